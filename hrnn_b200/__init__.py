@@ -1,0 +1,275 @@
+"""hrnn_b200: B200-native HRNN hot path behind the reference's index API.
+
+The Python class :class:`HRNN` mirrors the members of the reference's
+``hnswlib::HRNN<float>`` that its drivers call (include/hnswlib/hrnn.h) --
+same names, argument meaning and error messages -- and calls the C ABI of
+``libhrnn_b200.so`` (declared in include/hrnn_capi.h) through ctypes.  There is
+no CPU fallback: importing the package fails if the CUDA library is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libhrnn_b200.so")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(f"hrnn_b200: CUDA library {LIB_PATH} not built (run `make -C hrnn_b200`)")
+
+_lib = C.CDLL(LIB_PATH)
+
+OK, ERR_ARG, ERR_STATE, ERR_IO, ERR_FORMAT, ERR_CUDA, ERR_NOMEM, ERR_CAPACITY, ERR_LIMIT, ERR_TIMEOUT = range(10)
+
+# Every symbol include/hrnn_capi.h declares.
+EXPORTS = [
+    "hrnn_last_error", "hrnn_version", "hrnn_create", "hrnn_load", "hrnn_save", "hrnn_destroy",
+    "hrnn_add_points", "hrnn_refine_knng", "hrnn_build_rknng", "hrnn_build_rknng_mutable",
+    "hrnn_search_rknn", "hrnn_search_rknn_batch", "hrnn_search_rknn_batch_device",
+    "hrnn_compact_for_serving", "hrnn_insert_dynamic", "hrnn_set_ef", "hrnn_get_info",
+    "hrnn_get_search_stats", "hrnn_set_l2_order", "hrnn_detect_l2_order", "hrnn_get_knng",
+    "hrnn_set_knng", "hrnn_get_rknng", "hrnn_l2_batch",
+]
+
+
+class Info(C.Structure):
+    _fields_ = [
+        ("dim", C.c_uint64), ("max_elements", C.c_uint64), ("cur_element_count", C.c_uint64),
+        ("M", C.c_uint64), ("maxM", C.c_uint64), ("maxM0", C.c_uint64),
+        ("ef_construction", C.c_uint64), ("ef", C.c_uint64), ("K_knng", C.c_uint64),
+        ("maxlevel", C.c_int32), ("enterpoint", C.c_uint32),
+        ("knng_built", C.c_int32), ("rknng_built", C.c_int32), ("rknng_wide", C.c_int32),
+        ("rank_bits", C.c_uint32), ("rknng_entries", C.c_uint64),
+        ("serve_mode", C.c_int32), ("max_k_serve", C.c_uint64),
+        ("l2_lanes", C.c_int32), ("l2_fused", C.c_int32), ("device_bytes", C.c_uint64),
+    ]
+
+
+class SearchStats(C.Structure):
+    _fields_ = [(f, C.c_uint64) for f in (
+        "n_queries", "n_dist", "n_expanded", "n_posting", "n_cand", "n_verified", "n_result",
+        "n_lowp_decided", "n_fp32_decided", "n_fp64_decided")] + [
+        ("phase_a_ms", C.c_double), ("phase_b_ms", C.c_double), ("phase_c_ms", C.c_double)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+_vp = C.c_void_p
+_sz = C.c_size_t
+_lib.hrnn_last_error.restype = C.c_char_p
+_lib.hrnn_create.argtypes = [C.POINTER(_vp), _sz, _sz, _sz, _sz, _sz, _sz, C.c_int]
+_lib.hrnn_load.argtypes = [C.POINTER(_vp), C.c_char_p, _sz, _sz, C.c_int]
+_lib.hrnn_save.argtypes = [_vp, C.c_char_p]
+_lib.hrnn_destroy.argtypes = [_vp]
+_lib.hrnn_destroy.restype = None
+_lib.hrnn_add_points.argtypes = [_vp, _vp, _vp, _sz]
+_lib.hrnn_refine_knng.argtypes = [_vp, C.c_int, C.c_int]
+_lib.hrnn_build_rknng.argtypes = [_vp]
+_lib.hrnn_build_rknng_mutable.argtypes = [_vp]
+_lib.hrnn_search_rknn.argtypes = [_vp, _vp, _sz, C.c_float, _sz, _sz, _sz, _vp, _sz, C.POINTER(_sz)]
+_lib.hrnn_search_rknn_batch.argtypes = [_vp, _vp, _sz, _vp, _vp, _vp, C.c_float, C.c_uint32, _vp, _vp, _sz]
+_lib.hrnn_search_rknn_batch_device.argtypes = [_vp, _vp, _sz, _vp, _vp, _vp, C.c_float, C.c_uint32, _vp,
+                                               _vp, _sz, C.POINTER(C.c_uint64), _vp]
+_lib.hrnn_compact_for_serving.argtypes = [_vp, _sz]
+_lib.hrnn_insert_dynamic.argtypes = [_vp, _vp, _vp, _sz, C.c_uint, C.c_int]
+_lib.hrnn_set_ef.argtypes = [_vp, _sz]
+_lib.hrnn_get_info.argtypes = [_vp, C.POINTER(Info)]
+_lib.hrnn_get_search_stats.argtypes = [_vp, C.POINTER(SearchStats)]
+_lib.hrnn_set_l2_order.argtypes = [_vp, C.c_int, C.c_int]
+_lib.hrnn_detect_l2_order.argtypes = [C.POINTER(C.c_int), C.POINTER(C.c_int)]
+_lib.hrnn_get_knng.argtypes = [_vp, _vp, _vp, _vp]
+_lib.hrnn_set_knng.argtypes = [_vp, _vp, _vp, _vp]
+_lib.hrnn_get_rknng.argtypes = [_vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint32),
+                                C.POINTER(C.c_uint32), _vp, _vp, C.c_int]
+_lib.hrnn_l2_batch.argtypes = [_vp, _vp, _sz, _sz, C.c_int, C.c_int, _vp]
+
+
+class HrnnError(RuntimeError):
+    """std::runtime_error of the reference, carried with the C ABI status code."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(msg)
+        self.code = code
+
+
+def _check(rc: int):
+    if rc != OK:
+        raise HrnnError(rc, _lib.hrnn_last_error().decode())
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(_vp)
+
+
+def lib():
+    return _lib
+
+
+def detect_l2_order():
+    lanes, fused = C.c_int(0), C.c_int(0)
+    _check(_lib.hrnn_detect_l2_order(C.byref(lanes), C.byref(fused)))
+    return lanes.value, fused.value
+
+
+def l2_batch(A, B, lanes=16, fused=2) -> np.ndarray:
+    """Squared L2 of row pairs on the GPU in the reference's FP32 order."""
+    A = np.ascontiguousarray(A, np.float32)
+    B = np.ascontiguousarray(B, np.float32)
+    out = np.empty(A.shape[0], np.float32)
+    _check(_lib.hrnn_l2_batch(_p(A), _p(B), A.shape[0], A.shape[1], lanes, fused, _p(out)))
+    return out
+
+
+def _u32(x, n):
+    return np.ascontiguousarray(np.broadcast_to(np.asarray(x, dtype=np.uint32), (n,)))
+
+
+class HRNN:
+    """hnswlib::HRNN<float> with the hot path on the GPU (include/hnswlib/hrnn.h)."""
+
+    def __init__(self, dim: int, max_elements: int = 0, M: int = 16, ef_construction: int = 200,
+                 random_seed: int = 100, K_knng: int = 0, device: int = 0, _handle=None):
+        self.dim = int(dim)
+        self._h = _vp()
+        if _handle is not None:
+            self._h = _handle
+        else:
+            _check(_lib.hrnn_create(C.byref(self._h), self.dim, max_elements, M, ef_construction, random_seed,
+                                    K_knng, device))
+
+    @classmethod
+    def load(cls, path: str, dim: int, max_elements: int = 0, device: int = 0) -> "HRNN":
+        """HRNN(space, path, false, max_elements) -- hrnn.h:117."""
+        h = _vp()
+        _check(_lib.hrnn_load(C.byref(h), path.encode(), dim, max_elements, device))
+        return cls(dim, _handle=h)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.hrnn_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    # ---- build -------------------------------------------------------------
+    def addPoint(self, x, label: int):
+        self.add_points(np.asarray(x, np.float32)[None, :], np.asarray([label], np.uint64))
+
+    def add_points(self, X, labels=None):
+        X = np.ascontiguousarray(X, np.float32)
+        lab = None if labels is None else np.ascontiguousarray(labels, np.uint64)
+        _check(_lib.hrnn_add_points(self._h, _p(X), _p(lab) if lab is not None else None, X.shape[0]))
+
+    def refineKNNG(self, num_iters: int = 3, sample_size: int = 20):
+        _check(_lib.hrnn_refine_knng(self._h, num_iters, sample_size))
+
+    def buildRKNNG(self):
+        _check(_lib.hrnn_build_rknng(self._h))
+
+    def buildRKNNG_mutable(self):
+        _check(_lib.hrnn_build_rknng_mutable(self._h))
+
+    def insertPointDynamic(self, X, labels, m_update: int = 0, bidirectional: bool = False):
+        X = np.ascontiguousarray(np.atleast_2d(X), np.float32)
+        lab = np.ascontiguousarray(np.atleast_1d(labels), np.uint64)
+        _check(_lib.hrnn_insert_dynamic(self._h, _p(X), _p(lab), X.shape[0], m_update, int(bidirectional)))
+
+    def saveIndex(self, path: str):
+        _check(_lib.hrnn_save(self._h, path.encode()))
+
+    def compactForServing(self, max_k_serve: int):
+        _check(_lib.hrnn_compact_for_serving(self._h, max_k_serve))
+
+    def setEf(self, ef: int):
+        _check(_lib.hrnn_set_ef(self._h, ef))
+
+    def set_l2_order(self, lanes: int, fused: int):
+        _check(_lib.hrnn_set_l2_order(self._h, lanes, fused))
+
+    # ---- search ------------------------------------------------------------
+    def searchRknn(self, q, m: int, threshold: float, k: int, K_prime: int, ef_search: int) -> list:
+        """searchRknn -- hrnn.h:1966; labels in ascending internal-id order."""
+        return [int(x) for x in self.search_rknn_batch(np.asarray(q, np.float32)[None, :], m, K_prime,
+                                                       ef_search, threshold, k)[0]]
+
+    def search_rknn_batch(self, Q, m, K_prime, ef_search, threshold: float = 1.0, k: int = 10):
+        """Batch of searchRknn with host arrays; returns one label array per query."""
+        Q = np.ascontiguousarray(Q, np.float32)
+        nq = Q.shape[0]
+        mm, kp, ef = _u32(m, nq), _u32(K_prime, nq), _u32(ef_search, nq)
+        off = np.zeros(nq + 1, np.uint64)
+        cap = max(16, int(np.sum(mm.astype(np.int64)) * 64))
+        lab = np.zeros(cap, np.uint64)
+        rc = _lib.hrnn_search_rknn_batch(self._h, _p(Q), nq, _p(mm), _p(kp), _p(ef), threshold, k, _p(off),
+                                         _p(lab), cap)
+        if rc == ERR_CAPACITY:
+            cap = int(off[-1])
+            lab = np.zeros(max(cap, 1), np.uint64)
+            rc = _lib.hrnn_search_rknn_batch(self._h, _p(Q), nq, _p(mm), _p(kp), _p(ef), threshold, k,
+                                             _p(off), _p(lab), cap)
+        _check(rc)
+        return [lab[off[i]:off[i + 1]].copy() for i in range(nq)]
+
+    def search_rknn_batch_device(self, q_ptr, nq, m_ptr, kp_ptr, ef_ptr, threshold, k, off_ptr, lab_ptr,
+                                 cap, stream=0):
+        """Device-pointer batch (ints are raw CUDA pointers); returns the total result count."""
+        tot = C.c_uint64(0)
+        _check(_lib.hrnn_search_rknn_batch_device(self._h, _vp(q_ptr), nq, _vp(m_ptr), _vp(kp_ptr), _vp(ef_ptr),
+                                                  threshold, k, _vp(off_ptr), _vp(lab_ptr), cap, C.byref(tot),
+                                                  _vp(stream)))
+        return tot.value
+
+    # ---- inspection ----------------------------------------------------------
+    def info(self) -> dict:
+        i = Info()
+        _check(_lib.hrnn_get_info(self._h, C.byref(i)))
+        return {f: getattr(i, f) for f, _ in Info._fields_}
+
+    def last_search_stats(self) -> dict:
+        s = SearchStats()
+        _check(_lib.hrnn_get_search_stats(self._h, C.byref(s)))
+        return s.as_dict()
+
+    def getCurrentElementCount(self) -> int:
+        return self.info()["cur_element_count"]
+
+    @property
+    def K_knng_(self) -> int:
+        return self.info()["K_knng"]
+
+    @property
+    def knng_built_(self) -> bool:
+        return bool(self.info()["knng_built"])
+
+    @property
+    def rknng_built_(self) -> bool:
+        return bool(self.info()["rknng_built"])
+
+    def get_knng(self):
+        inf = self.info()
+        n, K = inf["cur_element_count"], inf["K_knng"]
+        ids = np.zeros((n, K), np.uint32)
+        d = np.zeros((n, K), np.float32)
+        cnt = np.zeros(n, np.uint32)
+        _check(_lib.hrnn_get_knng(self._h, _p(ids), _p(d), _p(cnt)))
+        return ids, d, cnt
+
+    def set_knng(self, ids, dists, cnt):
+        ids = np.ascontiguousarray(ids, np.uint32)
+        dists = np.ascontiguousarray(dists, np.float32)
+        cnt = np.ascontiguousarray(cnt, np.uint32)
+        _check(_lib.hrnn_set_knng(self._h, _p(ids), _p(dists), _p(cnt)))
+
+    def get_rknng(self, reference_order: bool = False):
+        no, ne = C.c_uint64(0), C.c_uint64(0)
+        eb, rb = C.c_uint32(0), C.c_uint32(0)
+        _check(_lib.hrnn_get_rknng(self._h, C.byref(no), C.byref(ne), C.byref(eb), C.byref(rb), None, None, 0))
+        off = np.zeros(no.value, np.uint64)
+        ent = np.zeros(max(ne.value, 1), np.uint64 if eb.value == 8 else np.uint32)
+        _check(_lib.hrnn_get_rknng(self._h, C.byref(no), C.byref(ne), C.byref(eb), C.byref(rb), _p(off), _p(ent),
+                                   int(reference_order)))
+        return off, ent[: ne.value], rb.value, eb.value == 8

@@ -1,0 +1,703 @@
+// Batched RkNN search, plain form: answers bit-identical to the reference's
+// searchRknn (hrnn.h:1966-2071) on the same index.
+//
+// Kernel A (one warp per query): greedy descent over the upper layers
+// (hrnn.h:1992-2013) and the best-first base-layer search searchBaseLayerST
+// (hrnn.h:484-616) with ef = max(ef_search, m), trimmed to m proxies.
+//
+//   The reference keeps a candidate min-heap and a result max-heap of size ef.
+//   Here the result set is one sorted list in shared memory ("beam") whose
+//   entries carry an expanded flag; the candidate heap is the set of unexpanded
+//   beam entries.  Equivalence (up to exact distance ties between different
+//   points): a candidate popped from the result heap has distance >= the new
+//   bound and can never be expanded again, so the first unexpanded beam entry is
+//   always the candidate the reference pops; and neighbour j of an expansion is
+//   accepted by the reference (size < ef || bound > d_j, evaluated after the
+//   earlier neighbours) iff fewer than ef elements of (beam before this expansion
+//   + earlier new neighbours) are <= d_j -- neighbours it rejected never move that
+//   count.  So all neighbour distances of an expansion are computed in parallel
+//   and the sequential acceptance is evaluated with one count per lane.
+//   The visited array becomes a lossy direct-mapped cache of ids plus an exact
+//   membership test against the beam: a point evicted from the cache and seen
+//   again is either in the beam (caught by the test) or was rejected/popped
+//   earlier, in which case the acceptance rule rejects it again.
+//
+// Kernel B (warp per query): length of each proxy's reverse-list prefix with
+// rank < K' (binary search: the segments are sorted by rank).
+//
+// Kernel C (warp per query): phase B posting scan into a per-warp open-address
+// table (score counts, the reference's score_buf), threshold filter and reset,
+// exact FP32 verification against the stored kNN radius, results in ascending
+// internal-id order (hrnn.h:2021-2070).
+#include <algorithm>
+#include <cfloat>
+#include <vector>
+
+#include "index.hpp"
+
+namespace hrnn {
+
+struct DevView {
+    const float* vec;
+    const uint32_t* adj0;
+    const uint32_t* upper;
+    const uint64_t* upper_off;
+    const uint32_t* knn_hdr;
+    const float* knn_dist;
+    const float* kdist_serve;
+    const uint64_t* csr_off;
+    const void* csr_ent;
+    const uint64_t* labels;
+    uint32_t n, dim, nb, W0, WU, K, mks, rank_bits;
+    int maxlevel;
+    uint32_t enterpoint;
+    int wide, lanes, fused;
+};
+
+namespace {
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+    uint32_t m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+__device__ __forceinline__ uint32_t hash32(uint32_t x) {
+    x ^= x >> 16;
+    x *= 0x7feb352dU;
+    x ^= x >> 15;
+    x *= 0x846ca68bU;
+    x ^= x >> 16;
+    return x;
+}
+
+// Distance of q to one vector, computed by the whole warp (both halves compute
+// the same value); returned in every lane.
+template <bool FUSED>
+__device__ __forceinline__ float warp_l2_one(const DevView& v, const float* q, uint32_t id) {
+    int l = threadIdx.x & 15;
+    if (v.lanes == 16 && v.dim % 16 == 0)
+        return l2_half16<FUSED>(q, v.vec + (size_t)id * v.dim, v.nb, l);
+    return l2_thread(q, v.vec + (size_t)id * v.dim, v.dim, v.lanes, v.fused);
+}
+
+// Distances of q to cnt (<= 32) vectors ids[0..cnt) -> dout[0..cnt).
+template <bool FUSED>
+__device__ __forceinline__ void warp_l2_list(const DevView& v, const float* q, const uint32_t* ids,
+                                             uint32_t cnt, float* dout) {
+    int lane = threadIdx.x & 31, half = lane >> 4, l = lane & 15;
+    if (v.lanes == 16 && v.dim % 16 == 0) {
+        for (uint32_t r = 0; r < cnt; r += 2) {
+            uint32_t t = r + half;
+            uint32_t id = ids[t < cnt ? t : r];
+            float d = l2_half16<FUSED>(q, v.vec + (size_t)id * v.dim, v.nb, l);
+            if (l == 0 && t < cnt) dout[t] = d;
+        }
+    } else {
+        if ((uint32_t)lane < cnt) dout[lane] = l2_thread(q, v.vec + (size_t)ids[lane] * v.dim, v.dim, v.lanes, v.fused);
+    }
+    __syncwarp();
+}
+
+struct WarpSmem {
+    float* q;
+    float* td;      // beam distances
+    uint32_t* ti;   // beam ids | kExpanded
+    float* xd;      // merge scratch
+    uint32_t* xi;
+    uint32_t* vis;  // visited cache
+    float* nd;      // neighbour distances
+    uint32_t* ni;   // neighbour ids
+    uint32_t* apos; // accepted insertion points
+};
+
+__host__ __device__ inline size_t warp_smem_bytes(uint32_t dim, uint32_t efc, uint32_t vc) {
+    return (size_t)dim * 4 + (size_t)efc * 8 + (size_t)(efc + 32) * 8 + (size_t)vc * 4 + 32 * 12;
+}
+
+__device__ inline WarpSmem carve(char* base, uint32_t dim, uint32_t efc, uint32_t vc) {
+    WarpSmem s;
+    s.q = (float*)base;
+    base += (size_t)dim * 4;
+    s.td = (float*)base;
+    base += (size_t)efc * 4;
+    s.ti = (uint32_t*)base;
+    base += (size_t)efc * 4;
+    s.xd = (float*)base;
+    base += (size_t)(efc + 32) * 4;
+    s.xi = (uint32_t*)base;
+    base += (size_t)(efc + 32) * 4;
+    s.vis = (uint32_t*)base;
+    base += (size_t)vc * 4;
+    s.nd = (float*)base;
+    base += 32 * 4;
+    s.ni = (uint32_t*)base;
+    base += 32 * 4;
+    s.apos = (uint32_t*)base;
+    return s;
+}
+
+// First index in td[0..n) with td[i] > x (upper bound), by one lane.
+__device__ __forceinline__ uint32_t upper_bound(const float* td, uint32_t n, float x) {
+    uint32_t lo = 0, hi = n;
+    while (lo < hi) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (td[mid] > x) hi = mid;
+        else lo = mid + 1;
+    }
+    return lo;
+}
+
+template <bool FUSED>
+__global__ void __launch_bounds__(128) k_phase_a(DevView v, const float* __restrict__ Q, uint32_t nq,
+                                                 const uint32_t* __restrict__ qm, const uint32_t* __restrict__ qef,
+                                                 uint32_t efc, uint32_t vc, uint32_t mmax,
+                                                 uint32_t* __restrict__ prox, uint32_t* __restrict__ nprox,
+                                                 SearchCounters* __restrict__ ctr) {
+    extern __shared__ char smem_raw[];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+    WarpSmem s = carve(smem_raw + (size_t)w * warp_smem_bytes(v.dim, efc, vc), v.dim, efc, vc);
+    unsigned long long c_dist = 0, c_exp = 0;
+    for (uint32_t qi = blockIdx.x * wpb + w; qi < nq; qi += gridDim.x * wpb) {
+        const uint32_t m = qm[qi];
+        const uint32_t EF = max(qef[qi], m);
+        if (v.n == 0 || m == 0) {
+            if (lane == 0) nprox[qi] = 0;
+            continue;
+        }
+        for (uint32_t i = lane; i < v.dim; i += 32) s.q[i] = Q[(size_t)qi * v.dim + i];
+        for (uint32_t i = lane; i < vc; i += 32) s.vis[i] = kInvalid;
+        __syncwarp();
+        // ---- greedy descent (hrnn.h:1992-2013) ----
+        uint32_t cur = v.enterpoint;
+        float curd = warp_l2_one<FUSED>(v, s.q, cur);
+        c_dist++;
+        for (int level = v.maxlevel; level > 0; --level) {
+            bool changed = true;
+            while (changed) {
+                changed = false;
+                const uint32_t* blk = v.upper + v.upper_off[cur] + (size_t)(level - 1) * v.WU;
+                uint32_t size = blk[0] & 0xFFFFu;
+                float bestd = curd;
+                uint32_t best = cur;
+                for (uint32_t base = 0; base < size; base += 32) {
+                    uint32_t cnt = min(32u, size - base);
+                    if ((uint32_t)lane < cnt) s.ni[lane] = blk[1 + base + lane];
+                    __syncwarp();
+                    warp_l2_list<FUSED>(v, s.q, s.ni, cnt, s.nd);
+                    c_dist += cnt;
+                    // first strict improvement of the running minimum, in list order
+                    float d = (uint32_t)lane < cnt ? s.nd[lane] : FLT_MAX;
+                    float mn = d;
+                    for (int o = 16; o; o >>= 1) mn = fminf(mn, __shfl_xor_sync(0xFFFFFFFFu, mn, o));
+                    uint32_t hit = __ballot_sync(0xFFFFFFFFu, (uint32_t)lane < cnt && d == mn);
+                    if (mn < bestd) {
+                        int src = __ffs(hit) - 1;
+                        bestd = mn;
+                        best = s.ni[src];
+                        changed = true;
+                    }
+                    __syncwarp();
+                }
+                cur = best;
+                curd = bestd;
+            }
+        }
+        // ---- base layer (hrnn.h:484-616) ----
+        uint32_t tsize = 1, cursor = 0;
+        if (lane == 0) {
+            s.td[0] = curd;
+            s.ti[0] = cur;
+            s.vis[hash32(cur) & (vc - 1)] = cur;
+        }
+        __syncwarp();
+        c_dist++;  // the reference evaluates the entry point again (hrnn.h:505)
+        for (;;) {
+            int found = -1;
+            for (uint32_t b = cursor; b < tsize; b += 32) {
+                uint32_t idx = b + lane;
+                bool u = idx < tsize && !(s.ti[idx] & kExpanded);
+                uint32_t bal = __ballot_sync(0xFFFFFFFFu, u);
+                if (bal) {
+                    found = (int)(b + __ffs(bal) - 1);
+                    break;
+                }
+            }
+            if (found < 0) break;
+            cursor = (uint32_t)found + 1;
+            const uint32_t c = s.ti[found] & kIdMask;
+            __syncwarp();
+            if (lane == 0) s.ti[found] |= kExpanded;
+            c_exp++;
+            const uint32_t* adj = v.adj0 + (size_t)c * v.W0;
+            const uint32_t size = adj[0] & 0xFFFFu;
+            for (uint32_t base = 0; base < size; base += 32) {
+                uint32_t j = base + lane;
+                uint32_t nid = j < size ? adj[1 + j] : kInvalid;
+                uint32_t slot = hash32(nid) & (vc - 1);
+                bool fresh = j < size && s.vis[slot] != nid;
+                __syncwarp();
+                uint32_t fb = __ballot_sync(0xFFFFFFFFu, fresh);
+                uint32_t cnt = __popc(fb);
+                if (fresh) {
+                    s.ni[__popc(fb & lanemask_lt())] = nid;
+                    s.vis[slot] = nid;
+                }
+                __syncwarp();
+                if (cnt == 0) continue;
+                warp_l2_list<FUSED>(v, s.q, s.ni, cnt, s.nd);
+                c_dist += cnt;
+                // exact membership test against the beam, then the acceptance count
+                float d = FLT_MAX;
+                uint32_t id = kInvalid, pos = 0;
+                bool ok = false;
+                if ((uint32_t)lane < cnt) {
+                    d = s.nd[lane];
+                    id = s.ni[lane];
+                    pos = upper_bound(s.td, tsize, d);
+                    ok = true;
+                    for (int k = (int)pos - 1; k >= 0 && s.td[k] == d; --k)
+                        if ((s.ti[k] & kIdMask) == id) {
+                            ok = false;
+                            break;
+                        }
+                }
+                uint32_t okb = __ballot_sync(0xFFFFFFFFu, ok);
+                uint32_t cp = 0;
+                for (uint32_t i = 0; i < cnt; ++i) {
+                    float di = __shfl_sync(0xFFFFFFFFu, d, i);
+                    if (((okb >> i) & 1u) && i < (uint32_t)lane && di <= d) cp++;
+                }
+                bool acc = ok && (pos + cp < EF);
+                uint32_t ab = __ballot_sync(0xFFFFFFFFu, acc);
+                if (!ab) continue;
+                uint32_t na = __popc(ab);
+                // new slot of each accepted neighbour among the accepted set
+                uint32_t before = 0;
+                for (uint32_t i = 0; i < cnt; ++i) {
+                    float di = __shfl_sync(0xFFFFFFFFu, d, i);
+                    if (((ab >> i) & 1u) && (di < d || (di == d && i < (uint32_t)lane))) before++;
+                }
+                uint32_t lo = acc ? pos : 0xFFFFFFFFu;
+                for (int o = 16; o; o >>= 1) lo = min(lo, __shfl_xor_sync(0xFFFFFFFFu, lo, o));
+                if (acc) s.apos[__popc(ab & lanemask_lt())] = pos;
+                __syncwarp();
+                const uint32_t newsize = min(tsize + na, EF);
+                // existing entries at or after lo shift by the number of accepted
+                // neighbours inserted at or before them
+                for (uint32_t k = lo + lane; k < tsize; k += 32) {
+                    uint32_t sh = 0;
+                    for (uint32_t a = 0; a < na; ++a) sh += (s.apos[a] <= k);
+                    uint32_t np = k + sh;
+                    if (np < newsize) {
+                        s.xd[np - lo] = s.td[k];
+                        s.xi[np - lo] = s.ti[k];
+                    }
+                }
+                uint32_t npos = pos + before;
+                if (acc && npos < newsize) {
+                    s.xd[npos - lo] = d;
+                    s.xi[npos - lo] = id;
+                }
+                uint32_t mnp = (acc && npos < newsize) ? npos : 0xFFFFFFFFu;
+                for (int o = 16; o; o >>= 1) mnp = min(mnp, __shfl_xor_sync(0xFFFFFFFFu, mnp, o));
+                __syncwarp();
+                for (uint32_t k = lo + lane; k < newsize; k += 32) {
+                    s.td[k] = s.xd[k - lo];
+                    s.ti[k] = s.xi[k - lo];
+                }
+                tsize = newsize;
+                cursor = min(cursor, mnp);
+                __syncwarp();
+            }
+        }
+        // ---- trim to m (hrnn.h:2018-2019): the m nearest, ascending ----
+        uint32_t np_ = min(m, tsize);
+        for (uint32_t i = lane; i < np_; i += 32) prox[(size_t)qi * mmax + i] = s.ti[i] & kIdMask;
+        if (lane == 0) nprox[qi] = np_;
+        __syncwarp();
+    }
+    if (lane == 0) {
+        atomicAdd(&ctr->n_dist, c_dist);
+        atomicAdd(&ctr->n_expanded, c_exp);
+    }
+}
+
+template <class E>
+__device__ __forceinline__ uint32_t entry_rank(const void* ent, uint64_t i, uint32_t rb) {
+    return (uint32_t)(((const E*)ent)[i] & (E)((1ull << rb) - 1));
+}
+template <class E>
+__device__ __forceinline__ uint32_t entry_owner(const void* ent, uint64_t i, uint32_t rb) {
+    return (uint32_t)(((const E*)ent)[i] >> rb);
+}
+
+// Prefix length (rank < K') of every proxy's reverse list and the per-query total.
+template <class E>
+__global__ void k_phase_b_count(DevView v, uint32_t nq, const uint32_t* __restrict__ Kp, uint32_t mmax,
+                                const uint32_t* __restrict__ prox, const uint32_t* __restrict__ nprox,
+                                uint32_t* __restrict__ plen, uint64_t* __restrict__ total) {
+    size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t qi = (uint32_t)(t / mmax), pi = (uint32_t)(t % mmax);
+    if (qi >= nq) return;
+    uint32_t len = 0;
+    if (pi < nprox[qi]) {
+        uint32_t p = prox[(size_t)qi * mmax + pi];
+        uint64_t b = v.csr_off[p], e = v.csr_off[p + 1];
+        uint32_t kp = Kp[qi];
+        uint64_t lo = b, hi = e;  // first entry with rank >= K'
+        while (lo < hi) {
+            uint64_t mid = (lo + hi) >> 1;
+            if (entry_rank<E>(v.csr_ent, mid, v.rank_bits) >= kp) hi = mid;
+            else lo = mid + 1;
+        }
+        len = (uint32_t)(lo - b);
+    }
+    plen[t] = len;
+    if (len) atomicAdd((unsigned long long*)&total[qi], (unsigned long long)len);
+}
+
+__device__ __forceinline__ float verify_kdist(const DevView& v, uint32_t id, uint32_t kidx) {
+    if (v.kdist_serve) return v.kdist_serve[(size_t)id * v.mks + kidx];   // hrnn.h:287-288
+    uint32_t cnt = v.knn_hdr[id] & 0xFFFFu;
+    if (kidx >= cnt) return FLT_MAX;                                     // hrnn.h:290-291
+    return v.knn_dist[(size_t)id * v.K + kidx];
+}
+
+// Phase B scan + phase C (hrnn.h:2021-2070), one warp per query.
+template <class E, bool FUSED>
+__global__ void __launch_bounds__(128) k_phase_bc(DevView v, const float* __restrict__ Q, uint32_t nq,
+                                                  uint32_t mmax, const uint32_t* __restrict__ prox,
+                                                  const uint32_t* __restrict__ nprox,
+                                                  const uint32_t* __restrict__ plen,
+                                                  const uint64_t* __restrict__ res_off, float threshold,
+                                                  uint32_t kidx, uint32_t hcap, uint32_t* __restrict__ hkey_pool,
+                                                  uint32_t* __restrict__ hcnt_pool, uint32_t* __restrict__ list_pool,
+                                                  size_t list_stride, uint64_t* __restrict__ resbuf,
+                                                  uint32_t* __restrict__ res_count, uint32_t* __restrict__ next_q,
+                                                  SearchCounters* __restrict__ ctr) {
+    extern __shared__ char smem_raw[];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+    const int half = lane >> 4, l = lane & 15;
+    float* q = (float*)(smem_raw + (size_t)w * (v.dim * 4 + 16));
+    uint32_t* nc_s = (uint32_t*)(q + v.dim);
+    const size_t gw = (size_t)blockIdx.x * wpb + w;
+    uint32_t* hkey = hkey_pool + gw * hcap;
+    uint32_t* hcnt = hcnt_pool + gw * hcap;
+    uint32_t* list = list_pool + gw * list_stride;
+    unsigned long long c_post = 0, c_cand = 0, c_ver = 0, c_res = 0;
+    for (;;) {
+        uint32_t qi = 0;
+        if (lane == 0) qi = atomicAdd(next_q, 1u);
+        qi = __shfl_sync(0xFFFFFFFFu, qi, 0);
+        if (qi >= nq) break;
+        const uint32_t np_ = nprox[qi];
+        for (uint32_t i = lane; i < v.dim; i += 32) q[i] = Q[(size_t)qi * v.dim + i];
+        if (lane == 0) *nc_s = 0;
+        __syncwarp();
+        // Phase B: farthest proxy first, like the reference's heap pops.
+        for (int pi = (int)np_ - 1; pi >= 0; --pi) {
+            uint32_t p = prox[(size_t)qi * mmax + pi];
+            uint32_t len = plen[(size_t)qi * mmax + pi];
+            uint64_t b = v.csr_off[p];
+            c_post += len;
+            for (uint32_t e = lane; e < len; e += 32) {
+                uint32_t owner = entry_owner<E>(v.csr_ent, b + e, v.rank_bits);
+                uint32_t slot = hash32(owner) & (hcap - 1);
+                for (;;) {
+                    uint32_t old = atomicCAS(&hkey[slot], kInvalid, owner);
+                    if (old == kInvalid) {
+                        atomicAdd(&hcnt[slot], 1u);
+                        list[atomicAdd(nc_s, 1u)] = slot;
+                        break;
+                    }
+                    if (old == owner) {
+                        atomicAdd(&hcnt[slot], 1u);
+                        break;
+                    }
+                    slot = (slot + 1) & (hcap - 1);
+                }
+            }
+        }
+        __syncwarp();
+        const uint32_t nc = *nc_s;
+        c_cand += nc;
+        // Phase C.1: threshold filter and table reset (hrnn.h:2043-2052).
+        uint32_t nv = 0;
+        for (uint32_t base = 0; base < nc; base += 32) {
+            uint32_t i = base + lane;
+            uint32_t id = kInvalid;
+            bool keep = false;
+            if (i < nc) {
+                uint32_t slot = list[i];
+                id = hkey[slot];
+                keep = (float)hcnt[slot] >= threshold;
+                hkey[slot] = kInvalid;
+                hcnt[slot] = 0;
+            }
+            uint32_t kb = __ballot_sync(0xFFFFFFFFu, keep);
+            __syncwarp();
+            if (keep) list[nv + __popc(kb & lanemask_lt())] = id;
+            nv += __popc(kb);
+            __syncwarp();
+        }
+        c_ver += nv;
+        // Phase C.2: exact FP32 verification (hrnn.h:2058-2069).
+        uint32_t na = 0;
+        if (v.lanes == 16 && v.dim % 16 == 0) {
+            for (uint32_t r = 0; r < nv; r += 2) {
+                uint32_t t = r + half;
+                uint32_t id = list[t < nv ? t : r];
+                float d = l2_half16<FUSED>(q, v.vec + (size_t)id * v.dim, v.nb, l);
+                bool a = t < nv && d <= verify_kdist(v, id, kidx);
+                uint32_t ab = __ballot_sync(0xFFFFFFFFu, a && l == 0);
+                __syncwarp();
+                if (lane == 0 && (ab & 1u)) list[na] = id;
+                if (lane == 16 && (ab & (1u << 16))) list[na + (ab & 1u)] = id;
+                na += __popc(ab);
+                __syncwarp();
+            }
+        } else {
+            for (uint32_t base = 0; base < nv; base += 32) {
+                uint32_t i = base + lane;
+                bool a = false;
+                uint32_t id = 0;
+                if (i < nv) {
+                    id = list[i];
+                    float d = l2_thread(q, v.vec + (size_t)id * v.dim, v.dim, v.lanes, v.fused);
+                    a = d <= verify_kdist(v, id, kidx);
+                }
+                uint32_t ab = __ballot_sync(0xFFFFFFFFu, a);
+                __syncwarp();
+                if (a) list[na + __popc(ab & lanemask_lt())] = id;
+                na += __popc(ab);
+                __syncwarp();
+            }
+        }
+        c_res += na;
+        // Results in ascending internal-id order (hrnn.h:2055): rank sort.
+        uint64_t ro = res_off[qi];
+        for (uint32_t i = lane; i < na; i += 32) {
+            uint32_t x = list[i], rk = 0;
+            for (uint32_t j = 0; j < na; ++j) rk += list[j] < x;
+            resbuf[ro + rk] = v.labels[x];
+        }
+        if (lane == 0) res_count[qi] = na;
+        __syncwarp();
+    }
+    if (lane == 0) {
+        atomicAdd(&ctr->n_posting, c_post);
+        atomicAdd(&ctr->n_cand, c_cand);
+        atomicAdd(&ctr->n_verified, c_ver);
+        atomicAdd(&ctr->n_result, c_res);
+    }
+}
+
+__global__ void k_pack_results(uint32_t nq, const uint64_t* __restrict__ res_off,
+                               const uint32_t* __restrict__ res_count, const uint64_t* __restrict__ out_off,
+                               const uint64_t* __restrict__ resbuf, uint64_t* __restrict__ out) {
+    uint32_t qi = blockIdx.x;
+    if (qi >= nq) return;
+    uint32_t c = res_count[qi];
+    for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) out[out_off[qi] + i] = resbuf[res_off[qi] + i];
+}
+
+__global__ void k_l2_pairs(const float* a, const float* b, size_t n, uint32_t dim, int lanes, int fused,
+                           float* out) {
+    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = l2_thread(a + i * dim, b + i * dim, dim, lanes, fused);
+}
+
+int sms(int dev) {
+    int v = 148;
+    cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+    return v;
+}
+
+}  // namespace
+
+DevView make_view(Index& ix) {
+    DevView v{};
+    v.vec = ix.vec.as<float>();
+    v.adj0 = ix.adj0.as<uint32_t>();
+    v.upper = ix.d_upper.as<uint32_t>();
+    v.upper_off = ix.d_upper_off.as<uint64_t>();
+    v.knn_hdr = ix.knn_hdr.as<uint32_t>();
+    v.knn_dist = ix.knn_dist.as<float>();
+    v.kdist_serve = ix.serve_mode ? ix.kdist_serve.as<float>() : nullptr;
+    v.csr_off = ix.csr_off.as<uint64_t>();
+    v.csr_ent = ix.csr_ent.p;
+    v.labels = ix.labels.as<uint64_t>();
+    v.n = (uint32_t)ix.cur;
+    v.dim = (uint32_t)ix.dim;
+    v.nb = (uint32_t)(ix.dim / 16);
+    v.W0 = (uint32_t)(1 + ix.maxM0);
+    v.WU = (uint32_t)(1 + ix.maxM);
+    v.K = (uint32_t)ix.K;
+    v.mks = (uint32_t)ix.max_k_serve;
+    v.rank_bits = ix.rank_bits;
+    v.maxlevel = ix.maxlevel;
+    v.enterpoint = ix.enterpoint;
+    v.wide = ix.wide;
+    v.lanes = ix.order.lanes;
+    v.fused = ix.order.fused;
+    return v;
+}
+
+uint64_t search_batch(Index& ix, const SearchArgs& a) {
+    if (!ix.rknng_built) fail(HRNN_ERR_STATE, "searchRknn: RKNNG not built");
+    cudaStream_t s = a.stream ? a.stream : ix.stream;
+    const size_t nq = a.nq;
+    if (ix.serve_mode && (a.k == 0 || a.k > ix.max_k_serve))
+        fail(HRNN_ERR_ARG, "searchRknn: k must be in [1, max_k_serve] in serve mode");
+    ix.sync_upper_to_device();
+    cudaEvent_t ev[4];
+    for (auto& e : ev) CUDA_CHECK(cudaEventCreate(&e));
+    CUDA_CHECK(cudaMemsetAsync(ix.counters.p, 0, sizeof(SearchCounters), s));
+    if (nq == 0) {
+        CUDA_CHECK(cudaMemsetAsync(a.d_out_offsets, 0, 8, s));
+        CUDA_CHECK(cudaStreamSynchronize(s));
+        for (auto& e : ev) cudaEventDestroy(e);
+        ix.last_stats = hrnn_search_stats{};
+        return 0;
+    }
+    // Per-batch maxima of m and ef (sizes the proxy table and the beam).
+    std::vector<uint32_t> hm(nq), hef(nq);
+    CUDA_CHECK(cudaMemcpyAsync(hm.data(), a.d_m, nq * 4, cudaMemcpyDeviceToHost, s));
+    CUDA_CHECK(cudaMemcpyAsync(hef.data(), a.d_ef, nq * 4, cudaMemcpyDeviceToHost, s));
+    CUDA_CHECK(cudaStreamSynchronize(s));
+    uint32_t mmax = 1, efmax = 1;
+    for (size_t i = 0; i < nq; ++i) {
+        mmax = std::max(mmax, hm[i]);
+        efmax = std::max(efmax, std::max(hef[i], hm[i]));
+    }
+    if (efmax > (1u << 16)) fail(HRNN_ERR_ARG, "searchRknn: ef_search/m too large (max 65536)");
+    DevView v = make_view(ix);
+    const uint32_t efc = (efmax + 31) & ~31u;
+    const uint32_t vc = 2048;
+    size_t wsm = warp_smem_bytes(v.dim, efc, vc);
+    int wpb = (int)std::max<size_t>(1, std::min<size_t>(4, (200 * 1024) / wsm));
+    size_t smem_a = wsm * wpb;
+    if (smem_a > 227 * 1024) fail(HRNN_ERR_ARG, "searchRknn: ef/dim too large for one warp's beam");
+    DevMem& prox = ix.scratch[0];
+    DevMem& nprox = ix.scratch[1];
+    DevMem& plen = ix.scratch[2];
+    DevMem& qtot = ix.scratch[3];
+    DevMem& tmp = ix.scratch[4];
+    prox.ensure(nq * mmax * 4);
+    nprox.ensure(nq * 4);
+    plen.ensure(nq * mmax * 4);
+    qtot.ensure((nq + 1) * 8 * 2 + (nq + 1) * 4 * 2 + 64);
+    uint64_t* d_total = qtot.as<uint64_t>();
+    uint64_t* d_resoff = d_total + (nq + 1);
+    uint32_t* d_rcount = (uint32_t*)(d_resoff + (nq + 1));
+    uint32_t* d_next = d_rcount + (nq + 1);
+    CUDA_CHECK(cudaMemsetAsync(d_total, 0, (nq + 1) * 8, s));
+    CUDA_CHECK(cudaMemsetAsync(d_rcount, 0, (nq + 1) * 4 + 4, s));
+    SearchCounters* ctr = ix.counters.as<SearchCounters>();
+    const bool fusedsimd = (ix.order.fused & 1) != 0;
+    const int nsm = sms(ix.device);
+    CUDA_CHECK(cudaEventRecord(ev[0], s));
+    {
+        unsigned grid = (unsigned)std::min<size_t>((nq + wpb - 1) / wpb, (size_t)nsm * 16);
+        auto kern = fusedsimd ? k_phase_a<true> : k_phase_a<false>;
+        CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_a));
+        kern<<<grid, wpb * 32, smem_a, s>>>(v, a.d_q, (uint32_t)nq, a.d_m, a.d_ef, efc, vc, mmax,
+                                            prox.as<uint32_t>(), nprox.as<uint32_t>(), ctr);
+        CUDA_LAUNCH_CHECK();
+    }
+    CUDA_CHECK(cudaEventRecord(ev[1], s));
+    {
+        size_t tot = nq * mmax;
+        auto kern = ix.wide ? k_phase_b_count<uint64_t> : k_phase_b_count<uint32_t>;
+        kern<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(v, (uint32_t)nq, a.d_Kp, mmax, prox.as<uint32_t>(),
+                                                           nprox.as<uint32_t>(), plen.as<uint32_t>(), d_total);
+        CUDA_LAUNCH_CHECK();
+    }
+    exclusive_scan_u64(d_total, d_resoff, nq + 1, s, tmp);
+    std::vector<uint64_t> htot(nq);
+    uint64_t sum_total = 0;
+    CUDA_CHECK(cudaMemcpyAsync(htot.data(), d_total, nq * 8, cudaMemcpyDeviceToHost, s));
+    CUDA_CHECK(cudaMemcpyAsync(&sum_total, d_resoff + nq, 8, cudaMemcpyDeviceToHost, s));
+    CUDA_CHECK(cudaStreamSynchronize(s));
+    uint64_t tmax = 1;
+    for (size_t i = 0; i < nq; ++i) tmax = std::max(tmax, htot[i]);
+    uint32_t hcap = 64;
+    while (hcap < 2 * tmax) hcap <<= 1;
+    // Warp slots for phase B/C, bounded by a scratch budget.
+    size_t per_slot = (size_t)hcap * 8 + tmax * 4;
+    size_t slots = std::max<size_t>(1, std::min<size_t>((size_t)nsm * 8 * 4, (size_t)(6ull << 30) / per_slot));
+    slots = std::min(slots, ((nq + 3) / 4) * 4);
+    slots = (slots + 3) / 4 * 4;
+    DevMem& hkey = ix.scratch[5];
+    DevMem& hcnt = ix.scratch[6];
+    DevMem& res = ix.scratch[7];
+    size_t need_h = slots * (size_t)hcap * 4;
+    if (hkey.bytes < need_h) {
+        hkey.alloc(need_h);
+        hcnt.alloc(need_h);
+        CUDA_CHECK(cudaMemsetAsync(hkey.p, 0xFF, need_h, s));
+        CUDA_CHECK(cudaMemsetAsync(hcnt.p, 0, need_h, s));
+    }
+    const size_t list_bytes = (slots * tmax * 4 + 255) & ~(size_t)255;
+    const size_t res_bytes = std::max<uint64_t>(sum_total, 1) * 8;
+    res.ensure(list_bytes + res_bytes);
+    uint32_t* list_pool = res.as<uint32_t>();
+    uint64_t* resbuf = (uint64_t*)(res.as<char>() + list_bytes);
+    CUDA_CHECK(cudaEventRecord(ev[2], s));
+    {
+        const uint32_t kidx = (uint32_t)(a.k - 1);
+        size_t smem = 4 * (v.dim * 4 + 16);
+        void (*kern)(DevView, const float*, uint32_t, uint32_t, const uint32_t*, const uint32_t*, const uint32_t*,
+                     const uint64_t*, float, uint32_t, uint32_t, uint32_t*, uint32_t*, uint32_t*, size_t, uint64_t*,
+                     uint32_t*, uint32_t*, SearchCounters*);
+        if (ix.wide) kern = fusedsimd ? k_phase_bc<uint64_t, true> : k_phase_bc<uint64_t, false>;
+        else kern = fusedsimd ? k_phase_bc<uint32_t, true> : k_phase_bc<uint32_t, false>;
+        kern<<<(unsigned)(slots / 4), 128, smem, s>>>(v, a.d_q, (uint32_t)nq, mmax, prox.as<uint32_t>(),
+                                                      nprox.as<uint32_t>(), plen.as<uint32_t>(), d_resoff,
+                                                      a.threshold, kidx, hcap, hkey.as<uint32_t>(),
+                                                      hcnt.as<uint32_t>(), list_pool, (size_t)tmax, resbuf,
+                                                      d_rcount, d_next, ctr);
+        CUDA_LAUNCH_CHECK();
+    }
+    exclusive_scan_u32_to_u64(d_rcount, a.d_out_offsets, nq + 1, s, tmp);
+    uint64_t total = 0;
+    CUDA_CHECK(cudaMemcpyAsync(&total, a.d_out_offsets + nq, 8, cudaMemcpyDeviceToHost, s));
+    CUDA_CHECK(cudaStreamSynchronize(s));
+    if (total <= a.cap && total > 0) {
+        k_pack_results<<<(unsigned)nq, 128, 0, s>>>((uint32_t)nq, d_resoff, d_rcount, a.d_out_offsets, resbuf,
+                                                     a.d_out_labels);
+        CUDA_LAUNCH_CHECK();
+    }
+    CUDA_CHECK(cudaEventRecord(ev[3], s));
+    CUDA_CHECK(cudaStreamSynchronize(s));
+    SearchCounters hc{};
+    CUDA_CHECK(cudaMemcpy(&hc, ix.counters.p, sizeof(hc), cudaMemcpyDeviceToHost));
+    hrnn_search_stats st{};
+    st.n_queries = nq;
+    st.n_dist = hc.n_dist;
+    st.n_expanded = hc.n_expanded;
+    st.n_posting = hc.n_posting;
+    st.n_cand = hc.n_cand;
+    st.n_verified = hc.n_verified;
+    st.n_result = hc.n_result;
+    float t01 = 0, t12 = 0, t23 = 0;
+    cudaEventElapsedTime(&t01, ev[0], ev[1]);
+    cudaEventElapsedTime(&t12, ev[1], ev[2]);
+    cudaEventElapsedTime(&t23, ev[2], ev[3]);
+    st.phase_a_ms = t01;
+    st.phase_b_ms = t12;
+    st.phase_c_ms = t23;
+    ix.last_stats = st;
+    for (auto& e : ev) cudaEventDestroy(e);
+    return total;
+}
+
+void l2_batch_device(const float* a, const float* b, size_t n, size_t dim, L2Order o, float* out,
+                     cudaStream_t s) {
+    if (!n) return;
+    k_l2_pairs<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(a, b, n, (uint32_t)dim, o.lanes, o.fused, out);
+    CUDA_LAUNCH_CHECK();
+}
+
+}  // namespace hrnn

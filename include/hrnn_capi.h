@@ -1,0 +1,188 @@
+/* hrnn_b200 -- C ABI of the B200-native HRNN hot path.
+ *
+ * This is the drop-in boundary.  Every entry point replaces one member of the
+ * reference's `hnswlib::HRNN<float>` (include/hnswlib/hrnn.h) that the three
+ * reference drivers call (src/hrnn_build.cpp:67-109, src/hrnn_search.cpp:137-178,
+ * src/hrnn_dynamic_test.cpp:224-393); the citation is on each declaration.
+ *
+ * Conventions
+ *  - Plain pointers and sizes only; no exceptions cross this boundary.
+ *  - Every call returns an hrnn_status (0 = HRNN_OK).  On failure the message of
+ *    the reference's std::runtime_error for the same condition (for example
+ *    "searchRknn: RKNNG not built", "Not an HRNN index file (bad magic)") is
+ *    available from hrnn_last_error() on the calling thread.
+ *  - Pointers named `d_*` are device pointers; all others are host pointers.
+ *  - `stream` is a cudaStream_t passed as void* (NULL = the handle's stream).
+ *    Calls on one handle must not overlap; use one handle per stream.
+ *  - Internal ids are assigned in insertion order; labels are the caller's u64
+ *    labels (labeltype = size_t, hnswlib.h:125).
+ */
+#ifndef HRNN_CAPI_H
+#define HRNN_CAPI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int hrnn_status;
+#define HRNN_OK 0
+#define HRNN_ERR_ARG 1      /* invalid argument                                   */
+#define HRNN_ERR_STATE 2    /* call not valid in the index's state                */
+#define HRNN_ERR_IO 3       /* file cannot be opened / read / written             */
+#define HRNN_ERR_FORMAT 4   /* not an HRNN .idx file, or a truncated one          */
+#define HRNN_ERR_CUDA 5     /* CUDA runtime error                                 */
+#define HRNN_ERR_NOMEM 6    /* device or host allocation failed                   */
+#define HRNN_ERR_CAPACITY 7 /* caller's output buffer too small (size reported)   */
+#define HRNN_ERR_LIMIT 8    /* element count exceeds max_elements                 */
+#define HRNN_ERR_TIMEOUT 9  /* a bounded device-side wait expired                 */
+
+typedef struct hrnn_index hrnn_index;
+
+/* Summary of an index (public fields and getters of HRNN<float>). */
+typedef struct {
+    uint64_t dim, max_elements, cur_element_count;   /* getCurrentElementCount hrnn.h:393 */
+    uint64_t M, maxM, maxM0, ef_construction, ef;    /* hrnn.h:38-42, setEf hrnn.h:226     */
+    uint64_t K_knng;                                 /* K_knng_ hrnn.h:83                  */
+    int32_t maxlevel;
+    uint32_t enterpoint;
+    int32_t knng_built, rknng_built, rknng_wide;    /* hrnn.h:86-87, 91                   */
+    uint32_t rank_bits;                              /* hrnn.h:93                          */
+    uint64_t rknng_entries;
+    int32_t serve_mode;                              /* compactForServing hrnn.h:109       */
+    uint64_t max_k_serve;
+    int32_t l2_lanes, l2_fused;                      /* FP32 summation order in use        */
+    uint64_t device_bytes;                           /* HBM held by the index              */
+} hrnn_info;
+
+/* Per-call counters of the last search (RknnProfile, hrnn.h:2077-2084, plus the
+ * work counts the roofline is computed from). */
+typedef struct {
+    uint64_t n_queries;
+    uint64_t n_dist;        /* FP32 distance evaluations, phase A              */
+    uint64_t n_expanded;    /* base-layer nodes expanded, phase A              */
+    uint64_t n_posting;     /* reverse-list entries read, phase B              */
+    uint64_t n_cand;        /* distinct candidates after phase B               */
+    uint64_t n_verified;    /* candidates passing the score threshold          */
+    uint64_t n_result;      /* accepted points                                 */
+    uint64_t n_lowp_decided;/* mixed precision: decided by the low-precision bound */
+    uint64_t n_fp32_decided;/* mixed precision: re-decided in exact FP32        */
+    uint64_t n_fp64_decided;/* mixed precision: re-decided in FP64 (tie band)   */
+    double phase_a_ms, phase_b_ms, phase_c_ms;   /* device time of each phase   */
+} hrnn_search_stats;
+
+/* Thread-local message of the last failing call on this thread ("" if none). */
+const char* hrnn_last_error(void);
+/* ABI version (major*10000 + minor*100 + patch). */
+int hrnn_version(void);
+
+/* HRNN(space, max_elements, M, ef_construction, random_seed, false, K_knng)
+ * -- hrnn.h:128-195.  device: CUDA ordinal. */
+hrnn_status hrnn_create(hrnn_index** out, size_t dim, size_t max_elements, size_t M,
+                        size_t ef_construction, size_t random_seed, size_t K_knng, int device);
+
+/* HRNN(space, path, false, max_elements) -> loadIndex -- hrnn.h:117-124, 930-1047.
+ * max_elements below the stored count keeps the stored capacity (hrnn.h:948-951). */
+hrnn_status hrnn_load(hrnn_index** out, const char* path, size_t dim, size_t max_elements,
+                      int device);
+
+/* saveIndex -- hrnn.h:861-927.  Byte layout identical to the reference's. */
+hrnn_status hrnn_save(hrnn_index* h, const char* path);
+
+/* ~HRNN -- hrnn.h:198-214. */
+void hrnn_destroy(hrnn_index* h);
+
+/* The addPoint loop of src/hrnn_build.cpp:75-88 (addPoint hrnn.h:1179, 1378-1517):
+ * HNSW insertion with the KNN-graph seed of hrnn.h:1479-1501, batched on the GPU.
+ * data: n x dim host floats; labels: n host labels (NULL = 0..n-1 offset by the
+ * current count). */
+hrnn_status hrnn_add_points(hrnn_index* h, const float* data, const uint64_t* labels, size_t n);
+
+/* refineKNNG(num_iters, sample_size) -- hrnn.h:1725-1862. */
+hrnn_status hrnn_refine_knng(hrnn_index* h, int num_iters, int sample_size);
+
+/* buildRKNNG() -- hrnn.h:1869-1935. */
+hrnn_status hrnn_build_rknng(hrnn_index* h);
+
+/* buildRKNNG_mutable() -- hrnn.h:1942-1959. */
+hrnn_status hrnn_build_rknng_mutable(hrnn_index* h);
+
+/* searchRknn(q, m, threshold, k, K_prime, ef_search) -- hrnn.h:1966-2071, one query,
+ * host buffers.  Labels are written in ascending internal-id order, as the
+ * reference returns them.  *out_count receives the result size; if it exceeds
+ * cap, HRNN_ERR_CAPACITY is returned and nothing past cap is written. */
+hrnn_status hrnn_search_rknn(hrnn_index* h, const float* query, size_t m, float threshold,
+                             size_t k, size_t K_prime, size_t ef_search, uint64_t* out_labels,
+                             size_t cap, size_t* out_count);
+
+/* A batch of searchRknn calls (the query loop of src/hrnn_search.cpp:168-180) with
+ * one (m, K', ef_search) per query, HOST buffers (copied in and out inside the
+ * call).  out_offsets: nq+1 entries; query i's labels are
+ * out_labels[out_offsets[i] .. out_offsets[i+1]).  On HRNN_ERR_CAPACITY,
+ * out_offsets is filled and out_offsets[nq] is the capacity needed. */
+hrnn_status hrnn_search_rknn_batch(hrnn_index* h, const float* queries, size_t nq,
+                                   const uint32_t* m, const uint32_t* K_prime,
+                                   const uint32_t* ef_search, float threshold, uint32_t k,
+                                   uint64_t* out_offsets, uint64_t* out_labels, size_t cap);
+
+/* Same with DEVICE buffers, stream-ordered (no host synchronisation except to
+ * size scratch).  d_out_offsets: nq+1 device u64; *out_total (host) receives the
+ * total result count. */
+hrnn_status hrnn_search_rknn_batch_device(hrnn_index* h, const float* d_queries, size_t nq,
+                                          const uint32_t* d_m, const uint32_t* d_K_prime,
+                                          const uint32_t* d_ef_search, float threshold,
+                                          uint32_t k, uint64_t* d_out_offsets,
+                                          uint64_t* d_out_labels, size_t cap,
+                                          uint64_t* out_total, void* stream);
+
+/* compactForServing(max_k_serve) -- hrnn.h:299-364: dense kdist[n x max_k_serve]. */
+hrnn_status hrnn_compact_for_serving(hrnn_index* h, size_t max_k_serve);
+
+/* insertPointDynamic(x, label, m_update, bidirectional) for n points --
+ * hrnn.h:2360-2534, as the insert loop of src/hrnn_dynamic_test.cpp:310-331. */
+hrnn_status hrnn_insert_dynamic(hrnn_index* h, const float* data, const uint64_t* labels, size_t n,
+                                unsigned m_update, int bidirectional);
+
+/* setEf -- hrnn.h:226-228. */
+hrnn_status hrnn_set_ef(hrnn_index* h, size_t ef);
+
+/* Public fields / getters (K_knng_, knng_built_, rknng_built_, getCurrentElementCount). */
+hrnn_status hrnn_get_info(hrnn_index* h, hrnn_info* info);
+
+/* Counters of the last search call. */
+hrnn_status hrnn_get_search_stats(hrnn_index* h, hrnn_search_stats* st);
+
+/* FP32 summation order of the L2 kernel (space_l2.h:214-238 picks it per host):
+ * lanes in {16, 8, 4}; fused bit 0 = SIMD multiply-add contracted, bit 1 = scalar
+ * tail contracted.  hrnn_detect_l2_order reports what the reference compiled with
+ * -march=native would use on this host (AVX-512 -> 16, AVX -> 8, else 4). */
+hrnn_status hrnn_set_l2_order(hrnn_index* h, int lanes, int fused);
+hrnn_status hrnn_detect_l2_order(int* lanes, int* fused);
+
+/* Read access to the KNN graph slot (get_knng_linklist hrnn.h:262-281):
+ * ids, dists: n x K_knng host arrays; cnt: n host counts.  Any may be NULL. */
+hrnn_status hrnn_get_knng(hrnn_index* h, uint32_t* ids, float* dists, uint32_t* cnt);
+/* Replace the KNN graph slot (e.g. to refine a graph produced elsewhere). */
+hrnn_status hrnn_set_knng(hrnn_index* h, const uint32_t* ids, const float* dists,
+                          const uint32_t* cnt);
+
+/* Reverse CSR (rknng_offsets_ / rknng_entries_*, hrnn.h:89-101).  Call with NULL
+ * arrays to get the sizes.  reference_order = 1 returns the entries in the exact
+ * byte order the reference's buildRKNNG_fill produces (its std::sort call is
+ * applied to the owner-ordered scatter on the host); 0 returns the device's
+ * canonical (rank, owner) order. */
+hrnn_status hrnn_get_rknng(hrnn_index* h, uint64_t* n_offsets, uint64_t* n_entries,
+                           uint32_t* entry_bytes, uint32_t* rank_bits, uint64_t* offsets,
+                           void* entries, int reference_order);
+
+/* Squared L2 of n pairs (a[i], b[i]) of dim floats on the device, in the order set by
+ * hrnn_set_l2_order.  Host arrays.  (L2Space::get_dist_func, space_l2.h:240-248.) */
+hrnn_status hrnn_l2_batch(const float* a, const float* b, size_t n, size_t dim, int lanes,
+                          int fused, float* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HRNN_CAPI_H */

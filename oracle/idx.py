@@ -125,3 +125,36 @@ def read_idx(path: str) -> IdxFile:
         (mask,) = struct.unpack_from("<Q" if eb == 8 else "<I", raw, pos)
         f.entry_bytes, f.rank_bits, f.csr_offsets, f.csr_entries, f.rank_mask = eb, rbits, offs, ents, mask
     return f
+
+
+def write_idx(path: str, X: np.ndarray, knn_ids: np.ndarray, knn_dists: np.ndarray, knn_cnt: np.ndarray,
+              M: int = 4, adj0: np.ndarray | None = None, labels: np.ndarray | None = None,
+              knng_built: bool = True) -> None:
+    """Writes a single-layer index in the reference's layout (test fixtures only):
+    level-0 links from adj0 ((n, 1+2M) u32, default empty), the given KNN slot,
+    no upper layers, no reverse CSR."""
+    n, d = X.shape
+    K = knn_ids.shape[1]
+    maxM0 = 2 * M
+    links = 4 * (1 + maxM0)
+    offK, slot = links, 4 + 8 * K
+    offD = offK + slot
+    labo = offD + 4 * d
+    sz = labo + 8
+    rec = np.zeros((n, sz), np.uint8)
+    if adj0 is not None:
+        rec[:, :links] = np.ascontiguousarray(adj0, np.uint32).view(np.uint8).reshape(n, links)
+    rec[:, offK:offK + 4] = np.ascontiguousarray(knn_cnt, np.uint32).view(np.uint8).reshape(n, 4)
+    pairs = np.empty((n, K, 2), np.uint32)
+    pairs[:, :, 0] = knn_ids
+    pairs[:, :, 1] = np.ascontiguousarray(knn_dists, np.float32).view(np.uint32)
+    rec[:, offK + 4:offK + slot] = pairs.view(np.uint8).reshape(n, 8 * K)
+    rec[:, offD:labo] = np.ascontiguousarray(X, np.float32).view(np.uint8).reshape(n, 4 * d)
+    lab = np.arange(n, dtype=np.uint64) if labels is None else np.asarray(labels, np.uint64)
+    rec[:, labo:sz] = lab.view(np.uint8).reshape(n, 8)
+    hdr = _HDR.pack(MAGIC, 0, n, n, sz, labo, offD, 0, 0, M, maxM0, M, 1.0 / np.log(M), 100, K, slot, offK,
+                    knng_built, False)
+    with open(path, "wb") as f:
+        f.write(hdr)
+        f.write(rec.tobytes())
+        f.write(np.zeros(n, np.uint32).tobytes())
