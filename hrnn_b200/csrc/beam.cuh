@@ -1,0 +1,290 @@
+// Warp-level graph search shared by the query path (search.cu) and the batched
+// HNSW construction (hnsw_build.cu): greedy descent over the upper layers and
+// the best-first beam search of one layer, with the exact FP32 distance order.
+//
+// Beam formulation of searchBaseLayerST (hrnn.h:484-616): the result max-heap of
+// size ef and the candidate min-heap are one ascending list in shared memory
+// whose entries carry an "expanded" flag.  The next node to expand is the first
+// unexpanded entry; neighbour j of an expansion is accepted iff fewer than ef
+// elements of (beam before the expansion + earlier fresh neighbours) are <= d_j,
+// which is the reference's sequential test (size < ef || bound > d_j) evaluated
+// after the earlier neighbours (neighbours it rejected never change the count).
+// The visited array is a lossy direct-mapped cache plus an exact membership test
+// against the beam; a point evicted from the cache and met again is either in
+// the beam (caught) or was rejected/popped before, in which case the acceptance
+// test rejects it again.  Equal distances of different points are the only case
+// in which the order can differ from the reference's heaps.
+#pragma once
+
+#include <cfloat>
+
+#include "common.cuh"
+
+namespace hrnn {
+
+struct DevView {
+    const float* vec;
+    const uint32_t* adj0;
+    const uint32_t* upper;
+    const uint64_t* upper_off;
+    const uint32_t* knn_hdr;
+    const float* knn_dist;
+    const float* kdist_serve;
+    const uint64_t* csr_off;
+    const void* csr_ent;
+    const uint64_t* labels;
+    uint32_t n, dim, nb, W0, WU, K, mks, rank_bits;
+    int maxlevel;
+    uint32_t enterpoint;
+    int wide, lanes, fused;
+};
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+    uint32_t m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+__device__ __forceinline__ uint32_t hash32(uint32_t x) {
+    x ^= x >> 16;
+    x *= 0x7feb352dU;
+    x ^= x >> 15;
+    x *= 0x846ca68bU;
+    x ^= x >> 16;
+    return x;
+}
+
+// Links of node c at `level`: word 0 = count (low 16 bits), then the ids.
+__device__ __forceinline__ const uint32_t* links_of(const DevView& v, uint32_t c, int level) {
+    if (level == 0) return v.adj0 + (size_t)c * v.W0;
+    return v.upper + v.upper_off[c] + (size_t)(level - 1) * v.WU;
+}
+
+// Distance of q (shared memory) to one stored vector, by the whole warp.
+template <bool FUSED>
+__device__ __forceinline__ float warp_l2_one(const DevView& v, const float* q, uint32_t id) {
+    int l = threadIdx.x & 15;
+    if (v.lanes == 16 && v.dim % 16 == 0) return l2_half16<FUSED>(q, v.vec + (size_t)id * v.dim, v.nb, l);
+    return l2_thread(q, v.vec + (size_t)id * v.dim, v.dim, v.lanes, v.fused);
+}
+
+// Distances of q to cnt (<= 32) stored vectors ids[0..cnt) -> dout[0..cnt).
+template <bool FUSED>
+__device__ __forceinline__ void warp_l2_list(const DevView& v, const float* q, const uint32_t* ids, uint32_t cnt,
+                                             float* dout) {
+    int lane = threadIdx.x & 31, half = lane >> 4, l = lane & 15;
+    if (v.lanes == 16 && v.dim % 16 == 0) {
+        for (uint32_t r = 0; r < cnt; r += 2) {
+            uint32_t t = r + half;
+            uint32_t id = ids[t < cnt ? t : r];
+            float d = l2_half16<FUSED>(q, v.vec + (size_t)id * v.dim, v.nb, l);
+            if (l == 0 && t < cnt) dout[t] = d;
+        }
+    } else {
+        if ((uint32_t)lane < cnt) dout[lane] = l2_thread(q, v.vec + (size_t)ids[lane] * v.dim, v.dim, v.lanes, v.fused);
+    }
+    __syncwarp();
+}
+
+struct WarpSmem {
+    float* q;
+    float* td;       // beam distances (ascending)
+    uint32_t* ti;    // beam ids | kExpanded
+    float* xd;       // merge scratch
+    uint32_t* xi;
+    uint32_t* vis;   // visited cache
+    float* nd;       // neighbour distances
+    uint32_t* ni;    // neighbour ids
+    uint32_t* apos;  // accepted insertion points
+};
+
+__host__ __device__ inline size_t warp_smem_bytes(uint32_t dim, uint32_t efc, uint32_t vc) {
+    return (size_t)dim * 4 + (size_t)efc * 8 + (size_t)(efc + 32) * 8 + (size_t)vc * 4 + 32 * 12;
+}
+
+__device__ inline WarpSmem carve(char* base, uint32_t dim, uint32_t efc, uint32_t vc) {
+    WarpSmem s;
+    s.q = (float*)base;
+    base += (size_t)dim * 4;
+    s.td = (float*)base;
+    base += (size_t)efc * 4;
+    s.ti = (uint32_t*)base;
+    base += (size_t)efc * 4;
+    s.xd = (float*)base;
+    base += (size_t)(efc + 32) * 4;
+    s.xi = (uint32_t*)base;
+    base += (size_t)(efc + 32) * 4;
+    s.vis = (uint32_t*)base;
+    base += (size_t)vc * 4;
+    s.nd = (float*)base;
+    base += 32 * 4;
+    s.ni = (uint32_t*)base;
+    base += 32 * 4;
+    s.apos = (uint32_t*)base;
+    return s;
+}
+
+// First index in td[0..n) with td[i] > x.
+__device__ __forceinline__ uint32_t upper_bound(const float* td, uint32_t n, float x) {
+    uint32_t lo = 0, hi = n;
+    while (lo < hi) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (td[mid] > x) hi = mid;
+        else lo = mid + 1;
+    }
+    return lo;
+}
+
+// Greedy descent over levels top..stop+1 (hrnn.h:1992-2013, 1438-1464): per level,
+// move to the first strict improvement of the running minimum in list order
+// until a whole list brings none.  cur/curd are updated in every lane.
+template <bool FUSED>
+__device__ void greedy_descent(const DevView& v, WarpSmem& s, int top, int stop, uint32_t& cur, float& curd,
+                               unsigned long long& c_dist) {
+    const int lane = threadIdx.x & 31;
+    for (int level = top; level > stop; --level) {
+        bool changed = true;
+        while (changed) {
+            changed = false;
+            const uint32_t* blk = links_of(v, cur, level);
+            uint32_t size = blk[0] & 0xFFFFu;
+            float bestd = curd;
+            uint32_t best = cur;
+            for (uint32_t base = 0; base < size; base += 32) {
+                uint32_t cnt = min(32u, size - base);
+                if ((uint32_t)lane < cnt) s.ni[lane] = blk[1 + base + lane];
+                __syncwarp();
+                warp_l2_list<FUSED>(v, s.q, s.ni, cnt, s.nd);
+                c_dist += cnt;
+                float d = (uint32_t)lane < cnt ? s.nd[lane] : FLT_MAX;
+                float mn = d;
+                for (int o = 16; o; o >>= 1) mn = fminf(mn, __shfl_xor_sync(0xFFFFFFFFu, mn, o));
+                uint32_t hit = __ballot_sync(0xFFFFFFFFu, (uint32_t)lane < cnt && d == mn);
+                if (mn < bestd) {
+                    bestd = mn;
+                    best = s.ni[__ffs(hit) - 1];
+                    changed = true;
+                }
+                __syncwarp();
+            }
+            cur = best;
+            curd = bestd;
+        }
+    }
+}
+
+// Best-first search of one layer from (ep, epd) with beam size EF (<= efc).
+// On return the beam s.td/s.ti[0..tsize) holds the EF nearest found, ascending
+// (ids still carry the expanded flag).  vc: visited-cache slots (power of two).
+template <bool FUSED>
+__device__ uint32_t beam_search(const DevView& v, WarpSmem& s, uint32_t ep, float epd, uint32_t EF, int level,
+                                uint32_t vc, unsigned long long& c_dist, unsigned long long& c_exp) {
+    const int lane = threadIdx.x & 31;
+    for (uint32_t i = lane; i < vc; i += 32) s.vis[i] = kInvalid;
+    __syncwarp();
+    uint32_t tsize = 1, cursor = 0;
+    if (lane == 0) {
+        s.td[0] = epd;
+        s.ti[0] = ep;
+        s.vis[hash32(ep) & (vc - 1)] = ep;
+    }
+    __syncwarp();
+    for (;;) {
+        int found = -1;
+        for (uint32_t b = cursor; b < tsize; b += 32) {
+            uint32_t idx = b + lane;
+            bool u = idx < tsize && !(s.ti[idx] & kExpanded);
+            uint32_t bal = __ballot_sync(0xFFFFFFFFu, u);
+            if (bal) {
+                found = (int)(b + __ffs(bal) - 1);
+                break;
+            }
+        }
+        if (found < 0) break;
+        cursor = (uint32_t)found + 1;
+        const uint32_t c = s.ti[found] & kIdMask;
+        __syncwarp();
+        if (lane == 0) s.ti[found] |= kExpanded;
+        c_exp++;
+        const uint32_t* adj = links_of(v, c, level);
+        const uint32_t size = adj[0] & 0xFFFFu;
+        for (uint32_t base = 0; base < size; base += 32) {
+            uint32_t j = base + lane;
+            uint32_t nid = j < size ? adj[1 + j] : kInvalid;
+            uint32_t slot = hash32(nid) & (vc - 1);
+            bool fresh = j < size && s.vis[slot] != nid;
+            __syncwarp();
+            uint32_t fb = __ballot_sync(0xFFFFFFFFu, fresh);
+            uint32_t cnt = __popc(fb);
+            if (fresh) {
+                s.ni[__popc(fb & lanemask_lt())] = nid;
+                s.vis[slot] = nid;
+            }
+            __syncwarp();
+            if (cnt == 0) continue;
+            warp_l2_list<FUSED>(v, s.q, s.ni, cnt, s.nd);
+            c_dist += cnt;
+            float d = FLT_MAX;
+            uint32_t id = kInvalid, pos = 0;
+            bool ok = false;
+            if ((uint32_t)lane < cnt) {
+                d = s.nd[lane];
+                id = s.ni[lane];
+                pos = upper_bound(s.td, tsize, d);
+                ok = true;
+                for (int k = (int)pos - 1; k >= 0 && s.td[k] == d; --k)
+                    if ((s.ti[k] & kIdMask) == id) {
+                        ok = false;
+                        break;
+                    }
+            }
+            uint32_t okb = __ballot_sync(0xFFFFFFFFu, ok);
+            uint32_t cp = 0;
+            for (uint32_t i = 0; i < cnt; ++i) {
+                float di = __shfl_sync(0xFFFFFFFFu, d, i);
+                if (((okb >> i) & 1u) && i < (uint32_t)lane && di <= d) cp++;
+            }
+            bool acc = ok && (pos + cp < EF);
+            uint32_t ab = __ballot_sync(0xFFFFFFFFu, acc);
+            if (!ab) continue;
+            uint32_t na = __popc(ab);
+            uint32_t before = 0;
+            for (uint32_t i = 0; i < cnt; ++i) {
+                float di = __shfl_sync(0xFFFFFFFFu, d, i);
+                if (((ab >> i) & 1u) && (di < d || (di == d && i < (uint32_t)lane))) before++;
+            }
+            uint32_t lo = acc ? pos : 0xFFFFFFFFu;
+            for (int o = 16; o; o >>= 1) lo = min(lo, __shfl_xor_sync(0xFFFFFFFFu, lo, o));
+            if (acc) s.apos[__popc(ab & lanemask_lt())] = pos;
+            __syncwarp();
+            const uint32_t newsize = min(tsize + na, EF);
+            for (uint32_t k = lo + lane; k < tsize; k += 32) {
+                uint32_t sh = 0;
+                for (uint32_t a = 0; a < na; ++a) sh += (s.apos[a] <= k);
+                uint32_t np = k + sh;
+                if (np < newsize) {
+                    s.xd[np - lo] = s.td[k];
+                    s.xi[np - lo] = s.ti[k];
+                }
+            }
+            uint32_t npos = pos + before;
+            if (acc && npos < newsize) {
+                s.xd[npos - lo] = d;
+                s.xi[npos - lo] = id;
+            }
+            uint32_t mnp = (acc && npos < newsize) ? npos : 0xFFFFFFFFu;
+            for (int o = 16; o; o >>= 1) mnp = min(mnp, __shfl_xor_sync(0xFFFFFFFFu, mnp, o));
+            __syncwarp();
+            for (uint32_t k = lo + lane; k < newsize; k += 32) {
+                s.td[k] = s.xd[k - lo];
+                s.ti[k] = s.xi[k - lo];
+            }
+            tsize = newsize;
+            cursor = min(cursor, mnp);
+            __syncwarp();
+        }
+    }
+    return tsize;
+}
+
+}  // namespace hrnn

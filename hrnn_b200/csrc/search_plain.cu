@@ -3,150 +3,27 @@
 //
 // Kernel A (one warp per query): greedy descent over the upper layers
 // (hrnn.h:1992-2013) and the best-first base-layer search searchBaseLayerST
-// (hrnn.h:484-616) with ef = max(ef_search, m), trimmed to m proxies.
+// (hrnn.h:484-616) with ef = max(ef_search, m), trimmed to the m nearest proxies
+// (hrnn.h:2016-2019).  The beam formulation and its equivalence argument are in
+// beam.cuh.
 //
-//   The reference keeps a candidate min-heap and a result max-heap of size ef.
-//   Here the result set is one sorted list in shared memory ("beam") whose
-//   entries carry an expanded flag; the candidate heap is the set of unexpanded
-//   beam entries.  Equivalence (up to exact distance ties between different
-//   points): a candidate popped from the result heap has distance >= the new
-//   bound and can never be expanded again, so the first unexpanded beam entry is
-//   always the candidate the reference pops; and neighbour j of an expansion is
-//   accepted by the reference (size < ef || bound > d_j, evaluated after the
-//   earlier neighbours) iff fewer than ef elements of (beam before this expansion
-//   + earlier new neighbours) are <= d_j -- neighbours it rejected never move that
-//   count.  So all neighbour distances of an expansion are computed in parallel
-//   and the sequential acceptance is evaluated with one count per lane.
-//   The visited array becomes a lossy direct-mapped cache of ids plus an exact
-//   membership test against the beam: a point evicted from the cache and seen
-//   again is either in the beam (caught by the test) or was rejected/popped
-//   earlier, in which case the acceptance rule rejects it again.
-//
-// Kernel B (warp per query): length of each proxy's reverse-list prefix with
-// rank < K' (binary search: the segments are sorted by rank).
+// Kernel B: length of each proxy's reverse-list prefix with rank < K' (binary
+// search: segments are sorted by rank), and the per-query total.
 //
 // Kernel C (warp per query): phase B posting scan into a per-warp open-address
-// table (score counts, the reference's score_buf), threshold filter and reset,
-// exact FP32 verification against the stored kNN radius, results in ascending
+// table (the reference's score_buf counts), threshold filter and reset, exact
+// FP32 verification against the stored kNN radius, results in ascending
 // internal-id order (hrnn.h:2021-2070).
 #include <algorithm>
 #include <cfloat>
 #include <vector>
 
+#include "beam.cuh"
 #include "index.hpp"
 
 namespace hrnn {
 
-struct DevView {
-    const float* vec;
-    const uint32_t* adj0;
-    const uint32_t* upper;
-    const uint64_t* upper_off;
-    const uint32_t* knn_hdr;
-    const float* knn_dist;
-    const float* kdist_serve;
-    const uint64_t* csr_off;
-    const void* csr_ent;
-    const uint64_t* labels;
-    uint32_t n, dim, nb, W0, WU, K, mks, rank_bits;
-    int maxlevel;
-    uint32_t enterpoint;
-    int wide, lanes, fused;
-};
-
 namespace {
-
-__device__ __forceinline__ uint32_t lanemask_lt() {
-    uint32_t m;
-    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
-    return m;
-}
-
-__device__ __forceinline__ uint32_t hash32(uint32_t x) {
-    x ^= x >> 16;
-    x *= 0x7feb352dU;
-    x ^= x >> 15;
-    x *= 0x846ca68bU;
-    x ^= x >> 16;
-    return x;
-}
-
-// Distance of q to one vector, computed by the whole warp (both halves compute
-// the same value); returned in every lane.
-template <bool FUSED>
-__device__ __forceinline__ float warp_l2_one(const DevView& v, const float* q, uint32_t id) {
-    int l = threadIdx.x & 15;
-    if (v.lanes == 16 && v.dim % 16 == 0)
-        return l2_half16<FUSED>(q, v.vec + (size_t)id * v.dim, v.nb, l);
-    return l2_thread(q, v.vec + (size_t)id * v.dim, v.dim, v.lanes, v.fused);
-}
-
-// Distances of q to cnt (<= 32) vectors ids[0..cnt) -> dout[0..cnt).
-template <bool FUSED>
-__device__ __forceinline__ void warp_l2_list(const DevView& v, const float* q, const uint32_t* ids,
-                                             uint32_t cnt, float* dout) {
-    int lane = threadIdx.x & 31, half = lane >> 4, l = lane & 15;
-    if (v.lanes == 16 && v.dim % 16 == 0) {
-        for (uint32_t r = 0; r < cnt; r += 2) {
-            uint32_t t = r + half;
-            uint32_t id = ids[t < cnt ? t : r];
-            float d = l2_half16<FUSED>(q, v.vec + (size_t)id * v.dim, v.nb, l);
-            if (l == 0 && t < cnt) dout[t] = d;
-        }
-    } else {
-        if ((uint32_t)lane < cnt) dout[lane] = l2_thread(q, v.vec + (size_t)ids[lane] * v.dim, v.dim, v.lanes, v.fused);
-    }
-    __syncwarp();
-}
-
-struct WarpSmem {
-    float* q;
-    float* td;      // beam distances
-    uint32_t* ti;   // beam ids | kExpanded
-    float* xd;      // merge scratch
-    uint32_t* xi;
-    uint32_t* vis;  // visited cache
-    float* nd;      // neighbour distances
-    uint32_t* ni;   // neighbour ids
-    uint32_t* apos; // accepted insertion points
-};
-
-__host__ __device__ inline size_t warp_smem_bytes(uint32_t dim, uint32_t efc, uint32_t vc) {
-    return (size_t)dim * 4 + (size_t)efc * 8 + (size_t)(efc + 32) * 8 + (size_t)vc * 4 + 32 * 12;
-}
-
-__device__ inline WarpSmem carve(char* base, uint32_t dim, uint32_t efc, uint32_t vc) {
-    WarpSmem s;
-    s.q = (float*)base;
-    base += (size_t)dim * 4;
-    s.td = (float*)base;
-    base += (size_t)efc * 4;
-    s.ti = (uint32_t*)base;
-    base += (size_t)efc * 4;
-    s.xd = (float*)base;
-    base += (size_t)(efc + 32) * 4;
-    s.xi = (uint32_t*)base;
-    base += (size_t)(efc + 32) * 4;
-    s.vis = (uint32_t*)base;
-    base += (size_t)vc * 4;
-    s.nd = (float*)base;
-    base += 32 * 4;
-    s.ni = (uint32_t*)base;
-    base += 32 * 4;
-    s.apos = (uint32_t*)base;
-    return s;
-}
-
-// First index in td[0..n) with td[i] > x (upper bound), by one lane.
-__device__ __forceinline__ uint32_t upper_bound(const float* td, uint32_t n, float x) {
-    uint32_t lo = 0, hi = n;
-    while (lo < hi) {
-        uint32_t mid = (lo + hi) >> 1;
-        if (td[mid] > x) hi = mid;
-        else lo = mid + 1;
-    }
-    return lo;
-}
 
 template <bool FUSED>
 __global__ void __launch_bounds__(128) k_phase_a(DevView v, const float* __restrict__ Q, uint32_t nq,
@@ -166,152 +43,13 @@ __global__ void __launch_bounds__(128) k_phase_a(DevView v, const float* __restr
             continue;
         }
         for (uint32_t i = lane; i < v.dim; i += 32) s.q[i] = Q[(size_t)qi * v.dim + i];
-        for (uint32_t i = lane; i < vc; i += 32) s.vis[i] = kInvalid;
         __syncwarp();
-        // ---- greedy descent (hrnn.h:1992-2013) ----
         uint32_t cur = v.enterpoint;
         float curd = warp_l2_one<FUSED>(v, s.q, cur);
         c_dist++;
-        for (int level = v.maxlevel; level > 0; --level) {
-            bool changed = true;
-            while (changed) {
-                changed = false;
-                const uint32_t* blk = v.upper + v.upper_off[cur] + (size_t)(level - 1) * v.WU;
-                uint32_t size = blk[0] & 0xFFFFu;
-                float bestd = curd;
-                uint32_t best = cur;
-                for (uint32_t base = 0; base < size; base += 32) {
-                    uint32_t cnt = min(32u, size - base);
-                    if ((uint32_t)lane < cnt) s.ni[lane] = blk[1 + base + lane];
-                    __syncwarp();
-                    warp_l2_list<FUSED>(v, s.q, s.ni, cnt, s.nd);
-                    c_dist += cnt;
-                    // first strict improvement of the running minimum, in list order
-                    float d = (uint32_t)lane < cnt ? s.nd[lane] : FLT_MAX;
-                    float mn = d;
-                    for (int o = 16; o; o >>= 1) mn = fminf(mn, __shfl_xor_sync(0xFFFFFFFFu, mn, o));
-                    uint32_t hit = __ballot_sync(0xFFFFFFFFu, (uint32_t)lane < cnt && d == mn);
-                    if (mn < bestd) {
-                        int src = __ffs(hit) - 1;
-                        bestd = mn;
-                        best = s.ni[src];
-                        changed = true;
-                    }
-                    __syncwarp();
-                }
-                cur = best;
-                curd = bestd;
-            }
-        }
-        // ---- base layer (hrnn.h:484-616) ----
-        uint32_t tsize = 1, cursor = 0;
-        if (lane == 0) {
-            s.td[0] = curd;
-            s.ti[0] = cur;
-            s.vis[hash32(cur) & (vc - 1)] = cur;
-        }
-        __syncwarp();
+        greedy_descent<FUSED>(v, s, v.maxlevel, 0, cur, curd, c_dist);
         c_dist++;  // the reference evaluates the entry point again (hrnn.h:505)
-        for (;;) {
-            int found = -1;
-            for (uint32_t b = cursor; b < tsize; b += 32) {
-                uint32_t idx = b + lane;
-                bool u = idx < tsize && !(s.ti[idx] & kExpanded);
-                uint32_t bal = __ballot_sync(0xFFFFFFFFu, u);
-                if (bal) {
-                    found = (int)(b + __ffs(bal) - 1);
-                    break;
-                }
-            }
-            if (found < 0) break;
-            cursor = (uint32_t)found + 1;
-            const uint32_t c = s.ti[found] & kIdMask;
-            __syncwarp();
-            if (lane == 0) s.ti[found] |= kExpanded;
-            c_exp++;
-            const uint32_t* adj = v.adj0 + (size_t)c * v.W0;
-            const uint32_t size = adj[0] & 0xFFFFu;
-            for (uint32_t base = 0; base < size; base += 32) {
-                uint32_t j = base + lane;
-                uint32_t nid = j < size ? adj[1 + j] : kInvalid;
-                uint32_t slot = hash32(nid) & (vc - 1);
-                bool fresh = j < size && s.vis[slot] != nid;
-                __syncwarp();
-                uint32_t fb = __ballot_sync(0xFFFFFFFFu, fresh);
-                uint32_t cnt = __popc(fb);
-                if (fresh) {
-                    s.ni[__popc(fb & lanemask_lt())] = nid;
-                    s.vis[slot] = nid;
-                }
-                __syncwarp();
-                if (cnt == 0) continue;
-                warp_l2_list<FUSED>(v, s.q, s.ni, cnt, s.nd);
-                c_dist += cnt;
-                // exact membership test against the beam, then the acceptance count
-                float d = FLT_MAX;
-                uint32_t id = kInvalid, pos = 0;
-                bool ok = false;
-                if ((uint32_t)lane < cnt) {
-                    d = s.nd[lane];
-                    id = s.ni[lane];
-                    pos = upper_bound(s.td, tsize, d);
-                    ok = true;
-                    for (int k = (int)pos - 1; k >= 0 && s.td[k] == d; --k)
-                        if ((s.ti[k] & kIdMask) == id) {
-                            ok = false;
-                            break;
-                        }
-                }
-                uint32_t okb = __ballot_sync(0xFFFFFFFFu, ok);
-                uint32_t cp = 0;
-                for (uint32_t i = 0; i < cnt; ++i) {
-                    float di = __shfl_sync(0xFFFFFFFFu, d, i);
-                    if (((okb >> i) & 1u) && i < (uint32_t)lane && di <= d) cp++;
-                }
-                bool acc = ok && (pos + cp < EF);
-                uint32_t ab = __ballot_sync(0xFFFFFFFFu, acc);
-                if (!ab) continue;
-                uint32_t na = __popc(ab);
-                // new slot of each accepted neighbour among the accepted set
-                uint32_t before = 0;
-                for (uint32_t i = 0; i < cnt; ++i) {
-                    float di = __shfl_sync(0xFFFFFFFFu, d, i);
-                    if (((ab >> i) & 1u) && (di < d || (di == d && i < (uint32_t)lane))) before++;
-                }
-                uint32_t lo = acc ? pos : 0xFFFFFFFFu;
-                for (int o = 16; o; o >>= 1) lo = min(lo, __shfl_xor_sync(0xFFFFFFFFu, lo, o));
-                if (acc) s.apos[__popc(ab & lanemask_lt())] = pos;
-                __syncwarp();
-                const uint32_t newsize = min(tsize + na, EF);
-                // existing entries at or after lo shift by the number of accepted
-                // neighbours inserted at or before them
-                for (uint32_t k = lo + lane; k < tsize; k += 32) {
-                    uint32_t sh = 0;
-                    for (uint32_t a = 0; a < na; ++a) sh += (s.apos[a] <= k);
-                    uint32_t np = k + sh;
-                    if (np < newsize) {
-                        s.xd[np - lo] = s.td[k];
-                        s.xi[np - lo] = s.ti[k];
-                    }
-                }
-                uint32_t npos = pos + before;
-                if (acc && npos < newsize) {
-                    s.xd[npos - lo] = d;
-                    s.xi[npos - lo] = id;
-                }
-                uint32_t mnp = (acc && npos < newsize) ? npos : 0xFFFFFFFFu;
-                for (int o = 16; o; o >>= 1) mnp = min(mnp, __shfl_xor_sync(0xFFFFFFFFu, mnp, o));
-                __syncwarp();
-                for (uint32_t k = lo + lane; k < newsize; k += 32) {
-                    s.td[k] = s.xd[k - lo];
-                    s.ti[k] = s.xi[k - lo];
-                }
-                tsize = newsize;
-                cursor = min(cursor, mnp);
-                __syncwarp();
-            }
-        }
-        // ---- trim to m (hrnn.h:2018-2019): the m nearest, ascending ----
+        uint32_t tsize = beam_search<FUSED>(v, s, cur, curd, EF, 0, vc, c_dist, c_exp);
         uint32_t np_ = min(m, tsize);
         for (uint32_t i = lane; i < np_; i += 32) prox[(size_t)qi * mmax + i] = s.ti[i] & kIdMask;
         if (lane == 0) nprox[qi] = np_;
