@@ -1,0 +1,479 @@
+#!/usr/bin/env python3
+"""Benchmark of the B200 HRNN hot path: RkNN queries/s at macro recall >= 0.95 (k=10)
+and the KNN-graph build time, on the 1M x 128, K_knng=500 Gaussian-mixture index.
+
+One step = one batch of queries (10,000 by default) answered by the batched
+search on an index resident in HBM.  `value` is whole-job queries/s over the
+timed steps (CUDA events on the launching stream, max over ranks); `e2e` is
+the same metric through the public host-buffer entry point
+(hrnn_search_rknn_batch: queries copied in, labels copied out inside the call).
+The index (GPU HNSW insertion + NNDescent + reverse CSR) is built first; its
+build times are reported under "knng_build".
+
+Multi-GPU: search does not shard (every query needs the whole index), so N ranks
+run N independent replicas, each answering its own query batch ("replicas only").
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+                  [--workload mixed-1M-d128-K500 | plain-100k-d128-K100]
+
+--impl reference times the reference's own searchRknn (oracle/_ref: include/
+hnswlib/hrnn.h compiled from its sources) with all host threads, on the same
+index file, workload, metric and parameters; rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # BASELINE configuration quoted for the metric: 1M x 128, Dirichlet(1) mixture of
+    # 256 Gaussians (centres ~ N(0, 4I), sigma 1, seed 2), K_knng=500.
+    "mixed-1M-d128-K500": dict(n=1_000_000, d=128, C=256, sigma=1.0, seed=2, dirichlet=True, nq=10_000,
+                               qseed=1002, M=16, efc=400, K=500, iters=10, S=50, k=10, Kp=500, ef=200,
+                               m_sweep=[1, 3, 5, 10, 20, 50]),
+    # The reference's CPU-runnable case: 100k x 128, 64 equal Gaussians (seed 0), K_knng=100.
+    "plain-100k-d128-K100": dict(n=100_000, d=128, C=64, sigma=1.0, seed=0, dirichlet=False, nq=1_000, qseed=1,
+                                 M=16, efc=400, K=100, iters=10, S=50, k=10, Kp=100, ef=200,
+                                 m_sweep=[1, 3, 5, 10, 20, 50]),
+}
+TARGET_RECALL = 0.95
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            j = json.load(f)
+        return float(j["hbm_gbs"]), float(j["bf16_tflops"]), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def start(self):
+        def run():
+            while not self._stop.is_set():
+                try:
+                    out = subprocess.run(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                         timeout=5).stdout.strip()
+                    if out:
+                        self.rows.append([x.strip() for x in out.split(",")])
+                except Exception:
+                    pass
+                self._stop.wait(0.2)
+
+        self._t = threading.Thread(target=run, daemon=True)
+        self._t.start()
+
+    def stop(self):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and r[5 + i] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+# ---------------------------------------------------------------------------
+# FP64 ground truth (measurement infrastructure; FP32 screen on the GPU with a
+# rigorous margin, every decision re-made in float64)
+# ---------------------------------------------------------------------------
+
+def kth_radius_fp64(torch, X: np.ndarray, k: int, dev) -> np.ndarray:
+    torch.backends.cuda.matmul.allow_tf32 = False
+    n = X.shape[0]
+    Xt = torch.from_numpy(X).to(dev)
+    nx = (Xt.double() ** 2).sum(1).float()
+    X64 = torch.from_numpy(X).to(dev).double()
+    out = torch.empty(n, dtype=torch.float64, device=dev)
+    pad = k + 16
+    bad_rows = []
+    B = 2048
+    for s in range(0, n, B):
+        e = min(n, s + B)
+        D = nx[s:e, None] - 2.0 * (Xt[s:e] @ Xt.T) + nx[None, :]
+        D[torch.arange(e - s, device=dev), torch.arange(s, e, device=dev)] = float("inf")
+        vals, idx = torch.topk(D, pad, dim=1, largest=False, sorted=True)
+        ex = ((X64[s:e, None, :] - X64[idx]) ** 2).sum(2)
+        ex_sorted, _ = torch.sort(ex, dim=1)
+        kth = ex_sorted[:, k - 1]
+        out[s:e] = kth
+        # rigorous screen: every point outside the candidates has fp32 distance >= the
+        # last candidate's, and the fp32 error is below `margin`
+        margin = 1e-4 * (nx[s:e].double() + nx.max().double()) + 1e-3
+        ok = (vals[:, -1].double() - margin) > kth
+        if not bool(ok.all()):
+            bad_rows.extend((torch.nonzero(~ok).flatten() + s).tolist())
+    for r in bad_rows:  # exact full row in float64
+        d = ((X64 - X64[r]) ** 2).sum(1)
+        d[r] = float("inf")
+        out[r] = torch.kthvalue(d, k).values
+    return out.cpu().numpy()
+
+
+def rknn_gt_fp64(torch, X: np.ndarray, Q: np.ndarray, kth: np.ndarray, dev):
+    torch.backends.cuda.matmul.allow_tf32 = False
+    Xt = torch.from_numpy(X).to(dev)
+    X64 = Xt.double()
+    nx = (X64 ** 2).sum(1)
+    kt = torch.from_numpy(kth).to(dev)
+    res = []
+    B = 256
+    for s in range(0, Q.shape[0], B):
+        q = torch.from_numpy(Q[s:s + B]).to(dev)
+        q64 = q.double()
+        nq_ = (q64 ** 2).sum(1)
+        D = (nq_[:, None] - 2.0 * (q @ Xt.T).double() + nx[None, :])
+        margin = 1e-4 * (nq_[:, None] + nx[None, :]) + 1e-3
+        cand = torch.nonzero(D <= kt[None, :] + margin)
+        qi, xi = cand[:, 0], cand[:, 1]
+        ex = ((q64[qi] - X64[xi]) ** 2).sum(1)
+        keep = ex <= kt[xi]
+        qi, xi = qi[keep].cpu().numpy(), xi[keep].cpu().numpy()
+        for j in range(q.shape[0]):
+            res.append(np.sort(xi[qi == j]).astype(np.uint32))
+    return res
+
+
+def macro_recall(gt, res) -> float:
+    s, c = 0.0, 0
+    for g, r in zip(gt, res):
+        if len(g) == 0:
+            continue
+        s += len(np.intersect1d(g, np.asarray(r, dtype=np.uint32))) / len(g)
+        c += 1
+    return s / c if c else 0.0
+
+
+# ---------------------------------------------------------------------------
+
+class StdoutToStderr:
+    """The library prints the reference's progress lines on stdout (hrnn.h:1855);
+    the bench keeps stdout for its one JSON line."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        os.dup2(2, 1)
+
+    def __exit__(self, *a):
+        sys.stdout.flush()
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+
+
+def build_index(H, W, X, dev_sync):
+    with StdoutToStderr():
+        return _build_index(H, W, X, dev_sync)
+
+
+def _build_index(H, W, X, dev_sync):
+    h = H.HRNN(W["d"], W["n"], W["M"], W["efc"], 100, W["K"])
+    t0 = time.perf_counter()
+    h.add_points(X)
+    dev_sync()
+    t1 = time.perf_counter()
+    h.refineKNNG(W["iters"], W["S"])
+    dev_sync()
+    t2 = time.perf_counter()
+    h.buildRKNNG()
+    dev_sync()
+    t3 = time.perf_counter()
+    return h, {"hnsw_insert_s": t1 - t0, "nndescent_s": t2 - t1, "rknng_csr_s": t3 - t2,
+               "knng_build_s": t3 - t1}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="mixed-1M-d128-K500", choices=list(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample", type=int, default=2000, help="queries in the CPU-baseline sample")
+    args = ap.parse_args()
+    W = WORKLOADS[args.workload]
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference" and rank != 0:
+        return  # the reference arm runs on rank 0 alone
+
+    import torch
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    import hrnn_b200 as H
+    from oracle import data as odata
+
+    def dev_sync():
+        torch.cuda.synchronize(dev)
+
+    t_gen = time.perf_counter()
+    X = odata.mixture(W["n"], W["d"], W["C"], W["sigma"], W["seed"], W["seed"], dirichlet=W["dirichlet"])
+    Q = odata.mixture(W["nq"], W["d"], W["C"], W["sigma"], W["seed"], W["qseed"] + rank, dirichlet=W["dirichlet"])
+    log(f"[bench] data {X.shape} queries {Q.shape} ({time.perf_counter() - t_gen:.1f}s)")
+
+    h, build = build_index(H, W, X, dev_sync)
+    rs = h.last_refine_stats()
+    log(f"[bench] build: {json.dumps(build)}")
+
+    # ---- ground truth and the recall sweep (untimed) ----
+    t_gt = time.perf_counter()
+    kth = kth_radius_fp64(torch, X, W["k"], dev)
+    gt = rknn_gt_fp64(torch, X, Q, kth, dev)
+    log(f"[bench] fp64 ground truth ({time.perf_counter() - t_gt:.1f}s), mean |RkNN| "
+        f"{np.mean([len(g) for g in gt]):.2f}, empty {sum(len(g) == 0 for g in gt)}")
+    # GT ids are data indices; index labels are data indices too.
+    sweep = {}
+    m_star = None
+    for m in W["m_sweep"]:
+        res = h.search_rknn_batch(Q, m, W["Kp"], W["ef"], threshold=1.0, k=W["k"])
+        sweep[m] = macro_recall(gt, res)
+        log(f"[bench] m={m}: macro recall {sweep[m]:.4f}")
+        if m_star is None and sweep[m] >= TARGET_RECALL:
+            m_star = m
+    if m_star is None:
+        m_star = W["m_sweep"][-1]
+    params = {"m": m_star, "K_prime": W["Kp"], "ef_search": W["ef"], "k": W["k"], "threshold": 1.0}
+
+    if args.impl == "reference":
+        run_reference_arm(args, W, h, Q, params, sweep, build)
+        return
+
+    # ---- timed device steps ----
+    nq, d = Q.shape
+    q_dev = torch.from_numpy(Q).to(dev)
+    m_dev = torch.full((nq,), m_star, dtype=torch.int32, device=dev)
+    kp_dev = torch.full((nq,), W["Kp"], dtype=torch.int32, device=dev)
+    ef_dev = torch.full((nq,), W["ef"], dtype=torch.int32, device=dev)
+    cap = nq * 512
+    off_dev = torch.zeros(nq + 1, dtype=torch.int64, device=dev)
+    lab_dev = torch.zeros(cap, dtype=torch.int64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        return h.search_rknn_batch_device(q_dev.data_ptr(), nq, m_dev.data_ptr(), kp_dev.data_ptr(),
+                                          ef_dev.data_ptr(), 1.0, W["k"], off_dev.data_ptr(), lab_dev.data_ptr(),
+                                          cap, stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        step()
+    clocks = ClockSampler(local)
+    if world > 1:
+        torch.distributed.barrier()
+    dev_sync()
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.nvtx.range_push("timed")  # profilers select the timed steps with this range
+    e0.record(stream)
+    launches = 0
+    for _ in range(args.steps):
+        step()
+        launches += h.last_search_stats()["n_launches"]
+    e1.record(stream)
+    dev_sync()
+    torch.cuda.nvtx.range_pop()
+    ck = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_per_step = ms / args.steps
+    qps = world * nq * args.steps / (ms / 1e3)
+    st = h.last_search_stats()
+
+    # ---- end to end through the host-buffer entry point ----
+    e2e_steps = max(1, args.steps)
+    Qh = np.ascontiguousarray(Q)
+    h.search_rknn_batch(Qh, m_star, W["Kp"], W["ef"], threshold=1.0, k=W["k"])
+    dev_sync()
+    t0 = time.perf_counter()
+    out = None
+    for _ in range(e2e_steps):
+        out = h.search_rknn_batch(Qh, m_star, W["Kp"], W["ef"], threshold=1.0, k=W["k"])
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_s], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    total_res = sum(len(x) for x in out)
+    e2e = {"value": world * nq * e2e_steps / e2e_s, "unit": "queries/s",
+           "h2d_bytes_per_step": int(nq * d * 4 + 3 * nq * 4), "d2h_bytes_per_step": int((nq + 1) * 8 + total_res * 8)}
+    recall_timed = macro_recall(gt, out)
+
+    # ---- roofline of the dominant phase ----
+    hbm, bf16, peak_kind = load_peaks()
+    E = 4
+    maxM0 = 2 * W["M"]
+    bytes_a = st["n_dist"] * d * 4 + st["n_expanded"] * (4 + 4 * maxM0)
+    bytes_bc = st["n_posting"] * E + st["n_verified"] * (d * 4 + 4) + st["n_result"] * 8
+    phases = {"phase_a_beam_search": (st["phase_a_ms"], bytes_a),
+              "phase_bc_posting_verify": (st["phase_c_ms"], bytes_bc)}
+    dom = max(phases, key=lambda k_: phases[k_][0])
+    tms, tb = phases[dom]
+    achieved = tb / (tms / 1e3) / 1e9 if tms > 0 else 0.0
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+                "frac": round(achieved / hbm, 4), "peak_source": peak_kind, "traffic": None,
+                "algorithmic_bytes_per_launch": int(tb), "launch_ms": round(tms, 3),
+                "per_query": {"n_dist": st["n_dist"] / nq, "n_expanded": st["n_expanded"] / nq,
+                              "n_posting": st["n_posting"] / nq, "n_verified": st["n_verified"] / nq,
+                              "n_result": st["n_result"] / nq},
+                "phase_ms": {"a": round(st["phase_a_ms"], 3), "b": round(st["phase_b_ms"], 3),
+                             "c": round(st["phase_c_ms"], 3)}}
+
+    # ---- NNDescent roofline (per iteration, the formula of the build) ----
+    it_bytes = []
+    for i in range(rs["iters"]):
+        b = 2 * W["n"] * W["K"] * 8 + rs["sample_entries"][i] * d * 4 + rs["proposals"][i] * (8 + 2 * d * 4)
+        it_bytes.append(b)
+    nnd_ms = sum(rs["ms"])
+    build["nndescent_iter_ms"] = [round(x, 2) for x in rs["ms"]]
+    build["nndescent_roofline"] = {"bound": "hbm", "achieved": round(sum(it_bytes) / (nnd_ms / 1e3) / 1e9, 1)
+                                   if nnd_ms > 0 else None, "peak": hbm, "unit": "GB/s",
+                                   "frac": round(sum(it_bytes) / (nnd_ms / 1e3) / 1e9 / hbm, 4) if nnd_ms else None,
+                                   "join_dists": rs["join_dists"], "proposals": rs["proposals"]}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(h, W, Q, params, args.cpu_sample)
+
+    line = {
+        "metric": "RkNN queries/s at recall>=0.95 (k=10)", "value": round(qps, 1), "unit": "queries/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded Gaussian mixture)",
+        "config": {"workload": args.workload, "n": W["n"], "dim": d, "K_knng": W["K"], "M": W["M"],
+                   "ef_construction": W["efc"], "queries_per_step": nq, "form": "plain (bit-exact)",
+                   **params, "recall_macro": round(recall_timed, 4),
+                   "recall_sweep": {str(k_): round(v, 4) for k_, v in sweep.items()},
+                   "parallelism": f"replicas{world}", "l2_flush": "inputs larger than L2 (index 7 GB)"},
+        "e2e": {k_: (round(v, 1) if isinstance(v, float) else v) for k_, v in e2e.items()},
+        "gpu_launches": int(launches), "roofline": roofline, "cpu_baseline": cpu, "clocks": ck,
+        "knng_build": {k_: (round(v, 3) if isinstance(v, float) else v) for k_, v in build.items()},
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+def _save_for_reference(h):
+    td = tempfile.mkdtemp(prefix="hrnn_bench_")
+    p = os.path.join(td, "index.idx")
+    t0 = time.perf_counter()
+    h.saveIndex(p)
+    log(f"[bench] saved index for the reference ({os.path.getsize(p) / 1e9:.2f} GB, "
+        f"{time.perf_counter() - t0:.1f}s)")
+    return td, p
+
+
+def cpu_baseline(h, W, Q, params, sample):
+    """The reference's searchRknn (oracle/_ref) on the same index on this host's
+    cores: all threads on `sample` queries, and one thread (the reference
+    protocol, src/hrnn_search.cpp:168-180) on a tenth of them."""
+    from oracle import ref
+    if not ref.available():
+        return {"value": None, "unit": "queries/s", "cores": 0, "kind": "reference",
+                "sample": "oracle/_ref not built"}
+    import shutil
+    td, p = _save_for_reference(h)
+    try:
+        t0 = time.perf_counter()
+        r = ref.RefIndex.load(p, W["d"])
+        log(f"[bench] reference loaded the index ({time.perf_counter() - t0:.1f}s)")
+        cores = os.cpu_count() or 1
+        Qs = Q[:sample]
+        _, secs = r.search_batch(Qs, params["m"], params["K_prime"], params["ef_search"], k=params["k"],
+                                 threads=cores, return_seconds=True)
+        n1 = max(20, sample // 10)
+        _, secs1 = r.search_batch(Q[:n1], params["m"], params["K_prime"], params["ef_search"], k=params["k"],
+                                  threads=1, return_seconds=True)
+        return {"value": round(len(Qs) / secs, 1), "unit": "queries/s", "cores": cores, "kind": "reference",
+                "sample": f"{len(Qs)} of the step's queries, {cores} threads (query-parallel searchRknn)",
+                "single_thread": {"value": round(n1 / secs1, 1), "sample": f"{n1} queries, 1 thread"}}
+    finally:
+        shutil.rmtree(td, ignore_errors=True)
+
+
+def run_reference_arm(args, W, h, Q, params, sweep, build):
+    from oracle import ref
+    if not ref.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (reference compiled from its sources) "
+                                                              "not built on this host"}))
+        return
+    import shutil
+    td, p = _save_for_reference(h)
+    try:
+        r = ref.RefIndex.load(p, W["d"])
+        cores = os.cpu_count() or 1
+        per_step = min(W["nq"], 2000)
+        for i in range(args.warmup):
+            r.search_batch(Q[:min(200, per_step)], params["m"], params["K_prime"], params["ef_search"],
+                           k=params["k"], threads=cores)
+        tot_q, tot_s = 0, 0.0
+        res_all = []
+        for i in range(args.steps):
+            Qs = Q[(i * per_step) % W["nq"]:][:per_step]
+            res, secs = r.search_batch(Qs, params["m"], params["K_prime"], params["ef_search"], k=params["k"],
+                                       threads=cores, return_seconds=True)
+            tot_q += len(Qs)
+            tot_s += secs
+        v = tot_q / tot_s
+        line = {"impl": "reference", "metric": "RkNN queries/s at recall>=0.95 (k=10)", "value": round(v, 1),
+                "unit": "queries/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": round(1e3 * tot_s / args.steps, 3), "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Gaussian mixture)",
+                "config": {"workload": args.workload, "n": W["n"], "dim": W["d"], "K_knng": W["K"],
+                           "queries_per_step": per_step, **params,
+                           "index": "the same .idx file (built by the GPU builder; the reference loads it "
+                                    "with HRNN(space, path))"},
+                "cpu_baseline": {"value": round(v, 1), "unit": "queries/s", "cores": cores, "kind": "reference",
+                                 "sample": f"{per_step} queries per step, {cores} threads"},
+                "e2e": {"value": round(v, 1), "unit": "queries/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+    finally:
+        shutil.rmtree(td, ignore_errors=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -29,7 +29,7 @@ EXPORTS = [
     "hrnn_add_points", "hrnn_refine_knng", "hrnn_build_rknng", "hrnn_build_rknng_mutable",
     "hrnn_search_rknn", "hrnn_search_rknn_batch", "hrnn_search_rknn_batch_device",
     "hrnn_compact_for_serving", "hrnn_insert_dynamic", "hrnn_set_ef", "hrnn_get_info",
-    "hrnn_get_search_stats", "hrnn_set_l2_order", "hrnn_detect_l2_order", "hrnn_get_knng",
+    "hrnn_get_search_stats", "hrnn_get_refine_stats", "hrnn_set_l2_order", "hrnn_detect_l2_order", "hrnn_get_knng",
     "hrnn_set_knng", "hrnn_get_rknng", "hrnn_l2_batch",
 ]
 
@@ -50,11 +50,24 @@ class Info(C.Structure):
 class SearchStats(C.Structure):
     _fields_ = [(f, C.c_uint64) for f in (
         "n_queries", "n_dist", "n_expanded", "n_posting", "n_cand", "n_verified", "n_result",
-        "n_lowp_decided", "n_fp32_decided", "n_fp64_decided")] + [
+        "n_lowp_decided", "n_fp32_decided", "n_fp64_decided", "n_launches")] + [
         ("phase_a_ms", C.c_double), ("phase_b_ms", C.c_double), ("phase_c_ms", C.c_double)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+MAX_ITERS = 64
+
+
+class RefineStats(C.Structure):
+    _fields_ = [("iters", C.c_int32)] + [
+        (f, C.c_uint64 * MAX_ITERS) for f in ("join_dists", "updates", "proposals", "sample_entries")] + [
+        ("ms", C.c_double * MAX_ITERS)]
+
+    def as_dict(self):
+        k = self.iters
+        return {"iters": k, **{f: list(getattr(self, f))[:k] for f, _ in self._fields_[1:]}}
 
 
 _vp = C.c_void_p
@@ -78,6 +91,7 @@ _lib.hrnn_insert_dynamic.argtypes = [_vp, _vp, _vp, _sz, C.c_uint, C.c_int]
 _lib.hrnn_set_ef.argtypes = [_vp, _sz]
 _lib.hrnn_get_info.argtypes = [_vp, C.POINTER(Info)]
 _lib.hrnn_get_search_stats.argtypes = [_vp, C.POINTER(SearchStats)]
+_lib.hrnn_get_refine_stats.argtypes = [_vp, C.POINTER(RefineStats)]
 _lib.hrnn_set_l2_order.argtypes = [_vp, C.c_int, C.c_int]
 _lib.hrnn_detect_l2_order.argtypes = [C.POINTER(C.c_int), C.POINTER(C.c_int)]
 _lib.hrnn_get_knng.argtypes = [_vp, _vp, _vp, _vp]
@@ -232,6 +246,11 @@ class HRNN:
     def last_search_stats(self) -> dict:
         s = SearchStats()
         _check(_lib.hrnn_get_search_stats(self._h, C.byref(s)))
+        return s.as_dict()
+
+    def last_refine_stats(self) -> dict:
+        s = RefineStats()
+        _check(_lib.hrnn_get_refine_stats(self._h, C.byref(s)))
         return s.as_dict()
 
     def getCurrentElementCount(self) -> int:

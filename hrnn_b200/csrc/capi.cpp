@@ -270,6 +270,14 @@ hrnn_status hrnn_get_search_stats(hrnn_index* h, hrnn_search_stats* st) {
     });
 }
 
+hrnn_status hrnn_get_refine_stats(hrnn_index* h, hrnn_refine_stats* st) {
+    return guard([&] {
+        need(h, "index");
+        need(st, "stats");
+        *st = h->ix.refine_stats;
+    });
+}
+
 hrnn_status hrnn_set_l2_order(hrnn_index* h, int lanes, int fused) {
     return guard([&] {
         need(h, "index");

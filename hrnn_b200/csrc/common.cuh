@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 #include <stdexcept>
@@ -29,8 +30,19 @@ inline void cuda_check(cudaError_t e, const char* what, const char* file, int li
         fail(e == cudaErrorMemoryAllocation ? HRNN_ERR_NOMEM : HRNN_ERR_CUDA, buf);
     }
 }
+// Number of kernels this library has launched (every launch site ends with
+// CUDA_LAUNCH_CHECK); per-call deltas are reported in the search statistics.
+inline std::atomic<unsigned long long>& launch_counter() {
+    static std::atomic<unsigned long long> c{0};
+    return c;
+}
+
 #define CUDA_CHECK(x) ::hrnn::cuda_check((x), #x, __FILE__, __LINE__)
-#define CUDA_LAUNCH_CHECK() ::hrnn::cuda_check(cudaGetLastError(), "kernel launch", __FILE__, __LINE__)
+#define CUDA_LAUNCH_CHECK()                                                              \
+    do {                                                                                 \
+        ::hrnn::launch_counter().fetch_add(1, std::memory_order_relaxed);                \
+        ::hrnn::cuda_check(cudaGetLastError(), "kernel launch", __FILE__, __LINE__);     \
+    } while (0)
 
 constexpr uint32_t kInvalid = 0xFFFFFFFFu;
 constexpr uint32_t kExpanded = 0x80000000u;   // flag bit in beam-list ids (ids < 2^31)

@@ -114,6 +114,7 @@ struct Index {
     DevMem io;           // host-buffer entry points stage their inputs/outputs here
     DevMem counters;     // SearchCounters
     hrnn_search_stats last_stats{};
+    hrnn_refine_stats refine_stats{};
 
     ~Index();
 

@@ -535,6 +535,7 @@ void refine_knng(Index& ix, int iters, int sample) {
     if (merge_smem > 227 * 1024) fail(HRNN_ERR_ARG, "refineKNNG: K_knng too large for the merge kernel");
     CUDA_CHECK(cudaFuncSetAttribute(k_merge, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)merge_smem));
     const int g1 = nsm * 16;
+    ix.refine_stats = hrnn_refine_stats{};
     for (int it = 0; it < iters; ++it) {
         cudaEvent_t e0, e1;
         CUDA_CHECK(cudaEventCreate(&e0));
@@ -558,6 +559,16 @@ void refine_knng(Index& ix, int iters, int sample) {
         k_sample_rev<<<g1, 256, 0, s>>>(n, R, cap, roff.as<uint64_t>(), rbuf.as<uint32_t>(), newl.as<uint32_t>(),
                                          newc.as<uint32_t>(), oldl.as<uint32_t>(), oldc.as<uint32_t>());
         CUDA_LAUNCH_CHECK();
+        // |new| + |old| summed over nodes (gather bytes of the join)
+        unsigned long long sample_entries = 0;
+        {
+            std::vector<uint32_t> a(n), b(n);
+            CUDA_CHECK(cudaMemcpyAsync(a.data(), newc.p, (size_t)n * 4, cudaMemcpyDeviceToHost, s));
+            CUDA_CHECK(cudaMemcpyAsync(b.data(), oldc.p, (size_t)n * 4, cudaMemcpyDeviceToHost, s));
+            CUDA_CHECK(cudaStreamSynchronize(s));
+            for (uint32_t i = 0; i < n; ++i) sample_entries += (unsigned long long)a[i] + b[i];
+        }
+        unsigned long long proposals = 0;
         // ---- phase 2, chunk by chunk ----
         uint32_t chunk = std::max<uint32_t>(1, std::min<uint32_t>(n, 4096));
         for (uint32_t node0 = 0; node0 < n;) {
@@ -604,6 +615,7 @@ void refine_knng(Index& ix, int iters, int sample) {
                                                                       isnew.as<uint8_t>(), hcap, d_nupd);
                 CUDA_LAUNCH_CHECK();
             }
+            proposals += np;
             node0 = node1;
             // Grow the chunk while proposals stay well inside the buffer.
             if (np < pcap / 8 && chunk < n) chunk = std::min<uint32_t>(n, chunk * 2);
@@ -618,6 +630,15 @@ void refine_knng(Index& ix, int iters, int sample) {
         cudaEventDestroy(e1);
         std::printf("      iter %d: %llu updates, %llu dists  (%.1f ms)\n", it, hc[2], hc[1], ms);
         std::fflush(stdout);
+        if (it < HRNN_MAX_ITERS) {
+            auto& rs = ix.refine_stats;
+            rs.iters = it + 1;
+            rs.join_dists[it] = hc[1];
+            rs.updates[it] = hc[2];
+            rs.proposals[it] = proposals;
+            rs.sample_entries[it] = sample_entries;
+            rs.ms[it] = ms;
+        }
     }
     ix.knng_built = true;                                 // hrnn.h:1861
 }

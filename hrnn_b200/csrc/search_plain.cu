@@ -292,6 +292,7 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
     cudaEvent_t ev[4];
     for (auto& e : ev) CUDA_CHECK(cudaEventCreate(&e));
     CUDA_CHECK(cudaMemsetAsync(ix.counters.p, 0, sizeof(SearchCounters), s));
+    const unsigned long long launches0 = launch_counter().load();
     if (nq == 0) {
         CUDA_CHECK(cudaMemsetAsync(a.d_out_offsets, 0, 8, s));
         CUDA_CHECK(cudaStreamSynchronize(s));
@@ -419,6 +420,7 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
     st.n_cand = hc.n_cand;
     st.n_verified = hc.n_verified;
     st.n_result = hc.n_result;
+    st.n_launches = launch_counter().load() - launches0;
     float t01 = 0, t12 = 0, t23 = 0;
     cudaEventElapsedTime(&t01, ev[0], ev[1]);
     cudaEventElapsedTime(&t12, ev[1], ev[2]);

@@ -70,8 +70,21 @@ typedef struct {
     uint64_t n_lowp_decided;/* mixed precision: decided by the low-precision bound */
     uint64_t n_fp32_decided;/* mixed precision: re-decided in exact FP32        */
     uint64_t n_fp64_decided;/* mixed precision: re-decided in FP64 (tie band)   */
+    uint64_t n_launches;    /* kernels this call launched                       */
     double phase_a_ms, phase_b_ms, phase_c_ms;   /* device time of each phase   */
 } hrnn_search_stats;
+
+/* Per-iteration counters of the last refineKNNG call (the reference prints the
+ * updates and distance counts per iteration, hrnn.h:1855-1859). */
+#define HRNN_MAX_ITERS 64
+typedef struct {
+    int32_t iters;
+    uint64_t join_dists[HRNN_MAX_ITERS];     /* pair distances of the local join     */
+    uint64_t updates[HRNN_MAX_ITERS];        /* entries inserted into lists          */
+    uint64_t proposals[HRNN_MAX_ITERS];      /* proposals that passed the bound      */
+    uint64_t sample_entries[HRNN_MAX_ITERS]; /* sum over nodes of |new| + |old|      */
+    double ms[HRNN_MAX_ITERS];               /* device time of the iteration         */
+} hrnn_refine_stats;
 
 /* Thread-local message of the last failing call on this thread ("" if none). */
 const char* hrnn_last_error(void);
@@ -153,6 +166,9 @@ hrnn_status hrnn_get_info(hrnn_index* h, hrnn_info* info);
 
 /* Counters of the last search call. */
 hrnn_status hrnn_get_search_stats(hrnn_index* h, hrnn_search_stats* st);
+
+/* Counters of the last refineKNNG call. */
+hrnn_status hrnn_get_refine_stats(hrnn_index* h, hrnn_refine_stats* st);
 
 /* FP32 summation order of the L2 kernel (space_l2.h:214-238 picks it per host):
  * lanes in {16, 8, 4}; fused bit 0 = SIMD multiply-add contracted, bit 1 = scalar
