@@ -42,6 +42,10 @@ WORKLOADS = {
     "mixed-1M-d128-K500": dict(n=1_000_000, d=128, C=256, sigma=1.0, seed=2, dirichlet=True, nq=10_000,
                                qseed=1002, M=16, efc=400, K=500, iters=10, S=50, k=10, Kp=500, ef=200,
                                m_sweep=[1, 3, 5, 10, 20, 50]),
+    # Profiling case: the same mixture at half the size (vectors 256 MB > L2), K_knng=250.
+    "mixed-500k-d128-K250": dict(n=500_000, d=128, C=256, sigma=1.0, seed=2, dirichlet=True, nq=2_000,
+                                 qseed=1002, M=16, efc=400, K=250, iters=10, S=50, k=10, Kp=250, ef=200,
+                                 m_sweep=[1, 3, 5, 10, 20, 50]),
     # The reference's CPU-runnable case: 100k x 128, 64 equal Gaussians (seed 0), K_knng=100.
     "plain-100k-d128-K100": dict(n=100_000, d=128, C=64, sigma=1.0, seed=0, dirichlet=False, nq=1_000, qseed=1,
                                  M=16, efc=400, K=100, iters=10, S=50, k=10, Kp=100, ef=200,

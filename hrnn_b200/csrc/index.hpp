@@ -113,6 +113,7 @@ struct Index {
     DevMem scratch[8];
     DevMem io;           // host-buffer entry points stage their inputs/outputs here
     DevMem counters;     // SearchCounters
+    DevMem kcol;         // f32 [n]: kdist(p, k-1) of the current search call
     hrnn_search_stats last_stats{};
     hrnn_refine_stats refine_stats{};
 

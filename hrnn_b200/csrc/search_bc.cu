@@ -1,0 +1,275 @@
+// Phase B + C of the batched search with one CTA per query (hrnn.h:2021-2070).
+//
+//   B: the reverse-list prefixes (rank < K') of the m proxies are scanned and the
+//      owners deduplicated/counted in an open-address table in shared memory --
+//      the reference's score_buf (hrnn.h:2029-2036).  To bound the table, the
+//      owner-id space is cut into P ranges processed one after the other (every
+//      posting is re-read P times; postings are 4 bytes, candidates 512).
+//   C: every distinct owner whose count reaches the threshold (hrnn.h:2043-2052)
+//      is verified in exact FP32, d(q,p) <= kdist(p, k-1) (hrnn.h:2058-2069):
+//      the warps sweep the table, compact candidates with a ballot and verify four
+//      per warp step (two per half-warp, loads issued together).  kdist(p, k-1) is
+//      read from kcol, a per-call column of the KNN-slot radius (FLT_MAX when the
+//      list is shorter than k, hrnn.h:290-291) that stays resident in L2.
+//   Accepted ids of one range are sorted (bitonic, shared memory) and appended as
+//   labels; ranges ascend, so the answer is in ascending internal-id order like
+//   the reference's (hrnn.h:2055).
+// A query whose table or accepted list overflows is flagged and answered by the
+// global-memory warp kernel instead.
+#include <cfloat>
+
+#include "beam.cuh"
+#include "index.hpp"
+
+namespace hrnn {
+
+namespace {
+
+constexpr uint32_t kHS = 8192;        // table slots
+constexpr uint32_t kPartTarget = 3072; // postings per range (load <= ~0.4)
+constexpr uint32_t kACap = 1024;      // accepted per range
+constexpr int kBCThreads = 256;
+
+template <class E>
+__device__ __forceinline__ uint32_t owner_of(const void* ent, uint64_t i, uint32_t rb) {
+    return (uint32_t)(((const E*)ent)[i] >> rb);
+}
+
+// Two exact distances per half-warp with the loads of both vectors in flight.
+template <bool FUSED>
+__device__ __forceinline__ void l2_half16_x2(const float* __restrict__ q, const float* __restrict__ x0,
+                                             const float* __restrict__ x1, uint32_t nb, int l, float& d0,
+                                             float& d1) {
+    float a0 = 0.f, a1 = 0.f;
+    uint32_t i = 0;
+    for (; i + 4 <= nb; i += 4) {
+        float u0 = __ldg(x0 + 16 * (i + 0) + l), u1 = __ldg(x0 + 16 * (i + 1) + l);
+        float u2 = __ldg(x0 + 16 * (i + 2) + l), u3 = __ldg(x0 + 16 * (i + 3) + l);
+        float w0 = __ldg(x1 + 16 * (i + 0) + l), w1 = __ldg(x1 + 16 * (i + 1) + l);
+        float w2 = __ldg(x1 + 16 * (i + 2) + l), w3 = __ldg(x1 + 16 * (i + 3) + l);
+        float q0 = q[16 * (i + 0) + l], q1 = q[16 * (i + 1) + l], q2 = q[16 * (i + 2) + l], q3 = q[16 * (i + 3) + l];
+        a0 = sq_step(a0, q0 - u0, FUSED);
+        a1 = sq_step(a1, q0 - w0, FUSED);
+        a0 = sq_step(a0, q1 - u1, FUSED);
+        a1 = sq_step(a1, q1 - w1, FUSED);
+        a0 = sq_step(a0, q2 - u2, FUSED);
+        a1 = sq_step(a1, q2 - w2, FUSED);
+        a0 = sq_step(a0, q3 - u3, FUSED);
+        a1 = sq_step(a1, q3 - w3, FUSED);
+    }
+    for (; i < nb; ++i) {
+        float qq = q[16 * i + l];
+        a0 = sq_step(a0, qq - __ldg(x0 + 16 * i + l), FUSED);
+        a1 = sq_step(a1, qq - __ldg(x1 + 16 * i + l), FUSED);
+    }
+    float s0 = __shfl_sync(0xFFFFFFFFu, a0, 0, 16), s1 = __shfl_sync(0xFFFFFFFFu, a1, 0, 16);
+#pragma unroll
+    for (int k = 1; k < 16; ++k) {
+        s0 = __fadd_rn(s0, __shfl_sync(0xFFFFFFFFu, a0, k, 16));
+        s1 = __fadd_rn(s1, __shfl_sync(0xFFFFFFFFu, a1, k, 16));
+    }
+    d0 = s0;
+    d1 = s1;
+}
+
+}  // namespace
+
+__global__ void k_kdist_column(DevView v, uint32_t kidx, float* __restrict__ kcol) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= v.n) return;
+    float kd;
+    if (v.kdist_serve) {
+        kd = v.kdist_serve[(size_t)i * v.mks + kidx];
+    } else {
+        uint32_t c = v.knn_hdr[i] & 0xFFFFu;
+        kd = kidx >= c ? FLT_MAX : v.knn_dist[(size_t)i * v.K + kidx];
+    }
+    kcol[i] = kd;
+}
+
+// dynamic shared memory: q[dim] | keys[kHS] | cnt[kHS] (threshold > 1 only) |
+// stage[warps][32] | acc[kACap] | ctl[8]
+__host__ size_t bc_cta_smem(uint32_t dim, bool counts) {
+    return (size_t)dim * 4 + (size_t)kHS * 4 + (counts ? (size_t)kHS * 4 : 0) + (kBCThreads / 32) * 32 * 4 +
+           (size_t)kACap * 4 + 64;
+}
+
+template <class E, bool FUSED, bool COUNTS>
+__global__ void __launch_bounds__(kBCThreads) k_phase_bc_cta(
+    DevView v, const float* __restrict__ Q, uint32_t nq, uint32_t mmax, const uint32_t* __restrict__ prox,
+    const uint32_t* __restrict__ nprox, const uint32_t* __restrict__ plen, const uint64_t* __restrict__ qtotal,
+    const uint64_t* __restrict__ res_off, float threshold, const float* __restrict__ kcol,
+    uint64_t* __restrict__ resbuf, uint32_t* __restrict__ res_count, uint32_t* __restrict__ next_q,
+    uint32_t* __restrict__ overflow_list, uint32_t* __restrict__ n_overflow, SearchCounters* __restrict__ ctr) {
+    extern __shared__ char smraw[];
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5, half = lane >> 4, l = lane & 15;
+    constexpr int NW = kBCThreads / 32;
+    float* q = (float*)smraw;
+    uint32_t* keys = (uint32_t*)(q + v.dim);
+    uint32_t* cnt = keys + kHS;
+    uint32_t* stage = COUNTS ? cnt + kHS : cnt;
+    uint32_t* acc = stage + NW * 32;
+    uint32_t* ctl = acc + kACap;  // 0: query, 1: accepted count, 2: overflow, 3: table full
+    unsigned long long c_post = 0, c_cand = 0, c_ver = 0, c_res = 0;
+    const bool fast = v.lanes == 16 && (v.dim % 16) == 0;
+    for (;;) {
+        __syncthreads();
+        if (tid == 0) ctl[0] = atomicAdd(next_q, 1u);
+        __syncthreads();
+        const uint32_t qi = ctl[0];
+        if (qi >= nq) break;
+        const uint64_t T = qtotal[qi];
+        const uint32_t np_ = nprox[qi];
+        if (T == 0) {
+            if (tid == 0) res_count[qi] = 0;
+            continue;
+        }
+        for (uint32_t i = tid; i < v.dim; i += kBCThreads) q[i] = Q[(size_t)qi * v.dim + i];
+        const uint32_t P = (uint32_t)((T + kPartTarget - 1) / kPartTarget);
+        const uint32_t width = (v.n + P - 1) / P;
+        const uint64_t ro = res_off[qi];
+        uint32_t written = 0;
+        bool overflow = false;
+        for (uint32_t part = 0; part < P && !overflow; ++part) {
+            const uint32_t lo = part * width, hi = min(v.n, lo + width);
+            for (uint32_t i = tid; i < kHS; i += kBCThreads) {
+                keys[i] = kInvalid;
+                if (COUNTS) cnt[i] = 0;
+            }
+            if (tid == 0) {
+                ctl[1] = 0;
+                ctl[3] = 0;
+            }
+            __syncthreads();
+            // ---- phase B: postings of this id range into the table ----
+            for (uint32_t pi = 0; pi < np_; ++pi) {
+                const uint32_t p = prox[(size_t)qi * mmax + pi];
+                const uint32_t len = plen[(size_t)qi * mmax + pi];
+                const uint64_t b = v.csr_off[p];
+                if (part == 0) c_post += (tid == 0) ? len : 0;
+                for (uint32_t e = tid; e < len; e += kBCThreads) {
+                    const uint32_t o = owner_of<E>(v.csr_ent, b + e, v.rank_bits);
+                    if (o < lo || o >= hi) continue;
+                    uint32_t slot = hash32(o) & (kHS - 1);
+                    uint32_t probes = 0;
+                    for (;;) {
+                        uint32_t old = atomicCAS(&keys[slot], kInvalid, o);
+                        if (old == kInvalid || old == o) {
+                            if (COUNTS) atomicAdd(&cnt[slot], 1u);
+                            break;
+                        }
+                        slot = (slot + 1) & (kHS - 1);
+                        if (++probes >= kHS) {
+                            ctl[3] = 1;
+                            break;
+                        }
+                    }
+                }
+            }
+            __syncthreads();
+            if (ctl[3]) {
+                overflow = true;
+                break;
+            }
+            // ---- phase C: verify the table's candidates ----
+            for (uint32_t base = w * 32; base < kHS; base += NW * 32) {
+                const uint32_t s = base + lane;
+                const uint32_t key = keys[s];
+                bool valid = key != kInvalid;
+                if (COUNTS && valid) valid = (float)cnt[s] >= threshold;
+                const uint32_t nonempty = __ballot_sync(0xFFFFFFFFu, key != kInvalid);
+                if (lane == 0) c_cand += __popc(nonempty);
+                const uint32_t bal = __ballot_sync(0xFFFFFFFFu, valid);
+                const uint32_t nv = __popc(bal);
+                uint32_t* st = stage + w * 32;
+                if (valid) st[__popc(bal & lanemask_lt())] = key;
+                __syncwarp();
+                if (lane == 0) c_ver += nv;
+                for (uint32_t r = 0; r < nv; r += 4) {
+                    const uint32_t t0 = r + half, t1 = r + 2 + half;
+                    const uint32_t id0 = st[t0 < nv ? t0 : r], id1 = st[t1 < nv ? t1 : r];
+                    const float k0 = __ldg(kcol + id0), k1 = __ldg(kcol + id1);
+                    float d0, d1;
+                    if (fast) {
+                        l2_half16_x2<FUSED>(q, v.vec + (size_t)id0 * v.dim, v.vec + (size_t)id1 * v.dim, v.nb, l, d0,
+                                            d1);
+                    } else {
+                        d0 = l2_thread(q, v.vec + (size_t)id0 * v.dim, v.dim, v.lanes, v.fused);
+                        d1 = l2_thread(q, v.vec + (size_t)id1 * v.dim, v.dim, v.lanes, v.fused);
+                    }
+                    if (l == 0) {
+                        if (t0 < nv && d0 <= k0) {
+                            uint32_t pos = atomicAdd(&ctl[1], 1u);
+                            if (pos < kACap) acc[pos] = id0;
+                        }
+                        if (t1 < nv && d1 <= k1) {
+                            uint32_t pos = atomicAdd(&ctl[1], 1u);
+                            if (pos < kACap) acc[pos] = id1;
+                        }
+                    }
+                }
+                __syncwarp();
+            }
+            __syncthreads();
+            const uint32_t na = ctl[1];
+            if (na > kACap) {
+                overflow = true;
+                break;
+            }
+            // ---- sort this range's accepted ids, append labels ----
+            uint32_t PP = 2;
+            while (PP < na) PP <<= 1;
+            for (uint32_t i = na + tid; i < PP; i += kBCThreads) acc[i] = kInvalid;
+            __syncthreads();
+            for (uint32_t k = 2; k <= PP; k <<= 1)
+                for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+                    for (uint32_t i = tid; i < PP; i += kBCThreads) {
+                        uint32_t y = i ^ j;
+                        if (y > i) {
+                            uint32_t a = acc[i], c = acc[y];
+                            if ((a > c) == ((i & k) == 0)) {
+                                acc[i] = c;
+                                acc[y] = a;
+                            }
+                        }
+                    }
+                    __syncthreads();
+                }
+            for (uint32_t i = tid; i < na; i += kBCThreads) resbuf[ro + written + i] = v.labels[acc[i]];
+            written += na;
+            __syncthreads();
+        }
+        if (tid == 0) {
+            if (overflow) {
+                overflow_list[atomicAdd(n_overflow, 1u)] = qi;
+            } else {
+                res_count[qi] = written;
+                c_res += written;
+            }
+        }
+    }
+    if (lane == 0) {
+        atomicAdd(&ctr->n_posting, c_post);
+        atomicAdd(&ctr->n_cand, c_cand);
+        atomicAdd(&ctr->n_verified, c_ver);
+        atomicAdd(&ctr->n_result, c_res);
+    }
+}
+
+// explicit instantiations used by search_plain.cu
+#define INST(E, F, C)                                                                                               \
+    template __global__ void k_phase_bc_cta<E, F, C>(DevView, const float*, uint32_t, uint32_t, const uint32_t*,    \
+                                                     const uint32_t*, const uint32_t*, const uint64_t*,             \
+                                                     const uint64_t*, float, const float*, uint64_t*, uint32_t*,    \
+                                                     uint32_t*, uint32_t*, uint32_t*, SearchCounters*);
+INST(uint32_t, false, false)
+INST(uint32_t, false, true)
+INST(uint32_t, true, false)
+INST(uint32_t, true, true)
+INST(uint64_t, false, false)
+INST(uint64_t, false, true)
+INST(uint64_t, true, false)
+INST(uint64_t, true, true)
+#undef INST
+
+}  // namespace hrnn

@@ -23,6 +23,14 @@
 
 namespace hrnn {
 
+// search_bc.cu
+template <class E, bool FUSED, bool COUNTS>
+__global__ void k_phase_bc_cta(DevView, const float*, uint32_t, uint32_t, const uint32_t*, const uint32_t*,
+                               const uint32_t*, const uint64_t*, const uint64_t*, float, const float*, uint64_t*,
+                               uint32_t*, uint32_t*, uint32_t*, uint32_t*, SearchCounters*);
+__global__ void k_kdist_column(DevView v, uint32_t kidx, float* kcol);
+size_t bc_cta_smem(uint32_t dim, bool counts);
+
 namespace {
 
 template <bool FUSED>
@@ -113,6 +121,7 @@ __global__ void __launch_bounds__(128) k_phase_bc(DevView v, const float* __rest
                                                   uint32_t* __restrict__ hcnt_pool, uint32_t* __restrict__ list_pool,
                                                   size_t list_stride, uint64_t* __restrict__ resbuf,
                                                   uint32_t* __restrict__ res_count, uint32_t* __restrict__ next_q,
+                                                  const uint32_t* __restrict__ qlist,
                                                   SearchCounters* __restrict__ ctr) {
     extern __shared__ char smem_raw[];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, wpb = blockDim.x >> 5;
@@ -129,6 +138,7 @@ __global__ void __launch_bounds__(128) k_phase_bc(DevView v, const float* __rest
         if (lane == 0) qi = atomicAdd(next_q, 1u);
         qi = __shfl_sync(0xFFFFFFFFu, qi, 0);
         if (qi >= nq) break;
+        if (qlist) qi = qlist[qi];
         const uint32_t np_ = nprox[qi];
         for (uint32_t i = lane; i < v.dim; i += 32) q[i] = Q[(size_t)qi * v.dim + i];
         if (lane == 0) *nc_s = 0;
@@ -332,7 +342,7 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
     uint32_t* d_rcount = (uint32_t*)(d_resoff + (nq + 1));
     uint32_t* d_next = d_rcount + (nq + 1);
     CUDA_CHECK(cudaMemsetAsync(d_total, 0, (nq + 1) * 8, s));
-    CUDA_CHECK(cudaMemsetAsync(d_rcount, 0, (nq + 1) * 4 + 4, s));
+    CUDA_CHECK(cudaMemsetAsync(d_rcount, 0, (nq + 1) * 4 + 16, s));
     SearchCounters* ctr = ix.counters.as<SearchCounters>();
     const bool fusedsimd = (ix.order.fused & 1) != 0;
     const int nsm = sms(ix.device);
@@ -359,45 +369,81 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
     CUDA_CHECK(cudaMemcpyAsync(htot.data(), d_total, nq * 8, cudaMemcpyDeviceToHost, s));
     CUDA_CHECK(cudaMemcpyAsync(&sum_total, d_resoff + nq, 8, cudaMemcpyDeviceToHost, s));
     CUDA_CHECK(cudaStreamSynchronize(s));
-    uint64_t tmax = 1;
-    for (size_t i = 0; i < nq; ++i) tmax = std::max(tmax, htot[i]);
-    uint32_t hcap = 64;
-    while (hcap < 2 * tmax) hcap <<= 1;
-    // Warp slots for phase B/C, bounded by a scratch budget.
-    size_t per_slot = (size_t)hcap * 8 + tmax * 4;
-    size_t slots = std::max<size_t>(1, std::min<size_t>((size_t)nsm * 8 * 4, (size_t)(6ull << 30) / per_slot));
-    slots = std::min(slots, ((nq + 3) / 4) * 4);
-    slots = (slots + 3) / 4 * 4;
     DevMem& hkey = ix.scratch[5];
     DevMem& hcnt = ix.scratch[6];
     DevMem& res = ix.scratch[7];
-    size_t need_h = slots * (size_t)hcap * 4;
-    if (hkey.bytes < need_h) {
-        hkey.alloc(need_h);
-        hcnt.alloc(need_h);
-        CUDA_CHECK(cudaMemsetAsync(hkey.p, 0xFF, need_h, s));
-        CUDA_CHECK(cudaMemsetAsync(hcnt.p, 0, need_h, s));
-    }
-    const size_t list_bytes = (slots * tmax * 4 + 255) & ~(size_t)255;
     const size_t res_bytes = std::max<uint64_t>(sum_total, 1) * 8;
-    res.ensure(list_bytes + res_bytes);
-    uint32_t* list_pool = res.as<uint32_t>();
-    uint64_t* resbuf = (uint64_t*)(res.as<char>() + list_bytes);
+    res.ensure(res_bytes + (nq + 1) * 4 + 256);
+    uint64_t* resbuf = res.as<uint64_t>();
+    uint32_t* ovl = (uint32_t*)(res.as<char>() + ((res_bytes + 255) & ~(size_t)255));
+    uint32_t* d_nov = d_next + 1;  // spare counters after d_next, zeroed with d_rcount
     CUDA_CHECK(cudaEventRecord(ev[2], s));
     {
+        // Per-call column of kdist(p, k-1) (hrnn.h:286-293), then one CTA per query.
         const uint32_t kidx = (uint32_t)(a.k - 1);
-        size_t smem = 4 * (v.dim * 4 + 16);
-        void (*kern)(DevView, const float*, uint32_t, uint32_t, const uint32_t*, const uint32_t*, const uint32_t*,
-                     const uint64_t*, float, uint32_t, uint32_t, uint32_t*, uint32_t*, uint32_t*, size_t, uint64_t*,
-                     uint32_t*, uint32_t*, SearchCounters*);
-        if (ix.wide) kern = fusedsimd ? k_phase_bc<uint64_t, true> : k_phase_bc<uint64_t, false>;
-        else kern = fusedsimd ? k_phase_bc<uint32_t, true> : k_phase_bc<uint32_t, false>;
-        kern<<<(unsigned)(slots / 4), 128, smem, s>>>(v, a.d_q, (uint32_t)nq, mmax, prox.as<uint32_t>(),
-                                                      nprox.as<uint32_t>(), plen.as<uint32_t>(), d_resoff,
-                                                      a.threshold, kidx, hcap, hkey.as<uint32_t>(),
-                                                      hcnt.as<uint32_t>(), list_pool, (size_t)tmax, resbuf,
-                                                      d_rcount, d_next, ctr);
+        ix.kcol.ensure((size_t)std::max<size_t>(ix.cur, 1) * 4);
+        k_kdist_column<<<(unsigned)((ix.cur + 255) / 256), 256, 0, s>>>(v, kidx, ix.kcol.as<float>());
         CUDA_LAUNCH_CHECK();
+        const bool counts = a.threshold > 1.0f;
+        const size_t smem = bc_cta_smem(v.dim, counts);
+        using KCta = void (*)(DevView, const float*, uint32_t, uint32_t, const uint32_t*, const uint32_t*,
+                              const uint32_t*, const uint64_t*, const uint64_t*, float, const float*, uint64_t*,
+                              uint32_t*, uint32_t*, uint32_t*, uint32_t*, SearchCounters*);
+        KCta kc;
+        if (ix.wide)
+            kc = fusedsimd ? (counts ? k_phase_bc_cta<uint64_t, true, true> : k_phase_bc_cta<uint64_t, true, false>)
+                           : (counts ? k_phase_bc_cta<uint64_t, false, true> : k_phase_bc_cta<uint64_t, false, false>);
+        else
+            kc = fusedsimd ? (counts ? k_phase_bc_cta<uint32_t, true, true> : k_phase_bc_cta<uint32_t, true, false>)
+                           : (counts ? k_phase_bc_cta<uint32_t, false, true> : k_phase_bc_cta<uint32_t, false, false>);
+        CUDA_CHECK(cudaFuncSetAttribute(kc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        int per_sm = 1;
+        CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kc, 256, smem));
+        unsigned grid = (unsigned)std::min<size_t>(nq, (size_t)nsm * std::max(per_sm, 1));
+        kc<<<grid, 256, smem, s>>>(v, a.d_q, (uint32_t)nq, mmax, prox.as<uint32_t>(), nprox.as<uint32_t>(),
+                                   plen.as<uint32_t>(), d_total, d_resoff, a.threshold, ix.kcol.as<float>(), resbuf,
+                                   d_rcount, d_next, ovl, d_nov, ctr);
+        CUDA_LAUNCH_CHECK();
+        // Queries whose shared-memory table or accepted list overflowed: the
+        // global-memory warp kernel, with a table sized for their posting count.
+        uint32_t nov = 0;
+        CUDA_CHECK(cudaMemcpyAsync(&nov, d_nov, 4, cudaMemcpyDeviceToHost, s));
+        CUDA_CHECK(cudaStreamSynchronize(s));
+        if (nov) {
+            std::vector<uint32_t> hov(nov);
+            CUDA_CHECK(cudaMemcpy(hov.data(), ovl, nov * 4, cudaMemcpyDeviceToHost));
+            uint64_t tmax = 1;
+            for (uint32_t qi : hov) tmax = std::max(tmax, htot[qi]);
+            uint32_t hcap = 64;
+            while (hcap < 2 * tmax) hcap <<= 1;
+            size_t per_slot = (size_t)hcap * 8 + tmax * 4;
+            size_t slots = std::max<size_t>(1, std::min<size_t>((size_t)nsm * 8 * 4, (size_t)(4ull << 30) / per_slot));
+            slots = std::min<size_t>(slots, ((size_t)nov + 3) / 4 * 4);
+            slots = (slots + 3) / 4 * 4;
+            size_t need_h = slots * (size_t)hcap * 4;
+            if (hkey.bytes < need_h) {
+                hkey.alloc(need_h);
+                hcnt.alloc(need_h);
+                CUDA_CHECK(cudaMemsetAsync(hkey.p, 0xFF, need_h, s));
+                CUDA_CHECK(cudaMemsetAsync(hcnt.p, 0, need_h, s));
+            }
+            DevMem& lp = ix.scratch[4];
+            lp.ensure(slots * tmax * 4 + 64);
+            uint32_t* d_next2 = d_next + 2;
+            CUDA_CHECK(cudaMemsetAsync(d_next2, 0, 4, s));
+            size_t smem_w = 4 * (v.dim * 4 + 16);
+            void (*kern)(DevView, const float*, uint32_t, uint32_t, const uint32_t*, const uint32_t*, const uint32_t*,
+                         const uint64_t*, float, uint32_t, uint32_t, uint32_t*, uint32_t*, uint32_t*, size_t,
+                         uint64_t*, uint32_t*, uint32_t*, const uint32_t*, SearchCounters*);
+            if (ix.wide) kern = fusedsimd ? k_phase_bc<uint64_t, true> : k_phase_bc<uint64_t, false>;
+            else kern = fusedsimd ? k_phase_bc<uint32_t, true> : k_phase_bc<uint32_t, false>;
+            kern<<<(unsigned)(slots / 4), 128, smem_w, s>>>(v, a.d_q, nov, mmax, prox.as<uint32_t>(),
+                                                            nprox.as<uint32_t>(), plen.as<uint32_t>(), d_resoff,
+                                                            a.threshold, kidx, hcap, hkey.as<uint32_t>(),
+                                                            hcnt.as<uint32_t>(), lp.as<uint32_t>(), (size_t)tmax,
+                                                            resbuf, d_rcount, d_next2, ovl, ctr);
+            CUDA_LAUNCH_CHECK();
+        }
     }
     exclusive_scan_u32_to_u64(d_rcount, a.d_out_offsets, nq + 1, s, tmp);
     uint64_t total = 0;

@@ -89,3 +89,15 @@ def test_reference_reads_gpu_index(built):
     a = r.search_batch(Q, 10, 64, 100, k=10)
     b = h.search_rknn_batch(Q, 10, 64, 100, k=10)
     assert all(np.array_equal(x, y) for x, y in zip(a, b))
+
+
+def test_large_answer_sets_match_oracle(built):
+    """k = K_knng and many proxies: answer sets of hundreds to thousands of points
+    (exercises the overflow path of the shared-memory phase B/C kernel)."""
+    X, Q, h, p, _ = built
+    O = port.OracleIndex(idx.read_idx(p))
+    for m, kp, k, th in ((50, 64, 64, 1.0), (40, 64, 64, 2.0), (30, 16, 40, 1.0)):
+        a = h.search_rknn_batch(Q[:60], m, kp, 100, threshold=th, k=k)
+        b = O.search_batch(Q[:60], m, kp, 100, threshold=th, k=k)
+        assert all(np.array_equal(x, y) for x, y in zip(a, b)), (m, kp, k, th)
+    assert max(len(x) for x in a) > 100
