@@ -312,6 +312,14 @@ __global__ void k_bucket_fill(const Prop* __restrict__ prop, unsigned long long 
 constexpr int kMergeWarps = 4;
 constexpr uint32_t kPiece = 1024;
 
+// Shared memory of one merge warp: keys (u64, first, so 8-byte alignment needs a
+// per-warp stride that is a multiple of 8), the list twice (d, id, flag), the id
+// table.  Rounded up to 16 bytes.
+__host__ __device__ inline size_t merge_warp_bytes(uint32_t K, uint32_t hcap) {
+    size_t b = (size_t)K * 18 + (size_t)kPiece * 8 + (size_t)hcap * 4 + 64;
+    return (b + 15) & ~(size_t)15;
+}
+
 __device__ __forceinline__ uint32_t hmix(uint32_t x) {
     x ^= x >> 16;
     x *= 0x7feb352dU;
@@ -328,7 +336,7 @@ __global__ void __launch_bounds__(kMergeWarps * 32) k_merge(uint32_t n, uint32_t
                                                            uint32_t hcap, unsigned long long* __restrict__ nupd) {
     extern __shared__ char smraw[];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const size_t per_warp = (size_t)K * 18 + (size_t)kPiece * 8 + (size_t)hcap * 4 + 64;
+    const size_t per_warp = merge_warp_bytes(K, hcap);  // multiple of 16: the u64 keys stay aligned
     char* base = smraw + w * per_warp;
     uint64_t* keys = (uint64_t*)base;
     float* Ld = (float*)(keys + kPiece);
@@ -531,7 +539,7 @@ void refine_knng(Index& ix, int iters, int sample) {
     }
     uint32_t hcap = 64;
     while (hcap < 2 * K) hcap <<= 1;
-    const size_t merge_smem = (size_t)kMergeWarps * ((size_t)K * 18 + (size_t)kPiece * 8 + (size_t)hcap * 4 + 64);
+    const size_t merge_smem = (size_t)kMergeWarps * merge_warp_bytes(K, hcap);
     if (merge_smem > 227 * 1024) fail(HRNN_ERR_ARG, "refineKNNG: K_knng too large for the merge kernel");
     CUDA_CHECK(cudaFuncSetAttribute(k_merge, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)merge_smem));
     const int g1 = nsm * 16;

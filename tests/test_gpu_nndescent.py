@@ -64,3 +64,27 @@ def test_refine_matches_live_reference_d128(tmp_path):
     exact = np.argsort(D, axis=1)[:, :80]
     rec = np.mean([len(np.intersect1d(exact[i], got[0][i, :got[2][i]])) / 80 for i in range(500)])
     assert rec > 0.9
+
+
+@pytest.mark.parametrize("K", [30, 7])
+def test_refine_odd_list_widths_match_oracle(golden_refine, tmp_path, K):
+    """K_knng values whose per-warp merge buffer is not a multiple of 8 bytes
+    before rounding (K * 18 % 8 != 0)."""
+    g = golden_refine
+    X = g["X"]
+    n = X.shape[0]
+    w = min(K, g["pre_ids"].shape[1])
+    ids = np.zeros((n, K), np.uint32)
+    d = np.zeros((n, K), np.float32)
+    ids[:, :w] = g["pre_ids"][:, :w]
+    d[:, :w] = g["pre_dists"][:, :w]
+    cnt = np.minimum(g["pre_cnt"], w).astype(np.uint32)
+    p = str(tmp_path / f"k{K}.idx")
+    idx.write_idx(p, X, ids, d, cnt, M=8)
+    h = H.HRNN.load(p, X.shape[1])
+    h.refineKNNG(3, 10)
+    got = h.get_knng()
+    oi, od, oc = ids.copy(), d.copy(), cnt.copy()
+    flags = (np.arange(K)[None, :] < oc[:, None]).astype(np.uint8)
+    port.refine(X, oi, od, oc, flags, 3, 10)
+    _same_lists(*got, oi, od, oc)
