@@ -68,20 +68,119 @@ __device__ __forceinline__ float warp_l2_one(const DevView& v, const float* q, u
     return l2_thread(q, v.vec + (size_t)id * v.dim, v.dim, v.lanes, v.fused);
 }
 
+// One thread, one row, 16-lane order (the AVX-512 path of space_l2.h:25-54):
+// accumulator l takes elements l, l+16, ...; the row is read with 16-byte loads,
+// two 64-byte blocks at a time, so a warp keeps up to 32 rows in flight.  q is
+// in shared memory (16-byte aligned); every thread reads the same q words.
+template <bool FUSED>
+__device__ __forceinline__ float l2_row16(const float* __restrict__ q, const float* __restrict__ x, uint32_t nb) {
+    float acc[16];
+#pragma unroll
+    for (int l = 0; l < 16; ++l) acc[l] = 0.f;
+    const float4* x4 = reinterpret_cast<const float4*>(x);
+    const float4* q4 = reinterpret_cast<const float4*>(q);
+    uint32_t i = 0;
+    for (; i + 2 <= nb; i += 2) {
+        float4 a[8];
+#pragma unroll
+        for (int c = 0; c < 8; ++c) a[c] = __ldg(x4 + 4 * i + c);
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            const float4 p = q4[4 * i + c];
+            const int l = (c & 3) * 4;
+            acc[l + 0] = sq_step(acc[l + 0], p.x - a[c].x, FUSED);
+            acc[l + 1] = sq_step(acc[l + 1], p.y - a[c].y, FUSED);
+            acc[l + 2] = sq_step(acc[l + 2], p.z - a[c].z, FUSED);
+            acc[l + 3] = sq_step(acc[l + 3], p.w - a[c].w, FUSED);
+        }
+    }
+    if (i < nb) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const float4 a = __ldg(x4 + 4 * i + c);
+            const float4 p = q4[4 * i + c];
+            const int l = c * 4;
+            acc[l + 0] = sq_step(acc[l + 0], p.x - a.x, FUSED);
+            acc[l + 1] = sq_step(acc[l + 1], p.y - a.y, FUSED);
+            acc[l + 2] = sq_step(acc[l + 2], p.z - a.z, FUSED);
+            acc[l + 3] = sq_step(acc[l + 3], p.w - a.w, FUSED);
+        }
+    }
+    float s = acc[0];
+#pragma unroll
+    for (int l = 1; l < 16; ++l) s = __fadd_rn(s, acc[l]);
+    return s;
+}
+
+// Two lanes per row (lane parity p owns accumulators 8p..8p+7, i.e. float4 #2p and
+// #2p+1 of every 16-element block); all of a lane's loads for its half row are
+// issued before the accumulation, so 16 rows of a warp cost one memory round trip.
+template <bool FUSED, int NB>
+__device__ __forceinline__ float l2_pair16(const float* __restrict__ q, const float* __restrict__ x, int p) {
+    const float4* x4 = reinterpret_cast<const float4*>(x);
+    const float4* q4 = reinterpret_cast<const float4*>(q);
+    float4 a[2 * NB];
+#pragma unroll
+    for (int i = 0; i < NB; ++i) {
+        a[2 * i] = __ldg(x4 + 4 * i + 2 * p);
+        a[2 * i + 1] = __ldg(x4 + 4 * i + 2 * p + 1);
+    }
+    float acc[8];
+#pragma unroll
+    for (int l = 0; l < 8; ++l) acc[l] = 0.f;
+#pragma unroll
+    for (int i = 0; i < NB; ++i) {
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            const float4 qq = q4[4 * i + 2 * p + c];
+            const float4 xx = a[2 * i + c];
+            acc[4 * c + 0] = sq_step(acc[4 * c + 0], qq.x - xx.x, FUSED);
+            acc[4 * c + 1] = sq_step(acc[4 * c + 1], qq.y - xx.y, FUSED);
+            acc[4 * c + 2] = sq_step(acc[4 * c + 2], qq.z - xx.z, FUSED);
+            acc[4 * c + 3] = sq_step(acc[4 * c + 3], qq.w - xx.w, FUSED);
+        }
+    }
+    // TmpRes[0] + ... + TmpRes[15] left to right: the even lane owns 0..7.
+    float hi[8];
+#pragma unroll
+    for (int l = 0; l < 8; ++l) hi[l] = __shfl_down_sync(0xFFFFFFFFu, acc[l], 1);
+    float s = acc[0];
+#pragma unroll
+    for (int l = 1; l < 8; ++l) s = __fadd_rn(s, acc[l]);
+#pragma unroll
+    for (int l = 0; l < 8; ++l) s = __fadd_rn(s, hi[l]);
+    return s;  // valid in the even lane
+}
+
+template <bool FUSED, int NB>
+__device__ __forceinline__ void warp_l2_pairs(const DevView& v, const float* q, const uint32_t* ids, uint32_t cnt,
+                                              float* dout) {
+    const int lane = threadIdx.x & 31, p = lane & 1;
+    for (uint32_t r = 0; r < cnt; r += 16) {
+        const uint32_t t = r + (lane >> 1);
+        const uint32_t id = ids[t < cnt ? t : r];
+        const float d = l2_pair16<FUSED, NB>(q, v.vec + (size_t)id * v.dim, p);
+        if (p == 0 && t < cnt) dout[t] = d;
+    }
+}
+
 // Distances of q to cnt (<= 32) stored vectors ids[0..cnt) -> dout[0..cnt).
+// dims 96/128/256 with the 16-lane order: two lanes per row (l2_pair16);
+// other multiples of 16: one row per lane; other dims or orders: l2_thread.
 template <bool FUSED>
 __device__ __forceinline__ void warp_l2_list(const DevView& v, const float* q, const uint32_t* ids, uint32_t cnt,
                                              float* dout) {
-    int lane = threadIdx.x & 31, half = lane >> 4, l = lane & 15;
-    if (v.lanes == 16 && v.dim % 16 == 0) {
-        for (uint32_t r = 0; r < cnt; r += 2) {
-            uint32_t t = r + half;
-            uint32_t id = ids[t < cnt ? t : r];
-            float d = l2_half16<FUSED>(q, v.vec + (size_t)id * v.dim, v.nb, l);
-            if (l == 0 && t < cnt) dout[t] = d;
-        }
-    } else {
-        if ((uint32_t)lane < cnt) dout[lane] = l2_thread(q, v.vec + (size_t)ids[lane] * v.dim, v.dim, v.lanes, v.fused);
+    const int lane = threadIdx.x & 31;
+    if (v.lanes == 16 && v.nb == 8 && v.dim == 128) {
+        warp_l2_pairs<FUSED, 8>(v, q, ids, cnt, dout);
+    } else if (v.lanes == 16 && v.nb == 6 && v.dim == 96) {
+        warp_l2_pairs<FUSED, 6>(v, q, ids, cnt, dout);
+    } else if (v.lanes == 16 && v.nb == 16 && v.dim == 256) {
+        warp_l2_pairs<FUSED, 16>(v, q, ids, cnt, dout);
+    } else if ((uint32_t)lane < cnt) {
+        const float* x = v.vec + (size_t)ids[lane] * v.dim;
+        dout[lane] = (v.lanes == 16 && v.dim % 16 == 0) ? l2_row16<FUSED>(q, x, v.nb)
+                                                         : l2_thread(q, x, v.dim, v.lanes, v.fused);
     }
     __syncwarp();
 }
@@ -99,7 +198,8 @@ struct WarpSmem {
 };
 
 __host__ __device__ inline size_t warp_smem_bytes(uint32_t dim, uint32_t efc, uint32_t vc) {
-    return (size_t)dim * 4 + (size_t)efc * 8 + (size_t)(efc + 32) * 8 + (size_t)vc * 4 + 32 * 12;
+    // multiple of 16 for dim % 4 == 0 and efc % 32 == 0 (q is read as float4)
+    return (size_t)dim * 4 + (size_t)(efc + 32) * 8 + (size_t)vc * 4 + 32 * 12 + 16;
 }
 
 __device__ inline WarpSmem carve(char* base, uint32_t dim, uint32_t efc, uint32_t vc) {
@@ -107,13 +207,11 @@ __device__ inline WarpSmem carve(char* base, uint32_t dim, uint32_t efc, uint32_
     s.q = (float*)base;
     base += (size_t)dim * 4;
     s.td = (float*)base;
-    base += (size_t)efc * 4;
+    base += (size_t)(efc + 32) * 4;
     s.ti = (uint32_t*)base;
-    base += (size_t)efc * 4;
-    s.xd = (float*)base;
     base += (size_t)(efc + 32) * 4;
-    s.xi = (uint32_t*)base;
-    base += (size_t)(efc + 32) * 4;
+    s.xd = nullptr;
+    s.xi = nullptr;
     s.vis = (uint32_t*)base;
     base += (size_t)vc * 4;
     s.nd = (float*)base;
@@ -258,27 +356,38 @@ __device__ uint32_t beam_search(const DevView& v, WarpSmem& s, uint32_t ep, floa
             if (acc) s.apos[__popc(ab & lanemask_lt())] = pos;
             __syncwarp();
             const uint32_t newsize = min(tsize + na, EF);
-            for (uint32_t k = lo + lane; k < tsize; k += 32) {
-                uint32_t sh = 0;
-                for (uint32_t a = 0; a < na; ++a) sh += (s.apos[a] <= k);
-                uint32_t np = k + sh;
-                if (np < newsize) {
-                    s.xd[np - lo] = s.td[k];
-                    s.xi[np - lo] = s.ti[k];
+            // In-place merge: existing entries at or after lo move right by the number
+            // of accepted neighbours inserted at or before them (at most 32), so the
+            // beam is shifted block by block from the right; every block is read
+            // before any lane writes, and its targets lie in itself or in blocks to
+            // its right that were already moved.
+            if (tsize > lo) {
+                for (int b = (int)lo + (int)(((tsize - lo - 1) / 32) * 32); b >= (int)lo; b -= 32) {
+                    const uint32_t k = (uint32_t)b + lane;
+                    float dk = 0.f;
+                    uint32_t ik = 0, np = 0xFFFFFFFFu;
+                    if (k < tsize) {
+                        dk = s.td[k];
+                        ik = s.ti[k];
+                        uint32_t sh = 0;
+                        for (uint32_t a = 0; a < na; ++a) sh += (s.apos[a] <= k);
+                        np = k + sh;
+                    }
+                    __syncwarp();
+                    if (np < newsize) {
+                        s.td[np] = dk;
+                        s.ti[np] = ik;
+                    }
+                    __syncwarp();
                 }
             }
             uint32_t npos = pos + before;
             if (acc && npos < newsize) {
-                s.xd[npos - lo] = d;
-                s.xi[npos - lo] = id;
+                s.td[npos] = d;
+                s.ti[npos] = id;
             }
             uint32_t mnp = (acc && npos < newsize) ? npos : 0xFFFFFFFFu;
             for (int o = 16; o; o >>= 1) mnp = min(mnp, __shfl_xor_sync(0xFFFFFFFFu, mnp, o));
-            __syncwarp();
-            for (uint32_t k = lo + lane; k < newsize; k += 32) {
-                s.td[k] = s.xd[k - lo];
-                s.ti[k] = s.xi[k - lo];
-            }
             tsize = newsize;
             cursor = min(cursor, mnp);
             __syncwarp();

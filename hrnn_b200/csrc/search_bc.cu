@@ -17,6 +17,7 @@
 // A query whose table or accepted list overflows is flagged and answered by the
 // global-memory warp kernel instead.
 #include <cfloat>
+#include <type_traits>
 
 #include "beam.cuh"
 #include "index.hpp"
@@ -90,7 +91,7 @@ __global__ void k_kdist_column(DevView v, uint32_t kidx, float* __restrict__ kco
 // dynamic shared memory: q[dim] | keys[kHS] | cnt[kHS] (threshold > 1 only) |
 // stage[warps][32] | acc[kACap] | ctl[8]
 __host__ size_t bc_cta_smem(uint32_t dim, bool counts) {
-    return (size_t)dim * 4 + (size_t)kHS * 4 + (counts ? (size_t)kHS * 4 : 0) + (kBCThreads / 32) * 32 * 4 +
+    return (size_t)dim * 4 + (size_t)kHS * 4 + (counts ? (size_t)kHS * 4 : 0) + (kBCThreads / 32) * 64 * 4 +
            (size_t)kACap * 4 + 64;
 }
 
@@ -108,7 +109,7 @@ __global__ void __launch_bounds__(kBCThreads) k_phase_bc_cta(
     uint32_t* keys = (uint32_t*)(q + v.dim);
     uint32_t* cnt = keys + kHS;
     uint32_t* stage = COUNTS ? cnt + kHS : cnt;
-    uint32_t* acc = stage + NW * 32;
+    uint32_t* acc = stage + NW * 64;
     uint32_t* ctl = acc + kACap;  // 0: query, 1: accepted count, 2: overflow, 3: table full
     unsigned long long c_post = 0, c_cand = 0, c_ver = 0, c_res = 0;
     const bool fast = v.lanes == 16 && (v.dim % 16) == 0;
@@ -172,6 +173,43 @@ __global__ void __launch_bounds__(kBCThreads) k_phase_bc_cta(
                 break;
             }
             // ---- phase C: verify the table's candidates ----
+            // Candidates are staged per warp until 32 are ready, then verified one
+            // row per lane (32 rows in flight per warp).
+            uint32_t* st = stage + w * 64;
+            uint32_t ns = 0;
+            auto accept = [&](uint32_t id) {
+                const uint32_t pos = atomicAdd(&ctl[1], 1u);
+                if (pos < kACap) acc[pos] = id;
+            };
+            // two lanes per row for the common dims (one memory round trip per 16
+            // rows), one row per lane otherwise
+            auto verify_pairs = [&](uint32_t cnt_, auto nbc) {
+                constexpr int NB = decltype(nbc)::value;
+                const int p = lane & 1;
+                for (uint32_t r = 0; r < cnt_; r += 16) {
+                    const uint32_t t = r + (lane >> 1);
+                    const uint32_t id = st[t < cnt_ ? t : r];
+                    const float kd = __ldg(kcol + id);
+                    const float d = l2_pair16<FUSED, NB>(q, v.vec + (size_t)id * v.dim, p);
+                    if (p == 0 && t < cnt_ && d <= kd) accept(id);
+                }
+            };
+            auto verify = [&](uint32_t cnt_) {
+                if (fast && v.dim == 128) {
+                    verify_pairs(cnt_, std::integral_constant<int, 8>{});
+                } else if (fast && v.dim == 96) {
+                    verify_pairs(cnt_, std::integral_constant<int, 6>{});
+                } else if (fast && v.dim == 256) {
+                    verify_pairs(cnt_, std::integral_constant<int, 16>{});
+                } else if ((uint32_t)lane < cnt_) {
+                    const uint32_t id = st[lane];
+                    const float kd = __ldg(kcol + id);
+                    const float* x = v.vec + (size_t)id * v.dim;
+                    const float d = fast ? l2_row16<FUSED>(q, x, v.nb) : l2_thread(q, x, v.dim, v.lanes, v.fused);
+                    if (d <= kd) accept(id);
+                }
+                __syncwarp();
+            };
             for (uint32_t base = w * 32; base < kHS; base += NW * 32) {
                 const uint32_t s = base + lane;
                 const uint32_t key = keys[s];
@@ -181,35 +219,21 @@ __global__ void __launch_bounds__(kBCThreads) k_phase_bc_cta(
                 if (lane == 0) c_cand += __popc(nonempty);
                 const uint32_t bal = __ballot_sync(0xFFFFFFFFu, valid);
                 const uint32_t nv = __popc(bal);
-                uint32_t* st = stage + w * 32;
-                if (valid) st[__popc(bal & lanemask_lt())] = key;
+                if (valid) st[ns + __popc(bal & lanemask_lt())] = key;
                 __syncwarp();
                 if (lane == 0) c_ver += nv;
-                for (uint32_t r = 0; r < nv; r += 4) {
-                    const uint32_t t0 = r + half, t1 = r + 2 + half;
-                    const uint32_t id0 = st[t0 < nv ? t0 : r], id1 = st[t1 < nv ? t1 : r];
-                    const float k0 = __ldg(kcol + id0), k1 = __ldg(kcol + id1);
-                    float d0, d1;
-                    if (fast) {
-                        l2_half16_x2<FUSED>(q, v.vec + (size_t)id0 * v.dim, v.vec + (size_t)id1 * v.dim, v.nb, l, d0,
-                                            d1);
-                    } else {
-                        d0 = l2_thread(q, v.vec + (size_t)id0 * v.dim, v.dim, v.lanes, v.fused);
-                        d1 = l2_thread(q, v.vec + (size_t)id1 * v.dim, v.dim, v.lanes, v.fused);
-                    }
-                    if (l == 0) {
-                        if (t0 < nv && d0 <= k0) {
-                            uint32_t pos = atomicAdd(&ctl[1], 1u);
-                            if (pos < kACap) acc[pos] = id0;
-                        }
-                        if (t1 < nv && d1 <= k1) {
-                            uint32_t pos = atomicAdd(&ctl[1], 1u);
-                            if (pos < kACap) acc[pos] = id1;
-                        }
-                    }
+                ns += nv;
+                if (ns >= 32) {
+                    verify(32);
+                    const uint32_t rest = ns - 32;
+                    const uint32_t mv = (uint32_t)lane < rest ? st[32 + lane] : 0;
+                    __syncwarp();
+                    if ((uint32_t)lane < rest) st[lane] = mv;
+                    __syncwarp();
+                    ns = rest;
                 }
-                __syncwarp();
             }
+            verify(ns);
             __syncthreads();
             const uint32_t na = ctl[1];
             if (na > kACap) {

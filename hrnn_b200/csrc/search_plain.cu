@@ -323,7 +323,7 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
     if (efmax > (1u << 16)) fail(HRNN_ERR_ARG, "searchRknn: ef_search/m too large (max 65536)");
     DevView v = make_view(ix);
     const uint32_t efc = (efmax + 31) & ~31u;
-    const uint32_t vc = 2048;
+    const uint32_t vc = 2048;  // visited-cache slots (lossy; misses cost a recomputed row)
     size_t wsm = warp_smem_bytes(v.dim, efc, vc);
     int wpb = (int)std::max<size_t>(1, std::min<size_t>(4, (200 * 1024) / wsm));
     size_t smem_a = wsm * wpb;
