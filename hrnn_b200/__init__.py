@@ -30,7 +30,7 @@ EXPORTS = [
     "hrnn_search_rknn", "hrnn_search_rknn_batch", "hrnn_search_rknn_batch_device",
     "hrnn_compact_for_serving", "hrnn_insert_dynamic", "hrnn_set_ef", "hrnn_get_info",
     "hrnn_get_search_stats", "hrnn_get_refine_stats", "hrnn_set_l2_order", "hrnn_detect_l2_order", "hrnn_get_knng",
-    "hrnn_set_knng", "hrnn_get_rknng", "hrnn_l2_batch",
+    "hrnn_set_knng", "hrnn_get_rknng", "hrnn_l2_batch", "hrnn_build_rknng_noalloc",
 ]
 
 
@@ -99,6 +99,8 @@ _lib.hrnn_set_knng.argtypes = [_vp, _vp, _vp, _vp]
 _lib.hrnn_get_rknng.argtypes = [_vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint32),
                                 C.POINTER(C.c_uint32), _vp, _vp, C.c_int]
 _lib.hrnn_l2_batch.argtypes = [_vp, _vp, _sz, _sz, C.c_int, C.c_int, _vp]
+_lib.hrnn_build_rknng_noalloc.argtypes = [_vp, _vp, _sz, _sz, _vp, _vp, _sz, C.POINTER(C.c_uint32),
+                                          C.POINTER(C.c_int), C.POINTER(C.c_uint64), _vp]
 
 
 class HrnnError(RuntimeError):
@@ -135,6 +137,17 @@ def l2_batch(A, B, lanes=16, fused=2) -> np.ndarray:
     out = np.empty(A.shape[0], np.float32)
     _check(_lib.hrnn_l2_batch(_p(A), _p(B), A.shape[0], A.shape[1], lanes, fused, _p(out)))
     return out
+
+
+def build_rknng_noalloc(d_knn_ids: int, d_knn_cnt: int, n: int, K: int, d_offsets: int, d_entries: int,
+                        entries_cap: int, stream: int = 0):
+    """Reverse-KNN CSR of a caller-owned device KNN graph, allocating nothing (for
+    callers that cannot call cudaMalloc).  Arguments are raw device pointers;
+    returns (rank_bits, wide, n_entries).  See include/hrnn_capi.h for the limits."""
+    rb, wide, ne = C.c_uint32(0), C.c_int(0), C.c_uint64(0)
+    _check(_lib.hrnn_build_rknng_noalloc(_vp(d_knn_ids), _vp(d_knn_cnt), n, K, _vp(d_offsets), _vp(d_entries),
+                                         entries_cap, C.byref(rb), C.byref(wide), C.byref(ne), _vp(stream)))
+    return rb.value, bool(wide.value), ne.value
 
 
 def _u32(x, n):

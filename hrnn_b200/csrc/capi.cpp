@@ -45,6 +45,10 @@ void set_device(hrnn_index* h) { CUDA_CHECK(cudaSetDevice(h->ix.device)); }
 
 }  // namespace
 
+namespace hrnn {
+void set_last_error(const std::string& m) { g_last_error = m; }
+}  // namespace hrnn
+
 extern "C" {
 
 const char* hrnn_last_error(void) { return g_last_error.c_str(); }

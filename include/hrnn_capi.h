@@ -193,6 +193,27 @@ hrnn_status hrnn_get_rknng(hrnn_index* h, uint64_t* n_offsets, uint64_t* n_entri
                            uint32_t* entry_bytes, uint32_t* rank_bits, uint64_t* offsets,
                            void* entries, int reference_order);
 
+/* Reverse-KNN CSR of a KNN graph the caller owns, with NO device allocation.
+ * No counterpart in the reference: it exists for callers that cannot call
+ * cudaMalloc (an arena that owns every device byte, or a serving loop that must
+ * not synchronise the device), and takes all buffers from the caller:
+ *   d_knn_ids  n x K u32 neighbour ids; d_knn_cnt n counts (low 16 bits used);
+ *   d_offsets  n+1 u64 out; d_entries entries_cap entries out -- u32 when
+ *              node_bits + rank_bits <= 32 (*wide = 0), else u64;
+ *   *n_entries receives the entry count (also on HRNN_ERR_CAPACITY).
+ * Same output as hrnn_build_rknng + hrnn_get_rknng(..., reference_order = 0).
+ * Its scratch is a fixed 32 MiB __device__ array in the library, held by every
+ * GPU that loads it: n is limited to 2,097,152 (HRNN_ERR_LIMIT beyond), and one
+ * reverse list to the scratch's staging size.  The first call on a device looks
+ * up the array's address (make it before any stream capture).  Calls share the
+ * array: calls that overlap on the GPU race; issue them one after another.
+ * Runs on `stream` (cudaStream_t) on the current device and returns after it
+ * finishes. */
+hrnn_status hrnn_build_rknng_noalloc(const uint32_t* d_knn_ids, const uint32_t* d_knn_cnt, size_t n,
+                                     size_t K, uint64_t* d_offsets, void* d_entries,
+                                     size_t entries_cap, uint32_t* rank_bits, int* wide,
+                                     uint64_t* n_entries, void* stream);
+
 /* Squared L2 of n pairs (a[i], b[i]) of dim floats on the device, in the order set by
  * hrnn_set_l2_order.  Host arrays.  (L2Space::get_dist_func, space_l2.h:240-248.) */
 hrnn_status hrnn_l2_batch(const float* a, const float* b, size_t n, size_t dim, int lanes,
