@@ -265,66 +265,112 @@ def main():
     log(f"[bench] fp64 ground truth ({time.perf_counter() - t_gt:.1f}s), mean |RkNN| "
         f"{np.mean([len(g) for g in gt]):.2f}, empty {sum(len(g) == 0 for g in gt)}")
     # GT ids are data indices; index labels are data indices too.
-    sweep = {}
-    m_star = None
-    for m in W["m_sweep"]:
-        res = h.search_rknn_batch(Q, m, W["Kp"], W["ef"], threshold=1.0, k=W["k"])
-        sweep[m] = macro_recall(gt, res)
-        log(f"[bench] m={m}: macro recall {sweep[m]:.4f}")
-        if m_star is None and sweep[m] >= TARGET_RECALL:
-            m_star = m
-    if m_star is None:
-        m_star = W["m_sweep"][-1]
-    params = {"m": m_star, "K_prime": W["Kp"], "ef_search": W["ef"], "k": W["k"], "threshold": 1.0}
+    nq, d = Q.shape
+    forms = {"plain": H.PREC_FP32_EXACT, "mixed": H.PREC_BF16}
+
+    def sweep_form(prec):
+        h.set_precision(prec)
+        sw, mstar = {}, None
+        for m in W["m_sweep"]:
+            res = h.search_rknn_batch(Q, m, W["Kp"], W["ef"], threshold=1.0, k=W["k"])
+            sw[m] = macro_recall(gt, res)
+            if mstar is None and sw[m] >= TARGET_RECALL:
+                mstar = m
+        return sw, (mstar if mstar is not None else W["m_sweep"][-1])
+
+    sweeps, mstars = {}, {}
+    for name, prec in forms.items():
+        sweeps[name], mstars[name] = sweep_form(prec)
+        log(f"[bench] {name}: recall sweep {json.dumps({k_: round(v_, 4) for k_, v_ in sweeps[name].items()})}"
+            f" -> m={mstars[name]}")
+    h.set_precision(H.PREC_FP32_EXACT)
+    params = {"m": mstars["plain"], "K_prime": W["Kp"], "ef_search": W["ef"], "k": W["k"], "threshold": 1.0}
 
     if args.impl == "reference":
-        run_reference_arm(args, W, h, Q, params, sweep, build)
+        run_reference_arm(args, W, h, Q, params, sweeps["plain"], build)
         return
 
-    # ---- timed device steps ----
-    nq, d = Q.shape
+    # ---- timed device steps, per form ----
     q_dev = torch.from_numpy(Q).to(dev)
-    m_dev = torch.full((nq,), m_star, dtype=torch.int32, device=dev)
     kp_dev = torch.full((nq,), W["Kp"], dtype=torch.int32, device=dev)
     ef_dev = torch.full((nq,), W["ef"], dtype=torch.int32, device=dev)
     cap = nq * 512
     off_dev = torch.zeros(nq + 1, dtype=torch.int64, device=dev)
     lab_dev = torch.zeros(cap, dtype=torch.int64, device=dev)
     stream = torch.cuda.current_stream(dev)
+    hbm, bf16, peak_kind = load_peaks()
+    maxM0 = 2 * W["M"]
 
-    def step():
-        return h.search_rknn_batch_device(q_dev.data_ptr(), nq, m_dev.data_ptr(), kp_dev.data_ptr(),
-                                          ef_dev.data_ptr(), 1.0, W["k"], off_dev.data_ptr(), lab_dev.data_ptr(),
-                                          cap, stream.cuda_stream)
+    def timed(prec, m_star, clocks=None):
+        h.set_precision(prec)
+        m_dev = torch.full((nq,), m_star, dtype=torch.int32, device=dev)
 
-    for _ in range(args.warmup):
-        step()
+        def step():
+            return h.search_rknn_batch_device(q_dev.data_ptr(), nq, m_dev.data_ptr(), kp_dev.data_ptr(),
+                                              ef_dev.data_ptr(), 1.0, W["k"], off_dev.data_ptr(),
+                                              lab_dev.data_ptr(), cap, stream.cuda_stream)
+
+        for _ in range(args.warmup):
+            step()
+        if world > 1:
+            torch.distributed.barrier()
+        dev_sync()
+        if clocks:
+            clocks.start()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.nvtx.range_push("timed")  # profilers select the timed steps with this range
+        e0.record(stream)
+        launches = 0
+        for _ in range(args.steps):
+            step()
+            launches += h.last_search_stats()["n_launches"]
+        e1.record(stream)
+        dev_sync()
+        torch.cuda.nvtx.range_pop()
+        ck = clocks.stop() if clocks else None
+        ms = e0.elapsed_time(e1)
+        if world > 1:
+            t = torch.tensor([ms], device=dev)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            ms = float(t.item())
+        st = h.last_search_stats()
+        # algorithmic bytes of the two phases (rows: 4 bytes/element FP32, 2 BF16)
+        rb = 2 if prec == H.PREC_BF16 else 4
+        bytes_a = st["n_dist"] * d * rb + st["n_expanded"] * (4 + 4 * maxM0)
+        bytes_bc = st["n_posting"] * 4 + st["n_verified"] * (d * rb + 4 + (4 if rb == 2 else 0)) + \
+            st["n_fp32_decided"] * d * 4 + st["n_result"] * 8
+        phases = {"phase_a_beam_search": (st["phase_a_ms"], bytes_a),
+                  "phase_bc_posting_verify": (st["phase_c_ms"], bytes_bc)}
+        dom = max(phases, key=lambda k_: phases[k_][0])
+        tms, tb = phases[dom]
+        achieved = tb / (tms / 1e3) / 1e9 if tms > 0 else 0.0
+        roof = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+                "frac": round(achieved / hbm, 4), "peak_source": peak_kind, "traffic": None,
+                "algorithmic_bytes_per_launch": int(tb), "launch_ms": round(tms, 3),
+                "per_query": {k_: round(st[k_] / nq, 3) for k_ in
+                              ("n_dist", "n_expanded", "n_posting", "n_verified", "n_result", "n_lowp_decided",
+                               "n_fp32_decided", "n_fp64_decided", "n_fp64_flipped")},
+                "phase_ms": {"a": round(st["phase_a_ms"], 3), "b": round(st["phase_b_ms"], 3),
+                             "c": round(st["phase_c_ms"], 3)}}
+        return {"qps": world * nq * args.steps / (ms / 1e3), "ms_per_step": ms / args.steps, "launches": launches,
+                "roofline": roof, "clocks": ck, "m": m_star, "recall_sweep": sweeps_of[prec]}
+
+    sweeps_of = {forms[k_]: v_ for k_, v_ in sweeps.items()}
+    results = {}
     clocks = ClockSampler(local)
-    if world > 1:
-        torch.distributed.barrier()
-    dev_sync()
-    clocks.start()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.nvtx.range_push("timed")  # profilers select the timed steps with this range
-    e0.record(stream)
-    launches = 0
-    for _ in range(args.steps):
-        step()
-        launches += h.last_search_stats()["n_launches"]
-    e1.record(stream)
-    dev_sync()
-    torch.cuda.nvtx.range_pop()
-    ck = clocks.stop()
-    ms = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([ms], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
-    ms_per_step = ms / args.steps
-    qps = world * nq * args.steps / (ms / 1e3)
-    st = h.last_search_stats()
+    results["plain"] = timed(forms["plain"], mstars["plain"])
+    results["mixed"] = timed(forms["mixed"], mstars["mixed"], clocks)
+    head = max(results, key=lambda k_: results[k_]["qps"])
+    R = results[head]
+    qps, ms_per_step, launches, roofline, ck = R["qps"], R["ms_per_step"], R["launches"], R["roofline"], R["clocks"]
+    if ck is None:
+        ck = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+    m_star = R["m"]
+    log(f"[bench] plain {results['plain']['qps']:.0f} q/s (m={mstars['plain']}), "
+        f"mixed {results['mixed']['qps']:.0f} q/s (m={mstars['mixed']})")
 
-    # ---- end to end through the host-buffer entry point ----
+    # ---- end to end through the host-buffer entry point (headline form) ----
+    h.set_precision(forms[head])
     e2e_steps = max(1, args.steps)
     Qh = np.ascontiguousarray(Q)
     h.search_rknn_batch(Qh, m_star, W["Kp"], W["ef"], threshold=1.0, k=W["k"])
@@ -342,26 +388,9 @@ def main():
     e2e = {"value": world * nq * e2e_steps / e2e_s, "unit": "queries/s",
            "h2d_bytes_per_step": int(nq * d * 4 + 3 * nq * 4), "d2h_bytes_per_step": int((nq + 1) * 8 + total_res * 8)}
     recall_timed = macro_recall(gt, out)
-
-    # ---- roofline of the dominant phase ----
-    hbm, bf16, peak_kind = load_peaks()
-    E = 4
-    maxM0 = 2 * W["M"]
-    bytes_a = st["n_dist"] * d * 4 + st["n_expanded"] * (4 + 4 * maxM0)
-    bytes_bc = st["n_posting"] * E + st["n_verified"] * (d * 4 + 4) + st["n_result"] * 8
-    phases = {"phase_a_beam_search": (st["phase_a_ms"], bytes_a),
-              "phase_bc_posting_verify": (st["phase_c_ms"], bytes_bc)}
-    dom = max(phases, key=lambda k_: phases[k_][0])
-    tms, tb = phases[dom]
-    achieved = tb / (tms / 1e3) / 1e9 if tms > 0 else 0.0
-    roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
-                "frac": round(achieved / hbm, 4), "peak_source": peak_kind, "traffic": None,
-                "algorithmic_bytes_per_launch": int(tb), "launch_ms": round(tms, 3),
-                "per_query": {"n_dist": st["n_dist"] / nq, "n_expanded": st["n_expanded"] / nq,
-                              "n_posting": st["n_posting"] / nq, "n_verified": st["n_verified"] / nq,
-                              "n_result": st["n_result"] / nq},
-                "phase_ms": {"a": round(st["phase_a_ms"], 3), "b": round(st["phase_b_ms"], 3),
-                             "c": round(st["phase_c_ms"], 3)}}
+    h.set_precision(H.PREC_FP32_EXACT)
+    params = {"m": m_star, "K_prime": W["Kp"], "ef_search": W["ef"], "k": W["k"], "threshold": 1.0}
+    sweep = sweeps[head]
 
     # ---- NNDescent roofline (per iteration, the formula of the build) ----
     it_bytes = []
@@ -382,13 +411,18 @@ def main():
     line = {
         "metric": "RkNN queries/s at recall>=0.95 (k=10)", "value": round(qps, 1), "unit": "queries/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "bf16 screen + f32/f64 decisions" if head == "mixed" else "f32",
         "data": "synthetic (seeded Gaussian mixture)",
         "config": {"workload": args.workload, "n": W["n"], "dim": d, "K_knng": W["K"], "M": W["M"],
-                   "ef_construction": W["efc"], "queries_per_step": nq, "form": "plain (bit-exact)",
+                   "ef_construction": W["efc"], "queries_per_step": nq, "form": head,
                    **params, "recall_macro": round(recall_timed, 4),
                    "recall_sweep": {str(k_): round(v, 4) for k_, v in sweep.items()},
                    "parallelism": f"replicas{world}", "l2_flush": "inputs larger than L2 (index 7 GB)"},
+        "forms": {k_: {"value": round(r_["qps"], 1), "ms_per_step": round(r_["ms_per_step"], 3), "m": r_["m"],
+                       "recall_sweep": {str(a_): round(b_, 4) for a_, b_ in r_["recall_sweep"].items()},
+                       "roofline": r_["roofline"]} for k_, r_ in results.items()},
+        "speedup_vs_plain": round(qps / results["plain"]["qps"], 3),
         "e2e": {k_: (round(v, 1) if isinstance(v, float) else v) for k_, v in e2e.items()},
         "gpu_launches": int(launches), "roofline": roofline, "cpu_baseline": cpu, "clocks": ck,
         "knng_build": {k_: (round(v, 3) if isinstance(v, float) else v) for k_, v in build.items()},

@@ -22,6 +22,7 @@ if not os.path.exists(LIB_PATH):
 _lib = C.CDLL(LIB_PATH)
 
 OK, ERR_ARG, ERR_STATE, ERR_IO, ERR_FORMAT, ERR_CUDA, ERR_NOMEM, ERR_CAPACITY, ERR_LIMIT, ERR_TIMEOUT = range(10)
+PREC_FP32_EXACT, PREC_BF16 = 0, 1
 
 # Every symbol include/hrnn_capi.h declares.
 EXPORTS = [
@@ -29,7 +30,7 @@ EXPORTS = [
     "hrnn_add_points", "hrnn_refine_knng", "hrnn_build_rknng", "hrnn_build_rknng_mutable",
     "hrnn_search_rknn", "hrnn_search_rknn_batch", "hrnn_search_rknn_batch_device",
     "hrnn_compact_for_serving", "hrnn_insert_dynamic", "hrnn_set_ef", "hrnn_get_info",
-    "hrnn_get_search_stats", "hrnn_get_refine_stats", "hrnn_set_l2_order", "hrnn_detect_l2_order", "hrnn_get_knng",
+    "hrnn_get_search_stats", "hrnn_get_refine_stats", "hrnn_set_precision", "hrnn_set_l2_order", "hrnn_detect_l2_order", "hrnn_get_knng",
     "hrnn_set_knng", "hrnn_get_rknng", "hrnn_l2_batch", "hrnn_build_rknng_noalloc",
 ]
 
@@ -50,7 +51,7 @@ class Info(C.Structure):
 class SearchStats(C.Structure):
     _fields_ = [(f, C.c_uint64) for f in (
         "n_queries", "n_dist", "n_expanded", "n_posting", "n_cand", "n_verified", "n_result",
-        "n_lowp_decided", "n_fp32_decided", "n_fp64_decided", "n_launches")] + [
+        "n_lowp_decided", "n_fp32_decided", "n_fp64_decided", "n_fp64_flipped", "n_launches")] + [
         ("phase_a_ms", C.c_double), ("phase_b_ms", C.c_double), ("phase_c_ms", C.c_double)]
 
     def as_dict(self):
@@ -92,6 +93,7 @@ _lib.hrnn_set_ef.argtypes = [_vp, _sz]
 _lib.hrnn_get_info.argtypes = [_vp, C.POINTER(Info)]
 _lib.hrnn_get_search_stats.argtypes = [_vp, C.POINTER(SearchStats)]
 _lib.hrnn_get_refine_stats.argtypes = [_vp, C.POINTER(RefineStats)]
+_lib.hrnn_set_precision.argtypes = [_vp, C.c_int]
 _lib.hrnn_set_l2_order.argtypes = [_vp, C.c_int, C.c_int]
 _lib.hrnn_detect_l2_order.argtypes = [C.POINTER(C.c_int), C.POINTER(C.c_int)]
 _lib.hrnn_get_knng.argtypes = [_vp, _vp, _vp, _vp]
@@ -216,6 +218,10 @@ class HRNN:
 
     def set_l2_order(self, lanes: int, fused: int):
         _check(_lib.hrnn_set_l2_order(self._h, lanes, fused))
+
+    def set_precision(self, precision: int):
+        """PREC_FP32_EXACT (bit-identical to the reference) or PREC_BF16."""
+        _check(_lib.hrnn_set_precision(self._h, precision))
 
     # ---- search ------------------------------------------------------------
     def searchRknn(self, q, m: int, threshold: float, k: int, K_prime: int, ef_search: int) -> list:

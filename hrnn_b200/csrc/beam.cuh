@@ -33,6 +33,9 @@ struct DevView {
     const uint64_t* csr_off;
     const void* csr_ent;
     const uint64_t* labels;
+    const uint16_t* vec_bf16;  // mixed precision: BF16 rows (or null)
+    const float* vec_err;      // ||x - bf16(x)||_2, rounded up
+    const uint32_t* knn_ids;   // KNN slot ids (FP64 radius re-decision)
     uint32_t n, dim, nb, W0, WU, K, mks, rank_bits;
     int maxlevel;
     uint32_t enterpoint;
@@ -222,6 +225,17 @@ __device__ inline WarpSmem carve(char* base, uint32_t dim, uint32_t efc, uint32_
     return s;
 }
 
+// Words of the link row of c at `level`, loaded unconditionally (no dependence on
+// the count): lane j gets word j (j < row width), lane 0 also word 32 (rows of 33
+// words, maxM0 = 32).  All loads stay inside the row.
+__device__ __forceinline__ void load_row(const DevView& v, uint32_t c, int level, uint32_t& w0, uint32_t& w1) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t W = level == 0 ? v.W0 : v.WU;
+    const uint32_t* row = links_of(v, c, level);
+    w0 = (uint32_t)lane < W ? __ldg(row + lane) : 0u;
+    w1 = (lane == 0 && W > 32) ? __ldg(row + 32) : 0u;
+}
+
 // First index in td[0..n) with td[i] > x.
 __device__ __forceinline__ uint32_t upper_bound(const float* td, uint32_t n, float x) {
     uint32_t lo = 0, hi = n;
@@ -233,10 +247,101 @@ __device__ __forceinline__ uint32_t upper_bound(const float* td, uint32_t n, flo
     return lo;
 }
 
+// ---------------------------------------------------------------------------
+// BF16 rows (mixed-precision search): vec_bf16[n][dim] holds round-to-nearest
+// copies of the FP32 rows.  These distances rank candidates only; every
+// accept/reject decision is re-made against the FP32 rows (search_bc.cu).
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ float bf16_lo(uint32_t w) { return __uint_as_float(w << 16); }
+__device__ __forceinline__ float bf16_hi(uint32_t w) { return __uint_as_float(w & 0xFFFF0000u); }
+
+// Two lanes per row, NB 16-element blocks: lane parity p reads bytes
+// [64p, 64p+64) of every 128-byte chunk, i.e. elements 32c + 16p .. 32c + 16p + 15
+// of chunk c; accumulation order is free (FP32, fused).
+template <int NB>
+__device__ __forceinline__ float bf16_pair(const float* __restrict__ q, const uint16_t* __restrict__ x, int p) {
+    const uint4* x4 = reinterpret_cast<const uint4*>(x);
+    constexpr int NC = NB / 2;  // 32-element chunks
+    uint4 a[2 * NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+        a[2 * c] = __ldg(x4 + 4 * c + 2 * p);
+        a[2 * c + 1] = __ldg(x4 + 4 * c + 2 * p + 1);
+    }
+    float s0 = 0.f, s1 = 0.f;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const uint4 w = a[2 * c + h];
+            const float* qq = q + 32 * c + 16 * p + 8 * h;
+            float t;
+            t = qq[0] - bf16_lo(w.x); s0 = fmaf(t, t, s0);
+            t = qq[1] - bf16_hi(w.x); s1 = fmaf(t, t, s1);
+            t = qq[2] - bf16_lo(w.y); s0 = fmaf(t, t, s0);
+            t = qq[3] - bf16_hi(w.y); s1 = fmaf(t, t, s1);
+            t = qq[4] - bf16_lo(w.z); s0 = fmaf(t, t, s0);
+            t = qq[5] - bf16_hi(w.z); s1 = fmaf(t, t, s1);
+            t = qq[6] - bf16_lo(w.w); s0 = fmaf(t, t, s0);
+            t = qq[7] - bf16_hi(w.w); s1 = fmaf(t, t, s1);
+        }
+    }
+    float s = s0 + s1;
+    return s + __shfl_xor_sync(0xFFFFFFFFu, s, 1);  // both lanes of the pair
+}
+
+// Any dim (one lane per row, scalar), for dims not a multiple of 32.
+__device__ __forceinline__ float bf16_thread(const float* __restrict__ q, const uint16_t* __restrict__ x, uint32_t d) {
+    float s = 0.f;
+    for (uint32_t e = 0; e < d; ++e) {
+        float t = q[e] - __uint_as_float((uint32_t)x[e] << 16);
+        s = fmaf(t, t, s);
+    }
+    return s;
+}
+
+template <int NB>
+__device__ __forceinline__ void warp_bf16_pairs(const DevView& v, const float* q, const uint32_t* ids, uint32_t cnt,
+                                                float* dout) {
+    const int lane = threadIdx.x & 31, p = lane & 1;
+    for (uint32_t r = 0; r < cnt; r += 16) {
+        const uint32_t t = r + (lane >> 1);
+        const uint32_t id = ids[t < cnt ? t : r];
+        const float d = bf16_pair<NB>(q, v.vec_bf16 + (size_t)id * v.dim, p);
+        if (p == 0 && t < cnt) dout[t] = d;
+    }
+}
+
+// Distance modes: 0 = exact FP32 unfused, 1 = exact FP32 fused, 2 = BF16 rows.
+template <int DM>
+__device__ __forceinline__ void warp_dist_list(const DevView& v, const float* q, const uint32_t* ids, uint32_t cnt,
+                                               float* dout) {
+    if constexpr (DM < 2) {
+        warp_l2_list<DM == 1>(v, q, ids, cnt, dout);
+    } else {
+        const int lane = threadIdx.x & 31;
+        if (v.dim == 128) warp_bf16_pairs<8>(v, q, ids, cnt, dout);
+        else if (v.dim == 96) warp_bf16_pairs<6>(v, q, ids, cnt, dout);
+        else if (v.dim == 256) warp_bf16_pairs<16>(v, q, ids, cnt, dout);
+        else if ((uint32_t)lane < cnt) dout[lane] = bf16_thread(q, v.vec_bf16 + (size_t)ids[lane] * v.dim, v.dim);
+        __syncwarp();
+    }
+}
+
+template <int DM>
+__device__ __forceinline__ float warp_dist_one(const DevView& v, const float* q, uint32_t id) {
+    if constexpr (DM < 2) {
+        return warp_l2_one<DM == 1>(v, q, id);
+    } else {
+        return bf16_thread(q, v.vec_bf16 + (size_t)id * v.dim, v.dim);
+    }
+}
+
 // Greedy descent over levels top..stop+1 (hrnn.h:1992-2013, 1438-1464): per level,
 // move to the first strict improvement of the running minimum in list order
 // until a whole list brings none.  cur/curd are updated in every lane.
-template <bool FUSED>
+template <int DM>
 __device__ void greedy_descent(const DevView& v, WarpSmem& s, int top, int stop, uint32_t& cur, float& curd,
                                unsigned long long& c_dist) {
     const int lane = threadIdx.x & 31;
@@ -252,7 +357,7 @@ __device__ void greedy_descent(const DevView& v, WarpSmem& s, int top, int stop,
                 uint32_t cnt = min(32u, size - base);
                 if ((uint32_t)lane < cnt) s.ni[lane] = blk[1 + base + lane];
                 __syncwarp();
-                warp_l2_list<FUSED>(v, s.q, s.ni, cnt, s.nd);
+                warp_dist_list<DM>(v, s.q, s.ni, cnt, s.nd);
                 c_dist += cnt;
                 float d = (uint32_t)lane < cnt ? s.nd[lane] : FLT_MAX;
                 float mn = d;
@@ -274,12 +379,14 @@ __device__ void greedy_descent(const DevView& v, WarpSmem& s, int top, int stop,
 // Best-first search of one layer from (ep, epd) with beam size EF (<= efc).
 // On return the beam s.td/s.ti[0..tsize) holds the EF nearest found, ascending
 // (ids still carry the expanded flag).  vc: visited-cache slots (power of two).
-template <bool FUSED>
+template <int DM>
 __device__ uint32_t beam_search(const DevView& v, WarpSmem& s, uint32_t ep, float epd, uint32_t EF, int level,
                                 uint32_t vc, unsigned long long& c_dist, unsigned long long& c_exp) {
     const int lane = threadIdx.x & 31;
     for (uint32_t i = lane; i < vc; i += 32) s.vis[i] = kInvalid;
     __syncwarp();
+    // Rows of at most 33 words (maxM0 <= 32) are read whole by the warp in one go.
+    const bool short_rows = (level == 0 ? v.W0 : v.WU) <= 33;
     uint32_t tsize = 1, cursor = 0;
     if (lane == 0) {
         s.td[0] = epd;
@@ -304,11 +411,23 @@ __device__ uint32_t beam_search(const DevView& v, WarpSmem& s, uint32_t ep, floa
         __syncwarp();
         if (lane == 0) s.ti[found] |= kExpanded;
         c_exp++;
+        // Links of c: one unconditional load of the row's words (no dependence on
+        // the count word).
+        uint32_t row0 = 0, row1 = 0;
+        if (short_rows) load_row(v, c, level, row0, row1);
         const uint32_t* adj = links_of(v, c, level);
-        const uint32_t size = adj[0] & 0xFFFFu;
+        if (!short_rows) row0 = adj[0];
+        const uint32_t size = __shfl_sync(0xFFFFFFFFu, row0, 0) & 0xFFFFu;
         for (uint32_t base = 0; base < size; base += 32) {
             uint32_t j = base + lane;
-            uint32_t nid = j < size ? adj[1 + j] : kInvalid;
+            uint32_t nid;
+            if (short_rows) {  // id j is word j + 1 of the row
+                const uint32_t a = __shfl_sync(0xFFFFFFFFu, row0, (lane + 1) & 31);
+                const uint32_t b = __shfl_sync(0xFFFFFFFFu, row1, 0);
+                nid = j < size ? (lane < 31 ? a : b) : kInvalid;
+            } else {
+                nid = j < size ? adj[1 + j] : kInvalid;
+            }
             uint32_t slot = hash32(nid) & (vc - 1);
             bool fresh = j < size && s.vis[slot] != nid;
             __syncwarp();
@@ -320,7 +439,7 @@ __device__ uint32_t beam_search(const DevView& v, WarpSmem& s, uint32_t ep, floa
             }
             __syncwarp();
             if (cnt == 0) continue;
-            warp_l2_list<FUSED>(v, s.q, s.ni, cnt, s.nd);
+            warp_dist_list<DM>(v, s.q, s.ni, cnt, s.nd);
             c_dist += cnt;
             float d = FLT_MAX;
             uint32_t id = kInvalid, pos = 0;

@@ -274,6 +274,15 @@ hrnn_status hrnn_get_search_stats(hrnn_index* h, hrnn_search_stats* st) {
     });
 }
 
+hrnn_status hrnn_set_precision(hrnn_index* h, int precision) {
+    return guard([&] {
+        need(h, "index");
+        if (precision != HRNN_PREC_FP32_EXACT && precision != HRNN_PREC_BF16)
+            hrnn::fail(HRNN_ERR_ARG, "set_precision: unknown precision");
+        h->ix.precision = precision;
+    });
+}
+
 hrnn_status hrnn_get_refine_stats(hrnn_index* h, hrnn_refine_stats* st) {
     return guard([&] {
         need(h, "index");

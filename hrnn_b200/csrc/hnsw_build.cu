@@ -119,9 +119,9 @@ __global__ void __launch_bounds__(128) k_build_batch(DevView v, uint32_t b0, uin
         const int L = levels[p];
         uint32_t cur = ep;
         float curd = warp_l2_one<FUSED>(v, s.q, cur);
-        if (L < maxlevel) greedy_descent<FUSED>(v, s, maxlevel, L, cur, curd, c_dist);  // hrnn.h:1438-1464
+        if (L < maxlevel) greedy_descent<FUSED ? 1 : 0>(v, s, maxlevel, L, cur, curd, c_dist);  // hrnn.h:1438-1464
         for (int level = min(L, maxlevel); level >= 0; --level) {
-            uint32_t tsize = beam_search<FUSED>(v, s, cur, curd, efc, level, vc, c_dist, c_exp);
+            uint32_t tsize = beam_search<FUSED ? 1 : 0>(v, s, cur, curd, efc, level, vc, c_dist, c_exp);
             for (uint32_t i = lane; i < tsize; i += 32) s.ti[i] &= kIdMask;
             __syncwarp();
             if (level == 0 && K > 0) {  // KNN-graph seed, hrnn.h:1479-1501
@@ -420,6 +420,7 @@ void add_points(Index& ix, const float* data, const uint64_t* labels, size_t n_a
     }
     CUDA_CHECK(cudaStreamSynchronize(s));
     ix.cur = end;
+    ix.bf16_valid = false;  // the BF16 copies are rebuilt on the next mixed-precision search
     // The device copy of the upper layers is now authoritative; mirror it back.
     if (!ix.upper.empty())
         CUDA_CHECK(cudaMemcpy(ix.upper.data(), ix.d_upper.p, ix.upper.size() * 4, cudaMemcpyDeviceToHost));

@@ -48,7 +48,7 @@ struct DevMem {
 // Per-search counters accumulated on the device (see hrnn_search_stats).
 struct SearchCounters {
     unsigned long long n_dist, n_expanded, n_posting, n_cand, n_verified, n_result;
-    unsigned long long n_lowp, n_fp32, n_fp64, overflow;
+    unsigned long long n_lowp, n_fp32, n_fp64, n_flip, overflow;
 };
 
 struct Index {
@@ -56,6 +56,7 @@ struct Index {
     int device = 0;
     cudaStream_t stream = nullptr;
     L2Order order;
+    int precision = HRNN_PREC_FP32_EXACT;
 
     // ---- header (hrnn.h names) -------------------------------------------
     size_t dim = 0, max_elements = 0, cur = 0;

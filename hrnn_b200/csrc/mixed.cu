@@ -1,0 +1,50 @@
+// BF16 copies of the stored vectors for the mixed-precision search, with the
+// per-vector rounding error e(x) = ||x - bf16(x)||_2 (computed in FP64, rounded
+// up to FP32) that makes the verification screen's bound rigorous:
+// | ||q - x|| - ||q - bf16(x)|| | <= e(x).
+#include <cuda_bf16.h>
+
+#include "index.hpp"
+
+namespace hrnn {
+
+namespace {
+
+__global__ void k_to_bf16(const float* __restrict__ vec, size_t n, uint32_t dim, uint16_t* __restrict__ out,
+                          float* __restrict__ err) {
+    size_t warp = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    size_t nw = ((size_t)gridDim.x * blockDim.x) >> 5;
+    for (size_t i = warp; i < n; i += nw) {
+        double e2 = 0.0;
+        for (uint32_t j = lane; j < dim; j += 32) {
+            float x = vec[i * dim + j];
+            __nv_bfloat16 b = __float2bfloat16_rn(x);
+            out[i * dim + j] = __bfloat16_as_ushort(b);
+            double dlt = (double)x - (double)__bfloat162float(b);
+            e2 += dlt * dlt;
+        }
+        for (int o = 16; o; o >>= 1) e2 += __shfl_xor_sync(0xFFFFFFFFu, e2, o);
+        if (lane == 0) err[i] = __double2float_ru(sqrt(e2) * (1.0 + 1e-12));
+    }
+}
+
+}  // namespace
+
+void ensure_bf16(Index& ix) {
+    if (ix.bf16_valid) return;
+    const size_t cap = std::max<size_t>(ix.max_elements, 1);
+    if (ix.vec_bf16.bytes < cap * ix.dim * 2) ix.vec_bf16.alloc(cap * ix.dim * 2);
+    if (ix.vec_norm.bytes < cap * 4) ix.vec_norm.alloc(cap * 4);
+    if (ix.cur) {
+        int nsm = 148;
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ix.device);
+        k_to_bf16<<<nsm * 16, 256, 0, ix.stream>>>(ix.vec.as<float>(), ix.cur, (uint32_t)ix.dim,
+                                                   ix.vec_bf16.as<uint16_t>(), ix.vec_norm.as<float>());
+        CUDA_LAUNCH_CHECK();
+        CUDA_CHECK(cudaStreamSynchronize(ix.stream));
+    }
+    ix.bf16_valid = true;
+}
+
+}  // namespace hrnn

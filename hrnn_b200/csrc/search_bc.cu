@@ -95,15 +95,18 @@ __host__ size_t bc_cta_smem(uint32_t dim, bool counts) {
            (size_t)kACap * 4 + 64;
 }
 
-template <class E, bool FUSED, bool COUNTS>
+constexpr float kTieUlps = 16.f;  // FP64 re-decision band around the radius, in ulps of kd
+
+template <class E, bool FUSED, bool COUNTS, bool MIXED>
 __global__ void __launch_bounds__(kBCThreads) k_phase_bc_cta(
     DevView v, const float* __restrict__ Q, uint32_t nq, uint32_t mmax, const uint32_t* __restrict__ prox,
     const uint32_t* __restrict__ nprox, const uint32_t* __restrict__ plen, const uint64_t* __restrict__ qtotal,
-    const uint64_t* __restrict__ res_off, float threshold, const float* __restrict__ kcol,
+    const uint64_t* __restrict__ res_off, float threshold, const float* __restrict__ kcol, uint32_t kidx,
     uint64_t* __restrict__ resbuf, uint32_t* __restrict__ res_count, uint32_t* __restrict__ next_q,
     uint32_t* __restrict__ overflow_list, uint32_t* __restrict__ n_overflow, SearchCounters* __restrict__ ctr) {
     extern __shared__ char smraw[];
-    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5, half = lane >> 4, l = lane & 15;
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    unsigned long long c_lowp = 0, c_fp32 = 0, c_fp64 = 0, c_flip = 0;
     constexpr int NW = kBCThreads / 32;
     float* q = (float*)smraw;
     uint32_t* keys = (uint32_t*)(q + v.dim);
@@ -194,7 +197,81 @@ __global__ void __launch_bounds__(kBCThreads) k_phase_bc_cta(
                     if (p == 0 && t < cnt_ && d <= kd) accept(id);
                 }
             };
+            // Mixed precision: a BF16 screen decides whatever its error bound allows;
+            // the rest is decided in exact FP32 (the reference's order), and inside a
+            // band of kTieUlps around the radius in FP64.
+            auto verify_mixed = [&](uint32_t cnt_, auto nbc) {
+                constexpr int NB = decltype(nbc)::value;
+                const int p = lane & 1;
+                for (uint32_t r = 0; r < cnt_; r += 16) {
+                    const uint32_t t = r + (lane >> 1);
+                    const bool live = t < cnt_;
+                    const uint32_t id = st[live ? t : r];
+                    const float kd = __ldg(kcol + id);
+                    const float D = bf16_pair<NB>(q, v.vec_bf16 + (size_t)id * v.dim, p);
+                    const float e = __ldg(v.vec_err + id);
+                    // ||q - x|| is within e of ||q - bf16(x)|| (triangle inequality);
+                    // rho covers the FP32 rounding of the screen's sum, of the
+                    // reference's own sum and of this bound's few operations (each
+                    // term is bounded by (dim + 8) * 2^-24 relative; 4x margin).
+                    const float rho = (4.f * v.dim + 64.f) * 5.9604645e-8f;
+                    const float sD = sqrtf(D);
+                    const float hi = sD * (1.f + rho) + e, lo = fmaxf(0.f, sD * (1.f - rho) - e);
+                    const float U = hi * hi * (1.f + rho), L = lo * lo * (1.f - rho);
+                    int decision;  // 1 accept, 0 reject, -1 undecided (same in both lanes)
+                    if (kd == FLT_MAX) decision = 1;
+                    else if (U < kd) decision = 1;
+                    else if (L > kd) decision = 0;
+                    else decision = -1;
+                    if (p == 0 && live && decision >= 0) c_lowp++;
+                    const uint32_t und = __ballot_sync(0xFFFFFFFFu, live && decision < 0);
+                    if (und) {  // exact FP32 for the undecided rows; all lanes take part
+                        float d32 = l2_pair16<FUSED, NB>(q, v.vec + (size_t)id * v.dim, p);
+                        d32 = __shfl_sync(0xFFFFFFFFu, d32, lane & ~1);
+                        const bool tie = live && decision < 0 && v.knn_ids && kidx < (v.knn_hdr[id] & 0xFFFFu) &&
+                                         fabsf(d32 - kd) <= kTieUlps * (nextafterf(kd, FLT_MAX) - kd);
+                        if (live && decision < 0) {
+                            decision = d32 <= kd;
+                            if (p == 0) c_fp32++;
+                        }
+                        if (__any_sync(0xFFFFFFFFu, tie)) {
+                            // FP64: d(q, x) against d(x, x_k), x_k the k-th neighbour of x
+                            double a = 0.0, b = 0.0;
+                            if (tie) {
+                                const uint32_t nk = v.knn_ids[(size_t)id * v.K + kidx];
+                                const float* x = v.vec + (size_t)id * v.dim;
+                                const float* y = v.vec + (size_t)nk * v.dim;
+                                for (uint32_t e2 = p; e2 < v.dim; e2 += 2) {
+                                    const double tq = (double)q[e2] - (double)x[e2];
+                                    const double ty = (double)x[e2] - (double)y[e2];
+                                    a += tq * tq;
+                                    b += ty * ty;
+                                }
+                            }
+                            a += __shfl_xor_sync(0xFFFFFFFFu, a, 1);
+                            b += __shfl_xor_sync(0xFFFFFFFFu, b, 1);
+                            if (tie) {
+                                const int d64 = a <= b;
+                                if (p == 0) {
+                                    c_fp64++;
+                                    if (d64 != decision) c_flip++;
+                                }
+                                decision = d64;
+                            }
+                        }
+                    }
+                    if (p == 0 && live && decision == 1) accept(id);
+                }
+            };
             auto verify = [&](uint32_t cnt_) {
+                if (MIXED && v.vec_bf16) {
+                    if (v.dim == 128) verify_mixed(cnt_, std::integral_constant<int, 8>{});
+                    else if (v.dim == 96) verify_mixed(cnt_, std::integral_constant<int, 6>{});
+                    else if (v.dim == 256) verify_mixed(cnt_, std::integral_constant<int, 16>{});
+                    else verify_pairs(cnt_, std::integral_constant<int, 8>{});  // unreachable: mixed needs 96/128/256
+                    __syncwarp();
+                    return;
+                }
                 if (fast && v.dim == 128) {
                     verify_pairs(cnt_, std::integral_constant<int, 8>{});
                 } else if (fast && v.dim == 96) {
@@ -278,22 +355,38 @@ __global__ void __launch_bounds__(kBCThreads) k_phase_bc_cta(
         atomicAdd(&ctr->n_verified, c_ver);
         atomicAdd(&ctr->n_result, c_res);
     }
+    if (MIXED) {  // per-lane counts: reduce over the warp first
+        for (int o = 16; o; o >>= 1) {
+            c_lowp += __shfl_xor_sync(0xFFFFFFFFu, c_lowp, o);
+            c_fp32 += __shfl_xor_sync(0xFFFFFFFFu, c_fp32, o);
+            c_fp64 += __shfl_xor_sync(0xFFFFFFFFu, c_fp64, o);
+            c_flip += __shfl_xor_sync(0xFFFFFFFFu, c_flip, o);
+        }
+        if (lane == 0) {
+            atomicAdd(&ctr->n_lowp, c_lowp);
+            atomicAdd(&ctr->n_fp32, c_fp32);
+            atomicAdd(&ctr->n_fp64, c_fp64);
+            atomicAdd(&ctr->n_flip, c_flip);
+        }
+    }
 }
 
 // explicit instantiations used by search_plain.cu
-#define INST(E, F, C)                                                                                               \
-    template __global__ void k_phase_bc_cta<E, F, C>(DevView, const float*, uint32_t, uint32_t, const uint32_t*,    \
-                                                     const uint32_t*, const uint32_t*, const uint64_t*,             \
-                                                     const uint64_t*, float, const float*, uint64_t*, uint32_t*,    \
-                                                     uint32_t*, uint32_t*, uint32_t*, SearchCounters*);
-INST(uint32_t, false, false)
-INST(uint32_t, false, true)
-INST(uint32_t, true, false)
-INST(uint32_t, true, true)
-INST(uint64_t, false, false)
-INST(uint64_t, false, true)
-INST(uint64_t, true, false)
-INST(uint64_t, true, true)
+#define INST(E, F, C, X)                                                                                            \
+    template __global__ void k_phase_bc_cta<E, F, C, X>(DevView, const float*, uint32_t, uint32_t, const uint32_t*, \
+                                                        const uint32_t*, const uint32_t*, const uint64_t*,          \
+                                                        const uint64_t*, float, const float*, uint32_t, uint64_t*,  \
+                                                        uint32_t*, uint32_t*, uint32_t*, uint32_t*, SearchCounters*);
+#define INST2(E, F, C) INST(E, F, C, false) INST(E, F, C, true)
+INST2(uint32_t, false, false)
+INST2(uint32_t, false, true)
+INST2(uint32_t, true, false)
+INST2(uint32_t, true, true)
+INST2(uint64_t, false, false)
+INST2(uint64_t, false, true)
+INST2(uint64_t, true, false)
+INST2(uint64_t, true, true)
+#undef INST2
 #undef INST
 
 }  // namespace hrnn

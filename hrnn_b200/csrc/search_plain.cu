@@ -24,16 +24,29 @@
 namespace hrnn {
 
 // search_bc.cu
-template <class E, bool FUSED, bool COUNTS>
+template <class E, bool FUSED, bool COUNTS, bool MIXED>
 __global__ void k_phase_bc_cta(DevView, const float*, uint32_t, uint32_t, const uint32_t*, const uint32_t*,
-                               const uint32_t*, const uint64_t*, const uint64_t*, float, const float*, uint64_t*,
-                               uint32_t*, uint32_t*, uint32_t*, uint32_t*, SearchCounters*);
+                               const uint32_t*, const uint64_t*, const uint64_t*, float, const float*, uint32_t,
+                               uint64_t*, uint32_t*, uint32_t*, uint32_t*, uint32_t*, SearchCounters*);
+using KCta = void (*)(DevView, const float*, uint32_t, uint32_t, const uint32_t*, const uint32_t*, const uint32_t*,
+                      const uint64_t*, const uint64_t*, float, const float*, uint32_t, uint64_t*, uint32_t*,
+                      uint32_t*, uint32_t*, uint32_t*, SearchCounters*);
+template <class E>
+KCta pick_bc(bool f, bool c, bool x) {
+    if (x)
+        return f ? (c ? k_phase_bc_cta<E, true, true, true> : k_phase_bc_cta<E, true, false, true>)
+                 : (c ? k_phase_bc_cta<E, false, true, true> : k_phase_bc_cta<E, false, false, true>);
+    return f ? (c ? k_phase_bc_cta<E, true, true, false> : k_phase_bc_cta<E, true, false, false>)
+             : (c ? k_phase_bc_cta<E, false, true, false> : k_phase_bc_cta<E, false, false, false>);
+}
+void ensure_bf16(Index& ix);  // mixed.cu
 __global__ void k_kdist_column(DevView v, uint32_t kidx, float* kcol);
 size_t bc_cta_smem(uint32_t dim, bool counts);
 
 namespace {
 
-template <bool FUSED>
+// DM: distance mode of beam.cuh (0/1 exact FP32 unfused/fused, 2 BF16 rows).
+template <int DM>
 __global__ void __launch_bounds__(128) k_phase_a(DevView v, const float* __restrict__ Q, uint32_t nq,
                                                  const uint32_t* __restrict__ qm, const uint32_t* __restrict__ qef,
                                                  uint32_t efc, uint32_t vc, uint32_t mmax,
@@ -53,11 +66,11 @@ __global__ void __launch_bounds__(128) k_phase_a(DevView v, const float* __restr
         for (uint32_t i = lane; i < v.dim; i += 32) s.q[i] = Q[(size_t)qi * v.dim + i];
         __syncwarp();
         uint32_t cur = v.enterpoint;
-        float curd = warp_l2_one<FUSED>(v, s.q, cur);
+        float curd = warp_dist_one<DM>(v, s.q, cur);
         c_dist++;
-        greedy_descent<FUSED>(v, s, v.maxlevel, 0, cur, curd, c_dist);
+        greedy_descent<DM>(v, s, v.maxlevel, 0, cur, curd, c_dist);
         c_dist++;  // the reference evaluates the entry point again (hrnn.h:505)
-        uint32_t tsize = beam_search<FUSED>(v, s, cur, curd, EF, 0, vc, c_dist, c_exp);
+        uint32_t tsize = beam_search<DM>(v, s, cur, curd, EF, 0, vc, c_dist, c_exp);
         uint32_t np_ = min(m, tsize);
         for (uint32_t i = lane; i < np_; i += 32) prox[(size_t)qi * mmax + i] = s.ti[i] & kIdMask;
         if (lane == 0) nprox[qi] = np_;
@@ -276,6 +289,9 @@ DevView make_view(Index& ix) {
     v.csr_off = ix.csr_off.as<uint64_t>();
     v.csr_ent = ix.csr_ent.p;
     v.labels = ix.labels.as<uint64_t>();
+    v.vec_bf16 = ix.bf16_valid ? ix.vec_bf16.as<uint16_t>() : nullptr;
+    v.vec_err = ix.bf16_valid ? ix.vec_norm.as<float>() : nullptr;
+    v.knn_ids = ix.knn_ids.as<uint32_t>();
     v.n = (uint32_t)ix.cur;
     v.dim = (uint32_t)ix.dim;
     v.nb = (uint32_t)(ix.dim / 16);
@@ -345,11 +361,19 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
     CUDA_CHECK(cudaMemsetAsync(d_rcount, 0, (nq + 1) * 4 + 16, s));
     SearchCounters* ctr = ix.counters.as<SearchCounters>();
     const bool fusedsimd = (ix.order.fused & 1) != 0;
+    // Mixed precision (hrnn_set_precision): BF16 rows for the beam and the
+    // verification screen; decisions still exact (FP32 / FP64 band).
+    const bool mixed = ix.precision == HRNN_PREC_BF16 && (v.dim == 96 || v.dim == 128 || v.dim == 256) &&
+                       v.lanes == 16;
+    if (mixed) {
+        ensure_bf16(ix);
+        v = make_view(ix);
+    }
     const int nsm = sms(ix.device);
     CUDA_CHECK(cudaEventRecord(ev[0], s));
     {
         unsigned grid = (unsigned)std::min<size_t>((nq + wpb - 1) / wpb, (size_t)nsm * 16);
-        auto kern = fusedsimd ? k_phase_a<true> : k_phase_a<false>;
+        auto kern = mixed ? k_phase_a<2> : (fusedsimd ? k_phase_a<1> : k_phase_a<0>);
         CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_a));
         kern<<<grid, wpb * 32, smem_a, s>>>(v, a.d_q, (uint32_t)nq, a.d_m, a.d_ef, efc, vc, mmax,
                                             prox.as<uint32_t>(), nprox.as<uint32_t>(), ctr);
@@ -386,23 +410,14 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
         CUDA_LAUNCH_CHECK();
         const bool counts = a.threshold > 1.0f;
         const size_t smem = bc_cta_smem(v.dim, counts);
-        using KCta = void (*)(DevView, const float*, uint32_t, uint32_t, const uint32_t*, const uint32_t*,
-                              const uint32_t*, const uint64_t*, const uint64_t*, float, const float*, uint64_t*,
-                              uint32_t*, uint32_t*, uint32_t*, uint32_t*, SearchCounters*);
-        KCta kc;
-        if (ix.wide)
-            kc = fusedsimd ? (counts ? k_phase_bc_cta<uint64_t, true, true> : k_phase_bc_cta<uint64_t, true, false>)
-                           : (counts ? k_phase_bc_cta<uint64_t, false, true> : k_phase_bc_cta<uint64_t, false, false>);
-        else
-            kc = fusedsimd ? (counts ? k_phase_bc_cta<uint32_t, true, true> : k_phase_bc_cta<uint32_t, true, false>)
-                           : (counts ? k_phase_bc_cta<uint32_t, false, true> : k_phase_bc_cta<uint32_t, false, false>);
+        KCta kc = ix.wide ? pick_bc<uint64_t>(fusedsimd, counts, mixed) : pick_bc<uint32_t>(fusedsimd, counts, mixed);
         CUDA_CHECK(cudaFuncSetAttribute(kc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         int per_sm = 1;
         CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kc, 256, smem));
         unsigned grid = (unsigned)std::min<size_t>(nq, (size_t)nsm * std::max(per_sm, 1));
         kc<<<grid, 256, smem, s>>>(v, a.d_q, (uint32_t)nq, mmax, prox.as<uint32_t>(), nprox.as<uint32_t>(),
-                                   plen.as<uint32_t>(), d_total, d_resoff, a.threshold, ix.kcol.as<float>(), resbuf,
-                                   d_rcount, d_next, ovl, d_nov, ctr);
+                                   plen.as<uint32_t>(), d_total, d_resoff, a.threshold, ix.kcol.as<float>(), kidx,
+                                   resbuf, d_rcount, d_next, ovl, d_nov, ctr);
         CUDA_LAUNCH_CHECK();
         // Queries whose shared-memory table or accepted list overflowed: the
         // global-memory warp kernel, with a table sized for their posting count.
@@ -466,6 +481,10 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
     st.n_cand = hc.n_cand;
     st.n_verified = hc.n_verified;
     st.n_result = hc.n_result;
+    st.n_lowp_decided = hc.n_lowp;
+    st.n_fp32_decided = hc.n_fp32;
+    st.n_fp64_decided = hc.n_fp64;
+    st.n_fp64_flipped = hc.n_flip;
     st.n_launches = launch_counter().load() - launches0;
     float t01 = 0, t12 = 0, t23 = 0;
     cudaEventElapsedTime(&t01, ev[0], ev[1]);

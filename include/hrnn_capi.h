@@ -70,6 +70,7 @@ typedef struct {
     uint64_t n_lowp_decided;/* mixed precision: decided by the low-precision bound */
     uint64_t n_fp32_decided;/* mixed precision: re-decided in exact FP32        */
     uint64_t n_fp64_decided;/* mixed precision: re-decided in FP64 (tie band)   */
+    uint64_t n_fp64_flipped;/* ... of which FP64 decided against FP32           */
     uint64_t n_launches;    /* kernels this call launched                       */
     double phase_a_ms, phase_b_ms, phase_c_ms;   /* device time of each phase   */
 } hrnn_search_stats;
@@ -169,6 +170,19 @@ hrnn_status hrnn_get_search_stats(hrnn_index* h, hrnn_search_stats* st);
 
 /* Counters of the last refineKNNG call. */
 hrnn_status hrnn_get_refine_stats(hrnn_index* h, hrnn_refine_stats* st);
+
+/* Precision of the search (new; the reference has FP32 only).
+ *  HRNN_PREC_FP32_EXACT (default): every distance is the reference's FP32 value;
+ *      answers are bit-identical to searchRknn.
+ *  HRNN_PREC_BF16: the beam search ranks with BF16 copies of the vectors and the
+ *      verification screens with them under a rigorous per-vector error bound;
+ *      every undecided accept/reject is re-decided with the reference's exact
+ *      FP32 distance, and within 16 ulps of the radius in FP64 against the
+ *      FP64 distance to the k-th neighbour.  Proxies may differ from the
+ *      reference's (recall, not membership); counts in hrnn_search_stats. */
+#define HRNN_PREC_FP32_EXACT 0
+#define HRNN_PREC_BF16 1
+hrnn_status hrnn_set_precision(hrnn_index* h, int precision);
 
 /* FP32 summation order of the L2 kernel (space_l2.h:214-238 picks it per host):
  * lanes in {16, 8, 4}; fused bit 0 = SIMD multiply-add contracted, bit 1 = scalar

@@ -101,3 +101,33 @@ def test_large_answer_sets_match_oracle(built):
         b = O.search_batch(Q[:60], m, kp, 100, threshold=th, k=k)
         assert all(np.array_equal(x, y) for x, y in zip(a, b)), (m, kp, k, th)
     assert max(len(x) for x in a) > 100
+
+
+def test_mixed_precision_decisions_and_recall(built):
+    """BF16 beam + screened verification: every returned point passes the exact
+    FP32 test (or the FP64 test inside the tie band), and recall stays at the plain
+    form's level."""
+    X, Q, h, p, _ = built
+    f = idx.read_idx(p)
+    V = f.vectors()
+    ids, d, cnt = f.knng()
+    lab2id = {int(l): i for i, l in enumerate(f.labels())}
+    kth = data.kth_nn_fp64(X, 10)
+    gt = data.rknn_gt_fp64(X, Q, kth)
+    plain = h.search_rknn_batch(Q, 10, 64, 100, k=10)
+    try:
+        h.set_precision(H.PREC_BF16)
+        mixed = h.search_rknn_batch(Q, 10, 64, 100, k=10)
+        st = h.last_search_stats()
+    finally:
+        h.set_precision(H.PREC_FP32_EXACT)
+    assert st["n_lowp_decided"] > 0.9 * (st["n_lowp_decided"] + st["n_fp32_decided"])
+    bad = 0
+    for qi, res in enumerate(mixed):
+        for lab in res:
+            i = lab2id[int(lab)]
+            d32 = port.l2(Q[qi], V[i])
+            kd = d[i, 9] if cnt[i] > 9 else np.float32(np.finfo(np.float32).max)
+            bad += not (d32 <= kd)
+    assert bad <= st["n_fp64_flipped"]
+    assert data.macro_recall(gt, mixed) >= data.macro_recall(gt, plain) - 0.01
