@@ -226,6 +226,8 @@ def main():
     ap.add_argument("--workload", default="mixed-1M-d128-K500", choices=list(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample", type=int, default=2000, help="queries in the CPU-baseline sample")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-budget form")
+    ap.add_argument("--budget-train", type=int, default=200_000, help="training queries of the budget MLP")
     args = ap.parse_args()
     W = WORKLOADS[args.workload]
 
@@ -290,6 +292,19 @@ def main():
         run_reference_arm(args, W, h, Q, params, sweeps["plain"], build)
         return
 
+    # ---- learned search budget: train on separate seeded queries (untimed) ----
+    budget_info = None
+    if not args.no_learned:
+        budget_info = train_budget(H, h, W, args, dev_sync)
+        h.set_precision(H.PREC_BF16)
+        h.set_budget(True, **BUDGET)
+        sw, mstar = sweep_form(H.PREC_BF16)
+        sweeps["learned"], mstars["learned"] = sw, mstar
+        log(f"[bench] learned: recall sweep (fallback m) {json.dumps({k_: round(v_, 4) for k_, v_ in sw.items()})}"
+            f" -> m={mstar}")
+        h.set_budget(False, **BUDGET)
+        h.set_precision(H.PREC_FP32_EXACT)
+
     # ---- timed device steps, per form ----
     q_dev = torch.from_numpy(Q).to(dev)
     kp_dev = torch.full((nq,), W["Kp"], dtype=torch.int32, device=dev)
@@ -301,8 +316,10 @@ def main():
     hbm, bf16, peak_kind = load_peaks()
     maxM0 = 2 * W["M"]
 
-    def timed(prec, m_star, clocks=None):
+    def timed(prec, m_star, clocks=None, learned=False):
         h.set_precision(prec)
+        if learned:
+            h.set_budget(True, **BUDGET)
         m_dev = torch.full((nq,), m_star, dtype=torch.int32, device=dev)
 
         def step():
@@ -352,25 +369,31 @@ def main():
                                "n_fp32_decided", "n_fp64_decided", "n_fp64_flipped")},
                 "phase_ms": {"a": round(st["phase_a_ms"], 3), "b": round(st["phase_b_ms"], 3),
                              "c": round(st["phase_c_ms"], 3)}}
+        if learned:
+            roof["budget_levels"] = st["n_budget"]
+            h.set_budget(False, **BUDGET)
         return {"qps": world * nq * args.steps / (ms / 1e3), "ms_per_step": ms / args.steps, "launches": launches,
-                "roofline": roof, "clocks": ck, "m": m_star, "recall_sweep": sweeps_of[prec]}
+                "roofline": roof, "clocks": ck, "m": m_star,
+                "recall_sweep": sweeps["learned" if learned else ("mixed" if prec == H.PREC_BF16 else "plain")]}
 
-    sweeps_of = {forms[k_]: v_ for k_, v_ in sweeps.items()}
     results = {}
     clocks = ClockSampler(local)
     results["plain"] = timed(forms["plain"], mstars["plain"])
-    results["mixed"] = timed(forms["mixed"], mstars["mixed"], clocks)
+    results["mixed"] = timed(forms["mixed"], mstars["mixed"], None if budget_info else clocks)
+    if budget_info:
+        results["learned"] = timed(H.PREC_BF16, mstars["learned"], clocks, learned=True)
     head = max(results, key=lambda k_: results[k_]["qps"])
     R = results[head]
     qps, ms_per_step, launches, roofline, ck = R["qps"], R["ms_per_step"], R["launches"], R["roofline"], R["clocks"]
     if ck is None:
         ck = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
     m_star = R["m"]
-    log(f"[bench] plain {results['plain']['qps']:.0f} q/s (m={mstars['plain']}), "
-        f"mixed {results['mixed']['qps']:.0f} q/s (m={mstars['mixed']})")
+    log("[bench] " + ", ".join(f"{k_} {r_['qps']:.0f} q/s (m={r_['m']})" for k_, r_ in results.items()))
 
     # ---- end to end through the host-buffer entry point (headline form) ----
-    h.set_precision(forms[head])
+    h.set_precision(H.PREC_FP32_EXACT if head == "plain" else H.PREC_BF16)
+    if head == "learned":
+        h.set_budget(True, **BUDGET)
     e2e_steps = max(1, args.steps)
     Qh = np.ascontiguousarray(Q)
     h.search_rknn_batch(Qh, m_star, W["Kp"], W["ef"], threshold=1.0, k=W["k"])
@@ -389,6 +412,8 @@ def main():
            "h2d_bytes_per_step": int(nq * d * 4 + 3 * nq * 4), "d2h_bytes_per_step": int((nq + 1) * 8 + total_res * 8)}
     recall_timed = macro_recall(gt, out)
     h.set_precision(H.PREC_FP32_EXACT)
+    if head == "learned":
+        h.set_budget(False, **BUDGET)
     params = {"m": m_star, "K_prime": W["Kp"], "ef_search": W["ef"], "k": W["k"], "threshold": 1.0}
     sweep = sweeps[head]
 
@@ -412,7 +437,8 @@ def main():
         "metric": "RkNN queries/s at recall>=0.95 (k=10)", "value": round(qps, 1), "unit": "queries/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "bf16 screen + f32/f64 decisions" if head == "mixed" else "f32",
+        "dtype": {"plain": "f32", "mixed": "bf16 screen + f32/f64 decisions",
+                  "learned": "bf16 screen + f32/f64 decisions; bf16 budget MLP"}[head],
         "data": "synthetic (seeded Gaussian mixture)",
         "config": {"workload": args.workload, "n": W["n"], "dim": d, "K_knng": W["K"], "M": W["M"],
                    "ef_construction": W["efc"], "queries_per_step": nq, "form": head,
@@ -423,6 +449,7 @@ def main():
                        "recall_sweep": {str(a_): round(b_, 4) for a_, b_ in r_["recall_sweep"].items()},
                        "roofline": r_["roofline"]} for k_, r_ in results.items()},
         "speedup_vs_plain": round(qps / results["plain"]["qps"], 3),
+        "learned_budget": budget_info,
         "e2e": {k_: (round(v, 1) if isinstance(v, float) else v) for k_, v in e2e.items()},
         "gpu_launches": int(launches), "roofline": roofline, "cpu_baseline": cpu, "clocks": ck,
         "knng_build": {k_: (round(v, 3) if isinstance(v, float) else v) for k_, v in build.items()},
@@ -432,6 +459,59 @@ def main():
     if world > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
+
+
+# Learned budget: level 0 = 1 proxy, level 1 = 3 proxies, both from one beam of
+# ef = 100; a query takes a level when the MLP gives that level's answer being
+# complete a probability >= 0.9, else the caller's (m, ef).
+BUDGET = dict(m0=1, m1=3, ef=100, confidence=0.9)
+LABEL_M, LABEL_EF = 50, 200  # the "complete" answer the labels compare against
+
+
+def _search_sets(h, Q, m, kp, ef, k, chunk=10_000):
+    out = []
+    for s in range(0, Q.shape[0], chunk):
+        out.extend(h.search_rknn_batch(Q[s:s + chunk], m, kp, ef, threshold=1.0, k=k))
+    return out
+
+
+def train_budget(H, h, W, args, dev_sync):
+    """Features and labels of `args.budget_train` seeded queries (a stream separate
+    from the timed ones) in the mixed-precision form, then MLP training on the GPU."""
+    from oracle import data as odata
+    t0 = time.perf_counter()
+    n = args.budget_train
+    Qtr = odata.mixture(n, W["d"], W["C"], W["sigma"], W["seed"], W["qseed"] + 7919, dirichlet=W["dirichlet"])
+    h.set_precision(H.PREC_BF16)
+    full = _search_sets(h, Qtr, LABEL_M, W["Kp"], LABEL_EF, W["k"])
+    Y = np.zeros((n, 2), np.uint8)
+    for j, ml in enumerate((BUDGET["m0"], BUDGET["m1"])):
+        got = _search_sets(h, Qtr, ml, W["Kp"], BUDGET["ef"], W["k"])
+        Y[:, j] = [np.isin(f, g, assume_unique=True).all() for f, g in zip(full, got)]
+    t1 = time.perf_counter()
+    h.set_budget(False, **BUDGET)
+    feat = np.concatenate([h.budget_features(Qtr[s:s + 50_000], W["k"]) for s in range(0, n, 50_000)])
+    dev_sync()
+    t2 = time.perf_counter()
+    loss = h.budget_train(feat, Y, epochs=20, batch=1024, lr=1e-3, seed=11)
+    dev_sync()
+    t3 = time.perf_counter()
+    z = h.budget_predict(feat[:20_000])
+    p = 1.0 / (1.0 + np.exp(-z.astype(np.float64)))
+    conf = BUDGET["confidence"]
+    take0 = p[:, 0] >= conf
+    take1 = ~take0 & (p[:, 1] >= conf)
+    wrong = (take0 & (Y[:20_000, 0] == 0)) | (take1 & (Y[:20_000, 1] == 0))
+    h.set_precision(H.PREC_FP32_EXACT)
+    info = {"train_queries": n, "levels": {"m0": BUDGET["m0"], "m1": BUDGET["m1"], "ef": BUDGET["ef"]},
+            "confidence": conf, "label_ref": {"m": LABEL_M, "ef": LABEL_EF},
+            "label_rate": [round(float(Y[:, 0].mean()), 4), round(float(Y[:, 1].mean()), 4)],
+            "final_loss": round(loss, 4), "train_level_share": [round(float(take0.mean()), 4),
+                                                                 round(float(take1.mean()), 4)],
+            "train_wrong_level_rate": round(float(wrong.mean()), 5),
+            "labels_s": round(t1 - t0, 1), "features_s": round(t2 - t1, 1), "train_s": round(t3 - t2, 1)}
+    log(f"[bench] learned budget: {json.dumps(info)}")
+    return info
 
 
 def _save_for_reference(h):

@@ -32,7 +32,14 @@ EXPORTS = [
     "hrnn_compact_for_serving", "hrnn_insert_dynamic", "hrnn_set_ef", "hrnn_get_info",
     "hrnn_get_search_stats", "hrnn_get_refine_stats", "hrnn_set_precision", "hrnn_set_l2_order", "hrnn_detect_l2_order", "hrnn_get_knng",
     "hrnn_set_knng", "hrnn_get_rknng", "hrnn_l2_batch", "hrnn_build_rknng_noalloc",
+    "hrnn_set_budget", "hrnn_budget_features", "hrnn_budget_train", "hrnn_budget_predict",
+    "hrnn_budget_gradients", "hrnn_budget_get_weights", "hrnn_budget_set_weights",
 ]
+
+# Learned-budget MLP: 256 -> 256 -> 256 -> 2; parameters W1 b1 W2 b2 W3 b3 (row-major [out, in]).
+BUDGET_IN, BUDGET_HIDDEN, BUDGET_OUT = 256, 256, 2
+BUDGET_SHAPES = [(256, 256), (256,), (256, 256), (256,), (2, 256), (2,)]
+BUDGET_PARAMS = sum(int(np.prod(s)) for s in BUDGET_SHAPES)
 
 
 class Info(C.Structure):
@@ -52,10 +59,13 @@ class SearchStats(C.Structure):
     _fields_ = [(f, C.c_uint64) for f in (
         "n_queries", "n_dist", "n_expanded", "n_posting", "n_cand", "n_verified", "n_result",
         "n_lowp_decided", "n_fp32_decided", "n_fp64_decided", "n_fp64_flipped", "n_launches")] + [
+        ("n_budget", C.c_uint64 * 3),
         ("phase_a_ms", C.c_double), ("phase_b_ms", C.c_double), ("phase_c_ms", C.c_double)]
 
     def as_dict(self):
-        return {f: getattr(self, f) for f, _ in self._fields_}
+        d = {f: getattr(self, f) for f, _ in self._fields_}
+        d["n_budget"] = list(self.n_budget)
+        return d
 
 
 MAX_ITERS = 64
@@ -101,6 +111,14 @@ _lib.hrnn_set_knng.argtypes = [_vp, _vp, _vp, _vp]
 _lib.hrnn_get_rknng.argtypes = [_vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint32),
                                 C.POINTER(C.c_uint32), _vp, _vp, C.c_int]
 _lib.hrnn_l2_batch.argtypes = [_vp, _vp, _sz, _sz, C.c_int, C.c_int, _vp]
+_lib.hrnn_set_budget.argtypes = [_vp, C.c_int, C.c_uint32, C.c_uint32, C.c_uint32, C.c_float]
+_lib.hrnn_budget_features.argtypes = [_vp, _vp, _sz, C.c_uint32, _vp]
+_lib.hrnn_budget_train.argtypes = [_vp, _vp, _vp, _sz, C.c_int, C.c_int, C.c_float, C.c_uint64,
+                                   C.POINTER(C.c_float)]
+_lib.hrnn_budget_predict.argtypes = [_vp, _vp, _sz, _vp]
+_lib.hrnn_budget_gradients.argtypes = [_vp, _vp, _vp, _sz, _vp, C.POINTER(C.c_float)]
+_lib.hrnn_budget_get_weights.argtypes = [_vp, _vp]
+_lib.hrnn_budget_set_weights.argtypes = [_vp, _vp]
 _lib.hrnn_build_rknng_noalloc.argtypes = [_vp, _vp, _sz, _sz, _vp, _vp, _sz, C.POINTER(C.c_uint32),
                                           C.POINTER(C.c_int), C.POINTER(C.c_uint64), _vp]
 
@@ -150,6 +168,15 @@ def build_rknng_noalloc(d_knn_ids: int, d_knn_cnt: int, n: int, K: int, d_offset
     _check(_lib.hrnn_build_rknng_noalloc(_vp(d_knn_ids), _vp(d_knn_cnt), n, K, _vp(d_offsets), _vp(d_entries),
                                          entries_cap, C.byref(rb), C.byref(wide), C.byref(ne), _vp(stream)))
     return rb.value, bool(wide.value), ne.value
+
+
+def _split_params(flat):
+    out, o = [], 0
+    for s in BUDGET_SHAPES:
+        k = int(np.prod(s))
+        out.append(flat[o:o + k].reshape(s).copy())
+        o += k
+    return out
 
 
 def _u32(x, n):
@@ -255,6 +282,53 @@ class HRNN:
                                                   threshold, k, _vp(off_ptr), _vp(lab_ptr), cap, C.byref(tot),
                                                   _vp(stream)))
         return tot.value
+
+    # ---- learned search budget (no counterpart in the reference) -------------
+    def set_budget(self, enable: bool, m0: int = 1, m1: int = 3, ef: int = 100, confidence: float = 0.9):
+        """Serve searches with the learned budget (levels m0 / m1 with beam ef) when enabled."""
+        _check(_lib.hrnn_set_budget(self._h, int(enable), m0, m1, ef, confidence))
+
+    def budget_features(self, Q, k: int) -> np.ndarray:
+        """The MLP's 256 features of each query (frontier pass with the budget's ef)."""
+        Q = np.ascontiguousarray(Q, np.float32)
+        f = np.zeros((Q.shape[0], BUDGET_IN), np.float32)
+        _check(_lib.hrnn_budget_features(self._h, _p(Q), Q.shape[0], k, _p(f)))
+        return f
+
+    def budget_train(self, feat, labels, epochs: int = 10, batch: int = 1024, lr: float = 1e-3,
+                     seed: int = 0) -> float:
+        feat = np.ascontiguousarray(feat, np.float32)
+        labels = np.ascontiguousarray(labels, np.uint8)
+        assert feat.shape[1:] == (BUDGET_IN,) and labels.shape == (feat.shape[0], BUDGET_OUT)
+        loss = C.c_float(0)
+        _check(_lib.hrnn_budget_train(self._h, _p(feat), _p(labels), feat.shape[0], epochs, batch, lr, seed,
+                                      C.byref(loss)))
+        return loss.value
+
+    def budget_predict(self, feat) -> np.ndarray:
+        feat = np.ascontiguousarray(feat, np.float32)
+        z = np.zeros((feat.shape[0], BUDGET_OUT), np.float32)
+        _check(_lib.hrnn_budget_predict(self._h, _p(feat), feat.shape[0], _p(z)))
+        return z
+
+    def budget_gradients(self, feat, labels):
+        """Gradients of the mean BCE (list in BUDGET_SHAPES order) and the loss."""
+        feat = np.ascontiguousarray(feat, np.float32)
+        labels = np.ascontiguousarray(labels, np.uint8)
+        g = np.zeros(BUDGET_PARAMS, np.float32)
+        loss = C.c_float(0)
+        _check(_lib.hrnn_budget_gradients(self._h, _p(feat), _p(labels), feat.shape[0], _p(g), C.byref(loss)))
+        return _split_params(g), loss.value
+
+    def budget_get_weights(self):
+        g = np.zeros(BUDGET_PARAMS, np.float32)
+        _check(_lib.hrnn_budget_get_weights(self._h, _p(g)))
+        return _split_params(g)
+
+    def budget_set_weights(self, params):
+        flat = np.concatenate([np.asarray(p, np.float32).ravel() for p in params])
+        assert flat.size == BUDGET_PARAMS
+        _check(_lib.hrnn_budget_set_weights(self._h, _p(flat)))
 
     # ---- inspection ----------------------------------------------------------
     def info(self) -> dict:

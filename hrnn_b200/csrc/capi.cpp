@@ -10,6 +10,9 @@
 #include <vector>
 
 #include "index.hpp"
+#include "mlp.hpp"
+
+static_assert(hrnn::kBudgetParams == HRNN_BUDGET_PARAMS, "budget parameter layout");
 
 struct hrnn_index {
     hrnn::Index ix;
@@ -280,6 +283,88 @@ hrnn_status hrnn_set_precision(hrnn_index* h, int precision) {
         if (precision != HRNN_PREC_FP32_EXACT && precision != HRNN_PREC_BF16)
             hrnn::fail(HRNN_ERR_ARG, "set_precision: unknown precision");
         h->ix.precision = precision;
+    });
+}
+
+hrnn_status hrnn_set_budget(hrnn_index* h, int enable, uint32_t m0, uint32_t m1, uint32_t ef,
+                            float confidence) {
+    return guard([&] {
+        need(h, "index");
+        set_device(h);
+        hrnn::budget_set(h->ix, enable != 0, m0, m1, ef, confidence);
+    });
+}
+
+hrnn_status hrnn_budget_features(hrnn_index* h, const float* queries, size_t nq, uint32_t k, float* feat) {
+    return guard([&] {
+        need(h, "index");
+        need(queries, "queries");
+        need(feat, "feat");
+        if (k == 0) hrnn::fail(HRNN_ERR_ARG, "budget_features: k must be >= 1");
+        set_device(h);
+        auto& ix = h->ix;
+        if (ix.serve_mode ? k > ix.max_k_serve : k > ix.K)
+            hrnn::fail(HRNN_ERR_ARG, "budget_features: k larger than the stored neighbour lists");
+        if (nq == 0) return;
+        hrnn::DevMem q, f;
+        q.alloc(nq * ix.dim * 4);
+        f.alloc(nq * hrnn::kMlpIn * 4);
+        CUDA_CHECK(cudaMemcpyAsync(q.p, queries, nq * ix.dim * 4, cudaMemcpyHostToDevice, ix.stream));
+        hrnn::budget_features(ix, q.as<float>(), nq, k, f.as<float>());
+        CUDA_CHECK(cudaMemcpy(feat, f.p, nq * hrnn::kMlpIn * 4, cudaMemcpyDeviceToHost));
+    });
+}
+
+hrnn_status hrnn_budget_train(hrnn_index* h, const float* feat, const uint8_t* labels, size_t n, int epochs,
+                              int batch, float lr, uint64_t seed, float* final_loss) {
+    return guard([&] {
+        need(h, "index");
+        need(feat, "feat");
+        need(labels, "labels");
+        set_device(h);
+        const float l = hrnn::budget_train(h->ix, feat, labels, n, epochs, batch, lr, seed);
+        if (final_loss) *final_loss = l;
+    });
+}
+
+hrnn_status hrnn_budget_predict(hrnn_index* h, const float* feat, size_t n, float* logits) {
+    return guard([&] {
+        need(h, "index");
+        need(feat, "feat");
+        need(logits, "logits");
+        set_device(h);
+        hrnn::budget_predict(h->ix, feat, n, logits);
+    });
+}
+
+hrnn_status hrnn_budget_gradients(hrnn_index* h, const float* feat, const uint8_t* labels, size_t n,
+                                  float* grads, float* loss) {
+    return guard([&] {
+        need(h, "index");
+        need(feat, "feat");
+        need(labels, "labels");
+        need(grads, "grads");
+        set_device(h);
+        const float l = hrnn::budget_gradients(h->ix, feat, labels, n, grads);
+        if (loss) *loss = l;
+    });
+}
+
+hrnn_status hrnn_budget_get_weights(hrnn_index* h, float* params) {
+    return guard([&] {
+        need(h, "index");
+        need(params, "params");
+        set_device(h);
+        hrnn::budget_get_weights(h->ix, params);
+    });
+}
+
+hrnn_status hrnn_budget_set_weights(hrnn_index* h, const float* params) {
+    return guard([&] {
+        need(h, "index");
+        need(params, "params");
+        set_device(h);
+        hrnn::budget_set_weights(h->ix, params);
     });
 }
 

@@ -10,8 +10,11 @@
 #include <fstream>
 
 #include "index.hpp"
+#include "mlp.hpp"
 
 namespace hrnn {
+
+Index::Index() = default;
 
 Index::~Index() {
     if (stream) cudaStreamDestroy(stream);

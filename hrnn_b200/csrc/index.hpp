@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <memory>
 #include <random>
 #include <string>
 #include <unordered_map>
@@ -17,6 +18,8 @@
 #include "common.cuh"
 
 namespace hrnn {
+
+struct Budget;  // mlp.hpp
 
 // Owning device allocation.
 struct DevMem {
@@ -117,7 +120,9 @@ struct Index {
     DevMem kcol;         // f32 [n]: kdist(p, k-1) of the current search call
     hrnn_search_stats last_stats{};
     hrnn_refine_stats refine_stats{};
+    std::unique_ptr<Budget> budget;  // learned search budget (hrnn_set_budget)
 
+    Index();
     ~Index();
 
     size_t n() const { return cur; }

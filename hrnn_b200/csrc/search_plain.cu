@@ -20,6 +20,7 @@
 
 #include "beam.cuh"
 #include "index.hpp"
+#include "mlp.hpp"
 
 namespace hrnn {
 
@@ -40,6 +41,14 @@ KCta pick_bc(bool f, bool c, bool x) {
              : (c ? k_phase_bc_cta<E, false, true, false> : k_phase_bc_cta<E, false, false, false>);
 }
 void ensure_bf16(Index& ix);  // mixed.cu
+// budget.cu
+__global__ void k_budget_features(DevView v, const float* Q, uint32_t nq, const uint32_t* prox, const float* proxd,
+                                  const uint32_t* nprox, uint32_t stride, const float* kcol, const float* proj,
+                                  float* feat);
+__global__ void k_budget_decide(const float* z, uint32_t nq, float conf, uint32_t m0, uint32_t m1, const uint32_t* qm,
+                                uint32_t* nprox,
+                                uint32_t* fb_list, uint32_t* fb_count, unsigned long long* levels);
+void ensure_projection(Index& ix, Budget& b);
 __global__ void k_kdist_column(DevView v, uint32_t kidx, float* kcol);
 size_t bc_cta_smem(uint32_t dim, bool counts);
 
@@ -51,14 +60,20 @@ __global__ void __launch_bounds__(128) k_phase_a(DevView v, const float* __restr
                                                  const uint32_t* __restrict__ qm, const uint32_t* __restrict__ qef,
                                                  uint32_t efc, uint32_t vc, uint32_t mmax,
                                                  uint32_t* __restrict__ prox, uint32_t* __restrict__ nprox,
-                                                 SearchCounters* __restrict__ ctr) {
+                                                 SearchCounters* __restrict__ ctr,
+                                                 const uint32_t* __restrict__ qlist, uint32_t m_over,
+                                                 uint32_t ef_over, float* __restrict__ proxd) {
+    // qlist: search only the listed queries (nq = list length); m_over / ef_over:
+    // one (m, ef) for every query instead of the arrays; proxd: also write the
+    // proxies' distances.
     extern __shared__ char smem_raw[];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, wpb = blockDim.x >> 5;
     WarpSmem s = carve(smem_raw + (size_t)w * warp_smem_bytes(v.dim, efc, vc), v.dim, efc, vc);
     unsigned long long c_dist = 0, c_exp = 0;
-    for (uint32_t qi = blockIdx.x * wpb + w; qi < nq; qi += gridDim.x * wpb) {
-        const uint32_t m = qm[qi];
-        const uint32_t EF = max(qef[qi], m);
+    for (uint32_t j = blockIdx.x * wpb + w; j < nq; j += gridDim.x * wpb) {
+        const uint32_t qi = qlist ? qlist[j] : j;
+        const uint32_t m = m_over ? m_over : qm[qi];
+        const uint32_t EF = max(ef_over ? ef_over : qef[qi], m);
         if (v.n == 0 || m == 0) {
             if (lane == 0) nprox[qi] = 0;
             continue;
@@ -72,7 +87,10 @@ __global__ void __launch_bounds__(128) k_phase_a(DevView v, const float* __restr
         c_dist++;  // the reference evaluates the entry point again (hrnn.h:505)
         uint32_t tsize = beam_search<DM>(v, s, cur, curd, EF, 0, vc, c_dist, c_exp);
         uint32_t np_ = min(m, tsize);
-        for (uint32_t i = lane; i < np_; i += 32) prox[(size_t)qi * mmax + i] = s.ti[i] & kIdMask;
+        for (uint32_t i = lane; i < np_; i += 32) {
+            prox[(size_t)qi * mmax + i] = s.ti[i] & kIdMask;
+            if (proxd) proxd[(size_t)qi * mmax + i] = s.td[i];
+        }
         if (lane == 0) nprox[qi] = np_;
         __syncwarp();
     }
@@ -337,6 +355,11 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
         efmax = std::max(efmax, std::max(hef[i], hm[i]));
     }
     if (efmax > (1u << 16)) fail(HRNN_ERR_ARG, "searchRknn: ef_search/m too large (max 65536)");
+    const bool learned = ix.budget && ix.budget->enabled && ix.budget->mlp.ready && ix.dim % 4 == 0;
+    if (learned) {  // the frontier pass keeps kFrontier proxies with ef = Budget::ef
+        mmax = std::max<uint32_t>(mmax, kFrontier);
+        efmax = std::max<uint32_t>(efmax, std::max<uint32_t>(ix.budget->ef, kFrontier));
+    }
     DevView v = make_view(ix);
     const uint32_t efc = (efmax + 31) & ~31u;
     const uint32_t vc = 2048;  // visited-cache slots (lossy; misses cost a recomputed row)
@@ -372,12 +395,54 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
     const int nsm = sms(ix.device);
     CUDA_CHECK(cudaEventRecord(ev[0], s));
     {
-        unsigned grid = (unsigned)std::min<size_t>((nq + wpb - 1) / wpb, (size_t)nsm * 16);
         auto kern = mixed ? k_phase_a<2> : (fusedsimd ? k_phase_a<1> : k_phase_a<0>);
         CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_a));
-        kern<<<grid, wpb * 32, smem_a, s>>>(v, a.d_q, (uint32_t)nq, a.d_m, a.d_ef, efc, vc, mmax,
-                                            prox.as<uint32_t>(), nprox.as<uint32_t>(), ctr);
-        CUDA_LAUNCH_CHECK();
+        auto grid_for = [&](size_t n) { return (unsigned)std::max<size_t>(1, std::min<size_t>((n + wpb - 1) / wpb, (size_t)nsm * 16)); };
+        if (!learned) {
+            kern<<<grid_for(nq), wpb * 32, smem_a, s>>>(v, a.d_q, (uint32_t)nq, a.d_m, a.d_ef, efc, vc, mmax,
+                                                        prox.as<uint32_t>(), nprox.as<uint32_t>(), ctr, nullptr, 0, 0,
+                                                        nullptr);
+            CUDA_LAUNCH_CHECK();
+        } else {
+            // Learned budget: frontier pass for every query, features, MLP, decision;
+            // the queries the MLP is not confident about are searched again with
+            // the caller's (m, ef).
+            Budget& b = *ix.budget;
+            ensure_projection(ix, b);
+            ix.kcol.ensure((size_t)std::max<size_t>(ix.cur, 1) * 4);
+            k_kdist_column<<<(unsigned)((ix.cur + 255) / 256), 256, 0, s>>>(v, (uint32_t)(a.k - 1), ix.kcol.as<float>());
+            CUDA_LAUNCH_CHECK();
+            b.feat.ensure(nq * kMlpIn * 4);
+            b.proxd.ensure(nq * mmax * 4);
+            b.fallback_list.ensure(nq * 4 + 64);
+            b.decided.ensure(64);
+            uint32_t* fb_count = b.decided.as<uint32_t>();
+            unsigned long long* levels = (unsigned long long*)(b.decided.as<char>() + 8);
+            CUDA_CHECK(cudaMemsetAsync(b.decided.p, 0, 64, s));
+            kern<<<grid_for(nq), wpb * 32, smem_a, s>>>(v, a.d_q, (uint32_t)nq, a.d_m, a.d_ef, efc, vc, mmax,
+                                                        prox.as<uint32_t>(), nprox.as<uint32_t>(), ctr, nullptr,
+                                                        kFrontier, b.ef, b.proxd.as<float>());
+            CUDA_LAUNCH_CHECK();
+            k_budget_features<<<(unsigned)((nq * 32 + 255) / 256), 256, 0, s>>>(
+                v, a.d_q, (uint32_t)nq, prox.as<uint32_t>(), b.proxd.as<float>(), nprox.as<uint32_t>(), mmax,
+                ix.kcol.as<float>(), b.proj.as<float>(), b.feat.as<float>());
+            CUDA_LAUNCH_CHECK();
+            b.mlp.forward(b.feat.as<float>(), (int)nq, s);
+            k_budget_decide<<<(unsigned)((nq + 255) / 256), 256, 0, s>>>(
+                b.mlp.z3.as<float>(), (uint32_t)nq, b.confidence, b.m[0], b.m[1], a.d_m, nprox.as<uint32_t>(),
+                b.fallback_list.as<uint32_t>(), fb_count, levels);
+            CUDA_LAUNCH_CHECK();
+            uint32_t nfb = 0;
+            CUDA_CHECK(cudaMemcpyAsync(&nfb, fb_count, 4, cudaMemcpyDeviceToHost, s));
+            CUDA_CHECK(cudaMemcpyAsync(b.n_level, levels, 24, cudaMemcpyDeviceToHost, s));
+            CUDA_CHECK(cudaStreamSynchronize(s));
+            if (nfb) {
+                kern<<<grid_for(nfb), wpb * 32, smem_a, s>>>(v, a.d_q, nfb, a.d_m, a.d_ef, efc, vc, mmax,
+                                                             prox.as<uint32_t>(), nprox.as<uint32_t>(), ctr,
+                                                             b.fallback_list.as<uint32_t>(), 0, 0, nullptr);
+                CUDA_LAUNCH_CHECK();
+            }
+        }
     }
     CUDA_CHECK(cudaEventRecord(ev[1], s));
     {
@@ -486,6 +551,8 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
     st.n_fp64_decided = hc.n_fp64;
     st.n_fp64_flipped = hc.n_flip;
     st.n_launches = launch_counter().load() - launches0;
+    if (learned)
+        for (int i = 0; i < 3; ++i) st.n_budget[i] = ix.budget->n_level[i];
     float t01 = 0, t12 = 0, t23 = 0;
     cudaEventElapsedTime(&t01, ev[0], ev[1]);
     cudaEventElapsedTime(&t12, ev[1], ev[2]);
@@ -503,6 +570,52 @@ void l2_batch_device(const float* a, const float* b, size_t n, size_t dim, L2Ord
     if (!n) return;
     k_l2_pairs<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(a, b, n, (uint32_t)dim, o.lanes, o.fused, out);
     CUDA_LAUNCH_CHECK();
+}
+
+Budget& budget_of(Index& ix) {
+    if (!ix.budget) ix.budget.reset(new Budget());
+    return *ix.budget;
+}
+
+// Features of nq queries (device buffers): the frontier pass (m = kFrontier,
+// ef = Budget::ef) and k_budget_features, in the index's precision mode.
+void budget_features(Index& ix, const float* d_q, size_t nq, uint32_t k, float* d_feat) {
+    if (!ix.rknng_built) fail(HRNN_ERR_STATE, "searchRknn: RKNNG not built");
+    if (ix.dim % 4 != 0) fail(HRNN_ERR_ARG, "budget: dim must be a multiple of 4");
+    if (nq == 0) return;
+    Budget& b = budget_of(ix);
+    cudaStream_t s = ix.stream;
+    ix.sync_upper_to_device();
+    const bool mixed = ix.precision == HRNN_PREC_BF16 && (ix.dim == 96 || ix.dim == 128 || ix.dim == 256) &&
+                       ix.order.lanes == 16;
+    if (mixed) ensure_bf16(ix);
+    DevView v = make_view(ix);
+    ensure_projection(ix, b);
+    const uint32_t mmax = kFrontier, efc = (std::max<uint32_t>(b.ef, kFrontier) + 31) & ~31u, vc = 2048;
+    const size_t wsm = warp_smem_bytes(v.dim, efc, vc);
+    const int wpb = (int)std::max<size_t>(1, std::min<size_t>(4, (200 * 1024) / wsm));
+    const size_t smem_a = wsm * wpb;
+    if (smem_a > 227 * 1024) fail(HRNN_ERR_ARG, "budget: ef/dim too large for one warp's beam");
+    DevMem prox, nprox, proxd;
+    prox.alloc(nq * mmax * 4);
+    nprox.alloc(nq * 4);
+    proxd.alloc(nq * mmax * 4);
+    ix.kcol.ensure((size_t)std::max<size_t>(ix.cur, 1) * 4);
+    k_kdist_column<<<(unsigned)((ix.cur + 255) / 256), 256, 0, s>>>(v, k - 1, ix.kcol.as<float>());
+    CUDA_LAUNCH_CHECK();
+    auto kern = mixed ? k_phase_a<2> : (((ix.order.fused & 1) != 0) ? k_phase_a<1> : k_phase_a<0>);
+    CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_a));
+    const int nsm = sms(ix.device);
+    unsigned grid = (unsigned)std::max<size_t>(1, std::min<size_t>((nq + wpb - 1) / wpb, (size_t)nsm * 16));
+    kern<<<grid, wpb * 32, smem_a, s>>>(v, d_q, (uint32_t)nq, nullptr, nullptr, efc, vc, mmax, prox.as<uint32_t>(),
+                                        nprox.as<uint32_t>(), ix.counters.as<SearchCounters>(), nullptr, kFrontier,
+                                        b.ef, proxd.as<float>());
+    CUDA_LAUNCH_CHECK();
+    k_budget_features<<<(unsigned)((nq * 32 + 255) / 256), 256, 0, s>>>(v, d_q, (uint32_t)nq, prox.as<uint32_t>(),
+                                                                       proxd.as<float>(), nprox.as<uint32_t>(), mmax,
+                                                                       ix.kcol.as<float>(), b.proj.as<float>(), d_feat);
+    CUDA_LAUNCH_CHECK();
+    CUDA_CHECK(cudaStreamSynchronize(s));
 }
 
 }  // namespace hrnn

@@ -72,6 +72,7 @@ typedef struct {
     uint64_t n_fp64_decided;/* mixed precision: re-decided in FP64 (tie band)   */
     uint64_t n_fp64_flipped;/* ... of which FP64 decided against FP32           */
     uint64_t n_launches;    /* kernels this call launched                       */
+    uint64_t n_budget[3];   /* learned budget: queries at level 0, 1, fallback */
     double phase_a_ms, phase_b_ms, phase_c_ms;   /* device time of each phase   */
 } hrnn_search_stats;
 
@@ -183,6 +184,35 @@ hrnn_status hrnn_get_refine_stats(hrnn_index* h, hrnn_refine_stats* st);
 #define HRNN_PREC_FP32_EXACT 0
 #define HRNN_PREC_BF16 1
 hrnn_status hrnn_set_precision(hrnn_index* h, int precision);
+
+/* Learned search budget (new; no counterpart in the reference).  A 256-256-256-2
+ * MLP with GELU and BF16 weights reads a query and its first beam frontier (a
+ * search with ef = `ef` keeping 32 entries) and outputs two logits: "the answer
+ * with m = m0 proxies from this frontier is complete" and "... with m = m1".  The
+ * batch search then uses the cheapest level whose probability reaches
+ * `confidence`, and the caller's (m, ef_search) otherwise.  Verification still
+ * decides every returned point: the budget changes work, never membership.
+ *   hrnn_set_budget: stores (m0, m1, ef, confidence) with 1 <= m0 <= m1 <= 32,
+ *     m1 <= ef, 0.5 < confidence <= 1, also when disabling; enabling needs weights.
+ *   hrnn_budget_features: the 256 features of nq host queries (host out, nq x 256)
+ *     for result size k, with the stored ef.
+ *   hrnn_budget_train: trains on the device with the library's BF16 kernels
+ *     (labels: nq x 2 bytes, 1 = complete at that level); returns the last loss.
+ *   hrnn_budget_predict / hrnn_budget_gradients: forward logits / parameter
+ *     gradients of the mean binary cross-entropy (W1 b1 W2 b2 W3 b3, FP32).
+ *   hrnn_budget_get_weights / _set_weights: the same parameter layout
+ *     (HRNN_BUDGET_PARAMS floats). */
+#define HRNN_BUDGET_PARAMS (256 * 256 + 256 + 256 * 256 + 256 + 2 * 256 + 2)
+hrnn_status hrnn_set_budget(hrnn_index* h, int enable, uint32_t m0, uint32_t m1, uint32_t ef,
+                            float confidence);
+hrnn_status hrnn_budget_features(hrnn_index* h, const float* queries, size_t nq, uint32_t k, float* feat);
+hrnn_status hrnn_budget_train(hrnn_index* h, const float* feat, const uint8_t* labels, size_t n,
+                              int epochs, int batch, float lr, uint64_t seed, float* final_loss);
+hrnn_status hrnn_budget_predict(hrnn_index* h, const float* feat, size_t n, float* logits);
+hrnn_status hrnn_budget_gradients(hrnn_index* h, const float* feat, const uint8_t* labels, size_t n,
+                                  float* grads, float* loss);
+hrnn_status hrnn_budget_get_weights(hrnn_index* h, float* params);
+hrnn_status hrnn_budget_set_weights(hrnn_index* h, const float* params);
 
 /* FP32 summation order of the L2 kernel (space_l2.h:214-238 picks it per host):
  * lanes in {16, 8, 4}; fused bit 0 = SIMD multiply-add contracted, bit 1 = scalar

@@ -85,3 +85,30 @@ def test_oracle_vs_live_reference(tmp_path):
         a = r.search_batch(Q, m, kp, ef, threshold=th, k=k)
         b = O.search_batch(Q, m, kp, ef, threshold=th, k=k)
         assert all(np.array_equal(x, y) for x, y in zip(a, b))
+
+
+def test_budget_mlp_oracle_finite_differences():
+    """The FP64 budget-MLP oracle's analytic gradients against central differences."""
+    from oracle import mlp
+    rng = np.random.default_rng(7)
+    params = [p.astype(np.float64) for p in mlp.init_params(3)]
+    X = rng.standard_normal((6, 256))
+    Y = rng.integers(0, 2, (6, 2)).astype(np.uint8)
+    _, grads = mlp.loss_and_grads(params, X, Y, bf16_ops=False)
+    h = 1e-6
+    for t, idxs in ((0, [(0, 0), (17, 200)]), (1, [(5,)]), (2, [(3, 9), (255, 1)]), (3, [(100,)]),
+                    (4, [(0, 7), (1, 255)]), (5, [(0,), (1,)])):
+        for ix in idxs:
+            pp = [p.copy() for p in params]
+            pp[t][ix] += h
+            lp = mlp.loss_of(mlp.forward(pp, X, bf16_ops=False)[4], Y)
+            pp[t][ix] -= 2 * h
+            lm = mlp.loss_of(mlp.forward(pp, X, bf16_ops=False)[4], Y)
+            num = (lp - lm) / (2 * h)
+            assert abs(num - grads[t][ix]) <= 1e-6 + 1e-5 * abs(num), (t, ix, num, grads[t][ix])
+
+
+def test_bf16_rounding_oracle():
+    from oracle import mlp
+    x = np.array([1.0, 1.0 + 2 ** -8, 1.0 + 3 * 2 ** -8, -2.5, 1.0 + 2 ** -9], np.float32)
+    assert np.array_equal(mlp.bf16(x), [1.0, 1.0, 1.0 + 4 * 2 ** -8, -2.5, 1.0])
