@@ -36,9 +36,10 @@ EXPORTS = [
     "hrnn_budget_gradients", "hrnn_budget_get_weights", "hrnn_budget_set_weights",
 ]
 
-# Learned-budget MLP: 256 -> 256 -> 256 -> 2; parameters W1 b1 W2 b2 W3 b3 (row-major [out, in]).
+# Learned-budget MLP: 256 -> 256 -> 256 -> 2; parameters W1 b1 W2 b2 W3 b3 (row-major
+# [out, in]), then the input normalisation mean and 1/std.
 BUDGET_IN, BUDGET_HIDDEN, BUDGET_OUT = 256, 256, 2
-BUDGET_SHAPES = [(256, 256), (256,), (256, 256), (256,), (2, 256), (2,)]
+BUDGET_SHAPES = [(256, 256), (256,), (256, 256), (256,), (2, 256), (2,), (256,), (256,)]
 BUDGET_PARAMS = sum(int(np.prod(s)) for s in BUDGET_SHAPES)
 
 
@@ -74,7 +75,7 @@ MAX_ITERS = 64
 class RefineStats(C.Structure):
     _fields_ = [("iters", C.c_int32)] + [
         (f, C.c_uint64 * MAX_ITERS) for f in ("join_dists", "updates", "proposals", "sample_entries")] + [
-        ("ms", C.c_double * MAX_ITERS)]
+        (f, C.c_double * MAX_ITERS) for f in ("ms", "sample_ms", "join_ms", "bucket_ms", "merge_ms")]
 
     def as_dict(self):
         k = self.iters
@@ -112,7 +113,7 @@ _lib.hrnn_get_rknng.argtypes = [_vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64
                                 C.POINTER(C.c_uint32), _vp, _vp, C.c_int]
 _lib.hrnn_l2_batch.argtypes = [_vp, _vp, _sz, _sz, C.c_int, C.c_int, _vp]
 _lib.hrnn_set_budget.argtypes = [_vp, C.c_int, C.c_uint32, C.c_uint32, C.c_uint32, C.c_float]
-_lib.hrnn_budget_features.argtypes = [_vp, _vp, _sz, C.c_uint32, _vp]
+_lib.hrnn_budget_features.argtypes = [_vp, _vp, _sz, C.c_uint32, C.c_uint32, C.c_uint32, _vp]
 _lib.hrnn_budget_train.argtypes = [_vp, _vp, _vp, _sz, C.c_int, C.c_int, C.c_float, C.c_uint64,
                                    C.POINTER(C.c_float)]
 _lib.hrnn_budget_predict.argtypes = [_vp, _vp, _sz, _vp]
@@ -284,15 +285,18 @@ class HRNN:
         return tot.value
 
     # ---- learned search budget (no counterpart in the reference) -------------
-    def set_budget(self, enable: bool, m0: int = 1, m1: int = 3, ef: int = 100, confidence: float = 0.9):
-        """Serve searches with the learned budget (levels m0 / m1 with beam ef) when enabled."""
+    def set_budget(self, enable: bool, m0: int = 1, m1: int = 3, ef: int = 0, confidence: float = 0.9):
+        """Serve searches with the learned budget when enabled: levels of m0 / m1
+        proxies; ef = 0 takes them from the caller's beam, ef > 0 from a beam of ef
+        (with a second search for the other queries)."""
         _check(_lib.hrnn_set_budget(self._h, int(enable), m0, m1, ef, confidence))
 
-    def budget_features(self, Q, k: int) -> np.ndarray:
-        """The MLP's 256 features of each query (frontier pass with the budget's ef)."""
+    def budget_features(self, Q, k: int, m: int = 1, ef_search: int = 1) -> np.ndarray:
+        """The MLP's 256 features of each query, from the frontier of a search with
+        (m, ef_search) -- the budget's (m1, ef) in two-pass mode."""
         Q = np.ascontiguousarray(Q, np.float32)
         f = np.zeros((Q.shape[0], BUDGET_IN), np.float32)
-        _check(_lib.hrnn_budget_features(self._h, _p(Q), Q.shape[0], k, _p(f)))
+        _check(_lib.hrnn_budget_features(self._h, _p(Q), Q.shape[0], k, m, ef_search, _p(f)))
         return f
 
     def budget_train(self, feat, labels, epochs: int = 10, batch: int = 1024, lr: float = 1e-3,
@@ -312,13 +316,13 @@ class HRNN:
         return z
 
     def budget_gradients(self, feat, labels):
-        """Gradients of the mean BCE (list in BUDGET_SHAPES order) and the loss."""
+        """Gradients of the mean BCE for W1 b1 W2 b2 W3 b3 and the loss."""
         feat = np.ascontiguousarray(feat, np.float32)
         labels = np.ascontiguousarray(labels, np.uint8)
         g = np.zeros(BUDGET_PARAMS, np.float32)
         loss = C.c_float(0)
         _check(_lib.hrnn_budget_gradients(self._h, _p(feat), _p(labels), feat.shape[0], _p(g), C.byref(loss)))
-        return _split_params(g), loss.value
+        return _split_params(g)[:6], loss.value
 
     def budget_get_weights(self):
         g = np.zeros(BUDGET_PARAMS, np.float32)

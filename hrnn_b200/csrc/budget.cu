@@ -1,17 +1,20 @@
 // Learned search budget: features of a query and its first beam frontier, the
 // MLP decision, and the host entry points for training and serving.
 //
-// Frontier pass: the beam search with ef = Budget::ef returning its kFrontier
-// nearest entries.  Features (256 per query): 128 values of a fixed Gaussian
+// Frontier pass: the beam search (the caller's, or the level ef in two-pass mode)
+// returning its kFrontier nearest entries.  Features (256 per query): 128 values of a fixed Gaussian
 // projection of the query (/ sqrt(dim)); for each of the 32 frontier entries
 // log(1 + d), log(1 + kdist(p, k-1)), d / kdist (clipped to [0, 4]) and the
 // reverse in-degree log(1 + |R(p)|) / 8 (missing entries: 0).
 // Decision: level 0 when sigmoid(z0) >= confidence, else level 1 when
-// sigmoid(z1) >= confidence, else the caller's (m, ef).  Levels 0 and 1 take the
-// first m of the frontier (the same proxies the plain search finds with that m and
-// ef); the fallback queries are searched again with the caller's budget.
+// sigmoid(z1) >= confidence, else the caller's m.  Levels take the first m0 / m1
+// entries of the frontier (the proxies the plain search finds with that m).
+// Single-pass mode (level ef 0): the frontier is the caller's own beam, so the
+// budget only trims proxies.  Two-pass mode: the frontier beam is the level ef
+// and the fallback queries are searched again with the caller's (m, ef).
 #include <algorithm>
 #include <cfloat>
+#include <cmath>
 #include <random>
 #include <vector>
 
@@ -57,10 +60,12 @@ __global__ void k_budget_features(DevView v, const float* __restrict__ Q, uint32
     f[224 + lane] = f3;
 }
 
-// Per query: budget level from the logits; nprox trimmed for levels 0/1,
-// fallback queries listed for a second search.
+// Per query: budget level from the logits; nprox trimmed for levels 0/1.
+// Fallback queries keep the caller's m (single pass) or are listed for a second
+// search (rerun).
 __global__ void k_budget_decide(const float* __restrict__ z, uint32_t nq, float conf, uint32_t m0, uint32_t m1,
-                                const uint32_t* __restrict__ qm, uint32_t* __restrict__ nprox, uint32_t* __restrict__ fb_list,
+                                const uint32_t* __restrict__ qm, int rerun, uint32_t* __restrict__ nprox,
+                                uint32_t* __restrict__ fb_list,
                                 uint32_t* __restrict__ fb_count, unsigned long long* __restrict__ levels) {
     const uint32_t qi = blockIdx.x * blockDim.x + threadIdx.x;
     if (qi >= nq) return;
@@ -72,7 +77,8 @@ __global__ void k_budget_decide(const float* __restrict__ z, uint32_t nq, float 
         nprox[qi] = min(nprox[qi], min(m1, qm[qi]));
         atomicAdd(&levels[1], 1ull);
     } else {
-        fb_list[atomicAdd(fb_count, 1u)] = qi;
+        if (rerun) fb_list[atomicAdd(fb_count, 1u)] = qi;
+        else nprox[qi] = min(nprox[qi], qm[qi]);
         atomicAdd(&levels[2], 1ull);
     }
 }
@@ -92,7 +98,7 @@ void budget_set(Index& ix, bool enable, uint32_t m0, uint32_t m1, uint32_t ef, f
     Budget& b = budget_of(ix);
     if (enable && !b.mlp.ready) fail(HRNN_ERR_STATE, "budget: train the model or set its weights first");
     if (m0 == 0 || m1 < m0 || m1 > (uint32_t)kFrontier) fail(HRNN_ERR_ARG, "budget: need 1 <= m0 <= m1 <= 32");
-    if (ef < m1 || ef > (1u << 16)) fail(HRNN_ERR_ARG, "budget: ef must be in [m1, 65536]");
+    if (ef != 0 && (ef < m1 || ef > (1u << 16))) fail(HRNN_ERR_ARG, "budget: ef must be 0 or in [m1, 65536]");
     if (!(confidence > 0.5f && confidence <= 1.f)) fail(HRNN_ERR_ARG, "budget: confidence must be in (0.5, 1]");
     if (ix.dim % 4 != 0) fail(HRNN_ERR_ARG, "budget: dim must be a multiple of 4");
     b.m[0] = m0;
@@ -118,6 +124,27 @@ float budget_train(Index& ix, const float* feat, const uint8_t* labels, size_t n
     if (n > 0xFFFFFFFFull) fail(HRNN_ERR_ARG, "budget_train: too many samples");
     Budget& b = budget_of(ix);
     cudaStream_t s = ix.stream;
+    if (!b.mlp.ready) {
+        // Fresh model: random weights and the training features' per-feature mean
+        // and 1/std (0 for constant features) as the input normalisation.
+        b.mlp.init(seed, s);
+        std::vector<double> mu(kMlpIn, 0.0), var(kMlpIn, 0.0);
+        for (size_t i = 0; i < n; ++i)
+            for (int f = 0; f < kMlpIn; ++f) mu[f] += feat[i * kMlpIn + f];
+        for (int f = 0; f < kMlpIn; ++f) mu[f] /= (double)n;
+        for (size_t i = 0; i < n; ++i)
+            for (int f = 0; f < kMlpIn; ++f) {
+                const double d = feat[i * kMlpIn + f] - mu[f];
+                var[f] += d * d;
+            }
+        std::vector<float> nr(2 * kMlpIn);
+        for (int f = 0; f < kMlpIn; ++f) {
+            const double sd = std::sqrt(var[f] / (double)n);
+            nr[f] = (float)mu[f];
+            nr[kMlpIn + f] = sd > 1e-12 ? (float)(1.0 / sd) : 0.f;
+        }
+        CUDA_CHECK(cudaMemcpyAsync(b.mlp.norm.p, nr.data(), nr.size() * 4, cudaMemcpyHostToDevice, s));
+    }
     DevMem X, Y;
     upload(X, feat, n * kMlpIn * 4, s);
     upload(Y, labels, n * 2, s);
@@ -157,6 +184,7 @@ float budget_gradients(Index& ix, const float* feat, const uint8_t* labels, size
         CUDA_CHECK(cudaMemcpyAsync(grads + off, b.mlp.gr[i].p, b.mlp.n[i] * 4, cudaMemcpyDeviceToHost, s));
         off += b.mlp.n[i];
     }
+    std::fill(grads + off, grads + off + 2 * kMlpIn, 0.f);
     float loss = 0.f;
     CUDA_CHECK(cudaMemcpyAsync(&loss, L.p, 4, cudaMemcpyDeviceToHost, s));
     CUDA_CHECK(cudaStreamSynchronize(s));
@@ -171,6 +199,7 @@ void budget_get_weights(Index& ix, float* params) {
         CUDA_CHECK(cudaMemcpy(params + off, b.mlp.p[i].p, b.mlp.n[i] * 4, cudaMemcpyDeviceToHost));
         off += b.mlp.n[i];
     }
+    CUDA_CHECK(cudaMemcpy(params + off, b.mlp.norm.p, 2 * kMlpIn * 4, cudaMemcpyDeviceToHost));
 }
 
 void budget_set_weights(Index& ix, const float* params) {
@@ -183,6 +212,7 @@ void budget_set_weights(Index& ix, const float* params) {
         CUDA_CHECK(cudaMemset(b.mlp.m2[i].p, 0, b.mlp.n[i] * 4));
         off += b.mlp.n[i];
     }
+    CUDA_CHECK(cudaMemcpy(b.mlp.norm.p, params + off, 2 * kMlpIn * 4, cudaMemcpyHostToDevice));
     b.mlp.step = 0;
 }
 

@@ -295,7 +295,8 @@ hrnn_status hrnn_set_budget(hrnn_index* h, int enable, uint32_t m0, uint32_t m1,
     });
 }
 
-hrnn_status hrnn_budget_features(hrnn_index* h, const float* queries, size_t nq, uint32_t k, float* feat) {
+hrnn_status hrnn_budget_features(hrnn_index* h, const float* queries, size_t nq, uint32_t k, uint32_t m,
+                                 uint32_t ef_search, float* feat) {
     return guard([&] {
         need(h, "index");
         need(queries, "queries");
@@ -310,7 +311,7 @@ hrnn_status hrnn_budget_features(hrnn_index* h, const float* queries, size_t nq,
         q.alloc(nq * ix.dim * 4);
         f.alloc(nq * hrnn::kMlpIn * 4);
         CUDA_CHECK(cudaMemcpyAsync(q.p, queries, nq * ix.dim * 4, cudaMemcpyHostToDevice, ix.stream));
-        hrnn::budget_features(ix, q.as<float>(), nq, k, f.as<float>());
+        hrnn::budget_features(ix, q.as<float>(), nq, k, m, ef_search, f.as<float>());
         CUDA_CHECK(cudaMemcpy(feat, f.p, nq * hrnn::kMlpIn * 4, cudaMemcpyDeviceToHost));
     });
 }

@@ -73,6 +73,16 @@ __device__ __forceinline__ float gelu_d(float x) {
     return 0.5f * (1.f + erff(x * 0.70710678f)) + x * 0.39894228f * expf(-0.5f * x * x);
 }
 
+// xn = (x - mean) * inv, per input feature (plain IEEE FP32 subtract and multiply).
+__global__ void k_normalize(const float* __restrict__ x, const float* __restrict__ nrm, float* __restrict__ xn,
+                            size_t n) {
+    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        const int f = (int)(i % kMlpIn);
+        xn[i] = __fmul_rn(__fsub_rn(x[i], nrm[f]), nrm[kMlpIn + f]);
+    }
+}
+
 __global__ void k_gelu(const float* __restrict__ z, float* __restrict__ a, size_t n) {
     size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) a[i] = gelu(z[i]);
@@ -158,6 +168,10 @@ void Mlp::init(uint64_t seed, cudaStream_t s) {
         CUDA_CHECK(cudaMemsetAsync(m1[i].p, 0, n[i] * 4, s));
         CUDA_CHECK(cudaMemsetAsync(m2[i].p, 0, n[i] * 4, s));
     }
+    std::vector<float> nr(2 * kMlpIn, 0.f);
+    for (int f = 0; f < kMlpIn; ++f) nr[kMlpIn + f] = 1.f;
+    norm.alloc(nr.size() * 4);
+    CUDA_CHECK(cudaMemcpyAsync(norm.p, nr.data(), nr.size() * 4, cudaMemcpyHostToDevice, s));
     step = 0;
     ready = true;
     CUDA_CHECK(cudaStreamSynchronize(s));
@@ -167,6 +181,7 @@ void Mlp::ensure_work(int B) {
     if (cap >= B) return;
     cap = B;
     const size_t b = (size_t)B;
+    xn.alloc(b * kMlpIn * 4);
     z1.alloc(b * kMlpH * 4);
     a1.alloc(b * kMlpH * 4);
     z2.alloc(b * kMlpH * 4);
@@ -179,7 +194,9 @@ void Mlp::ensure_work(int B) {
 
 void Mlp::forward(const float* X, int B, cudaStream_t s) {
     ensure_work(B);
-    gemm(false, true, X, w(0), z1.as<float>(), b(0), B, kMlpH, kMlpIn, kMlpIn, kMlpIn, 0.f, s);
+    k_normalize<<<blocks((size_t)B * kMlpIn), 256, 0, s>>>(X, norm.as<float>(), xn.as<float>(), (size_t)B * kMlpIn);
+    CUDA_LAUNCH_CHECK();
+    gemm(false, true, xn.as<float>(), w(0), z1.as<float>(), b(0), B, kMlpH, kMlpIn, kMlpIn, kMlpIn, 0.f, s);
     k_gelu<<<blocks((size_t)B * kMlpH), 256, 0, s>>>(z1.as<float>(), a1.as<float>(), (size_t)B * kMlpH);
     CUDA_LAUNCH_CHECK();
     gemm(false, true, a1.as<float>(), w(1), z2.as<float>(), b(1), B, kMlpH, kMlpH, kMlpH, kMlpH, 0.f, s);
@@ -188,8 +205,10 @@ void Mlp::forward(const float* X, int B, cudaStream_t s) {
     gemm(false, true, a2.as<float>(), w(2), z3.as<float>(), b(2), B, kMlpOut, kMlpH, kMlpH, kMlpH, 0.f, s);
 }
 
-// Gradients of the mean BCE over the batch into gr[] (forward must have run on X).
+// Gradients of the mean BCE over the batch into gr[] (forward must have run on X;
+// layer 1 reads the normalised copy it left in xn).
 void Mlp::backward(const float* X, const uint8_t* Y, int B, float* loss, cudaStream_t s) {
+    (void)X;
     k_bce<<<blocks((size_t)B * 2), 256, 0, s>>>(z3.as<float>(), Y, g3.as<float>(), B, loss);
     CUDA_LAUNCH_CHECK();
     // layer 3: dW3 = g3^T a2, db3 = colsum g3, g2 = g3 W3 * gelu'(z2)
@@ -209,7 +228,8 @@ void Mlp::backward(const float* X, const uint8_t* Y, int B, float* loss, cudaStr
     k_gelu_back<<<blocks((size_t)B * kMlpH), 256, 0, s>>>(z1.as<float>(), g1.as<float>(), (size_t)B * kMlpH);
     CUDA_LAUNCH_CHECK();
     // layer 1
-    gemm(true, false, g1.as<float>(), X, gr[0].as<float>(), nullptr, kMlpH, kMlpIn, B, kMlpH, kMlpIn, 0.f, s);
+    gemm(true, false, g1.as<float>(), xn.as<float>(), gr[0].as<float>(), nullptr, kMlpH, kMlpIn, B, kMlpH, kMlpIn,
+         0.f, s);
     k_colsum<<<1, 256, 0, s>>>(g1.as<float>(), gr[1].as<float>(), B, kMlpH);
     CUDA_LAUNCH_CHECK();
 }
@@ -227,7 +247,7 @@ void Mlp::adam(float lr, float wd, cudaStream_t s) {
 
 float Mlp::train(const float* d_X, const uint8_t* d_Y, size_t N, int epochs, int batch, float lr, uint64_t seed,
                  cudaStream_t s) {
-    if (!ready) init(seed, s);
+    if (!ready) fail(HRNN_ERR_STATE, "budget: model not initialised");
     DevMem idx, xb, yb, loss;
     idx.alloc(N * 4);
     xb.alloc((size_t)batch * kMlpIn * 4);

@@ -14,7 +14,8 @@ struct Mlp {
     // parameters: W1 [H x In], b1, W2 [H x H], b2, W3 [Out x H], b3 (FP32 masters)
     DevMem p[6], gr[6], m1[6], m2[6];
     size_t n[6];
-    DevMem z1, a1, z2, a2, z3, g1, g2, g3;  // activations / gradients of one batch
+    DevMem norm;  // input normalisation: mean[In], 1/std[In] (x -> (x - mean) * inv)
+    DevMem xn, z1, a1, z2, a2, z3, g1, g2, g3;  // normalised input, activations / gradients of one batch
     int cap = 0;
     long step = 0;
     bool ready = false;
@@ -22,31 +23,30 @@ struct Mlp {
     Mlp();
     float* w(int l) const { return p[2 * l].as<float>(); }
     float* b(int l) const { return p[2 * l + 1].as<float>(); }
-    void init(uint64_t seed, cudaStream_t s);
+    void init(uint64_t seed, cudaStream_t s);  // random weights, identity normalisation
     void ensure_work(int B);
     void forward(const float* X, int B, cudaStream_t s);  // logits in z3
     void backward(const float* X, const uint8_t* Y, int B, float* loss, cudaStream_t s);
     void adam(float lr, float wd, cudaStream_t s);
     float train(const float* d_X, const uint8_t* d_Y, size_t N, int epochs, int batch, float lr, uint64_t seed,
-                cudaStream_t s);
+                cudaStream_t s);  // d_X raw features; the model must be initialised
 };
 
 struct Budget {
     Mlp mlp;
     bool enabled = false;
     uint32_t m[2] = {1, 3};       // proxies of budget levels 0 and 1
-    uint32_t ef = 100;            // beam of the frontier pass (serves both levels)
+    uint32_t ef = 0;              // level beam (two-pass mode); 0: the caller's beam
     float confidence = 0.9f;      // probability cutoff for taking a level
     DevMem proj;                  // [dim x 128] fixed random projection of the query
     uint32_t proj_dim = 0;
-    DevMem feat, decided, fallback_list, proxd, kcache;
-    uint32_t kcache_k = 0xFFFFFFFFu;
+    DevMem feat, decided, fallback_list, proxd;  // per-call work buffers
     unsigned long long n_level[3] = {0, 0, 0};  // queries served at level 0 / 1 / fallback (last call)
 };
 
 // search_plain.cu
 Budget& budget_of(Index& ix);
-void budget_features(Index& ix, const float* d_q, size_t nq, uint32_t k, float* d_feat);
+void budget_features(Index& ix, const float* d_q, size_t nq, uint32_t k, uint32_t m, uint32_t ef, float* d_feat);
 
 // budget.cu: host entry points (host buffers unless named d_*)
 void budget_set(Index& ix, bool enable, uint32_t m0, uint32_t m1, uint32_t ef, float confidence);
@@ -56,7 +56,9 @@ void budget_predict(Index& ix, const float* feat, size_t n, float* logits);
 float budget_gradients(Index& ix, const float* feat, const uint8_t* labels, size_t n, float* grads);
 void budget_get_weights(Index& ix, float* params);
 void budget_set_weights(Index& ix, const float* params);
+// Parameter layout of get/set weights: W1 b1 W2 b2 W3 b3, then mean and 1/std of
+// the input normalisation.
 constexpr size_t kBudgetParams = (size_t)kMlpH * kMlpIn + kMlpH + (size_t)kMlpH * kMlpH + kMlpH +
-                                 (size_t)kMlpOut * kMlpH + kMlpOut;
+                                 (size_t)kMlpOut * kMlpH + kMlpOut + 2 * (size_t)kMlpIn;
 
 }  // namespace hrnn

@@ -174,11 +174,11 @@ __global__ void __launch_bounds__(256) k_join(const float* __restrict__ vec, uin
     const uint32_t stride = dim + 1;
     uint32_t* sid = (uint32_t*)(sm + (size_t)2 * cap * stride);
     float* sthr = (float*)(sid + 2 * cap);
-    uint32_t* rowoff = (uint32_t*)(sthr + 2 * cap);
     const int lane = threadIdx.x & 31;
     unsigned long long local_pairs = 0;
     for (uint32_t node = node0 + blockIdx.x; node < node1; node += gridDim.x) {
         const uint32_t nn = newc[node], no = oldc[node];
+        if (nn == 0) continue;  // no pairs (uniform over the block)
         const uint32_t tot = nn + no;
         __syncthreads();
         for (uint32_t r = threadIdx.x; r < tot; r += blockDim.x) {
@@ -193,16 +193,10 @@ __global__ void __launch_bounds__(256) k_join(const float* __restrict__ vec, uin
         }
         __syncthreads();
         // rows i in [0, nn); partners j in (i, tot): j < nn is new x new, j >= nn new x old.
-        // Pair t -> (i, j) through the row offsets rowoff[i] = sum_{i'<i} (tot-1-i').
-        if (threadIdx.x == 0) {
-            uint32_t acc = 0;
-            for (uint32_t i = 0; i <= nn; ++i) {
-                rowoff[i] = acc;
-                if (i < nn) acc += tot - 1 - i;
-            }
-        }
-        __syncthreads();
-        const uint32_t T = rowoff[nn];
+        // Pair t -> (i, j) through the row offsets off(i) = sum_{i'<i} (tot-1-i')
+        // = i (tot-1) - i (i-1) / 2.
+        auto rowoff = [tot](uint32_t i) { return i * (tot - 1) - i * (i - 1) / 2; };
+        const uint32_t T = rowoff(nn);
         for (uint32_t t0 = 0; t0 < T; t0 += blockDim.x) {
             const uint32_t t = t0 + threadIdx.x;
             bool emit_a = false, emit_b = false;
@@ -212,10 +206,10 @@ __global__ void __launch_bounds__(256) k_join(const float* __restrict__ vec, uin
                 uint32_t lo = 0, hi = nn;  // last row with rowoff <= t
                 while (hi - lo > 1) {
                     uint32_t mid = (lo + hi) >> 1;
-                    if (rowoff[mid] <= t) lo = mid;
+                    if (rowoff(mid) <= t) lo = mid;
                     else hi = mid;
                 }
-                const uint32_t i = lo, j = i + 1 + (t - rowoff[i]);
+                const uint32_t i = lo, j = i + 1 + (t - rowoff(i));
                 a = sid[i];
                 b = sid[j];
                 if (a != b) {
@@ -531,7 +525,7 @@ void refine_knng(Index& ix, int iters, int sample) {
     unsigned long long* d_njoin = d_pcount + 1;
     unsigned long long* d_nupd = d_pcount + 2;
     const bool fast = ix.order.lanes == 16 && ix.dim % 16 == 0;
-    const size_t join_smem = (size_t)2 * cap * (ix.dim + 1) * 4 + (size_t)2 * cap * 8 + ((size_t)cap + 1) * 4;
+    const size_t join_smem = (size_t)2 * cap * (ix.dim + 1) * 4 + (size_t)2 * cap * 8;
     if (fast) {
         auto kj = (ix.order.fused & 1) ? k_join<true> : k_join<false>;
         if (join_smem > 227 * 1024) fail(HRNN_ERR_ARG, "refineKNNG: sample size too large for dim");
@@ -544,10 +538,17 @@ void refine_knng(Index& ix, int iters, int sample) {
     CUDA_CHECK(cudaFuncSetAttribute(k_merge, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)merge_smem));
     const int g1 = nsm * 16;
     ix.refine_stats = hrnn_refine_stats{};
+    // Events bracketing sampling, and each chunk's join and bucket+merge.
+    cudaEvent_t ev[7];
+    for (auto& e : ev) CUDA_CHECK(cudaEventCreate(&e));
+    auto elapsed = [](cudaEvent_t a, cudaEvent_t b) {
+        float t = 0.f;
+        cudaEventElapsedTime(&t, a, b);
+        return (double)t;
+    };
     for (int it = 0; it < iters; ++it) {
-        cudaEvent_t e0, e1;
-        CUDA_CHECK(cudaEventCreate(&e0));
-        CUDA_CHECK(cudaEventCreate(&e1));
+        cudaEvent_t e0 = ev[0], e1 = ev[1];
+        double t_join = 0, t_bucket = 0, t_merge = 0, t_sample = 0;
         CUDA_CHECK(cudaEventRecord(e0, s));
         CUDA_CHECK(cudaMemsetAsync(ctr.p, 0, 64, s));
         // ---- phase 1 ----
@@ -567,6 +568,7 @@ void refine_knng(Index& ix, int iters, int sample) {
         k_sample_rev<<<g1, 256, 0, s>>>(n, R, cap, roff.as<uint64_t>(), rbuf.as<uint32_t>(), newl.as<uint32_t>(),
                                          newc.as<uint32_t>(), oldl.as<uint32_t>(), oldc.as<uint32_t>());
         CUDA_LAUNCH_CHECK();
+        CUDA_CHECK(cudaEventRecord(ev[2], s));
         // |new| + |old| summed over nodes (gather bytes of the join)
         unsigned long long sample_entries = 0;
         {
@@ -575,6 +577,7 @@ void refine_knng(Index& ix, int iters, int sample) {
             CUDA_CHECK(cudaMemcpyAsync(b.data(), oldc.p, (size_t)n * 4, cudaMemcpyDeviceToHost, s));
             CUDA_CHECK(cudaStreamSynchronize(s));
             for (uint32_t i = 0; i < n; ++i) sample_entries += (unsigned long long)a[i] + b[i];
+            t_sample = elapsed(e0, ev[2]);
         }
         unsigned long long proposals = 0;
         // ---- phase 2, chunk by chunk ----
@@ -584,6 +587,7 @@ void refine_knng(Index& ix, int iters, int sample) {
             k_thresholds<<<(n + 255) / 256, 256, 0, s>>>(hdr, dist, n, K, thr.as<float>());
             CUDA_LAUNCH_CHECK();
             CUDA_CHECK(cudaMemsetAsync(d_pcount, 0, 8, s));
+            CUDA_CHECK(cudaEventRecord(ev[3], s));
             unsigned grid = std::min<unsigned>(node1 - node0, (unsigned)nsm * 8);
             if (fast) {
                 auto kj = (ix.order.fused & 1) ? k_join<true> : k_join<false>;
@@ -598,9 +602,11 @@ void refine_knng(Index& ix, int iters, int sample) {
                                                     thr.as<float>(), prop.as<Prop>(), d_pcount, pcap, d_njoin);
             }
             CUDA_LAUNCH_CHECK();
+            CUDA_CHECK(cudaEventRecord(ev[4], s));
             unsigned long long np = 0;
             CUDA_CHECK(cudaMemcpyAsync(&np, d_pcount, 8, cudaMemcpyDeviceToHost, s));
             CUDA_CHECK(cudaStreamSynchronize(s));
+            t_join += elapsed(ev[3], ev[4]);
             if (np > pcap) {
                 if (chunk == 1) fail(HRNN_ERR_NOMEM, "refineKNNG: proposal buffer too small for one node");
                 chunk = std::max<uint32_t>(1, chunk / 4);  // redo this chunk smaller (the join is pure)
@@ -618,10 +624,15 @@ void refine_knng(Index& ix, int iters, int sample) {
                 k_bucket_fill<<<gb, 256, 0, s>>>(prop.as<Prop>(), np, toff.as<uint64_t>(), tcur.as<uint32_t>(),
                                                  bucket.as<uint64_t>());
                 CUDA_LAUNCH_CHECK();
+                CUDA_CHECK(cudaEventRecord(ev[6], s));
                 k_merge<<<nsm * 4, kMergeWarps * 32, merge_smem, s>>>(n, K, toff.as<uint64_t>(),
                                                                       bucket.as<uint64_t>(), hdr, ids, dist,
                                                                       isnew.as<uint8_t>(), hcap, d_nupd);
                 CUDA_LAUNCH_CHECK();
+                CUDA_CHECK(cudaEventRecord(ev[5], s));
+                CUDA_CHECK(cudaEventSynchronize(ev[5]));
+                t_bucket += elapsed(ev[4], ev[6]);
+                t_merge += elapsed(ev[6], ev[5]);
             }
             proposals += np;
             node0 = node1;
@@ -632,11 +643,9 @@ void refine_knng(Index& ix, int iters, int sample) {
         CUDA_CHECK(cudaEventRecord(e1, s));
         CUDA_CHECK(cudaMemcpyAsync(hc, ctr.p, 24, cudaMemcpyDeviceToHost, s));
         CUDA_CHECK(cudaStreamSynchronize(s));
-        float ms = 0;
-        cudaEventElapsedTime(&ms, e0, e1);
-        cudaEventDestroy(e0);
-        cudaEventDestroy(e1);
-        std::printf("      iter %d: %llu updates, %llu dists  (%.1f ms)\n", it, hc[2], hc[1], ms);
+        const double ms = elapsed(e0, e1);
+        std::printf("      iter %d: %llu updates, %llu dists  (%.1f ms: sample %.1f, join %.1f, bucket %.1f, "
+                    "merge %.1f)\n", it, hc[2], hc[1], ms, t_sample, t_join, t_bucket, t_merge);
         std::fflush(stdout);
         if (it < HRNN_MAX_ITERS) {
             auto& rs = ix.refine_stats;
@@ -646,8 +655,13 @@ void refine_knng(Index& ix, int iters, int sample) {
             rs.proposals[it] = proposals;
             rs.sample_entries[it] = sample_entries;
             rs.ms[it] = ms;
+            rs.sample_ms[it] = t_sample;
+            rs.join_ms[it] = t_join;
+            rs.bucket_ms[it] = t_bucket;
+            rs.merge_ms[it] = t_merge;
         }
     }
+    for (auto& e : ev) cudaEventDestroy(e);
     ix.knng_built = true;                                 // hrnn.h:1861
 }
 

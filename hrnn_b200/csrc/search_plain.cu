@@ -46,7 +46,7 @@ __global__ void k_budget_features(DevView v, const float* Q, uint32_t nq, const 
                                   const uint32_t* nprox, uint32_t stride, const float* kcol, const float* proj,
                                   float* feat);
 __global__ void k_budget_decide(const float* z, uint32_t nq, float conf, uint32_t m0, uint32_t m1, const uint32_t* qm,
-                                uint32_t* nprox,
+                                int rerun, uint32_t* nprox,
                                 uint32_t* fb_list, uint32_t* fb_count, unsigned long long* levels);
 void ensure_projection(Index& ix, Budget& b);
 __global__ void k_kdist_column(DevView v, uint32_t kidx, float* kcol);
@@ -62,10 +62,12 @@ __global__ void __launch_bounds__(128) k_phase_a(DevView v, const float* __restr
                                                  uint32_t* __restrict__ prox, uint32_t* __restrict__ nprox,
                                                  SearchCounters* __restrict__ ctr,
                                                  const uint32_t* __restrict__ qlist, uint32_t m_over,
-                                                 uint32_t ef_over, float* __restrict__ proxd) {
+                                                 uint32_t ef_over, uint32_t m_keep, float* __restrict__ proxd) {
     // qlist: search only the listed queries (nq = list length); m_over / ef_over:
-    // one (m, ef) for every query instead of the arrays; proxd: also write the
-    // proxies' distances.
+    // one (m, ef) for every query instead of the arrays (the beam is
+    // max(ef, m) as in the reference); m_keep: write at least this many beam
+    // entries (the learned budget's frontier; at most mmax); proxd: also write
+    // the entries' distances.
     extern __shared__ char smem_raw[];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, wpb = blockDim.x >> 5;
     WarpSmem s = carve(smem_raw + (size_t)w * warp_smem_bytes(v.dim, efc, vc), v.dim, efc, vc);
@@ -86,7 +88,7 @@ __global__ void __launch_bounds__(128) k_phase_a(DevView v, const float* __restr
         greedy_descent<DM>(v, s, v.maxlevel, 0, cur, curd, c_dist);
         c_dist++;  // the reference evaluates the entry point again (hrnn.h:505)
         uint32_t tsize = beam_search<DM>(v, s, cur, curd, EF, 0, vc, c_dist, c_exp);
-        uint32_t np_ = min(m, tsize);
+        uint32_t np_ = min(min(max(m, m_keep), mmax), tsize);
         for (uint32_t i = lane; i < np_; i += 32) {
             prox[(size_t)qi * mmax + i] = s.ti[i] & kIdMask;
             if (proxd) proxd[(size_t)qi * mmax + i] = s.td[i];
@@ -356,10 +358,11 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
     }
     if (efmax > (1u << 16)) fail(HRNN_ERR_ARG, "searchRknn: ef_search/m too large (max 65536)");
     const bool learned = ix.budget && ix.budget->enabled && ix.budget->mlp.ready && ix.dim % 4 == 0;
-    if (learned) {  // the frontier pass keeps kFrontier proxies with ef = Budget::ef
-        mmax = std::max<uint32_t>(mmax, kFrontier);
-        efmax = std::max<uint32_t>(efmax, std::max<uint32_t>(ix.budget->ef, kFrontier));
-    }
+    // Learned budget: the frontier keeps kFrontier beam entries; with a level ef
+    // (two-pass mode) the frontier beam is that ef.
+    const bool two_pass = learned && ix.budget->ef > 0;
+    if (learned) mmax = std::max<uint32_t>(mmax, kFrontier);
+    if (two_pass) efmax = std::max<uint32_t>(efmax, ix.budget->ef);
     DevView v = make_view(ix);
     const uint32_t efc = (efmax + 31) & ~31u;
     const uint32_t vc = 2048;  // visited-cache slots (lossy; misses cost a recomputed row)
@@ -401,12 +404,14 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
         if (!learned) {
             kern<<<grid_for(nq), wpb * 32, smem_a, s>>>(v, a.d_q, (uint32_t)nq, a.d_m, a.d_ef, efc, vc, mmax,
                                                         prox.as<uint32_t>(), nprox.as<uint32_t>(), ctr, nullptr, 0, 0,
-                                                        nullptr);
+                                                        0, nullptr);
             CUDA_LAUNCH_CHECK();
         } else {
-            // Learned budget: frontier pass for every query, features, MLP, decision;
-            // the queries the MLP is not confident about are searched again with
-            // the caller's (m, ef).
+            // Learned budget: frontier pass for every query, features, MLP,
+            // decision.  Single-pass mode: the frontier is the caller's own beam,
+            // levels only trim the proxies.  Two-pass mode: the frontier beam is
+            // the level ef, and the queries the MLP is not confident about are
+            // searched again with the caller's (m, ef).
             Budget& b = *ix.budget;
             ensure_projection(ix, b);
             ix.kcol.ensure((size_t)std::max<size_t>(ix.cur, 1) * 4);
@@ -421,7 +426,8 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
             CUDA_CHECK(cudaMemsetAsync(b.decided.p, 0, 64, s));
             kern<<<grid_for(nq), wpb * 32, smem_a, s>>>(v, a.d_q, (uint32_t)nq, a.d_m, a.d_ef, efc, vc, mmax,
                                                         prox.as<uint32_t>(), nprox.as<uint32_t>(), ctr, nullptr,
-                                                        kFrontier, b.ef, b.proxd.as<float>());
+                                                        two_pass ? b.m[1] : 0, two_pass ? b.ef : 0, kFrontier,
+                                                        b.proxd.as<float>());
             CUDA_LAUNCH_CHECK();
             k_budget_features<<<(unsigned)((nq * 32 + 255) / 256), 256, 0, s>>>(
                 v, a.d_q, (uint32_t)nq, prox.as<uint32_t>(), b.proxd.as<float>(), nprox.as<uint32_t>(), mmax,
@@ -429,18 +435,19 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
             CUDA_LAUNCH_CHECK();
             b.mlp.forward(b.feat.as<float>(), (int)nq, s);
             k_budget_decide<<<(unsigned)((nq + 255) / 256), 256, 0, s>>>(
-                b.mlp.z3.as<float>(), (uint32_t)nq, b.confidence, b.m[0], b.m[1], a.d_m, nprox.as<uint32_t>(),
-                b.fallback_list.as<uint32_t>(), fb_count, levels);
+                b.mlp.z3.as<float>(), (uint32_t)nq, b.confidence, b.m[0], b.m[1], a.d_m, two_pass ? 1 : 0,
+                nprox.as<uint32_t>(), b.fallback_list.as<uint32_t>(), fb_count, levels);
             CUDA_LAUNCH_CHECK();
-            uint32_t nfb = 0;
-            CUDA_CHECK(cudaMemcpyAsync(&nfb, fb_count, 4, cudaMemcpyDeviceToHost, s));
-            CUDA_CHECK(cudaMemcpyAsync(b.n_level, levels, 24, cudaMemcpyDeviceToHost, s));
-            CUDA_CHECK(cudaStreamSynchronize(s));
-            if (nfb) {
-                kern<<<grid_for(nfb), wpb * 32, smem_a, s>>>(v, a.d_q, nfb, a.d_m, a.d_ef, efc, vc, mmax,
-                                                             prox.as<uint32_t>(), nprox.as<uint32_t>(), ctr,
-                                                             b.fallback_list.as<uint32_t>(), 0, 0, nullptr);
-                CUDA_LAUNCH_CHECK();
+            if (two_pass) {
+                uint32_t nfb = 0;
+                CUDA_CHECK(cudaMemcpyAsync(&nfb, fb_count, 4, cudaMemcpyDeviceToHost, s));
+                CUDA_CHECK(cudaStreamSynchronize(s));
+                if (nfb) {
+                    kern<<<grid_for(nfb), wpb * 32, smem_a, s>>>(v, a.d_q, nfb, a.d_m, a.d_ef, efc, vc, mmax,
+                                                                 prox.as<uint32_t>(), nprox.as<uint32_t>(), ctr,
+                                                                 b.fallback_list.as<uint32_t>(), 0, 0, 0, nullptr);
+                    CUDA_LAUNCH_CHECK();
+                }
             }
         }
     }
@@ -538,6 +545,8 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
     CUDA_CHECK(cudaStreamSynchronize(s));
     SearchCounters hc{};
     CUDA_CHECK(cudaMemcpy(&hc, ix.counters.p, sizeof(hc), cudaMemcpyDeviceToHost));
+    if (learned)
+        CUDA_CHECK(cudaMemcpy(ix.budget->n_level, ix.budget->decided.as<char>() + 8, 24, cudaMemcpyDeviceToHost));
     hrnn_search_stats st{};
     st.n_queries = nq;
     st.n_dist = hc.n_dist;
@@ -577,13 +586,19 @@ Budget& budget_of(Index& ix) {
     return *ix.budget;
 }
 
-// Features of nq queries (device buffers): the frontier pass (m = kFrontier,
-// ef = Budget::ef) and k_budget_features, in the index's precision mode.
-void budget_features(Index& ix, const float* d_q, size_t nq, uint32_t k, float* d_feat) {
+// Features of nq queries (device buffers) as the learned search computes them:
+// the frontier pass of a search with (m, ef) -- (m1, level ef) in two-pass mode --
+// and k_budget_features, in the index's precision mode.
+void budget_features(Index& ix, const float* d_q, size_t nq, uint32_t k, uint32_t m, uint32_t ef, float* d_feat) {
     if (!ix.rknng_built) fail(HRNN_ERR_STATE, "searchRknn: RKNNG not built");
     if (ix.dim % 4 != 0) fail(HRNN_ERR_ARG, "budget: dim must be a multiple of 4");
     if (nq == 0) return;
     Budget& b = budget_of(ix);
+    if (b.ef > 0) {
+        m = b.m[1];
+        ef = b.ef;
+    }
+    if (m == 0 || std::max(m, ef) > (1u << 16)) fail(HRNN_ERR_ARG, "budget_features: need 1 <= m, ef <= 65536");
     cudaStream_t s = ix.stream;
     ix.sync_upper_to_device();
     const bool mixed = ix.precision == HRNN_PREC_BF16 && (ix.dim == 96 || ix.dim == 128 || ix.dim == 256) &&
@@ -591,7 +606,7 @@ void budget_features(Index& ix, const float* d_q, size_t nq, uint32_t k, float* 
     if (mixed) ensure_bf16(ix);
     DevView v = make_view(ix);
     ensure_projection(ix, b);
-    const uint32_t mmax = kFrontier, efc = (std::max<uint32_t>(b.ef, kFrontier) + 31) & ~31u, vc = 2048;
+    const uint32_t mmax = std::max<uint32_t>(m, kFrontier), efc = (std::max(m, ef) + 31) & ~31u, vc = 2048;
     const size_t wsm = warp_smem_bytes(v.dim, efc, vc);
     const int wpb = (int)std::max<size_t>(1, std::min<size_t>(4, (200 * 1024) / wsm));
     const size_t smem_a = wsm * wpb;
@@ -608,8 +623,8 @@ void budget_features(Index& ix, const float* d_q, size_t nq, uint32_t k, float* 
     const int nsm = sms(ix.device);
     unsigned grid = (unsigned)std::max<size_t>(1, std::min<size_t>((nq + wpb - 1) / wpb, (size_t)nsm * 16));
     kern<<<grid, wpb * 32, smem_a, s>>>(v, d_q, (uint32_t)nq, nullptr, nullptr, efc, vc, mmax, prox.as<uint32_t>(),
-                                        nprox.as<uint32_t>(), ix.counters.as<SearchCounters>(), nullptr, kFrontier,
-                                        b.ef, proxd.as<float>());
+                                        nprox.as<uint32_t>(), ix.counters.as<SearchCounters>(), nullptr, m, ef,
+                                        kFrontier, proxd.as<float>());
     CUDA_LAUNCH_CHECK();
     k_budget_features<<<(unsigned)((nq * 32 + 255) / 256), 256, 0, s>>>(v, d_q, (uint32_t)nq, prox.as<uint32_t>(),
                                                                        proxd.as<float>(), nprox.as<uint32_t>(), mmax,

@@ -86,6 +86,10 @@ typedef struct {
     uint64_t proposals[HRNN_MAX_ITERS];      /* proposals that passed the bound      */
     uint64_t sample_entries[HRNN_MAX_ITERS]; /* sum over nodes of |new| + |old|      */
     double ms[HRNN_MAX_ITERS];               /* device time of the iteration         */
+    double sample_ms[HRNN_MAX_ITERS];        /* ... of which sampling (phase 1)      */
+    double join_ms[HRNN_MAX_ITERS];          /* ... local joins                      */
+    double bucket_ms[HRNN_MAX_ITERS];        /* ... grouping proposals by target     */
+    double merge_ms[HRNN_MAX_ITERS];         /* ... list merges                      */
 } hrnn_refine_stats;
 
 /* Thread-local message of the last failing call on this thread ("" if none). */
@@ -186,26 +190,38 @@ hrnn_status hrnn_get_refine_stats(hrnn_index* h, hrnn_refine_stats* st);
 hrnn_status hrnn_set_precision(hrnn_index* h, int precision);
 
 /* Learned search budget (new; no counterpart in the reference).  A 256-256-256-2
- * MLP with GELU and BF16 weights reads a query and its first beam frontier (a
- * search with ef = `ef` keeping 32 entries) and outputs two logits: "the answer
- * with m = m0 proxies from this frontier is complete" and "... with m = m1".  The
- * batch search then uses the cheapest level whose probability reaches
- * `confidence`, and the caller's (m, ef_search) otherwise.  Verification still
- * decides every returned point: the budget changes work, never membership.
+ * MLP with GELU and BF16 weights reads a query and its beam frontier (the 32
+ * nearest beam entries) and outputs two logits: "the answer with m = m0 proxies
+ * is complete" and "... with m = m1".  The batch search then uses the cheapest
+ * level whose probability reaches `confidence`, and the caller's m otherwise.
+ * Verification still decides every returned point: the budget changes work,
+ * never membership.
+ *   ef = 0 (single pass): the frontier is the caller's own beam (ef_search), so a
+ *     level's answer equals the plain search with (m_l, ef_search).
+ *   ef > 0 (two pass): the frontier beam is ef; a level's answer equals the plain
+ *     search with (m_l, ef); the other queries are searched again with the
+ *     caller's (m, ef_search).
  *   hrnn_set_budget: stores (m0, m1, ef, confidence) with 1 <= m0 <= m1 <= 32,
- *     m1 <= ef, 0.5 < confidence <= 1, also when disabling; enabling needs weights.
+ *     ef = 0 or m1 <= ef, 0.5 < confidence <= 1, also when disabling; enabling
+ *     needs weights.
  *   hrnn_budget_features: the 256 features of nq host queries (host out, nq x 256)
- *     for result size k, with the stored ef.
+ *     for result size k, from the frontier of a search with (m, ef_search) --
+ *     (m1, ef) in two-pass mode.
  *   hrnn_budget_train: trains on the device with the library's BF16 kernels
- *     (labels: nq x 2 bytes, 1 = complete at that level); returns the last loss.
- *   hrnn_budget_predict / hrnn_budget_gradients: forward logits / parameter
- *     gradients of the mean binary cross-entropy (W1 b1 W2 b2 W3 b3, FP32).
- *   hrnn_budget_get_weights / _set_weights: the same parameter layout
- *     (HRNN_BUDGET_PARAMS floats). */
-#define HRNN_BUDGET_PARAMS (256 * 256 + 256 + 256 * 256 + 256 + 2 * 256 + 2)
+ *     (labels: nq x 2 bytes, 1 = complete at that level); returns the last
+ *     epoch's mean loss.  A model without weights is first initialised from
+ *     `seed`, with the training features' per-feature mean and 1/std as its
+ *     input normalisation (x -> (x - mean) * inv, applied before layer 1).
+ *   hrnn_budget_predict / hrnn_budget_gradients: forward logits / gradients of
+ *     the mean binary cross-entropy (summed over both outputs) with respect to
+ *     W1 b1 W2 b2 W3 b3, FP32 (the normalisation entries are left untouched).
+ *   hrnn_budget_get_weights / _set_weights: W1 [256x256] b1 W2 [256x256] b2
+ *     W3 [2x256] b3, then mean[256] and inv[256] (HRNN_BUDGET_PARAMS floats). */
+#define HRNN_BUDGET_PARAMS (256 * 256 + 256 + 256 * 256 + 256 + 2 * 256 + 2 + 2 * 256)
 hrnn_status hrnn_set_budget(hrnn_index* h, int enable, uint32_t m0, uint32_t m1, uint32_t ef,
                             float confidence);
-hrnn_status hrnn_budget_features(hrnn_index* h, const float* queries, size_t nq, uint32_t k, float* feat);
+hrnn_status hrnn_budget_features(hrnn_index* h, const float* queries, size_t nq, uint32_t k, uint32_t m,
+                                 uint32_t ef_search, float* feat);
 hrnn_status hrnn_budget_train(hrnn_index* h, const float* feat, const uint8_t* labels, size_t n,
                               int epochs, int batch, float lr, uint64_t seed, float* final_loss);
 hrnn_status hrnn_budget_predict(hrnn_index* h, const float* feat, size_t n, float* logits);

@@ -4,11 +4,12 @@ The budget model has no counterpart in the reference (it is an addition of this
 library), so this oracle is pinned by central finite differences of its own FP64
 loss (tests/test_oracle_pin.py) rather than by reference outputs.
 
-Model: 256 -> 256 -> 256 -> 2 with exact GELU (x * Phi(x)), parameters
-W1 b1 W2 b2 W3 b3 (W row-major [out, in]).  Loss: binary cross-entropy with
-logits on both outputs, summed over the outputs and averaged over the batch.
+Model: input normalisation x -> (x - mean) * inv (FP32, as the device computes
+it), then 256 -> 256 -> 256 -> 2 with exact GELU (x * Phi(x)); parameters
+W1 b1 W2 b2 W3 b3 mean inv (W row-major [out, in]).  Loss: binary cross-entropy
+with logits on both outputs, summed over the outputs and averaged over the batch.
 
-With ``bf16=True`` every GEMM operand is first rounded to float32 and then to
+With ``bf16_ops=True`` every GEMM operand is first rounded to float32 and then to
 bfloat16 (round to nearest even), the way the device kernels stage their tiles;
 biases and the elementwise steps stay unrounded.  Products and sums are FP64
 here, FP32 on the device.
@@ -18,7 +19,7 @@ from __future__ import annotations
 import numpy as np
 from scipy.special import erf
 
-SHAPES = [(256, 256), (256,), (256, 256), (256,), (2, 256), (2,)]
+SHAPES = [(256, 256), (256,), (256, 256), (256,), (2, 256), (2,), (256,), (256,)]
 
 
 def bf16(x) -> np.ndarray:
@@ -37,15 +38,23 @@ def gelu_d(x):
 
 
 def init_params(seed: int = 0):
+    """Random weights and biases, and a non-trivial normalisation (test values)."""
     g = np.random.default_rng(seed)
     out = []
-    for s in SHAPES:
-        fan_in = s[-1] if len(s) == 2 else 256
+    for s in SHAPES[:6]:
         if len(s) == 2:
-            out.append(g.uniform(-1, 1, s) / np.sqrt(fan_in))
+            out.append(g.uniform(-1, 1, s) / np.sqrt(s[1]))
         else:
             out.append(g.uniform(-0.1, 0.1, s))
+    out.append(g.normal(0, 0.5, 256))
+    out.append(g.uniform(0.5, 2.0, 256))
     return [np.asarray(p, np.float32) for p in out]
+
+
+def normalize(X, mean, inv) -> np.ndarray:
+    """(x - mean) * inv in IEEE FP32, one rounding per operation."""
+    X = np.asarray(X, np.float32)
+    return ((X - np.asarray(mean, np.float32)) * np.asarray(inv, np.float32)).astype(np.float32)
 
 
 def _r(x, on):
@@ -53,8 +62,8 @@ def _r(x, on):
 
 
 def forward(params, X, bf16_ops: bool = True):
-    W1, b1, W2, b2, W3, b3 = [np.asarray(p, np.float64) for p in params]
-    X = np.asarray(X, np.float64)
+    W1, b1, W2, b2, W3, b3 = [np.asarray(p, np.float64) for p in params[:6]]
+    X = normalize(X, params[6], params[7]).astype(np.float64)
     z1 = _r(X, bf16_ops) @ _r(W1, bf16_ops).T + b1
     a1 = gelu(z1)
     z2 = _r(a1, bf16_ops) @ _r(W2, bf16_ops).T + b2
@@ -71,9 +80,9 @@ def loss_of(z3, Y):
 
 def loss_and_grads(params, X, Y, bf16_ops: bool = True):
     """Mean BCE and its gradients (list in SHAPES order), mirroring the device backward."""
-    W1, b1, W2, b2, W3, b3 = [np.asarray(p, np.float64) for p in params]
-    X = np.asarray(X, np.float64)
+    W1, b1, W2, b2, W3, b3 = [np.asarray(p, np.float64) for p in params[:6]]
     z1, a1, z2, a2, z3 = forward(params, X, bf16_ops)
+    X = normalize(X, params[6], params[7]).astype(np.float64)
     B = X.shape[0]
     t = np.asarray(Y, np.float64)
     g3 = (1.0 / (1.0 + np.exp(-z3)) - t) / B

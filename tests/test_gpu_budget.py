@@ -32,8 +32,13 @@ def test_budget_forward_matches_oracle():
     X = np.random.default_rng(1).standard_normal((300, 256)).astype(np.float32)
     z = h.budget_predict(X)
     ref = mlp.forward(params, X, bf16_ops=True)[4]
-    # BF16 operands as on the device, FP32 accumulation vs FP64: |dz| <= 1e-4 * scale
-    assert np.max(np.abs(z - ref)) <= 1e-4 * max(1.0, np.max(np.abs(ref)))
+    # BF16 operands as on the device, FP32 accumulation vs FP64.  An activation
+    # within FP32 rounding of a BF16 rounding boundary can round the other way:
+    # one BF16 ulp of one operand moves a logit by ~2^-8 |a| |w| < 2e-3.
+    err = np.abs(z - ref)
+    assert np.median(err) <= 1e-6
+    assert np.mean(err > 1e-5) < 0.02
+    assert np.max(err) <= 2e-3
 
 
 @pytest.mark.parametrize("B", [1, 64, 333])
@@ -87,27 +92,30 @@ def _sets(res):
     return [frozenset(int(x) for x in r) for r in res]
 
 
-def test_learned_search_answers_equal_plain_searches(golden_idx):
+@pytest.mark.parametrize("efl", [0, 40])
+def test_learned_search_answers_equal_plain_searches(golden_idx, efl):
     """Every query's answer equals the plain search at the level the MLP chose
-    (m_l proxies, beam ef_l) or at the caller's budget for fallback queries."""
+    (m_l proxies from the caller's beam, or from a beam of efl in two-pass mode)
+    or at the caller's budget for the other queries."""
     h = H.HRNN.load(golden_idx, 32)
     m, kp, ef, k = 24, 24, 96, 10
-    m0, m1, efl, conf = 1, 3, 40, 0.8
+    m0, m1, conf = 1, 3, 0.8
+    ef_l = efl or ef
     Qtr = data.mixture(3000, 32, 12, 1.0, 11, 5)
     full = _sets(h.search_rknn_batch(Qtr, m, kp, ef, 1.0, k))
     lab = []
     for ml in (m0, m1):
-        got = _sets(h.search_rknn_batch(Qtr, ml, kp, efl, 1.0, k))
+        got = _sets(h.search_rknn_batch(Qtr, ml, kp, ef_l, 1.0, k))
         lab.append([f <= g for f, g in zip(full, got)])
     Y = np.array(lab, np.uint8).T
     h.budget_set_weights(mlp.init_params(1))
     h.set_budget(True, m0, m1, efl, conf)
-    feat = h.budget_features(Qtr, k)
+    feat = h.budget_features(Qtr, k, m, ef)
     assert feat.shape == (3000, 256) and np.all(np.isfinite(feat))
     h.budget_train(feat, Y, epochs=30, batch=256, lr=2e-3, seed=1)
 
     Q = data.mixture(700, 32, 12, 1.0, 11, 77)
-    z = h.budget_predict(h.budget_features(Q, k))
+    z = h.budget_predict(h.budget_features(Q, k, m, ef))
     p = 1.0 / (1.0 + np.exp(-z.astype(np.float64)))
     lvl = np.where(p[:, 0] >= conf, 0, np.where(p[:, 1] >= conf, 1, 2))
     got = h.search_rknn_batch(Q, m, kp, ef, 1.0, k)
@@ -118,21 +126,22 @@ def test_learned_search_answers_equal_plain_searches(golden_idx):
         assert st["n_budget"] == [int(np.sum(lvl == i)) for i in range(3)]
     h.set_budget(False)
     plain = {
-        0: h.search_rknn_batch(Q, m0, kp, efl, 1.0, k),
-        1: h.search_rknn_batch(Q, m1, kp, efl, 1.0, k),
+        0: h.search_rknn_batch(Q, m0, kp, ef_l, 1.0, k),
+        1: h.search_rknn_batch(Q, m1, kp, ef_l, 1.0, k),
         2: h.search_rknn_batch(Q, m, kp, ef, 1.0, k),
     }
     bad = [q for q in range(len(Q)) if not border[q] and not np.array_equal(got[q], plain[lvl[q]][q])]
     assert not bad, bad[:5]
 
 
+@pytest.mark.parametrize("efl", [0, 48])
 @pytest.mark.parametrize("level", [0, 1, 2])
-def test_learned_search_forced_levels(golden_idx, level):
+def test_learned_search_forced_levels(golden_idx, level, efl):
     """Weights that pin every query to one level: the answers equal that level's
     plain search, and switching the budget off restores the caller's search."""
     h = H.HRNN.load(golden_idx, 32)
     m, kp, ef, k = 20, 24, 80, 9
-    m0, m1, efl = 2, 5, 48
+    m0, m1 = 2, 5
     params = [np.zeros(s, np.float32) for s in H.BUDGET_SHAPES]
     params[5][:] = {0: (20, 20), 1: (-20, 20), 2: (-20, -20)}[level]
     h.budget_set_weights(params)
@@ -144,6 +153,7 @@ def test_learned_search_forced_levels(golden_idx, level):
     exp_counts[level] = len(Q)
     assert st["n_budget"] == exp_counts
     h.set_budget(False)
-    exp = h.search_rknn_batch(Q, (m0, m1, m)[level], kp, (efl, efl, ef)[level], 1.0, k)
+    ef_l = efl or ef
+    exp = h.search_rknn_batch(Q, (m0, m1, m)[level], kp, (ef_l, ef_l, ef)[level], 1.0, k)
     assert all(np.array_equal(a, b) for a, b in zip(got, exp))
     assert h.last_search_stats()["n_budget"] == [0, 0, 0]

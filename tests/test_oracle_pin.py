@@ -92,7 +92,7 @@ def test_budget_mlp_oracle_finite_differences():
     from oracle import mlp
     rng = np.random.default_rng(7)
     params = [p.astype(np.float64) for p in mlp.init_params(3)]
-    X = rng.standard_normal((6, 256))
+    X = rng.standard_normal((6, 256)).astype(np.float32)
     Y = rng.integers(0, 2, (6, 2)).astype(np.uint8)
     _, grads = mlp.loss_and_grads(params, X, Y, bf16_ops=False)
     h = 1e-6
