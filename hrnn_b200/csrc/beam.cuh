@@ -180,10 +180,12 @@ __device__ __forceinline__ void warp_l2_list(const DevView& v, const float* q, c
         warp_l2_pairs<FUSED, 6>(v, q, ids, cnt, dout);
     } else if (v.lanes == 16 && v.nb == 16 && v.dim == 256) {
         warp_l2_pairs<FUSED, 16>(v, q, ids, cnt, dout);
-    } else if ((uint32_t)lane < cnt) {
-        const float* x = v.vec + (size_t)ids[lane] * v.dim;
-        dout[lane] = (v.lanes == 16 && v.dim % 16 == 0) ? l2_row16<FUSED>(q, x, v.nb)
+    } else {
+        for (uint32_t t = lane; t < cnt; t += 32) {
+            const float* x = v.vec + (size_t)ids[t] * v.dim;
+            dout[t] = (v.lanes == 16 && v.dim % 16 == 0) ? l2_row16<FUSED>(q, x, v.nb)
                                                          : l2_thread(q, x, v.dim, v.lanes, v.fused);
+        }
     }
     __syncwarp();
 }
@@ -324,7 +326,8 @@ __device__ __forceinline__ void warp_dist_list(const DevView& v, const float* q,
         if (v.dim == 128) warp_bf16_pairs<8>(v, q, ids, cnt, dout);
         else if (v.dim == 96) warp_bf16_pairs<6>(v, q, ids, cnt, dout);
         else if (v.dim == 256) warp_bf16_pairs<16>(v, q, ids, cnt, dout);
-        else if ((uint32_t)lane < cnt) dout[lane] = bf16_thread(q, v.vec_bf16 + (size_t)ids[lane] * v.dim, v.dim);
+        else
+            for (uint32_t t = lane; t < cnt; t += 32) dout[t] = bf16_thread(q, v.vec_bf16 + (size_t)ids[t] * v.dim, v.dim);
         __syncwarp();
     }
 }
@@ -374,6 +377,84 @@ __device__ void greedy_descent(const DevView& v, WarpSmem& s, int top, int stop,
             curd = bestd;
         }
     }
+}
+
+// Inserts cnt (<= 32) scored neighbours (nd[i], ni[i]) into the beam: neighbour j
+// is accepted iff fewer than EF elements of (beam + accepted earlier neighbours of
+// this batch) are <= d_j, and not already in the beam; the beam stays sorted and
+// is cut to EF; cursor moves back to the first inserted position.
+__device__ __forceinline__ void beam_insert(WarpSmem& s, const float* nd, const uint32_t* ni, uint32_t cnt,
+                                            uint32_t EF, uint32_t& tsize, uint32_t& cursor) {
+    const int lane = threadIdx.x & 31;
+    float d = FLT_MAX;
+    uint32_t id = kInvalid, pos = 0;
+    bool ok = false;
+    if ((uint32_t)lane < cnt) {
+        d = nd[lane];
+        id = ni[lane];
+        pos = upper_bound(s.td, tsize, d);
+        ok = true;
+        for (int k = (int)pos - 1; k >= 0 && s.td[k] == d; --k)
+            if ((s.ti[k] & kIdMask) == id) {
+                ok = false;
+                break;
+            }
+    }
+    uint32_t okb = __ballot_sync(0xFFFFFFFFu, ok);
+    uint32_t cp = 0;
+    for (uint32_t i = 0; i < cnt; ++i) {
+        float di = __shfl_sync(0xFFFFFFFFu, d, i);
+        if (((okb >> i) & 1u) && i < (uint32_t)lane && di <= d) cp++;
+    }
+    bool acc = ok && (pos + cp < EF);
+    uint32_t ab = __ballot_sync(0xFFFFFFFFu, acc);
+    if (!ab) return;
+    uint32_t na = __popc(ab);
+    uint32_t before = 0;
+    for (uint32_t i = 0; i < cnt; ++i) {
+        float di = __shfl_sync(0xFFFFFFFFu, d, i);
+        if (((ab >> i) & 1u) && (di < d || (di == d && i < (uint32_t)lane))) before++;
+    }
+    uint32_t lo = acc ? pos : 0xFFFFFFFFu;
+    for (int o = 16; o; o >>= 1) lo = min(lo, __shfl_xor_sync(0xFFFFFFFFu, lo, o));
+    if (acc) s.apos[__popc(ab & lanemask_lt())] = pos;
+    __syncwarp();
+    const uint32_t newsize = min(tsize + na, EF);
+    // In-place merge: existing entries at or after lo move right by the number
+    // of accepted neighbours inserted at or before them (at most 32), so the
+    // beam is shifted block by block from the right; every block is read
+    // before any lane writes, and its targets lie in itself or in blocks to
+    // its right that were already moved.
+    if (tsize > lo) {
+        for (int b = (int)lo + (int)(((tsize - lo - 1) / 32) * 32); b >= (int)lo; b -= 32) {
+            const uint32_t k = (uint32_t)b + lane;
+            float dk = 0.f;
+            uint32_t ik = 0, np = 0xFFFFFFFFu;
+            if (k < tsize) {
+                dk = s.td[k];
+                ik = s.ti[k];
+                uint32_t sh = 0;
+                for (uint32_t a = 0; a < na; ++a) sh += (s.apos[a] <= k);
+                np = k + sh;
+            }
+            __syncwarp();
+            if (np < newsize) {
+                s.td[np] = dk;
+                s.ti[np] = ik;
+            }
+            __syncwarp();
+        }
+    }
+    uint32_t npos = pos + before;
+    if (acc && npos < newsize) {
+        s.td[npos] = d;
+        s.ti[npos] = id;
+    }
+    uint32_t mnp = (acc && npos < newsize) ? npos : 0xFFFFFFFFu;
+    for (int o = 16; o; o >>= 1) mnp = min(mnp, __shfl_xor_sync(0xFFFFFFFFu, mnp, o));
+    tsize = newsize;
+    cursor = min(cursor, mnp);
+    __syncwarp();
 }
 
 // Best-first search of one layer from (ep, epd) with beam size EF (<= efc).
@@ -441,75 +522,7 @@ __device__ uint32_t beam_search(const DevView& v, WarpSmem& s, uint32_t ep, floa
             if (cnt == 0) continue;
             warp_dist_list<DM>(v, s.q, s.ni, cnt, s.nd);
             c_dist += cnt;
-            float d = FLT_MAX;
-            uint32_t id = kInvalid, pos = 0;
-            bool ok = false;
-            if ((uint32_t)lane < cnt) {
-                d = s.nd[lane];
-                id = s.ni[lane];
-                pos = upper_bound(s.td, tsize, d);
-                ok = true;
-                for (int k = (int)pos - 1; k >= 0 && s.td[k] == d; --k)
-                    if ((s.ti[k] & kIdMask) == id) {
-                        ok = false;
-                        break;
-                    }
-            }
-            uint32_t okb = __ballot_sync(0xFFFFFFFFu, ok);
-            uint32_t cp = 0;
-            for (uint32_t i = 0; i < cnt; ++i) {
-                float di = __shfl_sync(0xFFFFFFFFu, d, i);
-                if (((okb >> i) & 1u) && i < (uint32_t)lane && di <= d) cp++;
-            }
-            bool acc = ok && (pos + cp < EF);
-            uint32_t ab = __ballot_sync(0xFFFFFFFFu, acc);
-            if (!ab) continue;
-            uint32_t na = __popc(ab);
-            uint32_t before = 0;
-            for (uint32_t i = 0; i < cnt; ++i) {
-                float di = __shfl_sync(0xFFFFFFFFu, d, i);
-                if (((ab >> i) & 1u) && (di < d || (di == d && i < (uint32_t)lane))) before++;
-            }
-            uint32_t lo = acc ? pos : 0xFFFFFFFFu;
-            for (int o = 16; o; o >>= 1) lo = min(lo, __shfl_xor_sync(0xFFFFFFFFu, lo, o));
-            if (acc) s.apos[__popc(ab & lanemask_lt())] = pos;
-            __syncwarp();
-            const uint32_t newsize = min(tsize + na, EF);
-            // In-place merge: existing entries at or after lo move right by the number
-            // of accepted neighbours inserted at or before them (at most 32), so the
-            // beam is shifted block by block from the right; every block is read
-            // before any lane writes, and its targets lie in itself or in blocks to
-            // its right that were already moved.
-            if (tsize > lo) {
-                for (int b = (int)lo + (int)(((tsize - lo - 1) / 32) * 32); b >= (int)lo; b -= 32) {
-                    const uint32_t k = (uint32_t)b + lane;
-                    float dk = 0.f;
-                    uint32_t ik = 0, np = 0xFFFFFFFFu;
-                    if (k < tsize) {
-                        dk = s.td[k];
-                        ik = s.ti[k];
-                        uint32_t sh = 0;
-                        for (uint32_t a = 0; a < na; ++a) sh += (s.apos[a] <= k);
-                        np = k + sh;
-                    }
-                    __syncwarp();
-                    if (np < newsize) {
-                        s.td[np] = dk;
-                        s.ti[np] = ik;
-                    }
-                    __syncwarp();
-                }
-            }
-            uint32_t npos = pos + before;
-            if (acc && npos < newsize) {
-                s.td[npos] = d;
-                s.ti[npos] = id;
-            }
-            uint32_t mnp = (acc && npos < newsize) ? npos : 0xFFFFFFFFu;
-            for (int o = 16; o; o >>= 1) mnp = min(mnp, __shfl_xor_sync(0xFFFFFFFFu, mnp, o));
-            tsize = newsize;
-            cursor = min(cursor, mnp);
-            __syncwarp();
+            beam_insert(s, s.nd, s.ni, cnt, EF, tsize, cursor);
         }
     }
     return tsize;

@@ -17,15 +17,16 @@
 //            new x old pair of a node in exact FP32 (the reference's order) and
 //            emits (target, source, d) proposals that can still enter the target's
 //            list (d below its current farthest when the list is full);
-//            k_bucket_* group them by target; k_merge sorts each target's
-//            proposals (bitonic, shared memory), drops duplicates and ids already
-//            listed, and merges them into the sorted list keeping K, marking the
-//            inserted entries new.  Chunking changes nothing in the result (the
-//            outcome is order-independent) but bounds the proposal buffer: lists
+//            k_bucket_* group them by target; k_merge_cta (one CTA per target)
+//            drops duplicates and ids already listed, selects the K-th distance
+//            of list U proposals by radix selection, sorts only the proposals at
+//            or below it and merges them into the sorted list keeping K, marking
+//            the inserted entries new.  Chunks bound the proposal buffer; lists
 //            fill during the first chunk, after which the threshold filters.
 //
 // Equal distances between different ids are the one place where the bulk merge and
-// the sequential insertion can order entries differently.
+// the sequential insertion can order entries differently (and where the chunk
+// boundaries can change which of two equal-distance proposals is kept).
 #include <algorithm>
 #include <cfloat>
 #include <cstdio>
@@ -58,9 +59,11 @@ __global__ void k_init_flags(const uint32_t* __restrict__ hdr, uint32_t n, uint3
 }
 
 // Counts reverse-sample candidates per (target, type) segment: seg = 2*nbr + (old?1:0).
+// thr[nbr]: the farthest entry of nbr's list, FLT_MAX when not full (so an empty
+// list never passes `d > thr`).
 __global__ void k_sample_count(const uint32_t* __restrict__ ids, const float* __restrict__ dist,
                                const uint32_t* __restrict__ hdr, const uint8_t* __restrict__ isnew, uint32_t n,
-                               uint32_t K, uint32_t* __restrict__ rcount) {
+                               uint32_t K, const float* __restrict__ thr, uint32_t* __restrict__ rcount) {
     size_t warp = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     int lane = threadIdx.x & 31;
     size_t nw = ((size_t)gridDim.x * blockDim.x) >> 5;
@@ -68,9 +71,7 @@ __global__ void k_sample_count(const uint32_t* __restrict__ ids, const float* __
         uint32_t c = hdr[i] & 0xFFFFu;
         for (uint32_t j = lane; j < c; j += 32) {
             uint32_t nbr = ids[i * K + j];
-            if ((hdr[nbr] & 0xFFFFu) == 0) continue;
-            if (dist[i * K + j] > worst_of(hdr, dist, K, nbr))
-                atomicAdd(&rcount[2 * (size_t)nbr + (isnew[i * K + j] ? 0 : 1)], 1u);
+            if (dist[i * K + j] > thr[nbr]) atomicAdd(&rcount[2 * (size_t)nbr + (isnew[i * K + j] ? 0 : 1)], 1u);
         }
     }
 }
@@ -79,7 +80,7 @@ __global__ void k_sample_count(const uint32_t* __restrict__ ids, const float* __
 // and clearing of the new flags.
 __global__ void k_sample_fill(const uint32_t* __restrict__ ids, const float* __restrict__ dist,
                               const uint32_t* __restrict__ hdr, uint8_t* __restrict__ isnew, uint32_t n, uint32_t K,
-                              uint32_t S, uint32_t cap, uint32_t* __restrict__ newl, uint32_t* __restrict__ newc,
+                              const float* __restrict__ thr, uint32_t S, uint32_t cap, uint32_t* __restrict__ newl, uint32_t* __restrict__ newc,
                               uint32_t* __restrict__ oldl, uint32_t* __restrict__ oldc,
                               const uint64_t* __restrict__ roff, uint32_t* __restrict__ rcur,
                               uint32_t* __restrict__ rbuf) {
@@ -106,7 +107,7 @@ __global__ void k_sample_fill(const uint32_t* __restrict__ ids, const float* __r
             }
             nn += __popc(bn);
             no += __popc(bo);
-            if (valid && (hdr[nbr] & 0xFFFFu) != 0 && dist[i * K + j] > worst_of(hdr, dist, K, nbr)) {
+            if (valid && dist[i * K + j] > thr[nbr]) {
                 size_t seg = 2 * (size_t)nbr + (isn ? 0 : 1);
                 rbuf[roff[seg] + atomicAdd(&rcur[seg], 1u)] = (uint32_t)i;
             }
@@ -120,9 +121,12 @@ __global__ void k_sample_fill(const uint32_t* __restrict__ ids, const float* __r
 
 // Appends the R smallest owners of each reverse segment, ascending, after the
 // forward samples (nn_old then stays within 2R = S + R, hrnn.h:1816-1817).
+// Also sums |new| + |old| over the nodes into *entries.
 __global__ void k_sample_rev(uint32_t n, uint32_t R, uint32_t cap, const uint64_t* __restrict__ roff,
                              const uint32_t* __restrict__ rbuf, uint32_t* __restrict__ newl,
-                             uint32_t* __restrict__ newc, uint32_t* __restrict__ oldl, uint32_t* __restrict__ oldc) {
+                             uint32_t* __restrict__ newc, uint32_t* __restrict__ oldl, uint32_t* __restrict__ oldc,
+                             unsigned long long* __restrict__ entries) {
+    unsigned long long my_entries = 0;
     size_t warp = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     int lane = threadIdx.x & 31;
     size_t nw = ((size_t)gridDim.x * blockDim.x) >> 5;
@@ -150,8 +154,10 @@ __global__ void k_sample_rev(uint32_t n, uint32_t R, uint32_t cap, const uint64_
             }
             __syncwarp();
             if (lane == 0) C[i] = base + take;
+            my_entries += base + take;
         }
     }
+    if (lane == 0 && my_entries) atomicAdd(entries, my_entries);
 }
 
 // ---- phase 2: join -----------------------------------------------------------
@@ -161,20 +167,50 @@ struct Prop {
     float d;
 };
 
-// One block per node of the chunk: exact FP32 distances of all sample pairs,
-// staged in shared memory (rows padded by one float against bank conflicts).
+// The proposal buffer is split into kShards segments with a counter each (block b
+// appends to segment b mod kShards), so no single counter takes every append.
+constexpr uint32_t kShards = 32;
+
+// Exclusive prefix of the segments' fill counts: flat proposal j lives in segment
+// s with pre[s] <= j < pre[s + 1], at prop[s * segcap + j - pre[s]].
+struct ShardMap {
+    unsigned long long pre[kShards + 1];
+    unsigned long long segcap;
+};
+
+__device__ __forceinline__ size_t shard_slot(const ShardMap& m, unsigned long long j) {
+    uint32_t lo = 0, hi = kShards;  // last segment with pre <= j
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (m.pre[mid] <= j) lo = mid;
+        else hi = mid;
+    }
+    return (size_t)lo * m.segcap + (size_t)(j - m.pre[lo]);
+}
+
+// One block per node of the chunk: exact FP32 distances of all sample pairs.
+// The node's rows are staged in shared memory (stride dim + 4 floats: 16-byte
+// aligned and free of bank conflicts for float4 reads).  A warp takes a tile of
+// 4 rows i x 32 columns j (lane = column): the 4 row vectors are read by every
+// lane at the same address (broadcast) and the lane's column vector once for all
+// 4 pairs.  Each pair keeps the reference's 16 accumulators (element e into
+// accumulator e mod 16, then summed left to right), so the tiling leaves every
+// distance bit-identical.  Proposals are appended with one atomic per warp tile.
 template <bool FUSED>
 __global__ void __launch_bounds__(256) k_join(const float* __restrict__ vec, uint32_t dim, uint32_t node0,
                                               uint32_t node1, uint32_t cap, const uint32_t* __restrict__ newl,
                                               const uint32_t* __restrict__ newc, const uint32_t* __restrict__ oldl,
                                               const uint32_t* __restrict__ oldc, const float* __restrict__ thr,
                                               Prop* __restrict__ prop, unsigned long long* __restrict__ pcount,
-                                              unsigned long long pcap, unsigned long long* __restrict__ njoin) {
-    extern __shared__ float sm[];
-    const uint32_t stride = dim + 1;
-    uint32_t* sid = (uint32_t*)(sm + (size_t)2 * cap * stride);
+                                              unsigned long long segcap, unsigned long long* __restrict__ njoin) {
+    extern __shared__ __align__(16) float sm[];
+    unsigned long long* const pc = pcount + blockIdx.x % kShards;
+    Prop* const seg = prop + (size_t)(blockIdx.x % kShards) * segcap;
+    const uint32_t SP = dim + 4;
+    uint32_t* sid = (uint32_t*)(sm + (size_t)2 * cap * SP);
     float* sthr = (float*)(sid + 2 * cap);
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const uint32_t d4 = dim >> 2;
     unsigned long long local_pairs = 0;
     for (uint32_t node = node0 + blockIdx.x; node < node1; node += gridDim.x) {
         const uint32_t nn = newc[node], no = oldc[node];
@@ -182,67 +218,86 @@ __global__ void __launch_bounds__(256) k_join(const float* __restrict__ vec, uin
         const uint32_t tot = nn + no;
         __syncthreads();
         for (uint32_t r = threadIdx.x; r < tot; r += blockDim.x) {
-            uint32_t id = r < nn ? newl[(size_t)node * cap + r] : oldl[(size_t)node * cap + (r - nn)];
+            const uint32_t id = r < nn ? newl[(size_t)node * cap + r] : oldl[(size_t)node * cap + (r - nn)];
             sid[r] = id;
             sthr[r] = thr[id];
         }
         __syncthreads();
-        for (uint32_t idx = threadIdx.x; idx < tot * dim; idx += blockDim.x) {
-            uint32_t r = idx / dim, e = idx % dim;
-            sm[r * stride + e] = vec[(size_t)sid[r] * dim + e];
+        for (uint32_t r = w; r < tot; r += nw) {  // a warp per row, float4 per lane
+            const float4* src = reinterpret_cast<const float4*>(vec + (size_t)sid[r] * dim);
+            float4* dst = reinterpret_cast<float4*>(sm + (size_t)r * SP);
+            for (uint32_t c = lane; c < d4; c += 32) dst[c] = __ldg(src + c);
         }
         __syncthreads();
-        // rows i in [0, nn); partners j in (i, tot): j < nn is new x new, j >= nn new x old.
-        // Pair t -> (i, j) through the row offsets off(i) = sum_{i'<i} (tot-1-i')
-        // = i (tot-1) - i (i-1) / 2.
-        auto rowoff = [tot](uint32_t i) { return i * (tot - 1) - i * (i - 1) / 2; };
-        const uint32_t T = rowoff(nn);
-        for (uint32_t t0 = 0; t0 < T; t0 += blockDim.x) {
-            const uint32_t t = t0 + threadIdx.x;
-            bool emit_a = false, emit_b = false;
-            uint32_t a = 0, b = 0;
-            float d = 0.f;
-            if (t < T) {
-                uint32_t lo = 0, hi = nn;  // last row with rowoff <= t
-                while (hi - lo > 1) {
-                    uint32_t mid = (lo + hi) >> 1;
-                    if (rowoff(mid) <= t) lo = mid;
-                    else hi = mid;
-                }
-                const uint32_t i = lo, j = i + 1 + (t - rowoff(i));
-                a = sid[i];
-                b = sid[j];
-                if (a != b) {
-                    const float* va = sm + (size_t)i * stride;
-                    const float* vb = sm + (size_t)j * stride;
-                    float acc[16];
+        const uint32_t ti_n = (nn + 3) >> 2, tj_n = (tot + 31) >> 5;
+        for (uint32_t t = w; t < ti_n * tj_n; t += nw) {
+            const uint32_t i0 = (t / tj_n) << 2, jb = (t % tj_n) << 5;
+            if (jb + 31 <= i0) continue;  // no j > i in this tile (uniform over the warp)
+            const uint32_t j = jb + lane;
+            const uint32_t jr = j < tot ? j : tot - 1;
+            float acc[4][16];
 #pragma unroll
-                    for (int l = 0; l < 16; ++l) acc[l] = 0.f;
-                    for (uint32_t e = 0; e < dim; e += 16) {
+            for (int r = 0; r < 4; ++r)
 #pragma unroll
-                        for (int l = 0; l < 16; ++l) acc[l] = sq_step(acc[l], va[e + l] - vb[e + l], FUSED);
+                for (int l = 0; l < 16; ++l) acc[r][l] = 0.f;
+            const float4* xb = reinterpret_cast<const float4*>(sm + (size_t)jr * SP);
+            const float4* xa = reinterpret_cast<const float4*>(sm + (size_t)i0 * SP);
+            const uint32_t sp4 = SP >> 2;
+            for (uint32_t e4 = 0; e4 < d4; e4 += 4) {
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    const float4 b = xb[e4 + c];
+#pragma unroll
+                    for (int r = 0; r < 4; ++r) {
+                        const float4 a = xa[(size_t)r * sp4 + e4 + c];
+                        acc[r][4 * c + 0] = sq_step(acc[r][4 * c + 0], a.x - b.x, FUSED);
+                        acc[r][4 * c + 1] = sq_step(acc[r][4 * c + 1], a.y - b.y, FUSED);
+                        acc[r][4 * c + 2] = sq_step(acc[r][4 * c + 2], a.z - b.z, FUSED);
+                        acc[r][4 * c + 3] = sq_step(acc[r][4 * c + 3], a.w - b.w, FUSED);
                     }
-                    d = acc[0];
-#pragma unroll
-                    for (int l = 1; l < 16; ++l) d = __fadd_rn(d, acc[l]);
-                    local_pairs++;
-                    emit_a = d < sthr[i];
-                    emit_b = d < sthr[j];
                 }
             }
-            // warp-aggregated append
-            const uint32_t ba = __ballot_sync(0xFFFFFFFFu, emit_a), bb = __ballot_sync(0xFFFFFFFFu, emit_b);
-            const uint32_t tot_w = __popc(ba) + __popc(bb);
-            if (tot_w) {
-                unsigned long long basep = 0;
-                if (lane == 0) basep = atomicAdd(pcount, (unsigned long long)tot_w);
-                basep = __shfl_sync(0xFFFFFFFFu, basep, 0);
-                unsigned long long p = basep + __popc(ba & lanemask_lt_()) + __popc(bb & lanemask_lt_());
-                if (emit_a) {
-                    if (p < pcap) prop[p] = Prop{a, b, d};
-                    p++;
+            float dd[4];
+            uint32_t emit = 0;  // bit 2r: i -> j proposal, bit 2r+1: j -> i
+            const uint32_t bj = sid[jr];
+            const float tj = sthr[jr];
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                float dv = acc[r][0];
+#pragma unroll
+                for (int l = 1; l < 16; ++l) dv = __fadd_rn(dv, acc[r][l]);
+                dd[r] = dv;
+                const uint32_t i = i0 + r;
+                if (i < nn && j > i && j < tot && sid[i] != bj) {
+                    local_pairs++;
+                    if (dv < sthr[i]) emit |= 1u << (2 * r);
+                    if (dv < tj) emit |= 2u << (2 * r);
                 }
-                if (emit_b && p < pcap) prop[p] = Prop{b, a, d};
+            }
+            const uint32_t ne = __popc(emit);
+            uint32_t incl = ne;
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            const uint32_t wt = __shfl_sync(0xFFFFFFFFu, incl, 31);
+            if (wt) {
+                unsigned long long basep = 0;
+                if (lane == 0) basep = atomicAdd(pc, (unsigned long long)wt);
+                basep = __shfl_sync(0xFFFFFFFFu, basep, 0);
+                unsigned long long p = basep + (incl - ne);
+#pragma unroll
+                for (int r = 0; r < 4; ++r) {
+                    const uint32_t ai = sid[(i0 + r) < tot ? i0 + r : 0];
+                    if ((emit >> (2 * r)) & 1u) {
+                        if (p < segcap) seg[p] = Prop{ai, bj, dd[r]};
+                        p++;
+                    }
+                    if ((emit >> (2 * r + 1)) & 1u) {
+                        if (p < segcap) seg[p] = Prop{bj, ai, dd[r]};
+                        p++;
+                    }
+                }
             }
         }
     }
@@ -256,7 +311,9 @@ __global__ void k_join_generic(const float* __restrict__ vec, uint32_t dim, int 
                                const uint32_t* __restrict__ newc, const uint32_t* __restrict__ oldl,
                                const uint32_t* __restrict__ oldc, const float* __restrict__ thr,
                                Prop* __restrict__ prop, unsigned long long* __restrict__ pcount,
-                               unsigned long long pcap, unsigned long long* __restrict__ njoin) {
+                               unsigned long long segcap, unsigned long long* __restrict__ njoin) {
+    unsigned long long* const pc = pcount + blockIdx.x % kShards;
+    Prop* const seg = prop + (size_t)(blockIdx.x % kShards) * segcap;
     unsigned long long local_pairs = 0;
     for (uint32_t node = node0 + blockIdx.x; node < node1; node += gridDim.x) {
         const uint32_t nn = newc[node], no = oldc[node], tot = nn + no;
@@ -271,9 +328,9 @@ __global__ void k_join_generic(const float* __restrict__ vec, uint32_t dim, int 
                 bool ea = d < thr[a], eb = d < thr[b];
                 uint32_t cnt = (uint32_t)ea + (uint32_t)eb;
                 if (cnt) {
-                    unsigned long long p = atomicAdd(pcount, (unsigned long long)cnt);
-                    if (ea && p < pcap) prop[p++] = Prop{a, b, d};
-                    if (eb && p < pcap) prop[p] = Prop{b, a, d};
+                    unsigned long long p = atomicAdd(pc, (unsigned long long)cnt);
+                    if (ea && p < segcap) seg[p++] = Prop{a, b, d};
+                    if (eb && p < segcap) seg[p] = Prop{b, a, d};
                 }
             }
         }
@@ -287,15 +344,17 @@ __global__ void k_thresholds(const uint32_t* __restrict__ hdr, const float* __re
     if (u < n) thr[u] = worst_of(hdr, dist, K, u);
 }
 
-__global__ void k_bucket_count(const Prop* __restrict__ prop, unsigned long long np, uint32_t* __restrict__ tcount) {
+__global__ void k_bucket_count(const Prop* __restrict__ prop, ShardMap m, uint32_t* __restrict__ tcount) {
+    const unsigned long long np = m.pre[kShards];
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < np; i += (size_t)gridDim.x * blockDim.x)
-        atomicAdd(&tcount[prop[i].target], 1u);
+        atomicAdd(&tcount[prop[shard_slot(m, i)].target], 1u);
 }
 
-__global__ void k_bucket_fill(const Prop* __restrict__ prop, unsigned long long np, const uint64_t* __restrict__ toff,
+__global__ void k_bucket_fill(const Prop* __restrict__ prop, ShardMap m, const uint64_t* __restrict__ toff,
                               uint32_t* __restrict__ tcur, uint64_t* __restrict__ bucket) {
+    const unsigned long long np = m.pre[kShards];
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < np; i += (size_t)gridDim.x * blockDim.x) {
-        Prop p = prop[i];
+        Prop p = prop[shard_slot(m, i)];
         uint64_t pos = toff[p.target] + atomicAdd(&tcur[p.target], 1u);
         bucket[pos] = ((uint64_t)__float_as_uint(p.d) << 32) | p.source;  // d >= 0: bit order = value order
     }
@@ -303,14 +362,21 @@ __global__ void k_bucket_fill(const Prop* __restrict__ prop, unsigned long long 
 
 // ---- phase 2: merge ----------------------------------------------------------
 
-constexpr int kMergeWarps = 4;
-constexpr uint32_t kPiece = 1024;
+constexpr int kMT = 256;          // merge CTA threads
+constexpr uint32_t kMH = 8192;    // source-id hash slots
+constexpr uint32_t kMS = 4096;    // survivor keys
 
-// Shared memory of one merge warp: keys (u64, first, so 8-byte alignment needs a
-// per-warp stride that is a multiple of 8), the list twice (d, id, flag), the id
-// table.  Rounded up to 16 bytes.
-__host__ __device__ inline size_t merge_warp_bytes(uint32_t K, uint32_t hcap) {
-    size_t b = (size_t)K * 18 + (size_t)kPiece * 8 + (size_t)hcap * 4 + 64;
+// Proposals one window holds: the hash keeps the list and the window's sources
+// at a load of at most 0.6.
+__host__ __device__ inline uint32_t merge_window(uint32_t K) {
+    const uint32_t w = kMH * 3 / 5 > K ? kMH * 3 / 5 - K : 0;
+    return w < kMS ? w : kMS;
+}
+
+// surv u64[kMS] | hash u32[kMH] | hist u32[256] | ctl u32[16] | two lists of
+// (d f32[K], id u32[K]) | two flag arrays u8[K].
+__host__ __device__ inline size_t merge_cta_bytes(uint32_t K) {
+    size_t b = (size_t)kMS * 8 + (size_t)kMH * 4 + 256 * 4 + 64 + (size_t)K * 16 + (size_t)K * 2;
     return (b + 15) & ~(size_t)15;
 }
 
@@ -321,153 +387,232 @@ __device__ __forceinline__ uint32_t hmix(uint32_t x) {
     return x;
 }
 
-// One warp per target with proposals.  Shared memory per warp: the list (d, id,
-// flag) twice, a piece of sorted proposal keys and an id hash of the list.
-__global__ void __launch_bounds__(kMergeWarps * 32) k_merge(uint32_t n, uint32_t K, const uint64_t* __restrict__ toff,
-                                                           const uint64_t* __restrict__ bucket,
-                                                           uint32_t* __restrict__ hdr, uint32_t* __restrict__ ids,
-                                                           float* __restrict__ dist, uint8_t* __restrict__ isnew,
-                                                           uint32_t hcap, unsigned long long* __restrict__ nupd) {
-    extern __shared__ char smraw[];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const size_t per_warp = merge_warp_bytes(K, hcap);  // multiple of 16: the u64 keys stay aligned
-    char* base = smraw + w * per_warp;
-    uint64_t* keys = (uint64_t*)base;
-    float* Ld = (float*)(keys + kPiece);
-    uint32_t* Li = (uint32_t*)(Ld + K);
-    float* Ld2 = (float*)(Li + K);
-    uint32_t* Li2 = (uint32_t*)(Ld2 + K);
-    uint32_t* hs = Li2 + K;
-    uint8_t* Lf = (uint8_t*)(hs + hcap);
-    uint8_t* Lf2 = Lf + K;
+// Bits of the rank-th smallest (1-based) of the non-negative floats Ld[0..cnt) and
+// hi32(surv[0..S)) (bit order = value order): four 8-bit radix passes.
+__device__ uint32_t block_select(const float* Ld, uint32_t cnt, const uint64_t* surv, uint32_t S, uint32_t rank,
+                                 uint32_t* hist, uint32_t* ctl) {
+    const int tid = threadIdx.x, lane = tid & 31;
+    uint32_t prefix = 0, mask = 0;
+    for (int shift = 24; shift >= 0; shift -= 8) {
+        for (int i = tid; i < 256; i += kMT) hist[i] = 0;
+        __syncthreads();
+        for (uint32_t j = tid; j < cnt; j += kMT) {
+            const uint32_t b = __float_as_uint(Ld[j]);
+            if ((b & mask) == prefix) atomicAdd(&hist[(b >> shift) & 255u], 1u);
+        }
+        for (uint32_t x = tid; x < S; x += kMT) {
+            const uint32_t b = (uint32_t)(surv[x] >> 32);
+            if ((b & mask) == prefix) atomicAdd(&hist[(b >> shift) & 255u], 1u);
+        }
+        __syncthreads();
+        if (tid < 32) {
+            uint32_t loc[8], sum = 0;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                loc[k] = hist[8 * lane + k];
+                sum += loc[k];
+            }
+            uint32_t incl = sum;
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            const uint32_t excl = incl - sum;
+            if (excl < rank && rank <= incl) {
+                uint32_t r = rank - excl;
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    if (r <= loc[k]) {
+                        ctl[3] = 8 * lane + k;
+                        ctl[4] = r;
+                        break;
+                    }
+                    r -= loc[k];
+                }
+            }
+        }
+        __syncthreads();
+        prefix |= ctl[3] << shift;
+        mask |= 0xFFu << shift;
+        rank = ctl[4];
+    }
+    return prefix;
+}
+
+// One CTA per target with proposals (targets handed out by *next_t).  Each window
+// of up to merge_window(K) proposals: drop those at or above the current farthest
+// entry (full list), those whose source is listed, and repeated sources (a
+// repeated pair has the same distance); find the K-th smallest distance tau of
+// (list U survivors) by radix selection; sort the survivors at or below tau by
+// (d, source) and merge them into the list, list entries first among equal
+// distances, keeping K.  Inserted entries are marked new.
+__global__ void __launch_bounds__(kMT) k_merge_cta(uint32_t n, uint32_t K, const uint64_t* __restrict__ toff,
+                                                   const uint64_t* __restrict__ bucket, uint32_t* __restrict__ hdr,
+                                                   uint32_t* __restrict__ ids, float* __restrict__ dist,
+                                                   uint8_t* __restrict__ isnew, unsigned long long* __restrict__ nupd,
+                                                   uint32_t* __restrict__ next_t) {
+    extern __shared__ __align__(16) char smraw[];
+    uint64_t* surv = (uint64_t*)smraw;
+    uint32_t* hk = (uint32_t*)(surv + kMS);
+    uint32_t* hist = hk + kMH;
+    uint32_t* ctl = hist + 256;  // 0 target, 1 survivors, 2 candidates, 3-4 select, 5 first changed
+    float* LdA = (float*)(ctl + 16);
+    uint32_t* LiA = (uint32_t*)(LdA + K);
+    float* LdB = (float*)(LiA + K);
+    uint32_t* LiB = (uint32_t*)(LdB + K);
+    uint8_t* LfA = (uint8_t*)(LiB + K);
+    uint8_t* LfB = LfA + K;
+    const int tid = threadIdx.x;
+    const uint32_t W = merge_window(K);
     unsigned long long upd = 0;
-    for (size_t u = (size_t)blockIdx.x * kMergeWarps + w; u < n; u += (size_t)gridDim.x * kMergeWarps) {
+    for (;;) {
+        __syncthreads();
+        if (tid == 0) ctl[0] = atomicAdd(next_t, 1u);
+        __syncthreads();
+        const uint32_t u = ctl[0];
+        if (u >= n) break;
         const uint64_t pb = toff[u], pe = toff[u + 1];
         if (pb == pe) continue;
+        float* Ld = LdA;
+        uint32_t* Li = LiA;
+        uint8_t* Lf = LfA;
+        float* Ld2 = LdB;
+        uint32_t* Li2 = LiB;
+        uint8_t* Lf2 = LfB;
         uint32_t cnt = hdr[u] & 0xFFFFu;
-        for (uint32_t j = lane; j < cnt; j += 32) {
-            Ld[j] = dist[u * K + j];
-            Li[j] = ids[u * K + j];
-            Lf[j] = isnew[u * K + j];
+        for (uint32_t j = tid; j < cnt; j += kMT) {
+            Ld[j] = dist[(size_t)u * K + j];
+            Li[j] = ids[(size_t)u * K + j];
+            Lf[j] = isnew[(size_t)u * K + j];
         }
-        uint32_t lo_written = cnt;  // first list position that changed
-        for (uint64_t p0 = pb; p0 < pe; p0 += kPiece) {
-            const uint32_t P = (pe - p0) < kPiece ? (uint32_t)(pe - p0) : kPiece;
-            uint32_t PP = 32;
-            while (PP < P) PP <<= 1;
-            for (uint32_t x = lane; x < PP; x += 32) keys[x] = x < P ? bucket[p0 + x] : ~0ull;
-            for (uint32_t x = lane; x < hcap; x += 32) hs[x] = kInvalid;
-            __syncwarp();
-            for (uint32_t j = lane; j < cnt; j += 32) {  // id hash of the current list
-                uint32_t id = Li[j], s = hmix(id) & (hcap - 1);
-                while (atomicCAS(&hs[s], kInvalid, id) != kInvalid) s = (s + 1) & (hcap - 1);
+        if (tid == 0) ctl[5] = cnt;
+        for (uint64_t w0 = pb; w0 < pe; w0 += W) {
+            const uint32_t P = (pe - w0) < W ? (uint32_t)(pe - w0) : W;
+            __syncthreads();  // the previous window's reads of ctl and the hash are done
+            for (uint32_t i = tid; i < kMH; i += kMT) hk[i] = kInvalid;
+            if (tid == 0) {
+                ctl[1] = 0;
+                ctl[2] = 0;
             }
-            // bitonic sort of the piece by (d, source)
+            __syncthreads();
+            for (uint32_t j = tid; j < cnt; j += kMT) {  // listed ids (distinct)
+                const uint32_t id = Li[j];
+                uint32_t sl = hmix(id) & (kMH - 1);
+                while (atomicCAS(&hk[sl], kInvalid, id) != kInvalid) sl = (sl + 1) & (kMH - 1);
+            }
+            __syncthreads();
+            const float worst = cnt >= K ? Ld[cnt - 1] : FLT_MAX;
+            for (uint32_t x = tid; x < P; x += kMT) {
+                const uint64_t key = bucket[w0 + x];
+                const float d = __uint_as_float((uint32_t)(key >> 32));
+                if (!(d < worst)) continue;
+                const uint32_t src = (uint32_t)key;
+                uint32_t sl = hmix(src) & (kMH - 1);
+                for (;;) {
+                    const uint32_t old = atomicCAS(&hk[sl], kInvalid, src);
+                    if (old == kInvalid) {
+                        surv[atomicAdd(&ctl[1], 1u)] = key;
+                        break;
+                    }
+                    if (old == src) break;
+                    sl = (sl + 1) & (kMH - 1);
+                }
+            }
+            __syncthreads();
+            const uint32_t S = ctl[1];
+            if (S == 0) continue;
+            // tau: bits of the K-th smallest distance of list U survivors
+            const uint32_t tau = cnt + S > K ? block_select(Ld, cnt, surv, S, K, hist, ctl) : 0xFFFFFFFFu;
+            // survivors at or below tau, compacted to the front
+            uint64_t loc[kMS / kMT];
+#pragma unroll
+            for (int k = 0; k < (int)(kMS / kMT); ++k) {
+                const uint32_t x = tid + k * kMT;
+                loc[k] = x < S ? surv[x] : ~0ull;
+            }
+            __syncthreads();
+#pragma unroll
+            for (int k = 0; k < (int)(kMS / kMT); ++k)
+                if (loc[k] != ~0ull && (uint32_t)(loc[k] >> 32) <= tau) surv[atomicAdd(&ctl[2], 1u)] = loc[k];
+            __syncthreads();
+            const uint32_t C = ctl[2];
+            uint32_t PP = 2;
+            while (PP < C) PP <<= 1;
+            for (uint32_t x = C + tid; x < PP; x += kMT) surv[x] = ~0ull;
+            __syncthreads();
             for (uint32_t k = 2; k <= PP; k <<= 1)
                 for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-                    __syncwarp();
-                    for (uint32_t x = lane; x < PP; x += 32) {
-                        uint32_t y = x ^ j;
+                    for (uint32_t x = tid; x < PP; x += kMT) {
+                        const uint32_t y = x ^ j;
                         if (y > x) {
-                            uint64_t a = keys[x], b = keys[y];
+                            const uint64_t a = surv[x], b = surv[y];
                             if ((a > b) == ((x & k) == 0)) {
-                                keys[x] = b;
-                                keys[y] = a;
+                                surv[x] = b;
+                                surv[y] = a;
                             }
                         }
                     }
+                    __syncthreads();
                 }
-            __syncwarp();
-            const float worst = cnt >= K ? Ld[cnt - 1] : FLT_MAX;
-            // keep: first of equal sources, not already listed, below the farthest
-            // entry when the list is full.  Compact kept keys to the front.
-            uint32_t kept = 0;
-            uint64_t carry = ~0ull;  // last original key of the previous group of 32
-            for (uint32_t x0 = 0; x0 < P; x0 += 32) {
-                uint32_t x = x0 + lane;
-                bool keep = false;
-                uint64_t kx = x < P ? keys[x] : ~0ull;
-                uint64_t prev = __shfl_up_sync(0xFFFFFFFFu, kx, 1);
-                if (lane == 0) prev = carry;
-                carry = __shfl_sync(0xFFFFFFFFu, kx, 31);
-                if (x < P) {
-                    uint32_t src = (uint32_t)kx;
-                    float d = __uint_as_float((uint32_t)(kx >> 32));
-                    keep = (x == 0 || prev != kx) && d < worst;
-                    if (keep) {
-                        uint32_t s = hmix(src) & (hcap - 1);
-                        while (hs[s] != kInvalid) {
-                            if (hs[s] == src) {
-                                keep = false;
-                                break;
-                            }
-                            s = (s + 1) & (hcap - 1);
-                        }
-                    }
-                }
-                uint32_t b = __ballot_sync(0xFFFFFFFFu, keep);
-                __syncwarp();
-                if (keep) keys[kept + __popc(b & lanemask_lt_())] = kx;
-                kept += __popc(b);
-                __syncwarp();
-            }
-            if (kept == 0) continue;
-            // merge list (cnt) with kept (sorted) -> K; ties: list entries first
-            const uint32_t ncnt = min(cnt + kept, K);
-            uint32_t lo = 0xFFFFFFFFu;
-            for (uint32_t j = lane; j < cnt; j += 32) {
-                float d = Ld[j];
-                uint32_t l2 = 0, h2 = kept;  // kept entries with distance < d
+            // merge (list entries first among equal distances), keep K
+            const uint32_t ncnt = min(cnt + C, K);
+            for (uint32_t j = tid; j < cnt; j += kMT) {
+                const float d = Ld[j];
+                const uint64_t bound = (uint64_t)__float_as_uint(d) << 32;  // candidates with distance < d
+                uint32_t l2 = 0, h2 = C;
                 while (l2 < h2) {
-                    uint32_t mid = (l2 + h2) >> 1;
-                    if (__uint_as_float((uint32_t)(keys[mid] >> 32)) < d) l2 = mid + 1;
+                    const uint32_t mid = (l2 + h2) >> 1;
+                    if (surv[mid] < bound) l2 = mid + 1;
                     else h2 = mid;
                 }
-                uint32_t pos = j + l2;
+                const uint32_t pos = j + l2;
                 if (pos < ncnt) {
                     Ld2[pos] = d;
                     Li2[pos] = Li[j];
                     Lf2[pos] = Lf[j];
                 }
-                if (l2 > 0) lo = min(lo, j);
             }
-            for (uint32_t x = lane; x < kept; x += 32) {
-                float d = __uint_as_float((uint32_t)(keys[x] >> 32));
+            for (uint32_t x = tid; x < C; x += kMT) {
+                const uint64_t key = surv[x];
+                const float d = __uint_as_float((uint32_t)(key >> 32));
                 uint32_t l2 = 0, h2 = cnt;  // list entries with distance <= d
                 while (l2 < h2) {
-                    uint32_t mid = (l2 + h2) >> 1;
+                    const uint32_t mid = (l2 + h2) >> 1;
                     if (Ld[mid] <= d) l2 = mid + 1;
                     else h2 = mid;
                 }
-                uint32_t pos = x + l2;
+                const uint32_t pos = x + l2;
                 if (pos < ncnt) {
                     Ld2[pos] = d;
-                    Li2[pos] = (uint32_t)keys[x];
+                    Li2[pos] = (uint32_t)key;
                     Lf2[pos] = 1;
-                    lo = min(lo, pos);
+                    atomicMin(&ctl[5], pos);
                     upd++;
                 }
             }
-            for (int o = 16; o; o >>= 1) lo = min(lo, __shfl_xor_sync(0xFFFFFFFFu, lo, o));
-            __syncwarp();
-            for (uint32_t j = lane; j < ncnt; j += 32) {
-                Ld[j] = Ld2[j];
-                Li[j] = Li2[j];
-                Lf[j] = Lf2[j];
-            }
+            __syncthreads();
+            float* t0 = Ld;
+            Ld = Ld2;
+            Ld2 = t0;
+            uint32_t* t1 = Li;
+            Li = Li2;
+            Li2 = t1;
+            uint8_t* t2 = Lf;
+            Lf = Lf2;
+            Lf2 = t2;
             cnt = ncnt;
-            lo_written = min(lo_written, lo);
-            __syncwarp();
         }
-        for (uint32_t j = lo_written + lane; j < cnt; j += 32) {
-            dist[u * K + j] = Ld[j];
-            ids[u * K + j] = Li[j];
-            isnew[u * K + j] = Lf[j];
+        __syncthreads();
+        const uint32_t lo = ctl[5];
+        for (uint32_t j = lo + tid; j < cnt; j += kMT) {
+            dist[(size_t)u * K + j] = Ld[j];
+            ids[(size_t)u * K + j] = Li[j];
+            isnew[(size_t)u * K + j] = Lf[j];
         }
-        if (lane == 0) hdr[u] = (hdr[u] & 0xFFFF0000u) | cnt;
-        __syncwarp();
+        if (tid == 0) hdr[u] = (hdr[u] & 0xFFFF0000u) | cnt;
     }
-    atomicAdd(nupd, upd);
+    for (int o = 16; o; o >>= 1) upd += __shfl_xor_sync(0xFFFFFFFFu, upd, o);
+    if ((tid & 31) == 0 && upd) atomicAdd(nupd, upd);
 }
 
 int smcount(int dev) {
@@ -495,6 +640,7 @@ void refine_knng(Index& ix, int iters, int sample) {
     // Device state of the refinement.
     DevMem isnew, newl, newc, oldl, oldc, rcount, roff, rcur, rbuf, thr, prop, tcount, toff, tcur, bucket, tmp, ctr;
     isnew.alloc((size_t)n * K + 16);
+    rbuf.alloc((size_t)n * K * 4 + 16);
     // INIT (hrnn.h:1744-1748): every existing entry is new.
     if (n) {
         size_t tot = (size_t)n * K;
@@ -514,29 +660,43 @@ void refine_knng(Index& ix, int iters, int sample) {
     toff.alloc(((size_t)n + 1) * 8);
     tcur.alloc(((size_t)n + 1) * 4);
     ctr.alloc(64);
-    const unsigned long long pcap = std::max<unsigned long long>(1 << 20, std::min<unsigned long long>(
-                                                                              400ull << 20, (unsigned long long)n * 512));
+    // Proposal buffer: every chunk's lists are merged once, at O(K) per touched
+    // target, so few large chunks are cheaper than many small ones.  Up to 2048
+    // proposals per node, 2^31 in all, and at most 40% of the free memory
+    // (20 bytes per proposal: the record and its bucket key).
+    size_t free_b = 0, total_b = 0;
+    CUDA_CHECK(cudaMemGetInfo(&free_b, &total_b));
+    const unsigned long long pcap = std::max<unsigned long long>(
+        1 << 20, std::min<unsigned long long>({(unsigned long long)n * 2048, 1ull << 31,
+                                               (unsigned long long)(free_b * 0.4 / 20)}));
     prop.alloc(pcap * sizeof(Prop));
     bucket.alloc(pcap * 8);
     uint32_t* hdr = ix.knn_hdr.as<uint32_t>();
     uint32_t* ids = ix.knn_ids.as<uint32_t>();
     float* dist = ix.knn_dist.as<float>();
-    unsigned long long* d_pcount = ctr.as<unsigned long long>();
-    unsigned long long* d_njoin = d_pcount + 1;
-    unsigned long long* d_nupd = d_pcount + 2;
+    unsigned long long* d_njoin = ctr.as<unsigned long long>() + 1;
+    unsigned long long* d_nupd = ctr.as<unsigned long long>() + 2;
+    uint32_t* d_nextt = (uint32_t*)(ctr.as<unsigned long long>() + 3);  // merge work counter
+    DevMem shard;  // per-segment proposal counts
+    shard.alloc(kShards * 8);
+    unsigned long long* d_pcount = shard.as<unsigned long long>();
+    const unsigned long long segcap = pcap / kShards;
     const bool fast = ix.order.lanes == 16 && ix.dim % 16 == 0;
-    const size_t join_smem = (size_t)2 * cap * (ix.dim + 1) * 4 + (size_t)2 * cap * 8;
+    const size_t join_smem = (size_t)2 * cap * (ix.dim + 4) * 4 + (size_t)2 * cap * 8;
     if (fast) {
         auto kj = (ix.order.fused & 1) ? k_join<true> : k_join<false>;
         if (join_smem > 227 * 1024) fail(HRNN_ERR_ARG, "refineKNNG: sample size too large for dim");
         CUDA_CHECK(cudaFuncSetAttribute(kj, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)join_smem));
     }
-    uint32_t hcap = 64;
-    while (hcap < 2 * K) hcap <<= 1;
-    const size_t merge_smem = (size_t)kMergeWarps * merge_warp_bytes(K, hcap);
-    if (merge_smem > 227 * 1024) fail(HRNN_ERR_ARG, "refineKNNG: K_knng too large for the merge kernel");
-    CUDA_CHECK(cudaFuncSetAttribute(k_merge, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)merge_smem));
+    const size_t merge_smem = merge_cta_bytes(K);
+    if (merge_smem > 227 * 1024 || merge_window(K) < 256)
+        fail(HRNN_ERR_ARG, "refineKNNG: K_knng too large for the merge kernel");
+    CUDA_CHECK(cudaFuncSetAttribute(k_merge_cta, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)merge_smem));
+    int merge_per_sm = 1;
+    CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&merge_per_sm, k_merge_cta, kMT, merge_smem));
+    const unsigned merge_grid = (unsigned)(nsm * std::max(merge_per_sm, 1));
     const int g1 = nsm * 16;
+    uint32_t chunk = std::max<uint32_t>(1, std::min<uint32_t>(n, 16384));
     ix.refine_stats = hrnn_refine_stats{};
     // Events bracketing sampling, and each chunk's join and bucket+merge.
     cudaEvent_t ev[7];
@@ -554,60 +714,68 @@ void refine_knng(Index& ix, int iters, int sample) {
         // ---- phase 1 ----
         CUDA_CHECK(cudaMemsetAsync(rcount.p, 0, rcount.bytes, s));
         CUDA_CHECK(cudaMemsetAsync(rcur.p, 0, rcur.bytes, s));
-        k_sample_count<<<g1, 256, 0, s>>>(ids, dist, hdr, isnew.as<uint8_t>(), n, K, rcount.as<uint32_t>());
+        k_thresholds<<<(n + 255) / 256, 256, 0, s>>>(hdr, dist, n, K, thr.as<float>());
+        CUDA_LAUNCH_CHECK();
+        k_sample_count<<<g1, 256, 0, s>>>(ids, dist, hdr, isnew.as<uint8_t>(), n, K, thr.as<float>(),
+                                           rcount.as<uint32_t>());
         CUDA_LAUNCH_CHECK();
         exclusive_scan_u32_to_u64(rcount.as<uint32_t>(), roff.as<uint64_t>(), (size_t)2 * n + 1, s, tmp);
         uint64_t rtot = 0;
         CUDA_CHECK(cudaMemcpyAsync(&rtot, roff.as<uint64_t>() + (size_t)2 * n, 8, cudaMemcpyDeviceToHost, s));
         CUDA_CHECK(cudaStreamSynchronize(s));
-        rbuf.ensure(std::max<uint64_t>(rtot, 1) * 4);
-        k_sample_fill<<<g1, 256, 0, s>>>(ids, dist, hdr, isnew.as<uint8_t>(), n, K, S, cap, newl.as<uint32_t>(),
+        rbuf.ensure(std::max<uint64_t>(rtot, 1) * 4);  // rtot <= n K: allocated once up front
+        k_sample_fill<<<g1, 256, 0, s>>>(ids, dist, hdr, isnew.as<uint8_t>(), n, K, thr.as<float>(), S, cap,
+                                          newl.as<uint32_t>(),
                                           newc.as<uint32_t>(), oldl.as<uint32_t>(), oldc.as<uint32_t>(),
                                           roff.as<uint64_t>(), rcur.as<uint32_t>(), rbuf.as<uint32_t>());
         CUDA_LAUNCH_CHECK();
         k_sample_rev<<<g1, 256, 0, s>>>(n, R, cap, roff.as<uint64_t>(), rbuf.as<uint32_t>(), newl.as<uint32_t>(),
-                                         newc.as<uint32_t>(), oldl.as<uint32_t>(), oldc.as<uint32_t>());
+                                         newc.as<uint32_t>(), oldl.as<uint32_t>(), oldc.as<uint32_t>(),
+                                         ctr.as<unsigned long long>() + 4);
         CUDA_LAUNCH_CHECK();
         CUDA_CHECK(cudaEventRecord(ev[2], s));
         // |new| + |old| summed over nodes (gather bytes of the join)
         unsigned long long sample_entries = 0;
-        {
-            std::vector<uint32_t> a(n), b(n);
-            CUDA_CHECK(cudaMemcpyAsync(a.data(), newc.p, (size_t)n * 4, cudaMemcpyDeviceToHost, s));
-            CUDA_CHECK(cudaMemcpyAsync(b.data(), oldc.p, (size_t)n * 4, cudaMemcpyDeviceToHost, s));
-            CUDA_CHECK(cudaStreamSynchronize(s));
-            for (uint32_t i = 0; i < n; ++i) sample_entries += (unsigned long long)a[i] + b[i];
-            t_sample = elapsed(e0, ev[2]);
-        }
+        CUDA_CHECK(cudaMemcpyAsync(&sample_entries, ctr.as<unsigned long long>() + 4, 8, cudaMemcpyDeviceToHost, s));
+        CUDA_CHECK(cudaStreamSynchronize(s));
+        t_sample = elapsed(e0, ev[2]);
         unsigned long long proposals = 0;
         // ---- phase 2, chunk by chunk ----
-        uint32_t chunk = std::max<uint32_t>(1, std::min<uint32_t>(n, 4096));
         for (uint32_t node0 = 0; node0 < n;) {
             uint32_t node1 = std::min<uint32_t>(n, node0 + chunk);
             k_thresholds<<<(n + 255) / 256, 256, 0, s>>>(hdr, dist, n, K, thr.as<float>());
             CUDA_LAUNCH_CHECK();
-            CUDA_CHECK(cudaMemsetAsync(d_pcount, 0, 8, s));
+            CUDA_CHECK(cudaMemsetAsync(d_pcount, 0, kShards * 8, s));
             CUDA_CHECK(cudaEventRecord(ev[3], s));
             unsigned grid = std::min<unsigned>(node1 - node0, (unsigned)nsm * 8);
             if (fast) {
                 auto kj = (ix.order.fused & 1) ? k_join<true> : k_join<false>;
                 kj<<<grid, 256, join_smem, s>>>(ix.vec.as<float>(), (uint32_t)ix.dim, node0, node1, cap,
                                                 newl.as<uint32_t>(), newc.as<uint32_t>(), oldl.as<uint32_t>(),
-                                                oldc.as<uint32_t>(), thr.as<float>(), prop.as<Prop>(), d_pcount, pcap,
+                                                oldc.as<uint32_t>(), thr.as<float>(), prop.as<Prop>(), d_pcount, segcap,
                                                 d_njoin);
             } else {
                 k_join_generic<<<grid, 128, 0, s>>>(ix.vec.as<float>(), (uint32_t)ix.dim, ix.order.lanes,
                                                     ix.order.fused, node0, node1, cap, newl.as<uint32_t>(),
                                                     newc.as<uint32_t>(), oldl.as<uint32_t>(), oldc.as<uint32_t>(),
-                                                    thr.as<float>(), prop.as<Prop>(), d_pcount, pcap, d_njoin);
+                                                    thr.as<float>(), prop.as<Prop>(), d_pcount, segcap, d_njoin);
             }
             CUDA_LAUNCH_CHECK();
             CUDA_CHECK(cudaEventRecord(ev[4], s));
-            unsigned long long np = 0;
-            CUDA_CHECK(cudaMemcpyAsync(&np, d_pcount, 8, cudaMemcpyDeviceToHost, s));
+            unsigned long long cnts[kShards];
+            CUDA_CHECK(cudaMemcpyAsync(cnts, d_pcount, sizeof(cnts), cudaMemcpyDeviceToHost, s));
             CUDA_CHECK(cudaStreamSynchronize(s));
             t_join += elapsed(ev[3], ev[4]);
-            if (np > pcap) {
+            ShardMap smap{};
+            smap.segcap = segcap;
+            unsigned long long np = 0, seg_max = 0;
+            for (uint32_t k = 0; k < kShards; ++k) {
+                smap.pre[k] = np;
+                np += cnts[k];
+                seg_max = std::max(seg_max, cnts[k]);
+            }
+            smap.pre[kShards] = np;
+            if (seg_max > segcap) {
                 if (chunk == 1) fail(HRNN_ERR_NOMEM, "refineKNNG: proposal buffer too small for one node");
                 chunk = std::max<uint32_t>(1, chunk / 4);  // redo this chunk smaller (the join is pure)
                 unsigned long long z = 0;
@@ -618,16 +786,16 @@ void refine_knng(Index& ix, int iters, int sample) {
                 CUDA_CHECK(cudaMemsetAsync(tcount.p, 0, tcount.bytes, s));
                 CUDA_CHECK(cudaMemsetAsync(tcur.p, 0, tcur.bytes, s));
                 unsigned gb = (unsigned)std::min<unsigned long long>((np + 255) / 256, (unsigned long long)nsm * 32);
-                k_bucket_count<<<gb, 256, 0, s>>>(prop.as<Prop>(), np, tcount.as<uint32_t>());
+                k_bucket_count<<<gb, 256, 0, s>>>(prop.as<Prop>(), smap, tcount.as<uint32_t>());
                 CUDA_LAUNCH_CHECK();
                 exclusive_scan_u32_to_u64(tcount.as<uint32_t>(), toff.as<uint64_t>(), (size_t)n + 1, s, tmp);
-                k_bucket_fill<<<gb, 256, 0, s>>>(prop.as<Prop>(), np, toff.as<uint64_t>(), tcur.as<uint32_t>(),
+                k_bucket_fill<<<gb, 256, 0, s>>>(prop.as<Prop>(), smap, toff.as<uint64_t>(), tcur.as<uint32_t>(),
                                                  bucket.as<uint64_t>());
                 CUDA_LAUNCH_CHECK();
                 CUDA_CHECK(cudaEventRecord(ev[6], s));
-                k_merge<<<nsm * 4, kMergeWarps * 32, merge_smem, s>>>(n, K, toff.as<uint64_t>(),
-                                                                      bucket.as<uint64_t>(), hdr, ids, dist,
-                                                                      isnew.as<uint8_t>(), hcap, d_nupd);
+                CUDA_CHECK(cudaMemsetAsync(d_nextt, 0, 4, s));
+                k_merge_cta<<<merge_grid, kMT, merge_smem, s>>>(n, K, toff.as<uint64_t>(), bucket.as<uint64_t>(),
+                                                                hdr, ids, dist, isnew.as<uint8_t>(), d_nupd, d_nextt);
                 CUDA_LAUNCH_CHECK();
                 CUDA_CHECK(cudaEventRecord(ev[5], s));
                 CUDA_CHECK(cudaEventSynchronize(ev[5]));
@@ -636,8 +804,10 @@ void refine_knng(Index& ix, int iters, int sample) {
             }
             proposals += np;
             node0 = node1;
-            // Grow the chunk while proposals stay well inside the buffer.
-            if (np < pcap / 8 && chunk < n) chunk = std::min<uint32_t>(n, chunk * 2);
+            // Keep the chunk's proposals between a quarter and three quarters of
+            // the buffer (the size carries over to the next iteration).
+            if (seg_max < segcap / 4 && chunk < n) chunk = std::min<uint32_t>(n, chunk * 2);
+            else if (seg_max > segcap / 4 * 3 && chunk > 1) chunk /= 2;
         }
         unsigned long long hc[3] = {0, 0, 0};
         CUDA_CHECK(cudaEventRecord(e1, s));

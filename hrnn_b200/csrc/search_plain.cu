@@ -62,17 +62,23 @@ __global__ void __launch_bounds__(128) k_phase_a(DevView v, const float* __restr
                                                  uint32_t* __restrict__ prox, uint32_t* __restrict__ nprox,
                                                  SearchCounters* __restrict__ ctr,
                                                  const uint32_t* __restrict__ qlist, uint32_t m_over,
-                                                 uint32_t ef_over, uint32_t m_keep, float* __restrict__ proxd) {
+                                                 uint32_t ef_over, uint32_t m_keep, float* __restrict__ proxd,
+                                                 uint32_t* __restrict__ next_q) {
     // qlist: search only the listed queries (nq = list length); m_over / ef_over:
     // one (m, ef) for every query instead of the arrays (the beam is
     // max(ef, m) as in the reference); m_keep: write at least this many beam
     // entries (the learned budget's frontier; at most mmax); proxd: also write
-    // the entries' distances.
+    // the entries' distances.  next_q: work counter, zero at launch; a warp takes
+    // the next query as soon as it finishes one.
     extern __shared__ char smem_raw[];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     WarpSmem s = carve(smem_raw + (size_t)w * warp_smem_bytes(v.dim, efc, vc), v.dim, efc, vc);
     unsigned long long c_dist = 0, c_exp = 0;
-    for (uint32_t j = blockIdx.x * wpb + w; j < nq; j += gridDim.x * wpb) {
+    for (;;) {
+        uint32_t j = 0;
+        if (lane == 0) j = atomicAdd(next_q, 1u);
+        j = __shfl_sync(0xFFFFFFFFu, j, 0);
+        if (j >= nq) break;
         const uint32_t qi = qlist ? qlist[j] : j;
         const uint32_t m = m_over ? m_over : qm[qi];
         const uint32_t EF = max(ef_over ? ef_over : qef[qi], m);
@@ -365,7 +371,10 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
     if (two_pass) efmax = std::max<uint32_t>(efmax, ix.budget->ef);
     DevView v = make_view(ix);
     const uint32_t efc = (efmax + 31) & ~31u;
-    const uint32_t vc = 2048;  // visited-cache slots (lossy; misses cost a recomputed row)
+    // Visited-cache slots (lossy; a miss costs a recomputed row).  1024 rather than
+    // more: the smaller per-warp shared memory keeps more warps resident, which
+    // pays for the ~10% extra rows at ef = 200.
+    const uint32_t vc = 1024;
     size_t wsm = warp_smem_bytes(v.dim, efc, vc);
     int wpb = (int)std::max<size_t>(1, std::min<size_t>(4, (200 * 1024) / wsm));
     size_t smem_a = wsm * wpb;
@@ -384,7 +393,7 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
     uint32_t* d_rcount = (uint32_t*)(d_resoff + (nq + 1));
     uint32_t* d_next = d_rcount + (nq + 1);
     CUDA_CHECK(cudaMemsetAsync(d_total, 0, (nq + 1) * 8, s));
-    CUDA_CHECK(cudaMemsetAsync(d_rcount, 0, (nq + 1) * 4 + 16, s));
+    CUDA_CHECK(cudaMemsetAsync(d_rcount, 0, (nq + 1) * 4 + 32, s));  // and the 8 counters after it
     SearchCounters* ctr = ix.counters.as<SearchCounters>();
     const bool fusedsimd = (ix.order.fused & 1) != 0;
     // Mixed precision (hrnn_set_precision): BF16 rows for the beam and the
@@ -400,11 +409,17 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
     {
         auto kern = mixed ? k_phase_a<2> : (fusedsimd ? k_phase_a<1> : k_phase_a<0>);
         CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_a));
-        auto grid_for = [&](size_t n) { return (unsigned)std::max<size_t>(1, std::min<size_t>((n + wpb - 1) / wpb, (size_t)nsm * 16)); };
+        // Persistent grid (every resident block), queries handed out by counters.
+        int per_sm = 1;
+        CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, wpb * 32, smem_a));
+        auto grid_for = [&](size_t n) {
+            return (unsigned)std::max<size_t>(1, std::min<size_t>((n + wpb - 1) / wpb, (size_t)nsm * std::max(per_sm, 1)));
+        };
+        uint32_t* d_qa = d_next + 4;  // work counters of the phase-A launches (zeroed with d_rcount)
         if (!learned) {
             kern<<<grid_for(nq), wpb * 32, smem_a, s>>>(v, a.d_q, (uint32_t)nq, a.d_m, a.d_ef, efc, vc, mmax,
                                                         prox.as<uint32_t>(), nprox.as<uint32_t>(), ctr, nullptr, 0, 0,
-                                                        0, nullptr);
+                                                        0, nullptr, d_qa);
             CUDA_LAUNCH_CHECK();
         } else {
             // Learned budget: frontier pass for every query, features, MLP,
@@ -427,7 +442,7 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
             kern<<<grid_for(nq), wpb * 32, smem_a, s>>>(v, a.d_q, (uint32_t)nq, a.d_m, a.d_ef, efc, vc, mmax,
                                                         prox.as<uint32_t>(), nprox.as<uint32_t>(), ctr, nullptr,
                                                         two_pass ? b.m[1] : 0, two_pass ? b.ef : 0, kFrontier,
-                                                        b.proxd.as<float>());
+                                                        b.proxd.as<float>(), d_qa);
             CUDA_LAUNCH_CHECK();
             k_budget_features<<<(unsigned)((nq * 32 + 255) / 256), 256, 0, s>>>(
                 v, a.d_q, (uint32_t)nq, prox.as<uint32_t>(), b.proxd.as<float>(), nprox.as<uint32_t>(), mmax,
@@ -445,7 +460,8 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
                 if (nfb) {
                     kern<<<grid_for(nfb), wpb * 32, smem_a, s>>>(v, a.d_q, nfb, a.d_m, a.d_ef, efc, vc, mmax,
                                                                  prox.as<uint32_t>(), nprox.as<uint32_t>(), ctr,
-                                                                 b.fallback_list.as<uint32_t>(), 0, 0, 0, nullptr);
+                                                                 b.fallback_list.as<uint32_t>(), 0, 0, 0, nullptr,
+                                                                 d_qa + 1);
                     CUDA_LAUNCH_CHECK();
                 }
             }
@@ -606,15 +622,17 @@ void budget_features(Index& ix, const float* d_q, size_t nq, uint32_t k, uint32_
     if (mixed) ensure_bf16(ix);
     DevView v = make_view(ix);
     ensure_projection(ix, b);
-    const uint32_t mmax = std::max<uint32_t>(m, kFrontier), efc = (std::max(m, ef) + 31) & ~31u, vc = 2048;
+    const uint32_t mmax = std::max<uint32_t>(m, kFrontier), efc = (std::max(m, ef) + 31) & ~31u, vc = 1024;
     const size_t wsm = warp_smem_bytes(v.dim, efc, vc);
     const int wpb = (int)std::max<size_t>(1, std::min<size_t>(4, (200 * 1024) / wsm));
     const size_t smem_a = wsm * wpb;
     if (smem_a > 227 * 1024) fail(HRNN_ERR_ARG, "budget: ef/dim too large for one warp's beam");
-    DevMem prox, nprox, proxd;
+    DevMem prox, nprox, proxd, next;
     prox.alloc(nq * mmax * 4);
     nprox.alloc(nq * 4);
     proxd.alloc(nq * mmax * 4);
+    next.alloc(16);
+    CUDA_CHECK(cudaMemsetAsync(next.p, 0, 16, s));
     ix.kcol.ensure((size_t)std::max<size_t>(ix.cur, 1) * 4);
     k_kdist_column<<<(unsigned)((ix.cur + 255) / 256), 256, 0, s>>>(v, k - 1, ix.kcol.as<float>());
     CUDA_LAUNCH_CHECK();
@@ -624,7 +642,7 @@ void budget_features(Index& ix, const float* d_q, size_t nq, uint32_t k, uint32_
     unsigned grid = (unsigned)std::max<size_t>(1, std::min<size_t>((nq + wpb - 1) / wpb, (size_t)nsm * 16));
     kern<<<grid, wpb * 32, smem_a, s>>>(v, d_q, (uint32_t)nq, nullptr, nullptr, efc, vc, mmax, prox.as<uint32_t>(),
                                         nprox.as<uint32_t>(), ix.counters.as<SearchCounters>(), nullptr, m, ef,
-                                        kFrontier, proxd.as<float>());
+                                        kFrontier, proxd.as<float>(), next.as<uint32_t>());
     CUDA_LAUNCH_CHECK();
     k_budget_features<<<(unsigned)((nq * 32 + 255) / 256), 256, 0, s>>>(v, d_q, (uint32_t)nq, prox.as<uint32_t>(),
                                                                        proxd.as<float>(), nprox.as<uint32_t>(), mmax,
