@@ -41,15 +41,20 @@ WORKLOADS = {
     # 256 Gaussians (centres ~ N(0, 4I), sigma 1, seed 2), K_knng=500.
     "mixed-1M-d128-K500": dict(n=1_000_000, d=128, C=256, sigma=1.0, seed=2, dirichlet=True, nq=10_000,
                                qseed=1002, M=16, efc=400, K=500, iters=10, S=50, k=10, Kp=500, ef=200,
-                               m_sweep=[1, 3, 5, 10, 20, 50]),
+                               m_sweep=[1, 2, 3, 4, 5, 6, 8, 10, 20, 50]),
     # Profiling case: the same mixture at half the size (vectors 256 MB > L2), K_knng=250.
     "mixed-500k-d128-K250": dict(n=500_000, d=128, C=256, sigma=1.0, seed=2, dirichlet=True, nq=2_000,
                                  qseed=1002, M=16, efc=400, K=250, iters=10, S=50, k=10, Kp=250, ef=200,
-                                 m_sweep=[1, 3, 5, 10, 20, 50]),
+                                 m_sweep=[1, 2, 3, 4, 5, 6, 8, 10, 20, 50]),
+    # Build profiling case: the 1M mixture's generator at 200k points, K_knng=500,
+    # two NNDescent iterations (used with --build-only).
+    "build-200k-d128-K500": dict(n=200_000, d=128, C=256, sigma=1.0, seed=2, dirichlet=True, nq=1_000,
+                                 qseed=1002, M=16, efc=400, K=500, iters=2, S=50, k=10, Kp=500, ef=200,
+                                 m_sweep=[5]),
     # The reference's CPU-runnable case: 100k x 128, 64 equal Gaussians (seed 0), K_knng=100.
     "plain-100k-d128-K100": dict(n=100_000, d=128, C=64, sigma=1.0, seed=0, dirichlet=False, nq=1_000, qseed=1,
                                  M=16, efc=400, K=100, iters=10, S=50, k=10, Kp=100, ef=200,
-                                 m_sweep=[1, 3, 5, 10, 20, 50]),
+                                 m_sweep=[1, 2, 3, 4, 5, 6, 8, 10, 20, 50]),
 }
 TARGET_RECALL = 0.95
 
@@ -227,6 +232,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample", type=int, default=2000, help="queries in the CPU-baseline sample")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-budget form")
+    ap.add_argument("--build-only", action="store_true", help="build the index, print its build times, exit")
     ap.add_argument("--budget-train", type=int, default=200_000, help="training queries of the budget MLP")
     args = ap.parse_args()
     W = WORKLOADS[args.workload]
@@ -259,6 +265,12 @@ def main():
     h, build = build_index(H, W, X, dev_sync)
     rs = h.last_refine_stats()
     log(f"[bench] build: {json.dumps(build)}")
+    if args.build_only:
+        if rank == 0:
+            print(json.dumps({"workload": args.workload, "build": build,
+                              "refine": {k_: rs[k_] for k_ in ("ms", "sample_ms", "join_ms", "bucket_ms", "merge_ms",
+                                                               "proposals", "join_dists", "updates")}}), flush=True)
+        return
 
     # ---- ground truth and the recall sweep (untimed) ----
     t_gt = time.perf_counter()
@@ -270,7 +282,7 @@ def main():
     nq, d = Q.shape
     forms = {"plain": H.PREC_FP32_EXACT, "mixed": H.PREC_BF16}
 
-    def sweep_form(prec):
+    def sweep_form(prec, stop=False):
         h.set_precision(prec)
         sw, mstar = {}, None
         for m in W["m_sweep"]:
@@ -278,6 +290,8 @@ def main():
             sw[m] = macro_recall(gt, res)
             if mstar is None and sw[m] >= TARGET_RECALL:
                 mstar = m
+                if stop:
+                    break
         return sw, (mstar if mstar is not None else W["m_sweep"][-1])
 
     sweeps, mstars = {}, {}
@@ -302,7 +316,7 @@ def main():
         for c in CONFIDENCES:
             BUDGET["confidence"] = c
             h.set_budget(True, **BUDGET)
-            sw, mstar = sweep_form(H.PREC_BF16)
+            sw, mstar = sweep_form(H.PREC_BF16, stop=True)
             log(f"[bench] learned (confidence {c}): recall sweep (fallback m) "
                 f"{json.dumps({k_: round(v_, 4) for k_, v_ in sw.items()})} -> m={mstar}")
             if sw[mstar] >= TARGET_RECALL:
@@ -487,7 +501,7 @@ def main():
 # own beam (single pass); a query takes a level when the MLP gives that level's
 # answer being complete a probability >= 0.9, else the caller's m.
 BUDGET = dict(m0=1, m1=3, ef=0, confidence=0.9)
-CONFIDENCES = (0.9, 0.95, 0.98, 0.99)
+CONFIDENCES = (0.95, 0.98, 0.99, 0.995, 0.998)
 LABEL_M, LABEL_EF = 50, 200  # the "complete" answer the labels compare against
 
 

@@ -167,27 +167,6 @@ struct Prop {
     float d;
 };
 
-// The proposal buffer is split into kShards segments with a counter each (block b
-// appends to segment b mod kShards), so no single counter takes every append.
-constexpr uint32_t kShards = 32;
-
-// Exclusive prefix of the segments' fill counts: flat proposal j lives in segment
-// s with pre[s] <= j < pre[s + 1], at prop[s * segcap + j - pre[s]].
-struct ShardMap {
-    unsigned long long pre[kShards + 1];
-    unsigned long long segcap;
-};
-
-__device__ __forceinline__ size_t shard_slot(const ShardMap& m, unsigned long long j) {
-    uint32_t lo = 0, hi = kShards;  // last segment with pre <= j
-    while (hi - lo > 1) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (m.pre[mid] <= j) lo = mid;
-        else hi = mid;
-    }
-    return (size_t)lo * m.segcap + (size_t)(j - m.pre[lo]);
-}
-
 // One block per node of the chunk: exact FP32 distances of all sample pairs.
 // The node's rows are staged in shared memory (stride dim + 4 floats: 16-byte
 // aligned and free of bank conflicts for float4 reads).  A warp takes a tile of
@@ -202,10 +181,8 @@ __global__ void __launch_bounds__(256) k_join(const float* __restrict__ vec, uin
                                               const uint32_t* __restrict__ newc, const uint32_t* __restrict__ oldl,
                                               const uint32_t* __restrict__ oldc, const float* __restrict__ thr,
                                               Prop* __restrict__ prop, unsigned long long* __restrict__ pcount,
-                                              unsigned long long segcap, unsigned long long* __restrict__ njoin) {
+                                              unsigned long long pcap, unsigned long long* __restrict__ njoin) {
     extern __shared__ __align__(16) float sm[];
-    unsigned long long* const pc = pcount + blockIdx.x % kShards;
-    Prop* const seg = prop + (size_t)(blockIdx.x % kShards) * segcap;
     const uint32_t SP = dim + 4;
     uint32_t* sid = (uint32_t*)(sm + (size_t)2 * cap * SP);
     float* sthr = (float*)(sid + 2 * cap);
@@ -283,18 +260,18 @@ __global__ void __launch_bounds__(256) k_join(const float* __restrict__ vec, uin
             const uint32_t wt = __shfl_sync(0xFFFFFFFFu, incl, 31);
             if (wt) {
                 unsigned long long basep = 0;
-                if (lane == 0) basep = atomicAdd(pc, (unsigned long long)wt);
+                if (lane == 0) basep = atomicAdd(pcount, (unsigned long long)wt);
                 basep = __shfl_sync(0xFFFFFFFFu, basep, 0);
                 unsigned long long p = basep + (incl - ne);
 #pragma unroll
                 for (int r = 0; r < 4; ++r) {
                     const uint32_t ai = sid[(i0 + r) < tot ? i0 + r : 0];
                     if ((emit >> (2 * r)) & 1u) {
-                        if (p < segcap) seg[p] = Prop{ai, bj, dd[r]};
+                        if (p < pcap) prop[p] = Prop{ai, bj, dd[r]};
                         p++;
                     }
                     if ((emit >> (2 * r + 1)) & 1u) {
-                        if (p < segcap) seg[p] = Prop{bj, ai, dd[r]};
+                        if (p < pcap) prop[p] = Prop{bj, ai, dd[r]};
                         p++;
                     }
                 }
@@ -311,9 +288,7 @@ __global__ void k_join_generic(const float* __restrict__ vec, uint32_t dim, int 
                                const uint32_t* __restrict__ newc, const uint32_t* __restrict__ oldl,
                                const uint32_t* __restrict__ oldc, const float* __restrict__ thr,
                                Prop* __restrict__ prop, unsigned long long* __restrict__ pcount,
-                               unsigned long long segcap, unsigned long long* __restrict__ njoin) {
-    unsigned long long* const pc = pcount + blockIdx.x % kShards;
-    Prop* const seg = prop + (size_t)(blockIdx.x % kShards) * segcap;
+                               unsigned long long pcap, unsigned long long* __restrict__ njoin) {
     unsigned long long local_pairs = 0;
     for (uint32_t node = node0 + blockIdx.x; node < node1; node += gridDim.x) {
         const uint32_t nn = newc[node], no = oldc[node], tot = nn + no;
@@ -328,9 +303,9 @@ __global__ void k_join_generic(const float* __restrict__ vec, uint32_t dim, int 
                 bool ea = d < thr[a], eb = d < thr[b];
                 uint32_t cnt = (uint32_t)ea + (uint32_t)eb;
                 if (cnt) {
-                    unsigned long long p = atomicAdd(pc, (unsigned long long)cnt);
-                    if (ea && p < segcap) seg[p++] = Prop{a, b, d};
-                    if (eb && p < segcap) seg[p] = Prop{b, a, d};
+                    unsigned long long p = atomicAdd(pcount, (unsigned long long)cnt);
+                    if (ea && p < pcap) prop[p++] = Prop{a, b, d};
+                    if (eb && p < pcap) prop[p] = Prop{b, a, d};
                 }
             }
         }
@@ -344,17 +319,15 @@ __global__ void k_thresholds(const uint32_t* __restrict__ hdr, const float* __re
     if (u < n) thr[u] = worst_of(hdr, dist, K, u);
 }
 
-__global__ void k_bucket_count(const Prop* __restrict__ prop, ShardMap m, uint32_t* __restrict__ tcount) {
-    const unsigned long long np = m.pre[kShards];
+__global__ void k_bucket_count(const Prop* __restrict__ prop, unsigned long long np, uint32_t* __restrict__ tcount) {
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < np; i += (size_t)gridDim.x * blockDim.x)
-        atomicAdd(&tcount[prop[shard_slot(m, i)].target], 1u);
+        atomicAdd(&tcount[prop[i].target], 1u);
 }
 
-__global__ void k_bucket_fill(const Prop* __restrict__ prop, ShardMap m, const uint64_t* __restrict__ toff,
+__global__ void k_bucket_fill(const Prop* __restrict__ prop, unsigned long long np, const uint64_t* __restrict__ toff,
                               uint32_t* __restrict__ tcur, uint64_t* __restrict__ bucket) {
-    const unsigned long long np = m.pre[kShards];
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < np; i += (size_t)gridDim.x * blockDim.x) {
-        Prop p = prop[shard_slot(m, i)];
+        Prop p = prop[i];
         uint64_t pos = toff[p.target] + atomicAdd(&tcur[p.target], 1u);
         bucket[pos] = ((uint64_t)__float_as_uint(p.d) << 32) | p.source;  // d >= 0: bit order = value order
     }
@@ -677,10 +650,7 @@ void refine_knng(Index& ix, int iters, int sample) {
     unsigned long long* d_njoin = ctr.as<unsigned long long>() + 1;
     unsigned long long* d_nupd = ctr.as<unsigned long long>() + 2;
     uint32_t* d_nextt = (uint32_t*)(ctr.as<unsigned long long>() + 3);  // merge work counter
-    DevMem shard;  // per-segment proposal counts
-    shard.alloc(kShards * 8);
-    unsigned long long* d_pcount = shard.as<unsigned long long>();
-    const unsigned long long segcap = pcap / kShards;
+    unsigned long long* d_pcount = ctr.as<unsigned long long>();  // proposal count of a chunk
     const bool fast = ix.order.lanes == 16 && ix.dim % 16 == 0;
     const size_t join_smem = (size_t)2 * cap * (ix.dim + 4) * 4 + (size_t)2 * cap * 8;
     if (fast) {
@@ -745,37 +715,28 @@ void refine_knng(Index& ix, int iters, int sample) {
             uint32_t node1 = std::min<uint32_t>(n, node0 + chunk);
             k_thresholds<<<(n + 255) / 256, 256, 0, s>>>(hdr, dist, n, K, thr.as<float>());
             CUDA_LAUNCH_CHECK();
-            CUDA_CHECK(cudaMemsetAsync(d_pcount, 0, kShards * 8, s));
+            CUDA_CHECK(cudaMemsetAsync(d_pcount, 0, 8, s));
             CUDA_CHECK(cudaEventRecord(ev[3], s));
             unsigned grid = std::min<unsigned>(node1 - node0, (unsigned)nsm * 8);
             if (fast) {
                 auto kj = (ix.order.fused & 1) ? k_join<true> : k_join<false>;
                 kj<<<grid, 256, join_smem, s>>>(ix.vec.as<float>(), (uint32_t)ix.dim, node0, node1, cap,
                                                 newl.as<uint32_t>(), newc.as<uint32_t>(), oldl.as<uint32_t>(),
-                                                oldc.as<uint32_t>(), thr.as<float>(), prop.as<Prop>(), d_pcount, segcap,
+                                                oldc.as<uint32_t>(), thr.as<float>(), prop.as<Prop>(), d_pcount, pcap,
                                                 d_njoin);
             } else {
                 k_join_generic<<<grid, 128, 0, s>>>(ix.vec.as<float>(), (uint32_t)ix.dim, ix.order.lanes,
                                                     ix.order.fused, node0, node1, cap, newl.as<uint32_t>(),
                                                     newc.as<uint32_t>(), oldl.as<uint32_t>(), oldc.as<uint32_t>(),
-                                                    thr.as<float>(), prop.as<Prop>(), d_pcount, segcap, d_njoin);
+                                                    thr.as<float>(), prop.as<Prop>(), d_pcount, pcap, d_njoin);
             }
             CUDA_LAUNCH_CHECK();
             CUDA_CHECK(cudaEventRecord(ev[4], s));
-            unsigned long long cnts[kShards];
-            CUDA_CHECK(cudaMemcpyAsync(cnts, d_pcount, sizeof(cnts), cudaMemcpyDeviceToHost, s));
+            unsigned long long np = 0;
+            CUDA_CHECK(cudaMemcpyAsync(&np, d_pcount, 8, cudaMemcpyDeviceToHost, s));
             CUDA_CHECK(cudaStreamSynchronize(s));
             t_join += elapsed(ev[3], ev[4]);
-            ShardMap smap{};
-            smap.segcap = segcap;
-            unsigned long long np = 0, seg_max = 0;
-            for (uint32_t k = 0; k < kShards; ++k) {
-                smap.pre[k] = np;
-                np += cnts[k];
-                seg_max = std::max(seg_max, cnts[k]);
-            }
-            smap.pre[kShards] = np;
-            if (seg_max > segcap) {
+            if (np > pcap) {
                 if (chunk == 1) fail(HRNN_ERR_NOMEM, "refineKNNG: proposal buffer too small for one node");
                 chunk = std::max<uint32_t>(1, chunk / 4);  // redo this chunk smaller (the join is pure)
                 unsigned long long z = 0;
@@ -786,10 +747,10 @@ void refine_knng(Index& ix, int iters, int sample) {
                 CUDA_CHECK(cudaMemsetAsync(tcount.p, 0, tcount.bytes, s));
                 CUDA_CHECK(cudaMemsetAsync(tcur.p, 0, tcur.bytes, s));
                 unsigned gb = (unsigned)std::min<unsigned long long>((np + 255) / 256, (unsigned long long)nsm * 32);
-                k_bucket_count<<<gb, 256, 0, s>>>(prop.as<Prop>(), smap, tcount.as<uint32_t>());
+                k_bucket_count<<<gb, 256, 0, s>>>(prop.as<Prop>(), np, tcount.as<uint32_t>());
                 CUDA_LAUNCH_CHECK();
                 exclusive_scan_u32_to_u64(tcount.as<uint32_t>(), toff.as<uint64_t>(), (size_t)n + 1, s, tmp);
-                k_bucket_fill<<<gb, 256, 0, s>>>(prop.as<Prop>(), smap, toff.as<uint64_t>(), tcur.as<uint32_t>(),
+                k_bucket_fill<<<gb, 256, 0, s>>>(prop.as<Prop>(), np, toff.as<uint64_t>(), tcur.as<uint32_t>(),
                                                  bucket.as<uint64_t>());
                 CUDA_LAUNCH_CHECK();
                 CUDA_CHECK(cudaEventRecord(ev[6], s));
@@ -806,8 +767,8 @@ void refine_knng(Index& ix, int iters, int sample) {
             node0 = node1;
             // Keep the chunk's proposals between a quarter and three quarters of
             // the buffer (the size carries over to the next iteration).
-            if (seg_max < segcap / 4 && chunk < n) chunk = std::min<uint32_t>(n, chunk * 2);
-            else if (seg_max > segcap / 4 * 3 && chunk > 1) chunk /= 2;
+            if (np < pcap / 4 && chunk < n) chunk = std::min<uint32_t>(n, chunk * 2);
+            else if (np > pcap / 4 * 3 && chunk > 1) chunk /= 2;
         }
         unsigned long long hc[3] = {0, 0, 0};
         CUDA_CHECK(cudaEventRecord(e1, s));

@@ -26,8 +26,12 @@ namespace hrnn {
 
 namespace {
 
-constexpr uint32_t kHS = 8192;        // table slots
-constexpr uint32_t kPartTarget = 3072; // postings per range (load <= ~0.4)
+// Candidate table: a power of two of slots, sized per query between 1024 and
+// table_max for a load of at most 0.4 postings per slot; queries with more
+// postings split the owner-id range into parts (one pass over the postings
+// each).  The mixed-precision kernel, whose registers already hold it to three
+// CTAs per SM, takes 16384 slots; the exact kernel keeps 8192 so that the
+// table's shared memory does not cut it below four.
 constexpr uint32_t kACap = 1024;      // accepted per range
 constexpr int kBCThreads = 256;
 
@@ -88,11 +92,13 @@ __global__ void k_kdist_column(DevView v, uint32_t kidx, float* __restrict__ kco
     kcol[i] = kd;
 }
 
-// dynamic shared memory: q[dim] | keys[kHS] | cnt[kHS] (threshold > 1 only) |
-// stage[warps][32] | acc[kACap] | ctl[8]
-__host__ size_t bc_cta_smem(uint32_t dim, bool counts) {
-    return (size_t)dim * 4 + (size_t)kHS * 4 + (counts ? (size_t)kHS * 4 : 0) + (kBCThreads / 32) * 64 * 4 +
-           (size_t)kACap * 4 + 64;
+__host__ __device__ constexpr uint32_t table_max(bool counts, bool mixed) { return mixed && !counts ? 16384 : 8192; }
+
+// dynamic shared memory: q[dim] | keys[H] | cnt[H] (threshold > 1 only) |
+// stage[warps][32] | acc[kACap] | ctl[8], H = table_max(counts, mixed)
+__host__ size_t bc_cta_smem(uint32_t dim, bool counts, bool mixed) {
+    const size_t H = table_max(counts, mixed);
+    return (size_t)dim * 4 + H * 4 + (counts ? H * 4 : 0) + (kBCThreads / 32) * 64 * 4 + (size_t)kACap * 4 + 64;
 }
 
 constexpr float kTieUlps = 16.f;  // FP64 re-decision band around the radius, in ulps of kd
@@ -110,8 +116,9 @@ __global__ void __launch_bounds__(kBCThreads) k_phase_bc_cta(
     constexpr int NW = kBCThreads / 32;
     float* q = (float*)smraw;
     uint32_t* keys = (uint32_t*)(q + v.dim);
-    uint32_t* cnt = keys + kHS;
-    uint32_t* stage = COUNTS ? cnt + kHS : cnt;
+    constexpr uint32_t HM = table_max(COUNTS, MIXED);
+    uint32_t* cnt = keys + HM;
+    uint32_t* stage = COUNTS ? cnt + HM : cnt;
     uint32_t* acc = stage + NW * 64;
     uint32_t* ctl = acc + kACap;  // 0: query, 1: accepted count, 2: overflow, 3: table full
     unsigned long long c_post = 0, c_cand = 0, c_ver = 0, c_res = 0;
@@ -129,14 +136,17 @@ __global__ void __launch_bounds__(kBCThreads) k_phase_bc_cta(
             continue;
         }
         for (uint32_t i = tid; i < v.dim; i += kBCThreads) q[i] = Q[(size_t)qi * v.dim + i];
-        const uint32_t P = (uint32_t)((T + kPartTarget - 1) / kPartTarget);
+        uint32_t HS = 1024;
+        while (HS < HM && (uint64_t)HS * 2 / 5 < T) HS <<= 1;
+        const uint32_t part_cap = HS * 2 / 5;
+        const uint32_t P = (uint32_t)((T + part_cap - 1) / part_cap);
         const uint32_t width = (v.n + P - 1) / P;
         const uint64_t ro = res_off[qi];
         uint32_t written = 0;
         bool overflow = false;
         for (uint32_t part = 0; part < P && !overflow; ++part) {
             const uint32_t lo = part * width, hi = min(v.n, lo + width);
-            for (uint32_t i = tid; i < kHS; i += kBCThreads) {
+            for (uint32_t i = tid; i < HS; i += kBCThreads) {
                 keys[i] = kInvalid;
                 if (COUNTS) cnt[i] = 0;
             }
@@ -154,7 +164,7 @@ __global__ void __launch_bounds__(kBCThreads) k_phase_bc_cta(
                 for (uint32_t e = tid; e < len; e += kBCThreads) {
                     const uint32_t o = owner_of<E>(v.csr_ent, b + e, v.rank_bits);
                     if (o < lo || o >= hi) continue;
-                    uint32_t slot = hash32(o) & (kHS - 1);
+                    uint32_t slot = hash32(o) & (HS - 1);
                     uint32_t probes = 0;
                     for (;;) {
                         uint32_t old = atomicCAS(&keys[slot], kInvalid, o);
@@ -162,8 +172,8 @@ __global__ void __launch_bounds__(kBCThreads) k_phase_bc_cta(
                             if (COUNTS) atomicAdd(&cnt[slot], 1u);
                             break;
                         }
-                        slot = (slot + 1) & (kHS - 1);
-                        if (++probes >= kHS) {
+                        slot = (slot + 1) & (HS - 1);
+                        if (++probes >= HS) {
                             ctl[3] = 1;
                             break;
                         }
@@ -287,7 +297,7 @@ __global__ void __launch_bounds__(kBCThreads) k_phase_bc_cta(
                 }
                 __syncwarp();
             };
-            for (uint32_t base = w * 32; base < kHS; base += NW * 32) {
+            for (uint32_t base = w * 32; base < HS; base += NW * 32) {
                 const uint32_t s = base + lane;
                 const uint32_t key = keys[s];
                 bool valid = key != kInvalid;

@@ -50,7 +50,7 @@ __global__ void k_budget_decide(const float* z, uint32_t nq, float conf, uint32_
                                 uint32_t* fb_list, uint32_t* fb_count, unsigned long long* levels);
 void ensure_projection(Index& ix, Budget& b);
 __global__ void k_kdist_column(DevView v, uint32_t kidx, float* kcol);
-size_t bc_cta_smem(uint32_t dim, bool counts);
+size_t bc_cta_smem(uint32_t dim, bool counts, bool mixed);
 
 namespace {
 
@@ -497,7 +497,7 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
         k_kdist_column<<<(unsigned)((ix.cur + 255) / 256), 256, 0, s>>>(v, kidx, ix.kcol.as<float>());
         CUDA_LAUNCH_CHECK();
         const bool counts = a.threshold > 1.0f;
-        const size_t smem = bc_cta_smem(v.dim, counts);
+        const size_t smem = bc_cta_smem(v.dim, counts, mixed);
         KCta kc = ix.wide ? pick_bc<uint64_t>(fusedsimd, counts, mixed) : pick_bc<uint32_t>(fusedsimd, counts, mixed);
         CUDA_CHECK(cudaFuncSetAttribute(kc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         int per_sm = 1;
