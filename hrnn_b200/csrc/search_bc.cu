@@ -29,9 +29,7 @@ namespace {
 // Candidate table: a power of two of slots, sized per query between 1024 and
 // table_max for a load of at most 0.4 postings per slot; queries with more
 // postings split the owner-id range into parts (one pass over the postings
-// each).  The mixed-precision kernel, whose registers already hold it to three
-// CTAs per SM, takes 16384 slots; the exact kernel keeps 8192 so that the
-// table's shared memory does not cut it below four.
+// each).  (16384-slot tables measured slower at m = 3 and no faster at m = 5.)
 constexpr uint32_t kACap = 1024;      // accepted per range
 constexpr int kBCThreads = 256;
 
@@ -92,7 +90,7 @@ __global__ void k_kdist_column(DevView v, uint32_t kidx, float* __restrict__ kco
     kcol[i] = kd;
 }
 
-__host__ __device__ constexpr uint32_t table_max(bool counts, bool mixed) { return mixed && !counts ? 16384 : 8192; }
+__host__ __device__ constexpr uint32_t table_max(bool, bool) { return 8192; }
 
 // dynamic shared memory: q[dim] | keys[H] | cnt[H] (threshold > 1 only) |
 // stage[warps][32] | acc[kACap] | ctl[8], H = table_max(counts, mixed)
