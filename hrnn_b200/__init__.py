@@ -33,7 +33,7 @@ EXPORTS = [
     "hrnn_get_search_stats", "hrnn_get_refine_stats", "hrnn_set_precision", "hrnn_set_l2_order", "hrnn_detect_l2_order", "hrnn_get_knng",
     "hrnn_set_knng", "hrnn_get_rknng", "hrnn_l2_batch", "hrnn_build_rknng_noalloc",
     "hrnn_set_budget", "hrnn_budget_features", "hrnn_budget_train", "hrnn_budget_predict",
-    "hrnn_budget_gradients", "hrnn_budget_get_weights", "hrnn_budget_set_weights",
+    "hrnn_budget_gradients", "hrnn_budget_get_weights", "hrnn_budget_set_weights", "hrnn_get_dynamic_stats",
 ]
 
 # Learned-budget MLP: 256 -> 256 -> 256 -> 2; parameters W1 b1 W2 b2 W3 b3 (row-major
@@ -82,6 +82,14 @@ class RefineStats(C.Structure):
         return {"iters": k, **{f: list(getattr(self, f))[:k] for f, _ in self._fields_[1:]}}
 
 
+class DynamicStats(C.Structure):
+    _fields_ = [(f, C.c_uint64) for f in ("n_inserted", "n_batches", "n_dist", "n_proposals", "n_updates")] + [
+        (f, C.c_double) for f in ("insert_ms", "rknng_ms", "maintain_ms")]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
 _vp = C.c_void_p
 _sz = C.c_size_t
 _lib.hrnn_last_error.restype = C.c_char_p
@@ -104,6 +112,7 @@ _lib.hrnn_set_ef.argtypes = [_vp, _sz]
 _lib.hrnn_get_info.argtypes = [_vp, C.POINTER(Info)]
 _lib.hrnn_get_search_stats.argtypes = [_vp, C.POINTER(SearchStats)]
 _lib.hrnn_get_refine_stats.argtypes = [_vp, C.POINTER(RefineStats)]
+_lib.hrnn_get_dynamic_stats.argtypes = [_vp, C.POINTER(DynamicStats)]
 _lib.hrnn_set_precision.argtypes = [_vp, C.c_int]
 _lib.hrnn_set_l2_order.argtypes = [_vp, C.c_int, C.c_int]
 _lib.hrnn_detect_l2_order.argtypes = [C.POINTER(C.c_int), C.POINTER(C.c_int)]
@@ -343,6 +352,11 @@ class HRNN:
     def last_search_stats(self) -> dict:
         s = SearchStats()
         _check(_lib.hrnn_get_search_stats(self._h, C.byref(s)))
+        return s.as_dict()
+
+    def last_dynamic_stats(self) -> dict:
+        s = DynamicStats()
+        _check(_lib.hrnn_get_dynamic_stats(self._h, C.byref(s)))
         return s.as_dict()
 
     def last_refine_stats(self) -> dict:

@@ -369,6 +369,14 @@ hrnn_status hrnn_budget_set_weights(hrnn_index* h, const float* params) {
     });
 }
 
+hrnn_status hrnn_get_dynamic_stats(hrnn_index* h, hrnn_dynamic_stats* st) {
+    return guard([&] {
+        need(h, "index");
+        need(st, "stats");
+        *st = h->ix.dyn_stats;
+    });
+}
+
 hrnn_status hrnn_get_refine_stats(hrnn_index* h, hrnn_refine_stats* st) {
     return guard([&] {
         need(h, "index");

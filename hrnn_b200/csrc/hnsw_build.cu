@@ -421,6 +421,9 @@ void add_points(Index& ix, const float* data, const uint64_t* labels, size_t n_a
     CUDA_CHECK(cudaStreamSynchronize(s));
     ix.cur = end;
     ix.bf16_valid = false;  // the BF16 copies are rebuilt on the next mixed-precision search
+    // The reverse lists no longer cover every point: searches need buildRKNNG first
+    // (the reference leaves its flag set and would read past its offsets array).
+    ix.rknng_built = false;
     // The device copy of the upper layers is now authoritative; mirror it back.
     if (!ix.upper.empty())
         CUDA_CHECK(cudaMemcpy(ix.upper.data(), ix.d_upper.p, ix.upper.size() * 4, cudaMemcpyDeviceToHost));

@@ -23,8 +23,7 @@ Index::~Index() {
 size_t Index::device_bytes() const {
     size_t s = 0;
     for (const DevMem* m : {&vec, &vec_bf16, &vec_norm, &adj0, &knn_hdr, &knn_ids, &knn_dist, &labels,
-                            &d_upper, &d_upper_off, &csr_off, &csr_ent, &mut_off, &mut_len, &mut_capv,
-                            &mut_ent, &kdist_serve, &counters, &io})
+                            &d_upper, &d_upper_off, &csr_off, &csr_ent, &kdist_serve, &counters, &io})
         s += m->bytes;
     for (const auto& m : scratch) s += m.bytes;
     return s;

@@ -101,12 +101,10 @@ struct Index {
     bool wide = false;
     bool csr_in_reference_order = false;  // loaded from a reference .idx
 
-    // ---- mutable reverse lists (buildRKNNG_mutable / insertPointDynamic) -
+    // ---- buildRKNNG_mutable / insertPointDynamic: the reverse lists are the
+    // CSR above, rebuilt after each batch of inserts (so they are exact).
     bool rknng_mutable = false;
-    DevMem mut_off;    // u64 [cap]: start of each list in mut_ent
-    DevMem mut_len;    // u32 [cap]
-    DevMem mut_capv;   // u32 [cap]: capacity of each list
-    DevMem mut_ent;    // u32 pool
+    hrnn_dynamic_stats dyn_stats{};
 
     // ---- serve mode (compactForServing, hrnn.h:299-364) -------------------
     bool serve_mode = false;

@@ -32,6 +32,7 @@
 #include <cstdio>
 #include <vector>
 
+#include "beam.cuh"
 #include "index.hpp"
 
 namespace hrnn {
@@ -418,7 +419,7 @@ __device__ uint32_t block_select(const float* Ld, uint32_t cnt, const uint64_t* 
 // repeated pair has the same distance); find the K-th smallest distance tau of
 // (list U survivors) by radix selection; sort the survivors at or below tau by
 // (d, source) and merge them into the list, list entries first among equal
-// distances, keeping K.  Inserted entries are marked new.
+// distances, keeping K.  Inserted entries are marked new (isnew may be null).
 __global__ void __launch_bounds__(kMT) k_merge_cta(uint32_t n, uint32_t K, const uint64_t* __restrict__ toff,
                                                    const uint64_t* __restrict__ bucket, uint32_t* __restrict__ hdr,
                                                    uint32_t* __restrict__ ids, float* __restrict__ dist,
@@ -456,7 +457,7 @@ __global__ void __launch_bounds__(kMT) k_merge_cta(uint32_t n, uint32_t K, const
         for (uint32_t j = tid; j < cnt; j += kMT) {
             Ld[j] = dist[(size_t)u * K + j];
             Li[j] = ids[(size_t)u * K + j];
-            Lf[j] = isnew[(size_t)u * K + j];
+            Lf[j] = isnew ? isnew[(size_t)u * K + j] : 0;
         }
         if (tid == 0) ctl[5] = cnt;
         for (uint64_t w0 = pb; w0 < pe; w0 += W) {
@@ -580,7 +581,7 @@ __global__ void __launch_bounds__(kMT) k_merge_cta(uint32_t n, uint32_t K, const
         for (uint32_t j = lo + tid; j < cnt; j += kMT) {
             dist[(size_t)u * K + j] = Ld[j];
             ids[(size_t)u * K + j] = Li[j];
-            isnew[(size_t)u * K + j] = Lf[j];
+            if (isnew) isnew[(size_t)u * K + j] = Lf[j];
         }
         if (tid == 0) hdr[u] = (hdr[u] & 0xFFFF0000u) | cnt;
     }
@@ -588,10 +589,214 @@ __global__ void __launch_bounds__(kMT) k_merge_cta(uint32_t n, uint32_t K, const
     if ((tid & 31) == 0 && upd) atomicAdd(nupd, upd);
 }
 
+// Groups np proposals by target (count, scan, scatter of (d, source) keys) and
+// merges each target's group into its list (k_merge_cta).  tcount / toff / tcur
+// hold n + 1 entries; `mid` is recorded between the grouping and the merge.
+void bucket_and_merge(uint32_t n, uint32_t K, const Prop* prop, unsigned long long np, DevMem& tcount, DevMem& toff,
+                      DevMem& tcur, uint64_t* bucket, DevMem& tmp, uint32_t* hdr, uint32_t* ids, float* dist,
+                      uint8_t* isnew, unsigned long long* d_nupd, uint32_t* d_nextt, size_t merge_smem,
+                      unsigned merge_grid, int nsm, cudaStream_t s, cudaEvent_t mid) {
+    CUDA_CHECK(cudaMemsetAsync(tcount.p, 0, ((size_t)n + 1) * 4, s));
+    CUDA_CHECK(cudaMemsetAsync(tcur.p, 0, ((size_t)n + 1) * 4, s));
+    const unsigned gb = (unsigned)std::min<unsigned long long>((np + 255) / 256, (unsigned long long)nsm * 32);
+    k_bucket_count<<<gb, 256, 0, s>>>(prop, np, tcount.as<uint32_t>());
+    CUDA_LAUNCH_CHECK();
+    exclusive_scan_u32_to_u64(tcount.as<uint32_t>(), toff.as<uint64_t>(), (size_t)n + 1, s, tmp);
+    k_bucket_fill<<<gb, 256, 0, s>>>(prop, np, toff.as<uint64_t>(), tcur.as<uint32_t>(), bucket);
+    CUDA_LAUNCH_CHECK();
+    if (mid) CUDA_CHECK(cudaEventRecord(mid, s));
+    CUDA_CHECK(cudaMemsetAsync(d_nextt, 0, 4, s));
+    k_merge_cta<<<merge_grid, kMT, merge_smem, s>>>(n, K, toff.as<uint64_t>(), bucket, hdr, ids, dist, isnew, d_nupd,
+                                                    d_nextt);
+    CUDA_LAUNCH_CHECK();
+}
+
 int smcount(int dev) {
     int v = 148;
     cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
     return v;
+}
+
+
+// ---- insertPointDynamic (hrnn.h:2360-2534), batched ------------------------
+//
+// The reference inserts one point at a time under per-node locks: HNSW insertion
+// with the KNN-graph seed (addPoint), registration of the point in its
+// neighbours' reverse lists, a self-query over the reverse lists of its first
+// m_update neighbours (all of them for m_update = 0) that skips the point and its
+// neighbours, and for every distinct candidate x_i an exact FP32 distance and
+// try_update_knng_evict(x_i, x_new, d) (insert when the list is not full or d is
+// below its farthest entry, evicting that entry); with `bidirectional` the new
+// point's own list becomes the K nearest of (its list U its candidates).
+//
+// Here a batch of points is inserted at once: add_points (the GPU HNSW builder),
+// a reverse-list rebuild (registers the batch in its neighbours' lists and drops
+// evicted entries exactly), then k_dyn_self_query emits the list updates of every
+// new point as proposals and bucket_and_merge applies them with the K-smallest
+// merge of the NNDescent path (the outcome of a sequence of evicting inserts).
+// Points of one batch see each other through the reverse lists but not through
+// each other's list updates; the reference's parallel insert loop has no fixed
+// order either.
+
+constexpr uint32_t kDX = 4096;  // excluded ids (the point and its list; K <= 2048)
+constexpr uint32_t kDC = 8192;  // candidate hash slots
+constexpr uint32_t kDB = 2048;  // candidates buffered before their distances are taken
+
+__device__ __forceinline__ bool hset_insert(uint32_t* h, uint32_t cap, uint32_t x) {
+    uint32_t sl = hmix(x) & (cap - 1);
+    for (uint32_t probes = 0; probes < cap; ++probes) {
+        const uint32_t old = atomicCAS(&h[sl], kInvalid, x);
+        if (old == kInvalid) return true;
+        if (old == x) return false;
+        sl = (sl + 1) & (cap - 1);
+    }
+    return false;  // full: treated as present (the callers keep the load below 0.6)
+}
+
+__device__ __forceinline__ bool hset_contains(const uint32_t* h, uint32_t cap, uint32_t x) {
+    uint32_t sl = hmix(x) & (cap - 1);
+    for (uint32_t probes = 0; probes < cap; ++probes) {
+        const uint32_t v = h[sl];
+        if (v == x) return true;
+        if (v == kInvalid) return false;
+        sl = (sl + 1) & (cap - 1);
+    }
+    return false;
+}
+
+// Exact FP32 distance of q (shared memory) to row x in the reference's order: two
+// lanes per row for the 16-lane order with dim 96/128/256, else one lane per row.
+template <bool FUSED>
+__device__ __forceinline__ void dyn_dists(const float* __restrict__ vec, uint32_t dim, int lanes, int fused,
+                                          const float* q, const uint32_t* ids, uint32_t cnt, float* out) {
+    const int lane = threadIdx.x & 31, p = lane & 1;
+    if (lanes == 16 && (dim == 128 || dim == 96 || dim == 256)) {
+        for (uint32_t r = 0; r < cnt; r += 16) {
+            const uint32_t t = r + (lane >> 1);
+            const uint32_t id = ids[t < cnt ? t : r];
+            const float* x = vec + (size_t)id * dim;
+            float d;
+            if (dim == 128) d = l2_pair16<FUSED, 8>(q, x, p);
+            else if (dim == 96) d = l2_pair16<FUSED, 6>(q, x, p);
+            else d = l2_pair16<FUSED, 16>(q, x, p);
+            if (p == 0 && t < cnt) out[t] = d;
+        }
+    } else {
+        for (uint32_t t = lane; t < cnt; t += 32) {
+            const float* x = vec + (size_t)ids[t] * dim;
+            out[t] = (lanes == 16 && dim % 16 == 0) ? l2_row16<FUSED>(q, x, dim / 16)
+                                                    : l2_thread(q, x, dim, lanes, fused);
+        }
+    }
+    __syncwarp();
+}
+
+// One CTA per new point x in [x0, x0 + nx) (handed out by *next): the self-query
+// and its proposals (x_i <- x when the distance is below x_i's farthest entry,
+// and x <- x_i under `bidir`).  The candidate hash dedups within a window of
+// about 0.6 kDC candidates; a repeat across windows only repeats a proposal,
+// which the merge drops.
+template <bool FUSED, class E>
+__global__ void __launch_bounds__(256) k_dyn_self_query(
+    const float* __restrict__ vec, uint32_t dim, int lanes, int fused, uint32_t x0, uint32_t nx,
+    const uint32_t* __restrict__ hdr, const uint32_t* __restrict__ ids, uint32_t K,
+    const uint64_t* __restrict__ csr_off, const void* __restrict__ csr_ent_v, uint32_t rb, uint32_t m_update, int bidir,
+    const float* __restrict__ thr, Prop* __restrict__ prop, unsigned long long* __restrict__ pcount,
+    unsigned long long pcap, unsigned long long* __restrict__ ndist, uint32_t* __restrict__ next) {
+    extern __shared__ __align__(16) char smraw[];
+    const E* __restrict__ csr_ent = static_cast<const E*>(csr_ent_v);
+    float* q = (float*)smraw;
+    uint32_t* xh = (uint32_t*)(q + dim);
+    uint32_t* ch = xh + kDX;
+    uint32_t* buf = ch + kDC;
+    float* bd = (float*)(buf + kDB);
+    uint32_t* ctl = (uint32_t*)(bd + kDB);  // 0 point, 1 buffered, 2 hashed since clear
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    constexpr int NW = 8;
+    unsigned long long c_dist = 0;
+    for (;;) {
+        __syncthreads();
+        if (tid == 0) ctl[0] = atomicAdd(next, 1u);
+        __syncthreads();
+        if (ctl[0] >= nx) break;
+        const uint32_t x = x0 + ctl[0];
+        const uint32_t cnt = hdr[x] & 0xFFFFu;
+        const uint32_t P = (m_update > 0 && m_update < cnt) ? m_update : cnt;
+        const float tx = thr[x];
+        for (uint32_t i = tid; i < dim; i += 256) q[i] = vec[(size_t)x * dim + i];
+        for (uint32_t i = tid; i < kDX; i += 256) xh[i] = kInvalid;
+        for (uint32_t i = tid; i < kDC; i += 256) ch[i] = kInvalid;
+        if (tid == 0) {
+            ctl[1] = 0;
+            ctl[2] = 0;
+        }
+        __syncthreads();
+        if (tid == 0) hset_insert(xh, kDX, x);
+        for (uint32_t j = tid; j < cnt; j += 256) hset_insert(xh, kDX, ids[(size_t)x * K + j]);
+        __syncthreads();
+        // distances and proposals of the buffered candidates, then an empty buffer
+        auto flush = [&]() {
+            const uint32_t nb = ctl[1];
+            for (uint32_t b0 = w * 32; b0 < nb; b0 += NW * 32) {
+                const uint32_t c = min(32u, nb - b0);
+                dyn_dists<FUSED>(vec, dim, lanes, fused, q, buf + b0, c, bd + b0);
+                uint32_t emit = 0, o = 0;
+                float d = 0.f;
+                if ((uint32_t)lane < c) {
+                    o = buf[b0 + lane];
+                    d = bd[b0 + lane];
+                    if (d < thr[o]) emit |= 1u;
+                    if (bidir && d < tx) emit |= 2u;
+                }
+                c_dist += (lane == 0) ? c : 0;
+                const uint32_t ne = __popc(emit);
+                uint32_t incl = ne;
+                for (int s2 = 1; s2 < 32; s2 <<= 1) {
+                    const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, s2);
+                    if (lane >= s2) incl += y;
+                }
+                const uint32_t wt = __shfl_sync(0xFFFFFFFFu, incl, 31);
+                if (wt) {
+                    unsigned long long base = 0;
+                    if (lane == 0) base = atomicAdd(pcount, (unsigned long long)wt);
+                    base = __shfl_sync(0xFFFFFFFFu, base, 0);
+                    unsigned long long pp = base + (incl - ne);
+                    if (emit & 1u) {
+                        if (pp < pcap) prop[pp] = Prop{o, x, d};
+                        pp++;
+                    }
+                    if ((emit & 2u) && pp < pcap) prop[pp] = Prop{x, o, d};
+                }
+            }
+            __syncthreads();
+            if (tid == 0) ctl[1] = 0;
+            if (ctl[2] + 256 > kDC * 3 / 5) {  // window full: start a new one
+                for (uint32_t i = tid; i < kDC; i += 256) ch[i] = kInvalid;
+                __syncthreads();
+                if (tid == 0) ctl[2] = 0;
+            }
+            __syncthreads();
+        };
+        for (uint32_t pi = 0; pi < P; ++pi) {
+            const uint32_t y = ids[(size_t)x * K + pi];
+            const uint64_t b = csr_off[y], e = csr_off[y + 1];
+            for (uint64_t e0 = b; e0 < e; e0 += 256) {
+                if (ctl[1] + 256 > kDB || ctl[2] + 256 > kDC * 3 / 5) flush();
+                const uint64_t idx = e0 + tid;
+                if (idx < e) {
+                    const uint32_t o = (uint32_t)(csr_ent[idx] >> rb);
+                    if (!hset_contains(xh, kDX, o) && hset_insert(ch, kDC, o)) {
+                        buf[atomicAdd(&ctl[1], 1u)] = o;
+                        atomicAdd(&ctl[2], 1u);
+                    }
+                }
+                __syncthreads();
+            }
+        }
+        flush();
+    }
+    for (int s2 = 16; s2; s2 >>= 1) c_dist += __shfl_xor_sync(0xFFFFFFFFu, c_dist, s2);
+    if (lane == 0 && c_dist) atomicAdd(ndist, c_dist);
 }
 
 }  // namespace
@@ -744,20 +949,8 @@ void refine_knng(Index& ix, int iters, int sample) {
                 continue;
             }
             if (np) {
-                CUDA_CHECK(cudaMemsetAsync(tcount.p, 0, tcount.bytes, s));
-                CUDA_CHECK(cudaMemsetAsync(tcur.p, 0, tcur.bytes, s));
-                unsigned gb = (unsigned)std::min<unsigned long long>((np + 255) / 256, (unsigned long long)nsm * 32);
-                k_bucket_count<<<gb, 256, 0, s>>>(prop.as<Prop>(), np, tcount.as<uint32_t>());
-                CUDA_LAUNCH_CHECK();
-                exclusive_scan_u32_to_u64(tcount.as<uint32_t>(), toff.as<uint64_t>(), (size_t)n + 1, s, tmp);
-                k_bucket_fill<<<gb, 256, 0, s>>>(prop.as<Prop>(), np, toff.as<uint64_t>(), tcur.as<uint32_t>(),
-                                                 bucket.as<uint64_t>());
-                CUDA_LAUNCH_CHECK();
-                CUDA_CHECK(cudaEventRecord(ev[6], s));
-                CUDA_CHECK(cudaMemsetAsync(d_nextt, 0, 4, s));
-                k_merge_cta<<<merge_grid, kMT, merge_smem, s>>>(n, K, toff.as<uint64_t>(), bucket.as<uint64_t>(),
-                                                                hdr, ids, dist, isnew.as<uint8_t>(), d_nupd, d_nextt);
-                CUDA_LAUNCH_CHECK();
+                bucket_and_merge(n, K, prop.as<Prop>(), np, tcount, toff, tcur, bucket.as<uint64_t>(), tmp, hdr, ids,
+                                 dist, isnew.as<uint8_t>(), d_nupd, d_nextt, merge_smem, merge_grid, nsm, s, ev[6]);
                 CUDA_CHECK(cudaEventRecord(ev[5], s));
                 CUDA_CHECK(cudaEventSynchronize(ev[5]));
                 t_bucket += elapsed(ev[4], ev[6]);
@@ -794,6 +987,134 @@ void refine_knng(Index& ix, int iters, int sample) {
     }
     for (auto& e : ev) cudaEventDestroy(e);
     ix.knng_built = true;                                 // hrnn.h:1861
+}
+
+void build_rknng_mutable(Index& ix) {
+    if (!ix.knng_built) fail(HRNN_ERR_STATE, "buildRKNNG_mutable: KNNG not built yet");  // hrnn.h:1943-1944
+    build_rknng(ix);
+    ix.rknng_mutable = true;
+    std::printf("    buildRKNNG_mutable: n=%zu total_entries=%zu\n", ix.cur, ix.csr_entries);
+    std::fflush(stdout);
+}
+
+void insert_dynamic(Index& ix, const float* data, const uint64_t* labels, size_t n, unsigned m_update,
+                    bool bidirectional) {
+    if (!ix.knng_built) fail(HRNN_ERR_STATE, "insertPointDynamic: KNNG not built yet");
+    if (!ix.rknng_mutable) fail(HRNN_ERR_STATE, "insertPointDynamic: buildRKNNG_mutable not called");
+    if (ix.serve_mode) fail(HRNN_ERR_STATE, "addPoint: index is in serve mode");
+    const uint32_t K = (uint32_t)ix.K;
+    if (K == 0 || K > kMaxK) fail(HRNN_ERR_ARG, "insertPointDynamic: K_knng must be in [1, 2048]");
+    if (ix.cur + n > ix.max_elements)
+        fail(HRNN_ERR_LIMIT, "The number of elements exceeds the specified limit");  // hrnn.h:1402-1404
+    hrnn_dynamic_stats st{};
+    ix.dyn_stats = st;
+    if (n == 0) return;
+    cudaStream_t s = ix.stream;
+    const int nsm = smcount(ix.device);
+    const size_t capn = ix.max_elements;
+    DevMem thr, prop, bucket, tcount, toff, tcur, tmp, ctr;
+    thr.alloc(capn * 4);
+    tcount.alloc((capn + 1) * 4);
+    toff.alloc((capn + 1) * 8);
+    tcur.alloc((capn + 1) * 4);
+    ctr.alloc(64);
+    size_t free_b = 0, total_b = 0;
+    CUDA_CHECK(cudaMemGetInfo(&free_b, &total_b));
+    const unsigned long long pcap = std::max<unsigned long long>(
+        1 << 20, std::min<unsigned long long>({(unsigned long long)n * 4096, 1ull << 30,
+                                               (unsigned long long)(free_b * 0.3 / 20)}));
+    prop.alloc(pcap * sizeof(Prop));
+    bucket.alloc(pcap * 8);
+    unsigned long long* d_pcount = ctr.as<unsigned long long>();
+    unsigned long long* d_ndist = d_pcount + 1;
+    unsigned long long* d_nupd = d_pcount + 2;
+    uint32_t* d_nextt = (uint32_t*)(d_pcount + 3);
+    uint32_t* d_next = (uint32_t*)(d_pcount + 4);
+    CUDA_CHECK(cudaMemsetAsync(ctr.p, 0, 64, s));
+    const size_t merge_smem = merge_cta_bytes(K);
+    CUDA_CHECK(cudaFuncSetAttribute(k_merge_cta, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)merge_smem));
+    int merge_per_sm = 1;
+    CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&merge_per_sm, k_merge_cta, kMT, merge_smem));
+    const unsigned merge_grid = (unsigned)(nsm * std::max(merge_per_sm, 1));
+    const size_t sq_smem = (size_t)ix.dim * 4 + (size_t)(kDX + kDC + 2 * kDB) * 4 + 64;
+    const bool fusedsimd = (ix.order.fused & 1) != 0;
+    cudaEvent_t ev[4];
+    for (auto& e : ev) CUDA_CHECK(cudaEventCreate(&e));
+    auto elapsed = [](cudaEvent_t a, cudaEvent_t b) {
+        float t = 0.f;
+        cudaEventElapsedTime(&t, a, b);
+        return (double)t;
+    };
+    uint32_t chunk = 1024;
+    size_t done = 0;
+    while (done < n) {
+        // Batches of an eighth of the index (at least 4096 points), so that later
+        // batches see the earlier ones' updates.
+        const size_t sb = std::min(n - done, std::max<size_t>(4096, ix.cur / 8));
+        const uint32_t x0 = (uint32_t)ix.cur;
+        CUDA_CHECK(cudaEventRecord(ev[0], s));
+        add_points(ix, data + done * ix.dim, labels ? labels + done : nullptr, sb);
+        CUDA_CHECK(cudaEventRecord(ev[1], s));
+        build_rknng(ix);  // the batch joins its neighbours' reverse lists
+        CUDA_CHECK(cudaEventRecord(ev[2], s));
+        const uint32_t nall = (uint32_t)ix.cur;
+        auto kq = ix.wide ? (fusedsimd ? k_dyn_self_query<true, uint64_t> : k_dyn_self_query<false, uint64_t>)
+                          : (fusedsimd ? k_dyn_self_query<true, uint32_t> : k_dyn_self_query<false, uint32_t>);
+        CUDA_CHECK(cudaFuncSetAttribute(kq, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sq_smem));
+        int sq_per_sm = 1;
+        CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sq_per_sm, kq, 256, sq_smem));
+        for (uint32_t a = 0; a < sb;) {
+            const uint32_t na = (uint32_t)std::min<size_t>(chunk, sb - a);
+            k_thresholds<<<(nall + 255) / 256, 256, 0, s>>>(ix.knn_hdr.as<uint32_t>(), ix.knn_dist.as<float>(), nall, K,
+                                                           thr.as<float>());
+            CUDA_LAUNCH_CHECK();
+            CUDA_CHECK(cudaMemsetAsync(d_pcount, 0, 8, s));
+            CUDA_CHECK(cudaMemsetAsync(d_next, 0, 4, s));
+            const unsigned grid = (unsigned)std::min<size_t>(na, (size_t)nsm * std::max(sq_per_sm, 1));
+            kq<<<grid, 256, sq_smem, s>>>(ix.vec.as<float>(), (uint32_t)ix.dim, ix.order.lanes, ix.order.fused,
+                                          x0 + a, na, ix.knn_hdr.as<uint32_t>(), ix.knn_ids.as<uint32_t>(), K,
+                                          ix.csr_off.as<uint64_t>(), ix.csr_ent.p, ix.rank_bits, m_update,
+                                          bidirectional ? 1 : 0, thr.as<float>(), prop.as<Prop>(), d_pcount, pcap,
+                                          d_ndist, d_next);
+            CUDA_LAUNCH_CHECK();
+            unsigned long long np = 0;
+            CUDA_CHECK(cudaMemcpyAsync(&np, d_pcount, 8, cudaMemcpyDeviceToHost, s));
+            CUDA_CHECK(cudaStreamSynchronize(s));
+            if (np > pcap) {  // the self-query is pure: redo this chunk smaller
+                if (chunk == 1) fail(HRNN_ERR_NOMEM, "insertPointDynamic: proposal buffer too small for one point");
+                chunk = std::max<uint32_t>(1, chunk / 4);
+                continue;
+            }
+            if (np)
+                bucket_and_merge(nall, K, prop.as<Prop>(), np, tcount, toff, tcur, bucket.as<uint64_t>(), tmp,
+                                 ix.knn_hdr.as<uint32_t>(), ix.knn_ids.as<uint32_t>(), ix.knn_dist.as<float>(), nullptr,
+                                 d_nupd, d_nextt, merge_smem, merge_grid, nsm, s, nullptr);
+            st.n_proposals += np;
+            a += na;
+            if (np < pcap / 4) chunk = std::min<uint32_t>(chunk * 2, 1u << 20);
+            else if (np > pcap / 4 * 3 && chunk > 1) chunk /= 2;
+        }
+        CUDA_CHECK(cudaEventRecord(ev[3], s));
+        CUDA_CHECK(cudaEventSynchronize(ev[3]));
+        st.insert_ms += elapsed(ev[0], ev[1]);
+        st.rknng_ms += elapsed(ev[1], ev[2]);
+        st.maintain_ms += elapsed(ev[2], ev[3]);
+        st.n_batches++;
+        done += sb;
+    }
+    CUDA_CHECK(cudaEventRecord(ev[0], s));
+    build_rknng(ix);  // reverse lists of the final graph
+    CUDA_CHECK(cudaEventRecord(ev[1], s));
+    unsigned long long hc[3] = {0, 0, 0};
+    CUDA_CHECK(cudaMemcpyAsync(hc, ctr.p, 24, cudaMemcpyDeviceToHost, s));
+    CUDA_CHECK(cudaStreamSynchronize(s));
+    st.rknng_ms += elapsed(ev[0], ev[1]);
+    for (auto& e : ev) cudaEventDestroy(e);
+    st.n_inserted = n;
+    st.n_dist = hc[1];
+    st.n_updates = hc[2];
+    ix.rknng_mutable = true;
+    ix.dyn_stats = st;
 }
 
 }  // namespace hrnn

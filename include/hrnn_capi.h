@@ -92,6 +92,18 @@ typedef struct {
     double merge_ms[HRNN_MAX_ITERS];         /* ... list merges                      */
 } hrnn_refine_stats;
 
+/* Counters of the last hrnn_insert_dynamic call. */
+typedef struct {
+    uint64_t n_inserted;     /* points added                                    */
+    uint64_t n_batches;      /* insertion batches                               */
+    uint64_t n_dist;         /* exact FP32 distances of the self-queries        */
+    uint64_t n_proposals;    /* list updates proposed                           */
+    uint64_t n_updates;      /* list entries inserted                           */
+    double insert_ms;        /* HNSW insertion and KNN-graph seeds              */
+    double rknng_ms;         /* reverse-list rebuilds                           */
+    double maintain_ms;      /* self-queries and list merges                    */
+} hrnn_dynamic_stats;
+
 /* Thread-local message of the last failing call on this thread ("" if none). */
 const char* hrnn_last_error(void);
 /* ABI version (major*10000 + minor*100 + patch). */
@@ -163,6 +175,9 @@ hrnn_status hrnn_compact_for_serving(hrnn_index* h, size_t max_k_serve);
  * hrnn.h:2360-2534, as the insert loop of src/hrnn_dynamic_test.cpp:310-331. */
 hrnn_status hrnn_insert_dynamic(hrnn_index* h, const float* data, const uint64_t* labels, size_t n,
                                 unsigned m_update, int bidirectional);
+
+/* Counters of the last hrnn_insert_dynamic call. */
+hrnn_status hrnn_get_dynamic_stats(hrnn_index* h, hrnn_dynamic_stats* st);
 
 /* setEf -- hrnn.h:226-228. */
 hrnn_status hrnn_set_ef(hrnn_index* h, size_t ef);
