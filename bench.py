@@ -114,64 +114,30 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------
-# FP64 ground truth (measurement infrastructure; FP32 screen on the GPU with a
-# rigorous margin, every decision re-made in float64)
+# Seeded synthetic inputs: Gaussian mixtures with the benchmark shapes (centres ~
+# N(0, 4 I) from default_rng(centre_seed), equal or Dirichlet(1) weights, points
+# = centre + N(0, sigma^2 I), float32).  The RkNN ground truth comes from
+# hrnn_b200.groundtruth (float64 decisions on the GPU).
 # ---------------------------------------------------------------------------
 
-def kth_radius_fp64(torch, X: np.ndarray, k: int, dev) -> np.ndarray:
-    torch.backends.cuda.matmul.allow_tf32 = False
-    n = X.shape[0]
-    Xt = torch.from_numpy(X).to(dev)
-    nx = (Xt.double() ** 2).sum(1).float()
-    X64 = torch.from_numpy(X).to(dev).double()
-    out = torch.empty(n, dtype=torch.float64, device=dev)
-    pad = k + 16
-    bad_rows = []
-    B = 2048
-    for s in range(0, n, B):
-        e = min(n, s + B)
-        D = nx[s:e, None] - 2.0 * (Xt[s:e] @ Xt.T) + nx[None, :]
-        D[torch.arange(e - s, device=dev), torch.arange(s, e, device=dev)] = float("inf")
-        vals, idx = torch.topk(D, pad, dim=1, largest=False, sorted=True)
-        ex = ((X64[s:e, None, :] - X64[idx]) ** 2).sum(2)
-        ex_sorted, _ = torch.sort(ex, dim=1)
-        kth = ex_sorted[:, k - 1]
-        out[s:e] = kth
-        # rigorous screen: every point outside the candidates has fp32 distance >= the
-        # last candidate's, and the fp32 error is below `margin`
-        margin = 1e-4 * (nx[s:e].double() + nx.max().double()) + 1e-3
-        ok = (vals[:, -1].double() - margin) > kth
-        if not bool(ok.all()):
-            bad_rows.extend((torch.nonzero(~ok).flatten() + s).tolist())
-    for r in bad_rows:  # exact full row in float64
-        d = ((X64 - X64[r]) ** 2).sum(1)
-        d[r] = float("inf")
-        out[r] = torch.kthvalue(d, k).values
-    return out.cpu().numpy()
+def mixture(n: int, d: int, C: int, sigma: float, centre_seed: int, draw_seed: int,
+            dirichlet: bool = False) -> np.ndarray:
+    rc = np.random.default_rng(centre_seed)
+    centres = rc.normal(0.0, 2.0, (C, d))
+    w = rc.dirichlet(np.ones(C)) if dirichlet else np.full(C, 1.0 / C)
+    r = np.random.default_rng(draw_seed)
+    lab = r.choice(C, size=n, p=w)
+    return (centres[lab] + r.normal(0.0, sigma, (n, d))).astype(np.float32)
 
 
-def rknn_gt_fp64(torch, X: np.ndarray, Q: np.ndarray, kth: np.ndarray, dev):
-    torch.backends.cuda.matmul.allow_tf32 = False
-    Xt = torch.from_numpy(X).to(dev)
-    X64 = Xt.double()
-    nx = (X64 ** 2).sum(1)
-    kt = torch.from_numpy(kth).to(dev)
-    res = []
-    B = 256
-    for s in range(0, Q.shape[0], B):
-        q = torch.from_numpy(Q[s:s + B]).to(dev)
-        q64 = q.double()
-        nq_ = (q64 ** 2).sum(1)
-        D = (nq_[:, None] - 2.0 * (q @ Xt.T).double() + nx[None, :])
-        margin = 1e-4 * (nq_[:, None] + nx[None, :]) + 1e-3
-        cand = torch.nonzero(D <= kt[None, :] + margin)
-        qi, xi = cand[:, 0], cand[:, 1]
-        ex = ((q64[qi] - X64[xi]) ** 2).sum(1)
-        keep = ex <= kt[xi]
-        qi, xi = qi[keep].cpu().numpy(), xi[keep].cpu().numpy()
-        for j in range(q.shape[0]):
-            res.append(np.sort(xi[qi == j]).astype(np.uint32))
-    return res
+def kth_radius_fp64(torch, X, k, dev):
+    from hrnn_b200 import groundtruth
+    return groundtruth.kth_radius_fp64(X, k, dev)
+
+
+def rknn_gt_fp64(torch, X, Q, kth, dev):
+    from hrnn_b200 import groundtruth
+    return [np.sort(ids) for ids, _ in groundtruth.rknn_fp64(X, Q, kth, dev)]
 
 
 def macro_recall(gt, res) -> float:
@@ -252,14 +218,12 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
 
     import hrnn_b200 as H
-    from oracle import data as odata
-
     def dev_sync():
         torch.cuda.synchronize(dev)
 
     t_gen = time.perf_counter()
-    X = odata.mixture(W["n"], W["d"], W["C"], W["sigma"], W["seed"], W["seed"], dirichlet=W["dirichlet"])
-    Q = odata.mixture(W["nq"], W["d"], W["C"], W["sigma"], W["seed"], W["qseed"] + rank, dirichlet=W["dirichlet"])
+    X = mixture(W["n"], W["d"], W["C"], W["sigma"], W["seed"], W["seed"], dirichlet=W["dirichlet"])
+    Q = mixture(W["nq"], W["d"], W["C"], W["sigma"], W["seed"], W["qseed"] + rank, dirichlet=W["dirichlet"])
     log(f"[bench] data {X.shape} queries {Q.shape} ({time.perf_counter() - t_gen:.1f}s)")
 
     h, build = build_index(H, W, X, dev_sync)
@@ -515,10 +479,9 @@ def _search_sets(h, Q, m, kp, ef, k, chunk=10_000):
 def train_budget(H, h, W, args, dev_sync):
     """Features and labels of `args.budget_train` seeded queries (a stream separate
     from the timed ones) in the mixed-precision form, then MLP training on the GPU."""
-    from oracle import data as odata
     t0 = time.perf_counter()
     n = args.budget_train
-    Qtr = odata.mixture(n, W["d"], W["C"], W["sigma"], W["seed"], W["qseed"] + 7919, dirichlet=W["dirichlet"])
+    Qtr = mixture(n, W["d"], W["C"], W["sigma"], W["seed"], W["qseed"] + 7919, dirichlet=W["dirichlet"])
     h.set_precision(H.PREC_BF16)
     full = _search_sets(h, Qtr, LABEL_M, W["Kp"], LABEL_EF, W["k"])
     Y = np.zeros((n, 2), np.uint8)
