@@ -130,6 +130,20 @@ def mixture(n: int, d: int, C: int, sigma: float, centre_seed: int, draw_seed: i
     return (centres[lab] + r.normal(0.0, sigma, (n, d))).astype(np.float32)
 
 
+def max_over_ranks(torch, value: float, device, world: int) -> float:
+    """Replicas report the slowest rank's time (every rank takes part)."""
+    if world <= 1:
+        return value
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_queries(W: dict, rank: int) -> np.ndarray:
+    """Each replica answers its own query stream (draw seed offset by the rank)."""
+    return mixture(W["nq"], W["d"], W["C"], W["sigma"], W["seed"], W["qseed"] + rank, dirichlet=W["dirichlet"])
+
+
 def kth_radius_fp64(torch, X, k, dev):
     from hrnn_b200 import groundtruth
     return groundtruth.kth_radius_fp64(X, k, dev)
@@ -223,7 +237,7 @@ def main():
 
     t_gen = time.perf_counter()
     X = mixture(W["n"], W["d"], W["C"], W["sigma"], W["seed"], W["seed"], dirichlet=W["dirichlet"])
-    Q = mixture(W["nq"], W["d"], W["C"], W["sigma"], W["seed"], W["qseed"] + rank, dirichlet=W["dirichlet"])
+    Q = replica_queries(W, rank)
     log(f"[bench] data {X.shape} queries {Q.shape} ({time.perf_counter() - t_gen:.1f}s)")
 
     h, build = build_index(H, W, X, dev_sync)
@@ -332,11 +346,7 @@ def main():
         dev_sync()
         torch.cuda.nvtx.range_pop()
         ck = clocks.stop() if clocks else None
-        ms = e0.elapsed_time(e1)
-        if world > 1:
-            t = torch.tensor([ms], device=dev)
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = max_over_ranks(torch, e0.elapsed_time(e1), dev, world)
         st = h.last_search_stats()
         # algorithmic bytes of the two phases (rows: 4 bytes/element FP32, 2 BF16)
         rb = 2 if prec == H.PREC_BF16 else 4
@@ -401,11 +411,7 @@ def main():
     out = None
     for _ in range(e2e_steps):
         out = h.search_rknn_batch(Qh, m_star, W["Kp"], W["ef"], threshold=1.0, k=W["k"])
-    e2e_s = time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([e2e_s], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(torch, time.perf_counter() - t0, dev, world)
     total_res = sum(len(x) for x in out)
     e2e = {"value": world * nq * e2e_steps / e2e_s, "unit": "queries/s",
            "h2d_bytes_per_step": int(nq * d * 4 + 3 * nq * 4), "d2h_bytes_per_step": int((nq + 1) * 8 + total_res * 8)}
