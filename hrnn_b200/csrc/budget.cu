@@ -164,6 +164,7 @@ void budget_predict(Index& ix, const float* feat, size_t n, float* logits) {
         b.mlp.forward(X.as<float>(), (int)c, s);
         CUDA_CHECK(cudaMemcpyAsync(logits + i0 * kMlpOut, b.mlp.z3.p, c * kMlpOut * 4, cudaMemcpyDeviceToHost, s));
         CUDA_CHECK(cudaStreamSynchronize(s));
+        b.mlp.check_tc();
     }
 }
 
@@ -188,6 +189,7 @@ float budget_gradients(Index& ix, const float* feat, const uint8_t* labels, size
     float loss = 0.f;
     CUDA_CHECK(cudaMemcpyAsync(&loss, L.p, 4, cudaMemcpyDeviceToHost, s));
     CUDA_CHECK(cudaStreamSynchronize(s));
+    b.mlp.check_tc();
     return loss;
 }
 

@@ -1,10 +1,13 @@
 // Learned search budget: a 256 -> 256 -> 256 -> 2 MLP (GELU) with BF16 weights,
 // trained and run on the device with the kernels below.
 //
-//   GEMMs: Y = X W^T + b (forward), dX = dY W, dW = dY^T X (backward), tiled in
-//   shared memory; both operands are rounded to BF16 (round to nearest) as they
-//   are staged, products are accumulated in FP32.  Master weights and Adam state
-//   are FP32.  Loss: binary cross-entropy with logits on both outputs.
+//   GEMMs: Y = X W^T + b (forward), dX = dY W, dW = dY^T X (backward); both
+//   operands are rounded to BF16 (round to nearest) as they are staged, products
+//   are accumulated in FP32.  The two 256 x 256 forward layers run on the tensor
+//   cores (tcgen05, mlp_tc.cu, GELU in the epilogue); the 2-output layer and the
+//   backward GEMMs on the CUDA cores (k_gemm, shared-memory tiles).  Master
+//   weights and Adam state are FP32.  Loss: binary cross-entropy with logits on
+//   both outputs.
 //
 // The two outputs are the logits of "the query's answer is complete with budget
 // level 0" and "... with level 1" (the levels are set by hrnn_set_budget); the
@@ -68,7 +71,6 @@ __global__ void k_gemm(const float* __restrict__ A, const float* __restrict__ B,
     }
 }
 
-__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.f + erff(x * 0.70710678f)); }
 __device__ __forceinline__ float gelu_d(float x) {
     return 0.5f * (1.f + erff(x * 0.70710678f)) + x * 0.39894228f * expf(-0.5f * x * x);
 }
@@ -81,11 +83,6 @@ __global__ void k_normalize(const float* __restrict__ x, const float* __restrict
         const int f = (int)(i % kMlpIn);
         xn[i] = __fmul_rn(__fsub_rn(x[i], nrm[f]), nrm[kMlpIn + f]);
     }
-}
-
-__global__ void k_gelu(const float* __restrict__ z, float* __restrict__ a, size_t n) {
-    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) a[i] = gelu(z[i]);
 }
 
 __global__ void k_gelu_back(const float* __restrict__ z, float* __restrict__ g, size_t n) {
@@ -172,6 +169,8 @@ void Mlp::init(uint64_t seed, cudaStream_t s) {
     for (int f = 0; f < kMlpIn; ++f) nr[kMlpIn + f] = 1.f;
     norm.alloc(nr.size() * 4);
     CUDA_CHECK(cudaMemcpyAsync(norm.p, nr.data(), nr.size() * 4, cudaMemcpyHostToDevice, s));
+    tc_err.alloc(16);
+    CUDA_CHECK(cudaMemsetAsync(tc_err.p, 0, 16, s));
     step = 0;
     ready = true;
     CUDA_CHECK(cudaStreamSynchronize(s));
@@ -196,12 +195,10 @@ void Mlp::forward(const float* X, int B, cudaStream_t s) {
     ensure_work(B);
     k_normalize<<<blocks((size_t)B * kMlpIn), 256, 0, s>>>(X, norm.as<float>(), xn.as<float>(), (size_t)B * kMlpIn);
     CUDA_LAUNCH_CHECK();
-    gemm(false, true, xn.as<float>(), w(0), z1.as<float>(), b(0), B, kMlpH, kMlpIn, kMlpIn, kMlpIn, 0.f, s);
-    k_gelu<<<blocks((size_t)B * kMlpH), 256, 0, s>>>(z1.as<float>(), a1.as<float>(), (size_t)B * kMlpH);
-    CUDA_LAUNCH_CHECK();
-    gemm(false, true, a1.as<float>(), w(1), z2.as<float>(), b(1), B, kMlpH, kMlpH, kMlpH, kMlpH, 0.f, s);
-    k_gelu<<<blocks((size_t)B * kMlpH), 256, 0, s>>>(z2.as<float>(), a2.as<float>(), (size_t)B * kMlpH);
-    CUDA_LAUNCH_CHECK();
+    // the two 256 x 256 layers on the tensor cores (GELU in the epilogue), the
+    // 2-output layer on the CUDA cores
+    mlp_layer_tc(xn.as<float>(), B, w(0), b(0), nullptr, z1.as<float>(), a1.as<float>(), true, tc_err.as<int>(), s);
+    mlp_layer_tc(a1.as<float>(), B, w(1), b(1), nullptr, z2.as<float>(), a2.as<float>(), true, tc_err.as<int>(), s);
     gemm(false, true, a2.as<float>(), w(2), z3.as<float>(), b(2), B, kMlpOut, kMlpH, kMlpH, kMlpH, 0.f, s);
 }
 
@@ -232,6 +229,12 @@ void Mlp::backward(const float* X, const uint8_t* Y, int B, float* loss, cudaStr
          0.f, s);
     k_colsum<<<1, 256, 0, s>>>(g1.as<float>(), gr[1].as<float>(), B, kMlpH);
     CUDA_LAUNCH_CHECK();
+}
+
+void Mlp::check_tc() {
+    int e = 0;
+    CUDA_CHECK(cudaMemcpy(&e, tc_err.p, 4, cudaMemcpyDeviceToHost));
+    if (e) fail(HRNN_ERR_TIMEOUT, "budget MLP: a tensor-core wait ran out");
 }
 
 void Mlp::adam(float lr, float wd, cudaStream_t s) {
@@ -273,6 +276,7 @@ float Mlp::train(const float* d_X, const uint8_t* d_Y, size_t N, int epochs, int
         float l = 0.f;
         CUDA_CHECK(cudaMemcpyAsync(&l, loss.p, 4, cudaMemcpyDeviceToHost, s));
         CUDA_CHECK(cudaStreamSynchronize(s));
+        check_tc();
         last = nb ? l / nb : 0.f;
     }
     return last;

@@ -15,6 +15,7 @@ struct Mlp {
     DevMem p[6], gr[6], m1[6], m2[6];
     size_t n[6];
     DevMem norm;  // input normalisation: mean[In], 1/std[In] (x -> (x - mean) * inv)
+    DevMem tc_err;  // set by the tensor-core layers when a bounded wait runs out
     DevMem xn, z1, a1, z2, a2, z3, g1, g2, g3;  // normalised input, activations / gradients of one batch
     int cap = 0;
     long step = 0;
@@ -28,6 +29,7 @@ struct Mlp {
     void forward(const float* X, int B, cudaStream_t s);  // logits in z3
     void backward(const float* X, const uint8_t* Y, int B, float* loss, cudaStream_t s);
     void adam(float lr, float wd, cudaStream_t s);
+    void check_tc();  // after a synchronisation: fails if a tensor-core wait ran out
     float train(const float* d_X, const uint8_t* d_Y, size_t N, int epochs, int batch, float lr, uint64_t seed,
                 cudaStream_t s);  // d_X raw features; the model must be initialised
 };
@@ -43,6 +45,10 @@ struct Budget {
     DevMem feat, decided, fallback_list, proxd;  // per-call work buffers
     unsigned long long n_level[3] = {0, 0, 0};  // queries served at level 0 / 1 / fallback (last call)
 };
+
+// mlp_tc.cu: tcgen05 layer out = act(norm(A) W^T + b), A [M x 256], W [256 x 256]
+void mlp_layer_tc(const float* A, int M, const float* W, const float* bias, const float* nrm, float* out_z,
+                  float* out_a, bool gelu, int* err, cudaStream_t s);
 
 // search_plain.cu
 Budget& budget_of(Index& ix);

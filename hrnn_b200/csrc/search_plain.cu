@@ -561,8 +561,10 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
     CUDA_CHECK(cudaStreamSynchronize(s));
     SearchCounters hc{};
     CUDA_CHECK(cudaMemcpy(&hc, ix.counters.p, sizeof(hc), cudaMemcpyDeviceToHost));
-    if (learned)
+    if (learned) {
         CUDA_CHECK(cudaMemcpy(ix.budget->n_level, ix.budget->decided.as<char>() + 8, 24, cudaMemcpyDeviceToHost));
+        ix.budget->mlp.check_tc();
+    }
     hrnn_search_stats st{};
     st.n_queries = nq;
     st.n_dist = hc.n_dist;
