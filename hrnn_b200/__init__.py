@@ -22,7 +22,7 @@ if not os.path.exists(LIB_PATH):
 _lib = C.CDLL(LIB_PATH)
 
 OK, ERR_ARG, ERR_STATE, ERR_IO, ERR_FORMAT, ERR_CUDA, ERR_NOMEM, ERR_CAPACITY, ERR_LIMIT, ERR_TIMEOUT = range(10)
-PREC_FP32_EXACT, PREC_BF16 = 0, 1
+PREC_FP32_EXACT, PREC_BF16, PREC_INT8 = 0, 1, 2
 
 # Every symbol include/hrnn_capi.h declares.
 EXPORTS = [

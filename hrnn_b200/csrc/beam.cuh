@@ -36,6 +36,8 @@ struct DevView {
     const uint16_t* vec_bf16;  // mixed precision: BF16 rows (or null)
     const float* vec_err;      // ||x - bf16(x)||_2, rounded up
     const uint32_t* knn_ids;   // KNN slot ids (FP64 radius re-decision)
+    const int8_t* vec_i8;      // INT8 beam: rows round(x / s) (or null)
+    const float4* i8_meta;     // (s, ||x - s c||, sum c^2, 0) per row
     uint32_t n, dim, nb, W0, WU, K, mks, rank_bits;
     int maxlevel;
     uint32_t enterpoint;
@@ -200,17 +202,25 @@ struct WarpSmem {
     float* nd;       // neighbour distances
     uint32_t* ni;    // neighbour ids
     uint32_t* apos;  // accepted insertion points
+    int* q8;         // INT8 beam: the query as packed int8 words (dim / 4)
+    float4* qm;      // (s_q^2 sum q8^2, s_q, ||q - s_q q8||, 0)
 };
 
 __host__ __device__ inline size_t warp_smem_bytes(uint32_t dim, uint32_t efc, uint32_t vc) {
     // multiple of 16 for dim % 4 == 0 and efc % 32 == 0 (q is read as float4)
-    return (size_t)dim * 4 + (size_t)(efc + 32) * 8 + (size_t)vc * 4 + 32 * 12 + 16;
+    return (size_t)dim * 4 + (((size_t)dim + 15) & ~(size_t)15) + 16 + (size_t)(efc + 32) * 8 + (size_t)vc * 4 +
+           32 * 12 + 16;
 }
 
+// q | q8 (dim bytes, padded to 16) | qm (16 bytes) | td | ti | vis | nd | ni | apos
 __device__ inline WarpSmem carve(char* base, uint32_t dim, uint32_t efc, uint32_t vc) {
     WarpSmem s;
     s.q = (float*)base;
     base += (size_t)dim * 4;
+    s.q8 = (int*)base;
+    base += ((size_t)dim + 15) & ~(size_t)15;
+    s.qm = (float4*)base;
+    base += 16;
     s.td = (float*)base;
     base += (size_t)(efc + 32) * 4;
     s.ti = (uint32_t*)base;
@@ -225,6 +235,14 @@ __device__ inline WarpSmem carve(char* base, uint32_t dim, uint32_t efc, uint32_
     base += 32 * 4;
     s.apos = (uint32_t*)base;
     return s;
+}
+
+// The INT8 query words and scalars that follow a warp's q (carve's layout).
+__device__ __forceinline__ const int* i8_q_words(const float* q, uint32_t dim) {
+    return reinterpret_cast<const int*>(q + dim);
+}
+__device__ __forceinline__ const float4* i8_q_meta(const float* q, uint32_t dim) {
+    return reinterpret_cast<const float4*>(reinterpret_cast<const char*>(q + dim) + ((dim + 15) & ~15u));
 }
 
 // Words of the link row of c at `level`, loaded unconditionally (no dependence on
@@ -303,6 +321,101 @@ __device__ __forceinline__ float bf16_thread(const float* __restrict__ q, const 
     return s;
 }
 
+// ---------------------------------------------------------------------------
+// INT8 rows (INT8 beam): x ~ s c, c in [-127, 127]; the query is quantised the
+// same way (s_q, q8) by the warp that searches it.  The approximate squared
+// distance ||s_q q8 - s c||^2 = s_q^2 sum q8^2 + s^2 sum c^2 - 2 s_q s (q8 . c)
+// takes integer dot products (dp4a) only; it ranks the beam, nothing else.
+// ---------------------------------------------------------------------------
+
+// The warp quantises s.q (FP32, dim floats) into s.q8 / s.qm.
+__device__ __forceinline__ void i8_prep_query(const WarpSmem& s, uint32_t dim) {
+    const int lane = threadIdx.x & 31;
+    float mx = 0.f;
+    for (uint32_t j = lane; j < dim; j += 32) mx = fmaxf(mx, fabsf(s.q[j]));
+    for (int o = 16; o; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, o));
+    const float sc = mx > 0.f ? mx / 127.f : 1.f;
+    int8_t* q8b = reinterpret_cast<int8_t*>(s.q8);
+    double e2 = 0.0;
+    int c2 = 0;
+    for (uint32_t j = lane; j < dim; j += 32) {
+        const int c = max(-127, min(127, __float2int_rn(s.q[j] / sc)));
+        q8b[j] = (int8_t)c;
+        const double dlt = (double)s.q[j] - (double)sc * (double)c;
+        e2 += dlt * dlt;
+        c2 += c * c;
+    }
+    for (int o = 16; o; o >>= 1) {
+        e2 += __shfl_xor_sync(0xFFFFFFFFu, e2, o);
+        c2 += __shfl_xor_sync(0xFFFFFFFFu, c2, o);
+    }
+    if (lane == 0) *s.qm = make_float4(sc * sc * (float)c2, sc, __double2float_ru(sqrt(e2)), 0.f);
+    __syncwarp();
+}
+
+// NW 16-byte words of one row (dim = 16 NW), all loaded before the dot products.
+template <int NW>
+__device__ __forceinline__ float i8_row(const int* __restrict__ q8, float4 qm, const int8_t* __restrict__ x,
+                                        float4 xm) {
+    const int4* x4 = reinterpret_cast<const int4*>(x);
+    int4 a[NW];
+#pragma unroll
+    for (int c = 0; c < NW; ++c) a[c] = __ldg(x4 + c);
+    int dot = 0;
+#pragma unroll
+    for (int c = 0; c < NW; ++c) {
+        dot = __dp4a(a[c].x, q8[4 * c + 0], dot);
+        dot = __dp4a(a[c].y, q8[4 * c + 1], dot);
+        dot = __dp4a(a[c].z, q8[4 * c + 2], dot);
+        dot = __dp4a(a[c].w, q8[4 * c + 3], dot);
+    }
+    return qm.x + xm.x * xm.x * xm.z - 2.f * qm.y * xm.x * (float)dot;
+}
+
+template <int NW>
+__device__ __forceinline__ void warp_i8_rows(const DevView& v, const int* q8, float4 qm, const uint32_t* ids,
+                                             uint32_t cnt, float* dout) {
+    const int lane = threadIdx.x & 31;
+    for (uint32_t r = 0; r < cnt; r += 32) {
+        const uint32_t t = r + lane;
+        const uint32_t id = ids[t < cnt ? t : r];
+        const float d = i8_row<NW>(q8, qm, v.vec_i8 + (size_t)id * v.dim, __ldg(v.i8_meta + id));
+        if (t < cnt) dout[t] = d;
+    }
+}
+
+__device__ __forceinline__ void warp_i8_list(const DevView& v, const int* q8, float4 qm, const uint32_t* ids,
+                                             uint32_t cnt, float* dout) {
+    // dim = 16 NW exactly (the precision setter allows multiples of 16 up to 256)
+    switch (v.dim >> 4) {
+#define HRNN_I8_CASE(W) \
+    case W: warp_i8_rows<W>(v, q8, qm, ids, cnt, dout); break;
+        HRNN_I8_CASE(1) HRNN_I8_CASE(2) HRNN_I8_CASE(3) HRNN_I8_CASE(4) HRNN_I8_CASE(5) HRNN_I8_CASE(6)
+        HRNN_I8_CASE(7) HRNN_I8_CASE(8) HRNN_I8_CASE(9) HRNN_I8_CASE(10) HRNN_I8_CASE(11) HRNN_I8_CASE(12)
+        HRNN_I8_CASE(13) HRNN_I8_CASE(14) HRNN_I8_CASE(15) HRNN_I8_CASE(16)
+#undef HRNN_I8_CASE
+        default: break;
+    }
+    __syncwarp();
+}
+
+// One row scored by every lane (the entry point of a search).
+__device__ __forceinline__ float i8_one(const DevView& v, const float* q, uint32_t id) {
+    const int* q8 = i8_q_words(q, v.dim);
+    const float4 qm = *i8_q_meta(q, v.dim);
+    const int8_t* x = v.vec_i8 + (size_t)id * v.dim;
+    const float4 xm = __ldg(v.i8_meta + id);
+    switch (v.dim >> 4) {
+#define HRNN_I8_ONE(W) \
+    case W: return i8_row<W>(q8, qm, x, xm);
+        HRNN_I8_ONE(1) HRNN_I8_ONE(2) HRNN_I8_ONE(3) HRNN_I8_ONE(4) HRNN_I8_ONE(5) HRNN_I8_ONE(6)
+        HRNN_I8_ONE(7) HRNN_I8_ONE(8) HRNN_I8_ONE(9) HRNN_I8_ONE(10) HRNN_I8_ONE(11) HRNN_I8_ONE(12)
+        HRNN_I8_ONE(13) HRNN_I8_ONE(14) HRNN_I8_ONE(15) HRNN_I8_ONE(16)
+#undef HRNN_I8_ONE
+        default: return 0.f;
+    }
+}
+
 template <int NB>
 __device__ __forceinline__ void warp_bf16_pairs(const DevView& v, const float* q, const uint32_t* ids, uint32_t cnt,
                                                 float* dout) {
@@ -319,7 +432,10 @@ __device__ __forceinline__ void warp_bf16_pairs(const DevView& v, const float* q
 template <int DM>
 __device__ __forceinline__ void warp_dist_list(const DevView& v, const float* q, const uint32_t* ids, uint32_t cnt,
                                                float* dout) {
-    if constexpr (DM < 2) {
+    if constexpr (DM == 3) {
+        // q is the warp's s.q; its INT8 copy and (s_q^2 sum q8^2, s_q, e_q) follow it
+        warp_i8_list(v, i8_q_words(q, v.dim), *i8_q_meta(q, v.dim), ids, cnt, dout);
+    } else if constexpr (DM < 2) {
         warp_l2_list<DM == 1>(v, q, ids, cnt, dout);
     } else {
         const int lane = threadIdx.x & 31;
@@ -336,6 +452,8 @@ template <int DM>
 __device__ __forceinline__ float warp_dist_one(const DevView& v, const float* q, uint32_t id) {
     if constexpr (DM < 2) {
         return warp_l2_one<DM == 1>(v, q, id);
+    } else if constexpr (DM == 3) {
+        return i8_one(v, q, id);
     } else {
         return bf16_thread(q, v.vec_bf16 + (size_t)id * v.dim, v.dim);
     }

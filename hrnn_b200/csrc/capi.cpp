@@ -280,8 +280,10 @@ hrnn_status hrnn_get_search_stats(hrnn_index* h, hrnn_search_stats* st) {
 hrnn_status hrnn_set_precision(hrnn_index* h, int precision) {
     return guard([&] {
         need(h, "index");
-        if (precision != HRNN_PREC_FP32_EXACT && precision != HRNN_PREC_BF16)
+        if (precision != HRNN_PREC_FP32_EXACT && precision != HRNN_PREC_BF16 && precision != HRNN_PREC_INT8)
             hrnn::fail(HRNN_ERR_ARG, "set_precision: unknown precision");
+        if (precision == HRNN_PREC_INT8 && (h->ix.dim % 16 != 0 || h->ix.dim > 256))
+            hrnn::fail(HRNN_ERR_ARG, "set_precision: INT8 needs dim a multiple of 16, at most 256");
         h->ix.precision = precision;
     });
 }

@@ -420,7 +420,8 @@ void add_points(Index& ix, const float* data, const uint64_t* labels, size_t n_a
     }
     CUDA_CHECK(cudaStreamSynchronize(s));
     ix.cur = end;
-    ix.bf16_valid = false;  // the BF16 copies are rebuilt on the next mixed-precision search
+    ix.bf16_valid = false;  // the BF16 / INT8 copies are rebuilt on the next search that uses them
+    ix.i8_valid = false;
     // The reverse lists no longer cover every point: searches need buildRKNNG first
     // (the reference leaves its flag set and would read past its offsets array).
     ix.rknng_built = false;

@@ -22,7 +22,7 @@ Index::~Index() {
 
 size_t Index::device_bytes() const {
     size_t s = 0;
-    for (const DevMem* m : {&vec, &vec_bf16, &vec_norm, &adj0, &knn_hdr, &knn_ids, &knn_dist, &labels,
+    for (const DevMem* m : {&vec, &vec_bf16, &vec_norm, &vec_i8, &i8_meta, &adj0, &knn_hdr, &knn_ids, &knn_dist, &labels,
                             &d_upper, &d_upper_off, &csr_off, &csr_ent, &kdist_serve, &counters, &io})
         s += m->bytes;
     for (const auto& m : scratch) s += m.bytes;

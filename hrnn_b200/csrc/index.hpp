@@ -85,6 +85,9 @@ struct Index {
     DevMem vec_bf16;   // bf16 [cap][dim] (mixed-precision search), built on demand
     DevMem vec_norm;   // f32 [cap]: ||x||, mixed-precision error bounds
     bool bf16_valid = false;
+    DevMem vec_i8;     // int8 [cap][dim]: round(x / s), s = max|x| / 127 (INT8 beam), built on demand
+    DevMem i8_meta;    // float4 [cap]: s, ||x - s c||_2 rounded up, sum c^2, 0
+    bool i8_valid = false;
     DevMem adj0;       // u32 [cap][1+maxM0]: raw level-0 link words
     DevMem knn_hdr;    // u32 [cap]: raw KNN-slot count word (count in low 16 bits)
     DevMem knn_ids;    // u32 [cap][K]

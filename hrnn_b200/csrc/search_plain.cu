@@ -41,6 +41,7 @@ KCta pick_bc(bool f, bool c, bool x) {
              : (c ? k_phase_bc_cta<E, false, true, false> : k_phase_bc_cta<E, false, false, false>);
 }
 void ensure_bf16(Index& ix);  // mixed.cu
+void ensure_i8(Index& ix);    // mixed.cu
 // budget.cu
 __global__ void k_budget_features(DevView v, const float* Q, uint32_t nq, const uint32_t* prox, const float* proxd,
                                   const uint32_t* nprox, uint32_t stride, const float* kcol, const float* proj,
@@ -54,7 +55,8 @@ size_t bc_cta_smem(uint32_t dim, bool counts, bool mixed);
 
 namespace {
 
-// DM: distance mode of beam.cuh (0/1 exact FP32 unfused/fused, 2 BF16 rows).
+// DM: distance mode of beam.cuh (0/1 exact FP32 unfused/fused, 2 BF16 rows, 3
+// INT8 rows against the INT8-quantised query).
 template <int DM>
 __global__ void __launch_bounds__(128) k_phase_a(DevView v, const float* __restrict__ Q, uint32_t nq,
                                                  const uint32_t* __restrict__ qm, const uint32_t* __restrict__ qef,
@@ -88,6 +90,7 @@ __global__ void __launch_bounds__(128) k_phase_a(DevView v, const float* __restr
         }
         for (uint32_t i = lane; i < v.dim; i += 32) s.q[i] = Q[(size_t)qi * v.dim + i];
         __syncwarp();
+        if constexpr (DM == 3) i8_prep_query(s, v.dim);
         uint32_t cur = v.enterpoint;
         float curd = warp_dist_one<DM>(v, s.q, cur);
         c_dist++;
@@ -317,6 +320,8 @@ DevView make_view(Index& ix) {
     v.labels = ix.labels.as<uint64_t>();
     v.vec_bf16 = ix.bf16_valid ? ix.vec_bf16.as<uint16_t>() : nullptr;
     v.vec_err = ix.bf16_valid ? ix.vec_norm.as<float>() : nullptr;
+    v.vec_i8 = ix.i8_valid ? ix.vec_i8.as<int8_t>() : nullptr;
+    v.i8_meta = ix.i8_valid ? ix.i8_meta.as<float4>() : nullptr;
     v.knn_ids = ix.knn_ids.as<uint32_t>();
     v.n = (uint32_t)ix.cur;
     v.dim = (uint32_t)ix.dim;
@@ -398,16 +403,16 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
     const bool fusedsimd = (ix.order.fused & 1) != 0;
     // Mixed precision (hrnn_set_precision): BF16 rows for the beam and the
     // verification screen; decisions still exact (FP32 / FP64 band).
-    const bool mixed = ix.precision == HRNN_PREC_BF16 && (v.dim == 96 || v.dim == 128 || v.dim == 256) &&
-                       v.lanes == 16;
-    if (mixed) {
-        ensure_bf16(ix);
-        v = make_view(ix);
-    }
+    const bool mixed = (ix.precision == HRNN_PREC_BF16 || ix.precision == HRNN_PREC_INT8) &&
+                       (v.dim == 96 || v.dim == 128 || v.dim == 256) && v.lanes == 16;
+    const bool int8 = ix.precision == HRNN_PREC_INT8 && v.dim % 16 == 0 && v.dim <= 256;
+    if (mixed) ensure_bf16(ix);
+    if (int8) ensure_i8(ix);
+    if (mixed || int8) v = make_view(ix);
     const int nsm = sms(ix.device);
     CUDA_CHECK(cudaEventRecord(ev[0], s));
     {
-        auto kern = mixed ? k_phase_a<2> : (fusedsimd ? k_phase_a<1> : k_phase_a<0>);
+        auto kern = int8 ? k_phase_a<3> : mixed ? k_phase_a<2> : (fusedsimd ? k_phase_a<1> : k_phase_a<0>);
         CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_a));
         // Persistent grid (every resident block), queries handed out by counters.
         int per_sm = 1;
@@ -619,9 +624,11 @@ void budget_features(Index& ix, const float* d_q, size_t nq, uint32_t k, uint32_
     if (m == 0 || std::max(m, ef) > (1u << 16)) fail(HRNN_ERR_ARG, "budget_features: need 1 <= m, ef <= 65536");
     cudaStream_t s = ix.stream;
     ix.sync_upper_to_device();
-    const bool mixed = ix.precision == HRNN_PREC_BF16 && (ix.dim == 96 || ix.dim == 128 || ix.dim == 256) &&
-                       ix.order.lanes == 16;
+    const bool mixed = (ix.precision == HRNN_PREC_BF16 || ix.precision == HRNN_PREC_INT8) &&
+                       (ix.dim == 96 || ix.dim == 128 || ix.dim == 256) && ix.order.lanes == 16;
+    const bool int8 = ix.precision == HRNN_PREC_INT8 && ix.dim % 16 == 0 && ix.dim <= 256;
     if (mixed) ensure_bf16(ix);
+    if (int8) ensure_i8(ix);
     DevView v = make_view(ix);
     ensure_projection(ix, b);
     const uint32_t mmax = std::max<uint32_t>(m, kFrontier), efc = (std::max(m, ef) + 31) & ~31u, vc = 1024;
@@ -638,7 +645,7 @@ void budget_features(Index& ix, const float* d_q, size_t nq, uint32_t k, uint32_
     ix.kcol.ensure((size_t)std::max<size_t>(ix.cur, 1) * 4);
     k_kdist_column<<<(unsigned)((ix.cur + 255) / 256), 256, 0, s>>>(v, k - 1, ix.kcol.as<float>());
     CUDA_LAUNCH_CHECK();
-    auto kern = mixed ? k_phase_a<2> : (((ix.order.fused & 1) != 0) ? k_phase_a<1> : k_phase_a<0>);
+    auto kern = int8 ? k_phase_a<3> : mixed ? k_phase_a<2> : (((ix.order.fused & 1) != 0) ? k_phase_a<1> : k_phase_a<0>);
     CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_a));
     const int nsm = sms(ix.device);
     unsigned grid = (unsigned)std::max<size_t>(1, std::min<size_t>((nq + wpb - 1) / wpb, (size_t)nsm * 16));

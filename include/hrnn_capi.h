@@ -199,9 +199,14 @@ hrnn_status hrnn_get_refine_stats(hrnn_index* h, hrnn_refine_stats* st);
  *      every undecided accept/reject is re-decided with the reference's exact
  *      FP32 distance, and within 16 ulps of the radius in FP64 against the
  *      FP64 distance to the k-th neighbour.  Proxies may differ from the
- *      reference's (recall, not membership); counts in hrnn_search_stats. */
+ *      reference's (recall, not membership); counts in hrnn_search_stats.
+ *  HRNN_PREC_INT8: as HRNN_PREC_BF16, but the beam search ranks with INT8 copies
+ *      of the vectors (per-vector scale) against an INT8 copy of the query
+ *      (integer dot products): the proxies are approximate, the decisions are
+ *      made as in HRNN_PREC_BF16.  Needs dim a multiple of 16, at most 256. */
 #define HRNN_PREC_FP32_EXACT 0
 #define HRNN_PREC_BF16 1
+#define HRNN_PREC_INT8 2
 hrnn_status hrnn_set_precision(hrnn_index* h, int precision);
 
 /* Learned search budget (new; no counterpart in the reference).  A 256-256-256-2

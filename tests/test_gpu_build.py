@@ -103,10 +103,11 @@ def test_large_answer_sets_match_oracle(built):
     assert max(len(x) for x in a) > 100
 
 
-def test_mixed_precision_decisions_and_recall(built):
-    """BF16 beam + screened verification: every returned point passes the exact
-    FP32 test (or the FP64 test inside the tie band), and recall stays at the plain
-    form's level."""
+@pytest.mark.parametrize("prec", [H.PREC_BF16, H.PREC_INT8])
+def test_mixed_precision_decisions_and_recall(built, prec):
+    """BF16 (or INT8) beam + BF16-screened verification: every returned point
+    passes the exact FP32 test (or the FP64 test inside the tie band), and recall
+    stays at the plain form's level."""
     X, Q, h, p, _ = built
     f = idx.read_idx(p)
     V = f.vectors()
@@ -116,7 +117,7 @@ def test_mixed_precision_decisions_and_recall(built):
     gt = data.rknn_gt_fp64(X, Q, kth)
     plain = h.search_rknn_batch(Q, 10, 64, 100, k=10)
     try:
-        h.set_precision(H.PREC_BF16)
+        h.set_precision(prec)
         mixed = h.search_rknn_batch(Q, 10, 64, 100, k=10)
         st = h.last_search_stats()
     finally:
