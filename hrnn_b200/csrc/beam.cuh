@@ -42,6 +42,7 @@ struct DevView {
     int maxlevel;
     uint32_t enterpoint;
     int wide, lanes, fused;
+    int i8_screen;             // verification screens with the INT8 rows first
 };
 
 __device__ __forceinline__ uint32_t lanemask_lt() {

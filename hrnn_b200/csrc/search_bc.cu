@@ -93,10 +93,12 @@ __global__ void k_kdist_column(DevView v, uint32_t kidx, float* __restrict__ kco
 __host__ __device__ constexpr uint32_t table_max(bool, bool) { return 8192; }
 
 // dynamic shared memory: q[dim] | keys[H] | cnt[H] (threshold > 1 only) |
-// stage[warps][32] | acc[kACap] | ctl[8], H = table_max(counts, mixed)
+// stage[warps][32] | acc[kACap] | ctl[16] | q8 (dim bytes, padded to 16) | qm,
+// H = table_max(counts, mixed)
 __host__ size_t bc_cta_smem(uint32_t dim, bool counts, bool mixed) {
     const size_t H = table_max(counts, mixed);
-    return (size_t)dim * 4 + H * 4 + (counts ? H * 4 : 0) + (kBCThreads / 32) * 64 * 4 + (size_t)kACap * 4 + 64;
+    return (size_t)dim * 4 + H * 4 + (counts ? H * 4 : 0) + (kBCThreads / 32) * 64 * 4 + (size_t)kACap * 4 + 64 +
+           (((size_t)dim + 15) & ~(size_t)15) + 16;
 }
 
 constexpr float kTieUlps = 16.f;  // FP64 re-decision band around the radius, in ulps of kd
@@ -119,6 +121,9 @@ __global__ void __launch_bounds__(kBCThreads) k_phase_bc_cta(
     uint32_t* stage = COUNTS ? cnt + HM : cnt;
     uint32_t* acc = stage + NW * 64;
     uint32_t* ctl = acc + kACap;  // 0: query, 1: accepted count, 2: overflow, 3: table full
+    int* q8 = (int*)(ctl + 16);   // INT8 screen: the query as packed int8 words
+    float4* qm = (float4*)((char*)q8 + ((v.dim + 15) & ~15u));  // (s_q^2 sum q8^2, s_q, ||q - s_q q8||, 0)
+    const bool i8s = MIXED && v.i8_screen && v.vec_i8 != nullptr;
     unsigned long long c_post = 0, c_cand = 0, c_ver = 0, c_res = 0;
     const bool fast = v.lanes == 16 && (v.dim % 16) == 0;
     for (;;) {
@@ -134,6 +139,30 @@ __global__ void __launch_bounds__(kBCThreads) k_phase_bc_cta(
             continue;
         }
         for (uint32_t i = tid; i < v.dim; i += kBCThreads) q[i] = Q[(size_t)qi * v.dim + i];
+        if (i8s) {  // quantise the query for the INT8 screen (warp 0)
+            __syncthreads();
+            if (w == 0) {
+                float mx = 0.f;
+                for (uint32_t j = lane; j < v.dim; j += 32) mx = fmaxf(mx, fabsf(q[j]));
+                for (int o = 16; o; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, o));
+                const float sc = mx > 0.f ? mx / 127.f : 1.f;
+                int8_t* qb = reinterpret_cast<int8_t*>(q8);
+                double e2 = 0.0;
+                int c2 = 0;
+                for (uint32_t j = lane; j < v.dim; j += 32) {
+                    const int c = max(-127, min(127, __float2int_rn(q[j] / sc)));
+                    qb[j] = (int8_t)c;
+                    const double dlt = (double)q[j] - (double)sc * (double)c;
+                    e2 += dlt * dlt;
+                    c2 += c * c;
+                }
+                for (int o = 16; o; o >>= 1) {
+                    e2 += __shfl_xor_sync(0xFFFFFFFFu, e2, o);
+                    c2 += __shfl_xor_sync(0xFFFFFFFFu, c2, o);
+                }
+                if (lane == 0) *qm = make_float4(sc * sc * (float)c2, sc, __double2float_ru(sqrt(e2)), 0.f);
+            }
+        }
         uint32_t HS = 1024;
         while (HS < HM && (uint64_t)HS * 2 / 5 < T) HS <<= 1;
         const uint32_t part_cap = HS * 2 / 5;
@@ -271,7 +300,41 @@ __global__ void __launch_bounds__(kBCThreads) k_phase_bc_cta(
                     if (p == 0 && live && decision == 1) accept(id);
                 }
             };
+            // INT8 screen (one row per lane, integer dot products) in front of the
+            // BF16 one: |sqrt(d) - sqrt(D)| <= e_q + e_x with D = ||s_q q8 - s c||^2,
+            // whose FP32 evaluation is within 8 ulps of (sqrt(s_q^2 sum q8^2) +
+            // s sqrt(sum c^2))^2; what it cannot decide goes on to verify_mixed.
+            auto verify_i8 = [&](uint32_t cnt_, auto nbc, auto nwc) {
+                constexpr int NWW = decltype(nwc)::value;
+                const bool live = (uint32_t)lane < cnt_;
+                const uint32_t id = st[live ? lane : 0];
+                const float kd = __ldg(kcol + id);
+                const float4 xm = __ldg(v.i8_meta + id);
+                const float4 qv = *qm;
+                const float D = i8_row<NWW>(q8, qv, v.vec_i8 + (size_t)id * v.dim, xm);
+                const float rq = sqrtf(qv.x), rx = xm.x * sqrtf(xm.z);
+                const float ef = 8.f * 5.9604645e-8f * (rq + rx) * (rq + rx);
+                const float e = qv.z + xm.y;
+                const float rho = (4.f * v.dim + 64.f) * 5.9604645e-8f;
+                const float hi = sqrtf(D + ef) * (1.f + rho) + e;
+                const float lo = fmaxf(0.f, sqrtf(fmaxf(0.f, D - ef)) * (1.f - rho) - e);
+                const float U = hi * hi * (1.f + rho), L = lo * lo * (1.f - rho);
+                const int decision = kd == FLT_MAX ? 1 : (U < kd ? 1 : (L > kd ? 0 : -1));
+                if (live && decision >= 0) c_lowp++;
+                if (live && decision == 1) accept(id);
+                const uint32_t und = __ballot_sync(0xFFFFFFFFu, live && decision < 0);
+                __syncwarp();
+                if (live && decision < 0) st[__popc(und & lanemask_lt())] = id;
+                __syncwarp();
+                if (und) verify_mixed((uint32_t)__popc(und), nbc);
+            };
             auto verify = [&](uint32_t cnt_) {
+                if (i8s && (v.dim == 128 || v.dim == 96)) {  // the dims with an unrolled BF16 screen behind it
+                    if (v.dim == 128) verify_i8(cnt_, std::integral_constant<int, 8>{}, std::integral_constant<int, 8>{});
+                    else verify_i8(cnt_, std::integral_constant<int, 6>{}, std::integral_constant<int, 6>{});
+                    __syncwarp();
+                    return;
+                }
                 if (MIXED && v.vec_bf16) {
                     if (v.dim == 128) verify_mixed(cnt_, std::integral_constant<int, 8>{});
                     else if (v.dim == 96) verify_mixed(cnt_, std::integral_constant<int, 6>{});

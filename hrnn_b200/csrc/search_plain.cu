@@ -409,6 +409,7 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
     if (mixed) ensure_bf16(ix);
     if (int8) ensure_i8(ix);
     if (mixed || int8) v = make_view(ix);
+    v.i8_screen = (mixed && int8) ? 1 : 0;
     const int nsm = sms(ix.device);
     CUDA_CHECK(cudaEventRecord(ev[0], s));
     {
