@@ -259,6 +259,8 @@ def main():
     # GT ids are data indices; index labels are data indices too.
     nq, d = Q.shape
     forms = {"plain": H.PREC_FP32_EXACT, "mixed": H.PREC_BF16}
+    if d % 16 == 0 and d <= 256:
+        forms["mixed_int8"] = H.PREC_INT8
 
     def sweep_form(prec, stop=False):
         h.set_precision(prec)
@@ -284,27 +286,6 @@ def main():
         run_reference_arm(args, W, h, Q, params, sweeps["plain"], build)
         return
 
-    # ---- learned search budget: train on separate seeded queries (untimed) ----
-    budget_info = None
-    if not args.no_learned:
-        budget_info = train_budget(H, h, W, args, dev_sync)
-        # (confidence, fallback m) candidates: the smallest fallback m reaching the
-        # recall target at each cutoff; the fastest of them is the learned form.
-        cands = []
-        for c in CONFIDENCES:
-            BUDGET["confidence"] = c
-            h.set_budget(True, **BUDGET)
-            sw, mstar = sweep_form(H.PREC_BF16, stop=True)
-            log(f"[bench] learned (confidence {c}): recall sweep (fallback m) "
-                f"{json.dumps({k_: round(v_, 4) for k_, v_ in sw.items()})} -> m={mstar}")
-            if sw[mstar] >= TARGET_RECALL:
-                cands.append((c, mstar, sw))
-        h.set_budget(False, **BUDGET)
-        h.set_precision(H.PREC_FP32_EXACT)
-        if not cands:
-            budget_info["candidates"] = []
-            budget_info = None
-
     # ---- timed device steps, per form ----
     q_dev = torch.from_numpy(Q).to(dev)
     kp_dev = torch.full((nq,), W["Kp"], dtype=torch.int32, device=dev)
@@ -316,8 +297,9 @@ def main():
     hbm, bf16, peak_kind = load_peaks()
     maxM0 = 2 * W["M"]
 
-    def timed(prec, m_star, clocks=None, learned=False, steps=None):
+    def timed(prec, m_star, learned=False, steps=None, name=None):
         steps = steps or args.steps
+        clocks = ClockSampler(local)
         h.set_precision(prec)
         if learned:
             h.set_budget(True, **BUDGET)
@@ -333,8 +315,7 @@ def main():
         if world > 1:
             torch.distributed.barrier()
         dev_sync()
-        if clocks:
-            clocks.start()
+        clocks.start()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.nvtx.range_push("timed")  # profilers select the timed steps with this range
         e0.record(stream)
@@ -345,13 +326,15 @@ def main():
         e1.record(stream)
         dev_sync()
         torch.cuda.nvtx.range_pop()
-        ck = clocks.stop() if clocks else None
+        ck = clocks.stop()
         ms = max_over_ranks(torch, e0.elapsed_time(e1), dev, world)
         st = h.last_search_stats()
-        # algorithmic bytes of the two phases (rows: 4 bytes/element FP32, 2 BF16)
-        rb = 2 if prec == H.PREC_BF16 else 4
-        bytes_a = st["n_dist"] * d * rb + st["n_expanded"] * (4 + 4 * maxM0)
-        bytes_bc = st["n_posting"] * 4 + st["n_verified"] * (d * rb + 4 + (4 if rb == 2 else 0)) + \
+        # algorithmic bytes of the two phases: rows of 4 bytes/element (FP32), 2 (BF16)
+        # or 1 plus 16 bytes of scale / error terms (INT8); the k-distance of each
+        # verified id; the FP32 rows of the screens' undecided ids
+        rb, rm = {H.PREC_FP32_EXACT: (4, 0), H.PREC_BF16: (2, 4), H.PREC_INT8: (1, 16)}[prec]
+        bytes_a = st["n_dist"] * (d * rb + rm) + st["n_expanded"] * (4 + 4 * maxM0)
+        bytes_bc = st["n_posting"] * 4 + st["n_verified"] * (d * rb + rm + 4) + \
             st["n_fp32_decided"] * d * 4 + st["n_result"] * 8
         phases = {"phase_a_beam_search": (st["phase_a_ms"], bytes_a),
                   "phase_bc_posting_verify": (st["phase_c_ms"], bytes_bc)}
@@ -370,37 +353,54 @@ def main():
             roof["budget_levels"] = st["n_budget"]
             h.set_budget(False, **BUDGET)
         return {"qps": world * nq * steps / (ms / 1e3), "ms_per_step": ms / steps, "launches": launches,
-                "roofline": roof, "clocks": ck, "m": m_star,
-                "recall_sweep": sweeps["learned" if learned else ("mixed" if prec == H.PREC_BF16 else "plain")]}
+                "roofline": roof, "clocks": ck, "m": m_star, "prec": prec, "recall_sweep": sweeps[name]}
 
     results = {}
-    clocks = ClockSampler(local)
-    results["plain"] = timed(forms["plain"], mstars["plain"])
-    results["mixed"] = timed(forms["mixed"], mstars["mixed"], None if budget_info else clocks)
-    if budget_info:
+    for name, prec in forms.items():
+        results[name] = timed(prec, mstars[name], name=name)
+
+    # ---- learned search budget on the faster reduced-precision form: trained on
+    # separate seeded queries (untimed), then the fastest (confidence, fallback m)
+    # pair reaching the recall target ----
+    budget_info = None
+    if not args.no_learned:
+        lp = max((f for f in forms if f != "plain"), key=lambda f: results[f]["qps"])
+        lprec = forms[lp]
+        budget_info = train_budget(H, h, W, args, dev_sync, lprec)
+        budget_info["precision_form"] = lp
+        cands = []
+        for c in CONFIDENCES:
+            BUDGET["confidence"] = c
+            h.set_budget(True, **BUDGET)
+            sw, mstar = sweep_form(lprec, stop=True)
+            log(f"[bench] learned (confidence {c}): recall sweep (fallback m) "
+                f"{json.dumps({k_: round(v_, 4) for k_, v_ in sw.items()})} -> m={mstar}")
+            if sw[mstar] >= TARGET_RECALL:
+                cands.append((c, mstar, sw))
+        h.set_budget(False, **BUDGET)
+        h.set_precision(H.PREC_FP32_EXACT)
         trial = []
         for c, mstar, sw in cands:
             BUDGET["confidence"] = c
             sweeps["learned"] = sw
-            r = timed(H.PREC_BF16, mstar, learned=True, steps=3)
+            r = timed(lprec, mstar, learned=True, steps=3, name="learned")
             trial.append({"confidence": c, "m": mstar, "recall": round(sw[mstar], 4), "value": round(r["qps"], 1)})
-        best = max(trial, key=lambda t_: t_["value"])
-        BUDGET["confidence"] = best["confidence"]
-        sweeps["learned"] = next(sw for c, _, sw in cands if c == best["confidence"])
-        mstars["learned"] = best["m"]
-        budget_info["confidence"] = best["confidence"]
         budget_info["candidates"] = trial
-        results["learned"] = timed(H.PREC_BF16, mstars["learned"], clocks, learned=True)
+        if trial:
+            best = max(trial, key=lambda t_: t_["value"])
+            BUDGET["confidence"] = best["confidence"]
+            sweeps["learned"] = next(sw for c, _, sw in cands if c == best["confidence"])
+            mstars["learned"] = best["m"]
+            budget_info["confidence"] = best["confidence"]
+            results["learned"] = timed(lprec, mstars["learned"], learned=True, name="learned")
     head = max(results, key=lambda k_: results[k_]["qps"])
     R = results[head]
     qps, ms_per_step, launches, roofline, ck = R["qps"], R["ms_per_step"], R["launches"], R["roofline"], R["clocks"]
-    if ck is None:
-        ck = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
     m_star = R["m"]
     log("[bench] " + ", ".join(f"{k_} {r_['qps']:.0f} q/s (m={r_['m']})" for k_, r_ in results.items()))
 
     # ---- end to end through the host-buffer entry point (headline form) ----
-    h.set_precision(H.PREC_FP32_EXACT if head == "plain" else H.PREC_BF16)
+    h.set_precision(R["prec"])
     if head == "learned":
         h.set_budget(True, **BUDGET)
     e2e_steps = max(1, args.steps)
@@ -443,8 +443,9 @@ def main():
         "metric": "RkNN queries/s at recall>=0.95 (k=10)", "value": round(qps, 1), "unit": "queries/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": {"plain": "f32", "mixed": "bf16 screen + f32/f64 decisions",
-                  "learned": "bf16 screen + f32/f64 decisions; bf16 budget MLP"}[head],
+        "dtype": {H.PREC_FP32_EXACT: "f32", H.PREC_BF16: "bf16 screen + f32/f64 decisions",
+                  H.PREC_INT8: "int8 beam; int8/bf16 screens + f32/f64 decisions"}[R["prec"]] +
+                 ("; bf16 budget MLP" if head == "learned" else ""),
         "data": "synthetic (seeded Gaussian mixture)",
         "config": {"workload": args.workload, "n": W["n"], "dim": d, "K_knng": W["K"], "M": W["M"],
                    "ef_construction": W["efc"], "queries_per_step": nq, "form": head,
@@ -452,6 +453,7 @@ def main():
                    "recall_sweep": {str(k_): round(v, 4) for k_, v in sweep.items()},
                    "parallelism": f"replicas{world}", "l2_flush": "inputs larger than L2 (index 7 GB)"},
         "forms": {k_: {"value": round(r_["qps"], 1), "ms_per_step": round(r_["ms_per_step"], 3), "m": r_["m"],
+                       "clocks": r_["clocks"],
                        "recall_sweep": {str(a_): round(b_, 4) for a_, b_ in r_["recall_sweep"].items()},
                        "roofline": r_["roofline"]} for k_, r_ in results.items()},
         "speedup_vs_plain": round(qps / results["plain"]["qps"], 3),
@@ -482,13 +484,13 @@ def _search_sets(h, Q, m, kp, ef, k, chunk=10_000):
     return out
 
 
-def train_budget(H, h, W, args, dev_sync):
+def train_budget(H, h, W, args, dev_sync, prec):
     """Features and labels of `args.budget_train` seeded queries (a stream separate
-    from the timed ones) in the mixed-precision form, then MLP training on the GPU."""
+    from the timed ones) in the serving precision `prec`, then MLP training on the GPU."""
     t0 = time.perf_counter()
     n = args.budget_train
     Qtr = mixture(n, W["d"], W["C"], W["sigma"], W["seed"], W["qseed"] + 7919, dirichlet=W["dirichlet"])
-    h.set_precision(H.PREC_BF16)
+    h.set_precision(prec)
     full = _search_sets(h, Qtr, LABEL_M, W["Kp"], LABEL_EF, W["k"])
     Y = np.zeros((n, 2), np.uint8)
     for j, ml in enumerate((BUDGET["m0"], BUDGET["m1"])):

@@ -502,6 +502,12 @@ __device__ void greedy_descent(const DevView& v, WarpSmem& s, int top, int stop,
 // is accepted iff fewer than EF elements of (beam + accepted earlier neighbours of
 // this batch) are <= d_j, and not already in the beam; the beam stays sorted and
 // is cut to EF; cursor moves back to the first inserted position.
+//
+// A neighbour no closer than the last entry of a full beam can be dropped before
+// the rest: it would land at position EF, and it only counts against neighbours
+// that are no closer than itself.  The accepted ones are ranked by (distance,
+// lane), which orders their insertion points too, so apos[] is sorted and the
+// shift of a beam entry is a binary search over it.
 __device__ __forceinline__ void beam_insert(WarpSmem& s, const float* nd, const uint32_t* ni, uint32_t cnt,
                                             uint32_t EF, uint32_t& tsize, uint32_t& cursor) {
     const int lane = threadIdx.x & 31;
@@ -511,33 +517,38 @@ __device__ __forceinline__ void beam_insert(WarpSmem& s, const float* nd, const 
     if ((uint32_t)lane < cnt) {
         d = nd[lane];
         id = ni[lane];
+        ok = !(tsize >= EF && d >= s.td[EF - 1]);
+    }
+    if (!__ballot_sync(0xFFFFFFFFu, ok)) return;
+    if (ok) {
         pos = upper_bound(s.td, tsize, d);
-        ok = true;
         for (int k = (int)pos - 1; k >= 0 && s.td[k] == d; --k)
             if ((s.ti[k] & kIdMask) == id) {
                 ok = false;
                 break;
             }
     }
-    uint32_t okb = __ballot_sync(0xFFFFFFFFu, ok);
+    const uint32_t okb = __ballot_sync(0xFFFFFFFFu, ok);
+    if (!okb) return;
     uint32_t cp = 0;
-    for (uint32_t i = 0; i < cnt; ++i) {
-        float di = __shfl_sync(0xFFFFFFFFu, d, i);
-        if (((okb >> i) & 1u) && i < (uint32_t)lane && di <= d) cp++;
+    for (uint32_t m = okb; m; m &= m - 1) {
+        const int i = __ffs(m) - 1;
+        const float di = __shfl_sync(0xFFFFFFFFu, d, i);
+        if (i < lane && di <= d) cp++;
     }
-    bool acc = ok && (pos + cp < EF);
-    uint32_t ab = __ballot_sync(0xFFFFFFFFu, acc);
+    const bool acc = ok && (pos + cp < EF);
+    const uint32_t ab = __ballot_sync(0xFFFFFFFFu, acc);
     if (!ab) return;
-    uint32_t na = __popc(ab);
+    const uint32_t na = __popc(ab);
     uint32_t before = 0;
-    for (uint32_t i = 0; i < cnt; ++i) {
-        float di = __shfl_sync(0xFFFFFFFFu, d, i);
-        if (((ab >> i) & 1u) && (di < d || (di == d && i < (uint32_t)lane))) before++;
+    for (uint32_t m = ab; m; m &= m - 1) {
+        const int i = __ffs(m) - 1;
+        const float di = __shfl_sync(0xFFFFFFFFu, d, i);
+        if (di < d || (di == d && i < lane)) before++;
     }
-    uint32_t lo = acc ? pos : 0xFFFFFFFFu;
-    for (int o = 16; o; o >>= 1) lo = min(lo, __shfl_xor_sync(0xFFFFFFFFu, lo, o));
-    if (acc) s.apos[__popc(ab & lanemask_lt())] = pos;
+    if (acc) s.apos[before] = pos;
     __syncwarp();
+    const uint32_t lo = s.apos[0], amax = s.apos[na - 1];
     const uint32_t newsize = min(tsize + na, EF);
     // In-place merge: existing entries at or after lo move right by the number
     // of accepted neighbours inserted at or before them (at most 32), so the
@@ -552,8 +563,16 @@ __device__ __forceinline__ void beam_insert(WarpSmem& s, const float* nd, const 
             if (k < tsize) {
                 dk = s.td[k];
                 ik = s.ti[k];
-                uint32_t sh = 0;
-                for (uint32_t a = 0; a < na; ++a) sh += (s.apos[a] <= k);
+                uint32_t sh = na;
+                if (k < amax) {  // number of insertion points <= k
+                    uint32_t a = 0, e = na - 1;
+                    while (a < e) {
+                        const uint32_t mid = (a + e) >> 1;
+                        if (s.apos[mid] <= k) a = mid + 1;
+                        else e = mid;
+                    }
+                    sh = a;
+                }
                 np = k + sh;
             }
             __syncwarp();
@@ -564,7 +583,7 @@ __device__ __forceinline__ void beam_insert(WarpSmem& s, const float* nd, const 
             __syncwarp();
         }
     }
-    uint32_t npos = pos + before;
+    const uint32_t npos = pos + before;
     if (acc && npos < newsize) {
         s.td[npos] = d;
         s.ti[npos] = id;
