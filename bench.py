@@ -214,8 +214,11 @@ def main():
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-budget form")
     ap.add_argument("--build-only", action="store_true", help="build the index, print its build times, exit")
     ap.add_argument("--budget-train", type=int, default=200_000, help="training queries of the budget MLP")
+    ap.add_argument("--queries", type=int, default=0, help="queries per step (default: the workload's)")
     args = ap.parse_args()
-    W = WORKLOADS[args.workload]
+    W = dict(WORKLOADS[args.workload])
+    if args.queries > 0:
+        W["nq"] = args.queries
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -29,7 +29,10 @@ namespace {
 // Candidate table: a power of two of slots, sized per query between 1024 and
 // table_max for a load of at most 0.4 postings per slot; queries with more
 // postings split the owner-id range into parts (one pass over the postings
-// each).  (16384-slot tables measured slower at m = 3 and no faster at m = 5.)
+// each, four postings per thread in flight).  Measured at m = 3 and 5, K' = 500:
+// 4096 slots or 0.25 load take more passes and are slower; 16384 slots or 0.5 -
+// 0.75 load take fewer passes but are slower too (more probes per insertion, and
+// the larger shared-memory footprint leaves less L1 for the verified rows).
 constexpr uint32_t kACap = 1024;      // accepted per range
 constexpr int kBCThreads = 256;
 
@@ -188,21 +191,31 @@ __global__ void __launch_bounds__(kBCThreads) k_phase_bc_cta(
                 const uint32_t len = plen[(size_t)qi * mmax + pi];
                 const uint64_t b = v.csr_off[p];
                 if (part == 0) c_post += (tid == 0) ? len : 0;
-                for (uint32_t e = tid; e < len; e += kBCThreads) {
-                    const uint32_t o = owner_of<E>(v.csr_ent, b + e, v.rank_bits);
-                    if (o < lo || o >= hi) continue;
-                    uint32_t slot = hash32(o) & (HS - 1);
-                    uint32_t probes = 0;
-                    for (;;) {
-                        uint32_t old = atomicCAS(&keys[slot], kInvalid, o);
-                        if (old == kInvalid || old == o) {
-                            if (COUNTS) atomicAdd(&cnt[slot], 1u);
-                            break;
-                        }
-                        slot = (slot + 1) & (HS - 1);
-                        if (++probes >= HS) {
-                            ctl[3] = 1;
-                            break;
+                // four postings per thread loaded together, then inserted
+                for (uint32_t e0 = tid; e0 < len; e0 += 4 * kBCThreads) {
+                    uint32_t ow[4];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const uint32_t e = e0 + (uint32_t)u * kBCThreads;
+                        ow[u] = e < len ? owner_of<E>(v.csr_ent, b + e, v.rank_bits) : hi;
+                    }
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const uint32_t o = ow[u];
+                        if (o < lo || o >= hi) continue;
+                        uint32_t slot = hash32(o) & (HS - 1);
+                        uint32_t probes = 0;
+                        for (;;) {
+                            uint32_t old = atomicCAS(&keys[slot], kInvalid, o);
+                            if (old == kInvalid || old == o) {
+                                if (COUNTS) atomicAdd(&cnt[slot], 1u);
+                                break;
+                            }
+                            slot = (slot + 1) & (HS - 1);
+                            if (++probes >= HS) {
+                                ctl[3] = 1;
+                                break;
+                            }
                         }
                     }
                 }

@@ -379,7 +379,7 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
     // Visited-cache slots (lossy; a miss costs a recomputed row).  1024 rather than
     // more: the smaller per-warp shared memory keeps more warps resident, which
     // pays for the ~10% extra rows at ef = 200.
-    const uint32_t vc = 1024;
+    const uint32_t vc = 512;
     size_t wsm = warp_smem_bytes(v.dim, efc, vc);
     int wpb = (int)std::max<size_t>(1, std::min<size_t>(4, (200 * 1024) / wsm));
     size_t smem_a = wsm * wpb;
