@@ -319,6 +319,10 @@ __global__ void __launch_bounds__(kBCThreads) k_phase_bc_cta(
             // s sqrt(sum c^2))^2; what it cannot decide goes on to verify_mixed.
             auto verify_i8 = [&](uint32_t cnt_, auto nbc, auto nwc) {
                 constexpr int NWW = decltype(nwc)::value;
+                // Every lane loads a row below (the idle ones st[0]'s), so an empty
+                // stage, whose st[0] was never written, loads nothing.  cnt_ is the
+                // same in all lanes of the warp.
+                if (cnt_ == 0) return;
                 const bool live = (uint32_t)lane < cnt_;
                 const uint32_t id = st[live ? lane : 0];
                 const float kd = __ldg(kcol + id);
