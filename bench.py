@@ -250,7 +250,8 @@ def main():
         if rank == 0:
             print(json.dumps({"workload": args.workload, "build": build,
                               "refine": {k_: rs[k_] for k_ in ("ms", "sample_ms", "join_ms", "bucket_ms", "merge_ms",
-                                                               "proposals", "join_dists", "updates")}}), flush=True)
+                                                               "proposals", "join_dists", "updates", "screen_survivors",
+                                                               "screen_dense_nodes", "join_mode")}}), flush=True)
         return
 
     # ---- ground truth and the recall sweep (untimed) ----
@@ -425,18 +426,29 @@ def main():
     params = {"m": m_star, "K_prime": W["Kp"], "ef_search": W["ef"], "k": W["k"], "threshold": 1.0}
     sweep = sweeps[head]
 
-    # ---- NNDescent roofline (per iteration, the formula of the build) ----
-    it_bytes = []
+    # ---- NNDescent roofline, per iteration: the lists read and written once
+    # (2 N K 8), every node's sample rows gathered once in FP32, every proposal
+    # (target, source, d) written once and read once (24 bytes).  The exact re-rank
+    # of the screened pairs reads the rows already staged on chip, so it moves no
+    # HBM bytes.  (Charging each proposal two FP32 rows from HBM instead,
+    # proposals * (8 + 2 d 4), gives the "per_proposal_rows" figure.) ----
+    it_bytes, it_bytes_rows = [], []
     for i in range(rs["iters"]):
-        b = 2 * W["n"] * W["K"] * 8 + rs["sample_entries"][i] * d * 4 + rs["proposals"][i] * (8 + 2 * d * 4)
-        it_bytes.append(b)
+        base = 2 * W["n"] * W["K"] * 8 + rs["sample_entries"][i] * d * 4
+        it_bytes.append(base + rs["proposals"][i] * 24)
+        it_bytes_rows.append(base + rs["proposals"][i] * (8 + 2 * d * 4))
     nnd_ms = sum(rs["ms"])
     build["nndescent_iter_ms"] = [round(x, 2) for x in rs["ms"]]
     build["nndescent_phase_ms"] = {k_: [round(x, 2) for x in rs[k_ + "_ms"]] for k_ in ("sample", "join", "bucket", "merge")}
     build["nndescent_roofline"] = {"bound": "hbm", "achieved": round(sum(it_bytes) / (nnd_ms / 1e3) / 1e9, 1)
                                    if nnd_ms > 0 else None, "peak": hbm, "unit": "GB/s",
                                    "frac": round(sum(it_bytes) / (nnd_ms / 1e3) / 1e9 / hbm, 4) if nnd_ms else None,
-                                   "join_dists": rs["join_dists"], "proposals": rs["proposals"]}
+                                   "bytes_per_iter": it_bytes,
+                                   "per_proposal_rows_frac": round(sum(it_bytes_rows) / (nnd_ms / 1e3) / 1e9 / hbm, 4)
+                                   if nnd_ms else None,
+                                   "join_dists": rs["join_dists"], "proposals": rs["proposals"],
+                                   "join_mode": rs["join_mode"], "screen_survivors": rs["screen_survivors"],
+                                   "screen_dense_nodes": rs["screen_dense_nodes"]}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

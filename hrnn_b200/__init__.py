@@ -23,6 +23,7 @@ _lib = C.CDLL(LIB_PATH)
 
 OK, ERR_ARG, ERR_STATE, ERR_IO, ERR_FORMAT, ERR_CUDA, ERR_NOMEM, ERR_CAPACITY, ERR_LIMIT, ERR_TIMEOUT = range(10)
 PREC_FP32_EXACT, PREC_BF16, PREC_INT8 = 0, 1, 2
+JOIN_EXACT, JOIN_TENSOR, JOIN_AUDIT = 0, 1, 2
 
 # Every symbol include/hrnn_capi.h declares.
 EXPORTS = [
@@ -30,7 +31,7 @@ EXPORTS = [
     "hrnn_add_points", "hrnn_refine_knng", "hrnn_build_rknng", "hrnn_build_rknng_mutable",
     "hrnn_search_rknn", "hrnn_search_rknn_batch", "hrnn_search_rknn_batch_device",
     "hrnn_compact_for_serving", "hrnn_insert_dynamic", "hrnn_set_ef", "hrnn_get_info",
-    "hrnn_get_search_stats", "hrnn_get_refine_stats", "hrnn_set_precision", "hrnn_set_l2_order", "hrnn_detect_l2_order", "hrnn_get_knng",
+    "hrnn_get_search_stats", "hrnn_get_refine_stats", "hrnn_set_precision", "hrnn_set_join_mode", "hrnn_set_l2_order", "hrnn_detect_l2_order", "hrnn_get_knng",
     "hrnn_set_knng", "hrnn_get_rknng", "hrnn_l2_batch", "hrnn_build_rknng_noalloc",
     "hrnn_set_budget", "hrnn_budget_features", "hrnn_budget_train", "hrnn_budget_predict",
     "hrnn_budget_gradients", "hrnn_budget_get_weights", "hrnn_budget_set_weights", "hrnn_get_dynamic_stats",
@@ -75,11 +76,15 @@ MAX_ITERS = 64
 class RefineStats(C.Structure):
     _fields_ = [("iters", C.c_int32)] + [
         (f, C.c_uint64 * MAX_ITERS) for f in ("join_dists", "updates", "proposals", "sample_entries")] + [
-        (f, C.c_double * MAX_ITERS) for f in ("ms", "sample_ms", "join_ms", "bucket_ms", "merge_ms")]
+        (f, C.c_double * MAX_ITERS) for f in ("ms", "sample_ms", "join_ms", "bucket_ms", "merge_ms")] + [
+        (f, C.c_uint64 * MAX_ITERS) for f in ("screen_survivors", "screen_dense_nodes", "screen_misses")] + [
+        ("join_mode", C.c_int32)]
 
     def as_dict(self):
         k = self.iters
-        return {"iters": k, **{f: list(getattr(self, f))[:k] for f, _ in self._fields_[1:]}}
+        d = {"iters": k, "join_mode": self.join_mode}
+        d.update({f: list(getattr(self, f))[:k] for f, _ in self._fields_[1:-1]})
+        return d
 
 
 class DynamicStats(C.Structure):
@@ -114,6 +119,7 @@ _lib.hrnn_get_search_stats.argtypes = [_vp, C.POINTER(SearchStats)]
 _lib.hrnn_get_refine_stats.argtypes = [_vp, C.POINTER(RefineStats)]
 _lib.hrnn_get_dynamic_stats.argtypes = [_vp, C.POINTER(DynamicStats)]
 _lib.hrnn_set_precision.argtypes = [_vp, C.c_int]
+_lib.hrnn_set_join_mode.argtypes = [_vp, C.c_int]
 _lib.hrnn_set_l2_order.argtypes = [_vp, C.c_int, C.c_int]
 _lib.hrnn_detect_l2_order.argtypes = [C.POINTER(C.c_int), C.POINTER(C.c_int)]
 _lib.hrnn_get_knng.argtypes = [_vp, _vp, _vp, _vp]
@@ -257,8 +263,14 @@ class HRNN:
         _check(_lib.hrnn_set_l2_order(self._h, lanes, fused))
 
     def set_precision(self, precision: int):
-        """PREC_FP32_EXACT (bit-identical to the reference) or PREC_BF16."""
+        """PREC_FP32_EXACT (bit-identical to the reference), PREC_BF16 or PREC_INT8."""
         _check(_lib.hrnn_set_precision(self._h, precision))
+
+    def set_join_mode(self, mode: int):
+        """Local join of refineKNNG: JOIN_EXACT (the default), JOIN_TENSOR (BF16
+        tensor-core screen, exact FP32 for the pairs it keeps; same lists), or
+        JOIN_AUDIT (screen decisions checked against every pair's exact distance)."""
+        _check(_lib.hrnn_set_join_mode(self._h, mode))
 
     # ---- search ------------------------------------------------------------
     def searchRknn(self, q, m: int, threshold: float, k: int, K_prime: int, ef_search: int) -> list:

@@ -288,6 +288,15 @@ hrnn_status hrnn_set_precision(hrnn_index* h, int precision) {
     });
 }
 
+hrnn_status hrnn_set_join_mode(hrnn_index* h, int mode) {
+    return guard([&] {
+        need(h, "index");
+        if (mode != HRNN_JOIN_EXACT && mode != HRNN_JOIN_TENSOR && mode != HRNN_JOIN_AUDIT)
+            hrnn::fail(HRNN_ERR_ARG, "set_join_mode: unknown join mode");
+        h->ix.join_mode = mode;
+    });
+}
+
 hrnn_status hrnn_set_budget(hrnn_index* h, int enable, uint32_t m0, uint32_t m1, uint32_t ef,
                             float confidence) {
     return guard([&] {

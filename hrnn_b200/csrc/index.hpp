@@ -60,6 +60,7 @@ struct Index {
     cudaStream_t stream = nullptr;
     L2Order order;
     int precision = HRNN_PREC_FP32_EXACT;
+    int join_mode = 0;  // refineKNNG local join (HRNN_JOIN_EXACT; HRNN_JOIN_TENSOR screens on the tensor cores)
 
     // ---- header (hrnn.h names) -------------------------------------------
     size_t dim = 0, max_elements = 0, cur = 0;

@@ -30,10 +30,12 @@
 #include <algorithm>
 #include <cfloat>
 #include <cstdio>
+#include <cstdlib>
 #include <vector>
 
 #include "beam.cuh"
 #include "index.hpp"
+#include "join.cuh"
 
 namespace hrnn {
 
@@ -162,11 +164,6 @@ __global__ void k_sample_rev(uint32_t n, uint32_t R, uint32_t cap, const uint64_
 }
 
 // ---- phase 2: join -----------------------------------------------------------
-
-struct Prop {
-    uint32_t target, source;
-    float d;
-};
 
 // One block per node of the chunk: exact FP32 distances of all sample pairs.
 // The node's rows are staged in shared memory (stride dim + 4 floats: 16-byte
@@ -837,7 +834,7 @@ void refine_knng(Index& ix, int iters, int sample) {
     tcount.alloc(((size_t)n + 1) * 4);
     toff.alloc(((size_t)n + 1) * 8);
     tcur.alloc(((size_t)n + 1) * 4);
-    ctr.alloc(64);
+    ctr.alloc(128);  // counters (64 bytes), then the tensor-core join's
     // Proposal buffer: every chunk's lists are merged once, at O(K) per touched
     // target, so few large chunks are cheaper than many small ones.  Up to 2048
     // proposals per node, 2^31 in all, and at most 40% of the free memory
@@ -847,6 +844,14 @@ void refine_knng(Index& ix, int iters, int sample) {
     const unsigned long long pcap = std::max<unsigned long long>(
         1 << 20, std::min<unsigned long long>({(unsigned long long)n * 2048, 1ull << 31,
                                                (unsigned long long)(free_b * 0.4 / 20)}));
+    // Proposals one chunk aims for (HRNN_REFINE_CHUNK_PROPOSALS, default the whole
+    // buffer): smaller chunks merge more often, so lists that start short fill
+    // sooner and later chunks are filtered by finite thresholds.
+    unsigned long long ptarget = pcap;
+    if (const char* e = std::getenv("HRNN_REFINE_CHUNK_PROPOSALS")) {
+        const unsigned long long v = std::strtoull(e, nullptr, 10);
+        if (v >= 4096) ptarget = std::min(pcap, v);
+    }
     prop.alloc(pcap * sizeof(Prop));
     bucket.alloc(pcap * 8);
     uint32_t* hdr = ix.knn_hdr.as<uint32_t>();
@@ -857,6 +862,9 @@ void refine_knng(Index& ix, int iters, int sample) {
     uint32_t* d_nextt = (uint32_t*)(ctr.as<unsigned long long>() + 3);  // merge work counter
     unsigned long long* d_pcount = ctr.as<unsigned long long>();  // proposal count of a chunk
     const bool fast = ix.order.lanes == 16 && ix.dim % 16 == 0;
+    // Tensor-core screened join where the dims and sample sizes allow it.
+    const bool tcj = fast && ix.join_mode != kJoinExact && join_tc_supported((uint32_t)ix.dim, cap);
+    JoinTcCounters* d_jc = reinterpret_cast<JoinTcCounters*>(ctr.as<char>() + 64);
     const size_t join_smem = (size_t)2 * cap * (ix.dim + 4) * 4 + (size_t)2 * cap * 8;
     if (fast) {
         auto kj = (ix.order.fused & 1) ? k_join<true> : k_join<false>;
@@ -885,7 +893,7 @@ void refine_knng(Index& ix, int iters, int sample) {
         cudaEvent_t e0 = ev[0], e1 = ev[1];
         double t_join = 0, t_bucket = 0, t_merge = 0, t_sample = 0;
         CUDA_CHECK(cudaEventRecord(e0, s));
-        CUDA_CHECK(cudaMemsetAsync(ctr.p, 0, 64, s));
+        CUDA_CHECK(cudaMemsetAsync(ctr.p, 0, 128, s));
         // ---- phase 1 ----
         CUDA_CHECK(cudaMemsetAsync(rcount.p, 0, rcount.bytes, s));
         CUDA_CHECK(cudaMemsetAsync(rcur.p, 0, rcur.bytes, s));
@@ -923,7 +931,12 @@ void refine_knng(Index& ix, int iters, int sample) {
             CUDA_CHECK(cudaMemsetAsync(d_pcount, 0, 8, s));
             CUDA_CHECK(cudaEventRecord(ev[3], s));
             unsigned grid = std::min<unsigned>(node1 - node0, (unsigned)nsm * 8);
-            if (fast) {
+            if (tcj) {
+                join_tc(ix.vec.as<float>(), (uint32_t)ix.dim, node0, node1, cap, newl.as<uint32_t>(),
+                        newc.as<uint32_t>(), oldl.as<uint32_t>(), oldc.as<uint32_t>(), thr.as<float>(),
+                        prop.as<Prop>(), d_pcount, pcap, d_njoin, d_jc, (ix.order.fused & 1) != 0, ix.join_mode, nsm,
+                        s);
+            } else if (fast) {
                 auto kj = (ix.order.fused & 1) ? k_join<true> : k_join<false>;
                 kj<<<grid, 256, join_smem, s>>>(ix.vec.as<float>(), (uint32_t)ix.dim, node0, node1, cap,
                                                 newl.as<uint32_t>(), newc.as<uint32_t>(), oldl.as<uint32_t>(),
@@ -960,13 +973,16 @@ void refine_knng(Index& ix, int iters, int sample) {
             node0 = node1;
             // Keep the chunk's proposals between a quarter and three quarters of
             // the buffer (the size carries over to the next iteration).
-            if (np < pcap / 4 && chunk < n) chunk = std::min<uint32_t>(n, chunk * 2);
-            else if (np > pcap / 4 * 3 && chunk > 1) chunk /= 2;
+            if (np < ptarget / 4 && chunk < n) chunk = std::min<uint32_t>(n, chunk * 2);
+            else if (np > ptarget / 4 * 3 && chunk > 1) chunk /= 2;
         }
         unsigned long long hc[3] = {0, 0, 0};
+        JoinTcCounters hj{};
         CUDA_CHECK(cudaEventRecord(e1, s));
         CUDA_CHECK(cudaMemcpyAsync(hc, ctr.p, 24, cudaMemcpyDeviceToHost, s));
+        CUDA_CHECK(cudaMemcpyAsync(&hj, d_jc, sizeof(hj), cudaMemcpyDeviceToHost, s));
         CUDA_CHECK(cudaStreamSynchronize(s));
+        if (hj.err) fail(HRNN_ERR_TIMEOUT, "refineKNNG: tensor-core join: wait on the MMA commit expired");
         const double ms = elapsed(e0, e1);
         std::printf("      iter %d: %llu updates, %llu dists  (%.1f ms: sample %.1f, join %.1f, bucket %.1f, "
                     "merge %.1f)\n", it, hc[2], hc[1], ms, t_sample, t_join, t_bucket, t_merge);
@@ -983,6 +999,10 @@ void refine_knng(Index& ix, int iters, int sample) {
             rs.join_ms[it] = t_join;
             rs.bucket_ms[it] = t_bucket;
             rs.merge_ms[it] = t_merge;
+            rs.screen_survivors[it] = tcj ? hj.survivors : 0;
+            rs.screen_dense_nodes[it] = tcj ? hj.dense_nodes : 0;
+            rs.screen_misses[it] = tcj ? hj.misses : 0;
+            rs.join_mode = tcj ? ix.join_mode : kJoinExact;
         }
     }
     for (auto& e : ev) cudaEventDestroy(e);

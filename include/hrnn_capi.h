@@ -90,6 +90,11 @@ typedef struct {
     double join_ms[HRNN_MAX_ITERS];          /* ... local joins                      */
     double bucket_ms[HRNN_MAX_ITERS];        /* ... grouping proposals by target     */
     double merge_ms[HRNN_MAX_ITERS];         /* ... list merges                      */
+    uint64_t screen_survivors[HRNN_MAX_ITERS];   /* tensor-core join: pairs given exact FP32 */
+    uint64_t screen_dense_nodes[HRNN_MAX_ITERS]; /* ... nodes joined densely (list overflow) */
+    uint64_t screen_misses[HRNN_MAX_ITERS];      /* ... audit mode: proposals the screen
+                                                    would have dropped (0 when the bound holds) */
+    int32_t join_mode;                           /* join mode the last call ran          */
 } hrnn_refine_stats;
 
 /* Counters of the last hrnn_insert_dynamic call. */
@@ -208,6 +213,23 @@ hrnn_status hrnn_get_refine_stats(hrnn_index* h, hrnn_refine_stats* st);
 #define HRNN_PREC_BF16 1
 #define HRNN_PREC_INT8 2
 hrnn_status hrnn_set_precision(hrnn_index* h, int precision);
+
+/* Local join of refineKNNG (new; the reference computes every sample pair's FP32
+ * distance, hrnn.h:1823-1853).  Every mode yields the same proposals, hence the
+ * same lists:
+ *  HRNN_JOIN_EXACT (default):  exact FP32 distance of every pair on the CUDA cores.
+ *  HRNN_JOIN_TENSOR: a BF16 Gram matrix of each node's sample rows on
+ *      the tensor cores bounds every pair's FP32 distance from below; pairs whose
+ *      bound reaches both ends' farthest entries are dropped, the rest get the
+ *      exact FP32 distance.  Used for dim a multiple of 16 up to 128 and sample
+ *      sizes up to 64 (16-lane L2 order); otherwise the exact join runs.
+ *  HRNN_JOIN_AUDIT:  the screen's decisions recorded, then every pair exact;
+ *      proposals the screen would have dropped are counted in
+ *      hrnn_refine_stats.screen_misses. */
+#define HRNN_JOIN_EXACT 0
+#define HRNN_JOIN_TENSOR 1
+#define HRNN_JOIN_AUDIT 2
+hrnn_status hrnn_set_join_mode(hrnn_index* h, int mode);
 
 /* Learned search budget (new; no counterpart in the reference).  A 256-256-256-2
  * MLP with GELU and BF16 weights reads a query and its beam frontier (the 32
