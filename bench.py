@@ -154,6 +154,35 @@ def rknn_gt_fp64(torch, X, Q, kth, dev):
     return [np.sort(ids) for ids, _ in groundtruth.rknn_fp64(X, Q, kth, dev)]
 
 
+def knng_quality(torch, h, X, K, dev, sample=1000, seed=5):
+    """Recall of the KNN graph against exact kNN, and the relative error of its
+    stored FP32 distances against FP64 ones, on `sample` seeded nodes (FP64 on the
+    device; internal ids are data indices, the build inserts in data order)."""
+    ids, dists, cnt = h.get_knng()
+    n = X.shape[0]
+    S = np.sort(np.random.default_rng(seed).choice(n, min(sample, n), replace=False))
+    Xd = torch.from_numpy(X).to(dev, torch.float64)
+    nx = (Xd * Xd).sum(1)
+    rec, errs = [], []
+    for c0 in range(0, len(S), 250):
+        sl = torch.from_numpy(S[c0:c0 + 250].astype(np.int64)).to(dev)
+        xs = Xd[sl]
+        D = nx[sl][:, None] - 2.0 * (xs @ Xd.T) + nx[None, :]
+        D[torch.arange(len(sl), device=dev), sl] = float("inf")
+        exact = torch.topk(D, K, dim=1, largest=False).indices.cpu().numpy()
+        for r, u in enumerate(S[c0:c0 + 250]):
+            c = int(cnt[u])
+            rec.append(len(np.intersect1d(exact[r], ids[u, :c])) / K)
+            nb = torch.from_numpy(ids[u, :c].astype(np.int64)).to(dev)
+            d64 = ((Xd[nb] - xs[r][None, :]) ** 2).sum(1).cpu().numpy()
+            d32 = dists[u, :c].astype(np.float64)
+            errs.append(np.abs(d32 - d64) / np.maximum(d64, 1e-300))
+        del D
+    e = np.concatenate(errs) if errs else np.zeros(1)
+    return {"recall_at_K": round(float(np.mean(rec)), 5), "nodes_sampled": int(len(S)),
+            "dist_rel_err_max": float(e.max()), "dist_rel_err_mean": float(e.mean())}
+
+
 def macro_recall(gt, res) -> float:
     s, c = 0.0, 0
     for g, r in zip(gt, res):
@@ -246,6 +275,8 @@ def main():
     h, build = build_index(H, W, X, dev_sync)
     rs = h.last_refine_stats()
     log(f"[bench] build: {json.dumps(build)}")
+    build["knng_quality"] = knng_quality(torch, h, X, W["K"], dev)
+    log(f"[bench] KNN graph: {json.dumps(build['knng_quality'])}")
     if args.build_only:
         if rank == 0:
             print(json.dumps({"workload": args.workload, "build": build,

@@ -30,8 +30,9 @@ EXPORTS = [
     "hrnn_last_error", "hrnn_version", "hrnn_create", "hrnn_load", "hrnn_save", "hrnn_destroy",
     "hrnn_add_points", "hrnn_refine_knng", "hrnn_build_rknng", "hrnn_build_rknng_mutable",
     "hrnn_search_rknn", "hrnn_search_rknn_batch", "hrnn_search_rknn_batch_device",
+    "hrnn_search_plan_create", "hrnn_search_plan_run", "hrnn_search_plan_result", "hrnn_search_plan_destroy",
     "hrnn_compact_for_serving", "hrnn_insert_dynamic", "hrnn_set_ef", "hrnn_get_info",
-    "hrnn_get_search_stats", "hrnn_get_refine_stats", "hrnn_set_precision", "hrnn_set_join_mode", "hrnn_set_l2_order", "hrnn_detect_l2_order", "hrnn_get_knng",
+    "hrnn_get_search_stats", "hrnn_get_refine_stats", "hrnn_set_precision", "hrnn_set_join_mode", "hrnn_set_autotune", "hrnn_set_l2_order", "hrnn_detect_l2_order", "hrnn_get_knng",
     "hrnn_set_knng", "hrnn_get_rknng", "hrnn_l2_batch", "hrnn_build_rknng_noalloc",
     "hrnn_set_budget", "hrnn_budget_features", "hrnn_budget_train", "hrnn_budget_predict",
     "hrnn_budget_gradients", "hrnn_budget_get_weights", "hrnn_budget_set_weights", "hrnn_get_dynamic_stats",
@@ -62,7 +63,8 @@ class SearchStats(C.Structure):
         "n_queries", "n_dist", "n_expanded", "n_posting", "n_cand", "n_verified", "n_result",
         "n_lowp_decided", "n_fp32_decided", "n_fp64_decided", "n_fp64_flipped", "n_launches")] + [
         ("n_budget", C.c_uint64 * 3),
-        ("phase_a_ms", C.c_double), ("phase_b_ms", C.c_double), ("phase_c_ms", C.c_double)]
+        ("phase_a_ms", C.c_double), ("phase_b_ms", C.c_double), ("phase_c_ms", C.c_double),
+        ("a_warps_per_block", C.c_uint32), ("a_visit_slots", C.c_uint32)]
 
     def as_dict(self):
         d = {f: getattr(self, f) for f, _ in self._fields_}
@@ -109,6 +111,12 @@ _lib.hrnn_build_rknng.argtypes = [_vp]
 _lib.hrnn_build_rknng_mutable.argtypes = [_vp]
 _lib.hrnn_search_rknn.argtypes = [_vp, _vp, _sz, C.c_float, _sz, _sz, _sz, _vp, _sz, C.POINTER(_sz)]
 _lib.hrnn_search_rknn_batch.argtypes = [_vp, _vp, _sz, _vp, _vp, _vp, C.c_float, C.c_uint32, _vp, _vp, _sz]
+_lib.hrnn_search_plan_create.argtypes = [_vp, _vp, _sz, _vp, _vp, _vp, C.c_uint32, C.c_uint32, C.c_float,
+                                         C.c_uint32, _vp, _vp, _sz, _vp, C.POINTER(_vp)]
+_lib.hrnn_search_plan_run.argtypes = [_vp, _vp]
+_lib.hrnn_search_plan_result.argtypes = [_vp, _vp, C.POINTER(C.c_uint64), C.POINTER(C.c_int)]
+_lib.hrnn_search_plan_destroy.argtypes = [_vp]
+_lib.hrnn_search_plan_destroy.restype = None
 _lib.hrnn_search_rknn_batch_device.argtypes = [_vp, _vp, _sz, _vp, _vp, _vp, C.c_float, C.c_uint32, _vp,
                                                _vp, _sz, C.POINTER(C.c_uint64), _vp]
 _lib.hrnn_compact_for_serving.argtypes = [_vp, _sz]
@@ -120,6 +128,7 @@ _lib.hrnn_get_refine_stats.argtypes = [_vp, C.POINTER(RefineStats)]
 _lib.hrnn_get_dynamic_stats.argtypes = [_vp, C.POINTER(DynamicStats)]
 _lib.hrnn_set_precision.argtypes = [_vp, C.c_int]
 _lib.hrnn_set_join_mode.argtypes = [_vp, C.c_int]
+_lib.hrnn_set_autotune.argtypes = [_vp, C.c_int]
 _lib.hrnn_set_l2_order.argtypes = [_vp, C.c_int, C.c_int]
 _lib.hrnn_detect_l2_order.argtypes = [C.POINTER(C.c_int), C.POINTER(C.c_int)]
 _lib.hrnn_get_knng.argtypes = [_vp, _vp, _vp, _vp]
@@ -266,6 +275,10 @@ class HRNN:
         """PREC_FP32_EXACT (bit-identical to the reference), PREC_BF16 or PREC_INT8."""
         _check(_lib.hrnn_set_precision(self._h, precision))
 
+    def set_autotune(self, enable: bool):
+        """Time the beam-search launch shapes on the first large batch (default on)."""
+        _check(_lib.hrnn_set_autotune(self._h, 1 if enable else 0))
+
     def set_join_mode(self, mode: int):
         """Local join of refineKNNG: JOIN_EXACT (the default), JOIN_TENSOR (BF16
         tensor-core screen, exact FP32 for the pairs it keeps; same lists), or
@@ -304,6 +317,16 @@ class HRNN:
                                                   threshold, k, _vp(off_ptr), _vp(lab_ptr), cap, C.byref(tot),
                                                   _vp(stream)))
         return tot.value
+
+    def search_plan(self, q_ptr, nq, m_ptr, kp_ptr, ef_ptr, m_max, ef_max, threshold, k, off_ptr, lab_ptr, cap,
+                    stream=0) -> "SearchPlan":
+        """A captured search plan over fixed device buffers (ints are raw CUDA
+        pointers): run() replays the whole batch search as one CUDA graph."""
+        out = _vp()
+        _check(_lib.hrnn_search_plan_create(self._h, _vp(q_ptr), nq, _vp(m_ptr), _vp(kp_ptr), _vp(ef_ptr), m_max,
+                                            ef_max, threshold, k, _vp(off_ptr), _vp(lab_ptr), cap, _vp(stream),
+                                            C.byref(out)))
+        return SearchPlan(self, out)
 
     # ---- learned search budget (no counterpart in the reference) -------------
     def set_budget(self, enable: bool, m0: int = 1, m1: int = 3, ef: int = 0, confidence: float = 0.9):
@@ -415,3 +438,31 @@ class HRNN:
         _check(_lib.hrnn_get_rknng(self._h, C.byref(no), C.byref(ne), C.byref(eb), C.byref(rb), _p(off), _p(ent),
                                    int(reference_order)))
         return off, ent[: ne.value], rb.value, eb.value == 8
+
+
+class SearchPlan:
+    """hrnn_search_plan_*: the batch search recorded once as a CUDA graph."""
+
+    def __init__(self, index, handle):
+        self._index = index  # keeps the index alive while the plan exists
+        self._p = handle
+
+    def run(self, stream=0):
+        _check(_lib.hrnn_search_plan_run(self._p, _vp(stream)))
+
+    def result(self, stream=0):
+        """Waits for the stream; returns (total results, clamped flag)."""
+        tot, cl = C.c_uint64(0), C.c_int(0)
+        _check(_lib.hrnn_search_plan_result(self._p, _vp(stream), C.byref(tot), C.byref(cl)))
+        return tot.value, bool(cl.value)
+
+    def close(self):
+        if self._p:
+            _lib.hrnn_search_plan_destroy(self._p)
+            self._p = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -10,12 +10,18 @@
 #include <vector>
 
 #include "index.hpp"
+#include "plan.hpp"
 #include "mlp.hpp"
 
 static_assert(hrnn::kBudgetParams == HRNN_BUDGET_PARAMS, "budget parameter layout");
 
 struct hrnn_index {
     hrnn::Index ix;
+};
+
+struct hrnn_search_plan {
+    hrnn_index* h;
+    hrnn::SearchPlan p;
 };
 
 namespace {
@@ -104,6 +110,7 @@ void hrnn_destroy(hrnn_index* h) {
 hrnn_status hrnn_add_points(hrnn_index* h, const float* data, const uint64_t* labels, size_t n) {
     return guard([&] {
         need(h, "index");
+        h->ix.generation++;
         if (n) need(data, "data");
         set_device(h);
         hrnn::add_points(h->ix, data, labels, n);
@@ -113,6 +120,7 @@ hrnn_status hrnn_add_points(hrnn_index* h, const float* data, const uint64_t* la
 hrnn_status hrnn_refine_knng(hrnn_index* h, int iters, int sample) {
     return guard([&] {
         need(h, "index");
+        h->ix.generation++;
         set_device(h);
         hrnn::refine_knng(h->ix, iters, sample);
     });
@@ -121,6 +129,7 @@ hrnn_status hrnn_refine_knng(hrnn_index* h, int iters, int sample) {
 hrnn_status hrnn_build_rknng(hrnn_index* h) {
     return guard([&] {
         need(h, "index");
+        h->ix.generation++;
         set_device(h);
         hrnn::build_rknng(h->ix);
     });
@@ -129,6 +138,7 @@ hrnn_status hrnn_build_rknng(hrnn_index* h) {
 hrnn_status hrnn_build_rknng_mutable(hrnn_index* h) {
     return guard([&] {
         need(h, "index");
+        h->ix.generation++;
         set_device(h);
         hrnn::build_rknng_mutable(h->ix);
     });
@@ -213,9 +223,73 @@ hrnn_status hrnn_search_rknn(hrnn_index* h, const float* query, size_t m, float 
     return st;
 }
 
+hrnn_status hrnn_search_plan_create(hrnn_index* h, const float* d_queries, size_t nq, const uint32_t* d_m,
+                                    const uint32_t* d_K_prime, const uint32_t* d_ef_search, uint32_t m_max,
+                                    uint32_t ef_max, float threshold, uint32_t k, uint64_t* d_out_offsets,
+                                    uint64_t* d_out_labels, size_t cap, void* stream, hrnn_search_plan** out) {
+    return guard([&] {
+        need(h, "index");
+        need(out, "out");
+        need(d_queries, "queries");
+        need(d_m, "m");
+        need(d_K_prime, "K_prime");
+        need(d_ef_search, "ef_search");
+        need(d_out_offsets, "out_offsets");
+        if (cap > 0) need(d_out_labels, "out_labels");
+        set_device(h);
+        auto* pl = new hrnn_search_plan{h, {}};
+        try {
+            hrnn::SearchPlan& p = pl->p;
+            p.ix = &h->ix;
+            p.nq = nq;
+            p.cap = cap;
+            p.m_max = m_max;
+            p.ef_max = ef_max;
+            p.k = k;
+            p.threshold = threshold;
+            p.d_q = d_queries;
+            p.d_m = d_m;
+            p.d_kp = d_K_prime;
+            p.d_ef = d_ef_search;
+            p.d_out_off = d_out_offsets;
+            p.d_out_lab = d_out_labels;
+            hrnn::plan_create(p, stream ? (cudaStream_t)stream : h->ix.stream);
+        } catch (...) {
+            delete pl;
+            throw;
+        }
+        *out = pl;
+    });
+}
+
+hrnn_status hrnn_search_plan_run(hrnn_search_plan* plan, void* stream) {
+    return guard([&] {
+        need(plan, "plan");
+        set_device(plan->h);
+        hrnn::plan_run(plan->p, stream ? (cudaStream_t)stream : plan->h->ix.stream);
+    });
+}
+
+hrnn_status hrnn_search_plan_result(hrnn_search_plan* plan, void* stream, uint64_t* total, int* clamped) {
+    return guard([&] {
+        need(plan, "plan");
+        set_device(plan->h);
+        const uint64_t t = hrnn::plan_result(plan->p, stream ? (cudaStream_t)stream : plan->h->ix.stream, clamped);
+        if (total) *total = t;
+        if (t > plan->p.cap) hrnn::fail(HRNN_ERR_CAPACITY, "search plan: results exceed the capacity; labels not written");
+    });
+}
+
+void hrnn_search_plan_destroy(hrnn_search_plan* plan) {
+    if (!plan) return;
+    cudaSetDevice(plan->h->ix.device);
+    delete plan;
+}
+
 hrnn_status hrnn_compact_for_serving(hrnn_index* h, size_t mks) {
     return guard([&] {
         need(h, "index");
+        h->ix.generation++;
         set_device(h);
         hrnn::compact_for_serving(h->ix, mks);
     });
@@ -225,6 +299,7 @@ hrnn_status hrnn_insert_dynamic(hrnn_index* h, const float* data, const uint64_t
                                 unsigned m_update, int bidirectional) {
     return guard([&] {
         need(h, "index");
+        h->ix.generation++;
         if (n) need(data, "data");
         set_device(h);
         hrnn::insert_dynamic(h->ix, data, labels, n, m_update, bidirectional != 0);
@@ -234,6 +309,7 @@ hrnn_status hrnn_insert_dynamic(hrnn_index* h, const float* data, const uint64_t
 hrnn_status hrnn_set_ef(hrnn_index* h, size_t ef) {
     return guard([&] {
         need(h, "index");
+        h->ix.generation++;
         h->ix.ef = ef;
     });
 }
@@ -280,11 +356,19 @@ hrnn_status hrnn_get_search_stats(hrnn_index* h, hrnn_search_stats* st) {
 hrnn_status hrnn_set_precision(hrnn_index* h, int precision) {
     return guard([&] {
         need(h, "index");
+        h->ix.generation++;
         if (precision != HRNN_PREC_FP32_EXACT && precision != HRNN_PREC_BF16 && precision != HRNN_PREC_INT8)
             hrnn::fail(HRNN_ERR_ARG, "set_precision: unknown precision");
         if (precision == HRNN_PREC_INT8 && (h->ix.dim % 16 != 0 || h->ix.dim > 256))
             hrnn::fail(HRNN_ERR_ARG, "set_precision: INT8 needs dim a multiple of 16, at most 256");
         h->ix.precision = precision;
+    });
+}
+
+hrnn_status hrnn_set_autotune(hrnn_index* h, int enable) {
+    return guard([&] {
+        need(h, "index");
+        h->ix.autotune = enable != 0;
     });
 }
 
@@ -399,6 +483,7 @@ hrnn_status hrnn_get_refine_stats(hrnn_index* h, hrnn_refine_stats* st) {
 hrnn_status hrnn_set_l2_order(hrnn_index* h, int lanes, int fused) {
     return guard([&] {
         need(h, "index");
+        h->ix.generation++;
         if (lanes != 16 && lanes != 8 && lanes != 4) hrnn::fail(HRNN_ERR_ARG, "lanes must be 16, 8 or 4");
         if (fused < 0 || fused > 3) hrnn::fail(HRNN_ERR_ARG, "fused must be in [0, 3]");
         h->ix.order.lanes = lanes;
@@ -428,6 +513,7 @@ hrnn_status hrnn_get_knng(hrnn_index* h, uint32_t* ids, float* dists, uint32_t* 
 hrnn_status hrnn_set_knng(hrnn_index* h, const uint32_t* ids, const float* dists, const uint32_t* cnt) {
     return guard([&] {
         need(h, "index");
+        h->ix.generation++;
         need(ids, "ids");
         need(dists, "dists");
         need(cnt, "cnt");

@@ -60,6 +60,9 @@ struct Index {
     cudaStream_t stream = nullptr;
     L2Order order;
     int precision = HRNN_PREC_FP32_EXACT;
+    bool autotune = true;                                   // hrnn_set_autotune
+    std::unordered_map<uint64_t, std::pair<uint32_t, uint32_t>> a_shape;  // (mode, beam) -> (warps/block, slots)
+    uint64_t generation = 0;  // bumped by every call that changes the index (captured plans check it)
     int join_mode = 0;  // refineKNNG local join (HRNN_JOIN_EXACT; HRNN_JOIN_TENSOR screens on the tensor cores)
 
     // ---- header (hrnn.h names) -------------------------------------------

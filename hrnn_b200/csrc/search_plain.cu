@@ -21,6 +21,7 @@
 #include "beam.cuh"
 #include "index.hpp"
 #include "mlp.hpp"
+#include "plan.hpp"
 
 namespace hrnn {
 
@@ -164,10 +165,13 @@ __global__ void __launch_bounds__(128) k_phase_bc(DevView v, const float* __rest
                                                   size_t list_stride, uint64_t* __restrict__ resbuf,
                                                   uint32_t* __restrict__ res_count, uint32_t* __restrict__ next_q,
                                                   const uint32_t* __restrict__ qlist,
-                                                  SearchCounters* __restrict__ ctr) {
+                                                  SearchCounters* __restrict__ ctr,
+                                                  const uint32_t* __restrict__ nq_dev) {
+    // nq_dev: the query count in device memory (a captured plan), else nq.
     extern __shared__ char smem_raw[];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, wpb = blockDim.x >> 5;
     const int half = lane >> 4, l = lane & 15;
+    if (nq_dev) nq = *nq_dev;
     float* q = (float*)(smem_raw + (size_t)w * (v.dim * 4 + 16));
     uint32_t* nc_s = (uint32_t*)(q + v.dim);
     const size_t gw = (size_t)blockIdx.x * wpb + w;
@@ -304,6 +308,29 @@ int sms(int dev) {
     return v;
 }
 
+// Captured plans: each query's m and ef clamped to the plan's maxima (flag set
+// when one was above), so the beam and the proxy table never outgrow their sizes.
+__global__ void k_plan_inputs(const uint32_t* __restrict__ m_in, const uint32_t* __restrict__ ef_in, uint32_t nq,
+                              uint32_t m_max, uint32_t ef_max, uint32_t* __restrict__ m_out,
+                              uint32_t* __restrict__ ef_out, uint32_t* __restrict__ flag) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nq) return;
+    const uint32_t m = m_in[i], ef = ef_in[i];
+    if (m > m_max || ef > ef_max) atomicOr(flag, 1u);
+    m_out[i] = min(m, m_max);
+    ef_out[i] = min(ef, ef_max);
+}
+
+// k_pack_results when the total (out_off[nq]) fits the caller's capacity.
+__global__ void k_pack_results_capped(uint32_t nq, const uint64_t* __restrict__ res_off,
+                                      const uint32_t* __restrict__ res_count, const uint64_t* __restrict__ out_off,
+                                      const uint64_t* __restrict__ resbuf, uint64_t* __restrict__ out, size_t cap) {
+    const uint32_t qi = blockIdx.x;
+    if (qi >= nq || out_off[nq] > cap) return;
+    const uint32_t c = res_count[qi];
+    for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) out[out_off[qi] + i] = resbuf[res_off[qi] + i];
+}
+
 }  // namespace
 
 DevView make_view(Index& ix) {
@@ -379,7 +406,7 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
     // Visited-cache slots (lossy; a miss costs a recomputed row).  1024 rather than
     // more: the smaller per-warp shared memory keeps more warps resident, which
     // pays for the ~10% extra rows at ef = 200.
-    const uint32_t vc = 512;
+    uint32_t vc = 512;
     size_t wsm = warp_smem_bytes(v.dim, efc, vc);
     int wpb = (int)std::max<size_t>(1, std::min<size_t>(4, (200 * 1024) / wsm));
     size_t smem_a = wsm * wpb;
@@ -414,6 +441,58 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
     CUDA_CHECK(cudaEventRecord(ev[0], s));
     {
         auto kern = int8 ? k_phase_a<3> : mixed ? k_phase_a<2> : (fusedsimd ? k_phase_a<1> : k_phase_a<0>);
+        uint32_t* d_qa = d_next + 4;  // work counters of the phase-A launches (zeroed with d_rcount)
+        // Launch shape: the tuned one of this (distance mode, beam size), else timed
+        // now on this batch when autotuning is on and the batch is large enough.
+        const uint64_t shape_key = ((uint64_t)(int8 ? 3 : mixed ? 2 : fusedsimd ? 1 : 0) << 32) | efc;
+        auto shape = ix.autotune ? ix.a_shape.find(shape_key) : ix.a_shape.end();
+        if (shape != ix.a_shape.end()) {
+            wpb = (int)shape->second.first;
+            vc = shape->second.second;
+        } else if (ix.autotune && !learned && nq >= 1024) {
+            float best = FLT_MAX;
+            int bw = wpb;
+            uint32_t bv = vc;
+            cudaEvent_t t0, t1;
+            CUDA_CHECK(cudaEventCreate(&t0));
+            CUDA_CHECK(cudaEventCreate(&t1));
+            for (uint32_t cv : {256u, 512u, 1024u}) {
+                for (int cw : {2, 4}) {
+                    const size_t sm = warp_smem_bytes(v.dim, efc, cv) * (size_t)cw;
+                    if (sm > 200 * 1024) continue;
+                    CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+                    int ps = 1;
+                    CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ps, kern, cw * 32, sm));
+                    const unsigned g = (unsigned)std::max<size_t>(
+                        1, std::min<size_t>((nq + cw - 1) / cw, (size_t)nsm * std::max(ps, 1)));
+                    CUDA_CHECK(cudaMemsetAsync(d_qa, 0, 4, s));
+                    CUDA_CHECK(cudaEventRecord(t0, s));
+                    kern<<<g, cw * 32, sm, s>>>(v, a.d_q, (uint32_t)nq, a.d_m, a.d_ef, efc, cv, mmax,
+                                                 prox.as<uint32_t>(), nprox.as<uint32_t>(), ctr, nullptr, 0, 0, 0,
+                                                 nullptr, d_qa);
+                    CUDA_LAUNCH_CHECK();
+                    CUDA_CHECK(cudaEventRecord(t1, s));
+                    CUDA_CHECK(cudaEventSynchronize(t1));
+                    float ms = 0.f;
+                    CUDA_CHECK(cudaEventElapsedTime(&ms, t0, t1));
+                    if (ms < best) {
+                        best = ms;
+                        bw = cw;
+                        bv = cv;
+                    }
+                }
+            }
+            cudaEventDestroy(t0);
+            cudaEventDestroy(t1);
+            wpb = bw;
+            vc = bv;
+            ix.a_shape[shape_key] = {(uint32_t)wpb, vc};
+            // the trials' counts and work counter start over
+            CUDA_CHECK(cudaMemsetAsync(ctr, 0, sizeof(SearchCounters), s));
+            CUDA_CHECK(cudaMemsetAsync(d_qa, 0, 4, s));
+            CUDA_CHECK(cudaEventRecord(ev[0], s));
+        }
+        smem_a = warp_smem_bytes(v.dim, efc, vc) * (size_t)wpb;
         CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_a));
         // Persistent grid (every resident block), queries handed out by counters.
         int per_sm = 1;
@@ -421,7 +500,6 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
         auto grid_for = [&](size_t n) {
             return (unsigned)std::max<size_t>(1, std::min<size_t>((n + wpb - 1) / wpb, (size_t)nsm * std::max(per_sm, 1)));
         };
-        uint32_t* d_qa = d_next + 4;  // work counters of the phase-A launches (zeroed with d_rcount)
         if (!learned) {
             kern<<<grid_for(nq), wpb * 32, smem_a, s>>>(v, a.d_q, (uint32_t)nq, a.d_m, a.d_ef, efc, vc, mmax,
                                                         prox.as<uint32_t>(), nprox.as<uint32_t>(), ctr, nullptr, 0, 0,
@@ -543,14 +621,14 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
             size_t smem_w = 4 * (v.dim * 4 + 16);
             void (*kern)(DevView, const float*, uint32_t, uint32_t, const uint32_t*, const uint32_t*, const uint32_t*,
                          const uint64_t*, float, uint32_t, uint32_t, uint32_t*, uint32_t*, uint32_t*, size_t,
-                         uint64_t*, uint32_t*, uint32_t*, const uint32_t*, SearchCounters*);
+                         uint64_t*, uint32_t*, uint32_t*, const uint32_t*, SearchCounters*, const uint32_t*);
             if (ix.wide) kern = fusedsimd ? k_phase_bc<uint64_t, true> : k_phase_bc<uint64_t, false>;
             else kern = fusedsimd ? k_phase_bc<uint32_t, true> : k_phase_bc<uint32_t, false>;
             kern<<<(unsigned)(slots / 4), 128, smem_w, s>>>(v, a.d_q, nov, mmax, prox.as<uint32_t>(),
                                                             nprox.as<uint32_t>(), plen.as<uint32_t>(), d_resoff,
                                                             a.threshold, kidx, hcap, hkey.as<uint32_t>(),
                                                             hcnt.as<uint32_t>(), lp.as<uint32_t>(), (size_t)tmax,
-                                                            resbuf, d_rcount, d_next2, ovl, ctr);
+                                                            resbuf, d_rcount, d_next2, ovl, ctr, nullptr);
             CUDA_LAUNCH_CHECK();
         }
     }
@@ -590,6 +668,8 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
     cudaEventElapsedTime(&t01, ev[0], ev[1]);
     cudaEventElapsedTime(&t12, ev[1], ev[2]);
     cudaEventElapsedTime(&t23, ev[2], ev[3]);
+    st.a_warps_per_block = (uint32_t)wpb;
+    st.a_visit_slots = vc;
     st.phase_a_ms = t01;
     st.phase_b_ms = t12;
     st.phase_c_ms = t23;
@@ -659,6 +739,200 @@ void budget_features(Index& ix, const float* d_q, size_t nq, uint32_t k, uint32_
                                                                        ix.kcol.as<float>(), b.proj.as<float>(), d_feat);
     CUDA_LAUNCH_CHECK();
     CUDA_CHECK(cudaStreamSynchronize(s));
+}
+
+// ---- captured search plans ---------------------------------------------------
+//
+// The sequence of search_batch for one batch shape, with its four host reads
+// replaced by bounds fixed at creation:
+//   - the maxima of m and ef: the plan's m_max / ef_max (inputs clamped on the
+//     device, k_plan_inputs);
+//   - the result staging size: nq * m_max * (longest reverse list), an upper bound
+//     of every query's posting count;
+//   - the overflow count: the overflow kernel always runs, reads the count from
+//     device memory and sizes its tables for the same bound;
+//   - the total before packing: k_pack_results_capped checks it on the device.
+// Device layout of qtot as in search_batch: total[nq+1] u64 | res_off[nq+1] u64 |
+// rcount[nq+1] u32 | counters u32[8] (BC work, overflow count, overflow work,
+// -, phase-A work x2, -, -).
+
+namespace {
+
+struct PlanLaunch {
+    uint32_t efc, vc, mmax, wpb, grid_a, grid_bc, kidx, slots, hcap;
+    size_t smem_a, smem_bc, smem_w, tmax;
+    bool mixed, int8, fusedsimd, counts;
+};
+
+PlanLaunch plan_launch_shape(Index& ix, const SearchPlan& p) {
+    PlanLaunch L{};
+    DevView v = make_view(ix);
+    L.mmax = std::max<uint32_t>(1, p.m_max);
+    const uint32_t efmax = std::max(std::max<uint32_t>(1, p.ef_max), L.mmax);
+    L.efc = (efmax + 31) & ~31u;
+    L.vc = 512;
+    const size_t wsm = warp_smem_bytes(v.dim, L.efc, L.vc);
+    L.wpb = (uint32_t)std::max<size_t>(1, std::min<size_t>(4, (200 * 1024) / wsm));
+    L.smem_a = wsm * L.wpb;
+    L.fusedsimd = (ix.order.fused & 1) != 0;
+    L.mixed = (ix.precision == HRNN_PREC_BF16 || ix.precision == HRNN_PREC_INT8) &&
+              (v.dim == 96 || v.dim == 128 || v.dim == 256) && v.lanes == 16;
+    L.int8 = ix.precision == HRNN_PREC_INT8 && v.dim % 16 == 0 && v.dim <= 256;
+    const uint64_t shape_key = ((uint64_t)(L.int8 ? 3 : L.mixed ? 2 : L.fusedsimd ? 1 : 0) << 32) | L.efc;
+    auto shape = ix.autotune ? ix.a_shape.find(shape_key) : ix.a_shape.end();  // tuned by an earlier batch call
+    if (shape != ix.a_shape.end()) {
+        L.wpb = shape->second.first;
+        L.vc = shape->second.second;
+        L.smem_a = warp_smem_bytes(v.dim, L.efc, L.vc) * L.wpb;
+    }
+    L.counts = p.threshold > 1.0f;
+    L.kidx = p.k - 1;
+    L.smem_bc = bc_cta_smem(v.dim, L.counts, L.mixed);
+    L.smem_w = 4 * (v.dim * 4 + 16);
+    return L;
+}
+
+}  // namespace
+
+void plan_create(SearchPlan& p, cudaStream_t s) {
+    Index& ix = *p.ix;
+    if (!ix.rknng_built) fail(HRNN_ERR_STATE, "searchRknn: RKNNG not built");
+    if (ix.budget && ix.budget->enabled)
+        fail(HRNN_ERR_STATE, "search plan: the learned budget is not captured; disable it first");
+    if (p.nq == 0 || p.nq > (1u << 30)) fail(HRNN_ERR_ARG, "search plan: nq must be in [1, 2^30]");
+    if (p.m_max == 0 || p.ef_max == 0) fail(HRNN_ERR_ARG, "search plan: m_max and ef_max must be >= 1");
+    if (std::max(p.m_max, p.ef_max) > (1u << 16)) fail(HRNN_ERR_ARG, "searchRknn: ef_search/m too large (max 65536)");
+    if (p.k == 0) fail(HRNN_ERR_ARG, "search plan: k must be >= 1");
+    if (ix.serve_mode && p.k > ix.max_k_serve) fail(HRNN_ERR_ARG, "searchRknn: k must be in [1, max_k_serve] in serve mode");
+    ix.sync_upper_to_device();
+    PlanLaunch L = plan_launch_shape(ix, p);
+    if (L.smem_a > 227 * 1024) fail(HRNN_ERR_ARG, "searchRknn: ef/dim too large for one warp's beam");
+    if (L.mixed) ensure_bf16(ix);
+    if (L.int8) ensure_i8(ix);
+    DevView v = make_view(ix);
+    v.i8_screen = (L.mixed && L.int8) ? 1 : 0;
+    const size_t nq = p.nq;
+    // longest reverse list: bounds every proxy's posting prefix
+    std::vector<uint64_t> off(ix.cur + 1);
+    CUDA_CHECK(cudaMemcpy(off.data(), ix.csr_off.p, off.size() * 8, cudaMemcpyDeviceToHost));
+    uint64_t maxdeg = 1;
+    for (size_t i = 0; i < ix.cur; ++i) maxdeg = std::max<uint64_t>(maxdeg, off[i + 1] - off[i]);
+    L.tmax = (size_t)L.mmax * maxdeg;
+    const size_t res_entries = nq * L.tmax;
+    size_t free_b = 0, total_b = 0;
+    CUDA_CHECK(cudaMemGetInfo(&free_b, &total_b));
+    if (res_entries * 8 > free_b / 2)
+        fail(HRNN_ERR_NOMEM, "search plan: result bound nq * m_max * longest reverse list does not fit; lower m_max or nq");
+    const int nsm = sms(ix.device);
+    // overflow tables: a fixed pool of warp slots, each sized for the bound
+    uint32_t hcap = 64;
+    while (hcap < 2 * L.tmax) hcap <<= 1;
+    L.hcap = hcap;
+    const size_t per_slot = (size_t)hcap * 8 + L.tmax * 4;
+    size_t slots = std::max<size_t>(4, std::min<size_t>((size_t)nsm * 4, (free_b / 8) / per_slot) / 4 * 4);
+    L.slots = (uint32_t)slots;
+    // buffers
+    p.inputs.alloc((3 * nq + 8) * 4);  // m | ef | flag, 3 spare | overflow list
+    p.prox.alloc(nq * L.mmax * 4);
+    p.nprox.alloc(nq * 4);
+    p.plen.alloc(nq * L.mmax * 4);
+    p.qtot.alloc((nq + 1) * 8 * 2 + (nq + 1) * 4 + 64);
+    p.res.alloc(std::max<size_t>(res_entries, 1) * 8);
+    p.kcol.alloc(std::max<size_t>(ix.cur, 1) * 4);
+    p.hkey.alloc(slots * hcap * 4);
+    p.hcnt.alloc(slots * hcap * 4);
+    p.lp.alloc(slots * L.tmax * 4 + 64);
+    p.ctr.alloc(sizeof(SearchCounters));
+    CUDA_CHECK(cudaMemsetAsync(p.hkey.p, 0xFF, p.hkey.bytes, s));
+    CUDA_CHECK(cudaMemsetAsync(p.hcnt.p, 0, p.hcnt.bytes, s));
+    CUDA_CHECK(cudaMemsetAsync(p.qtot.p, 0, p.qtot.bytes, s));
+    uint64_t* d_total = p.qtot.as<uint64_t>();
+    uint64_t* d_resoff = d_total + (nq + 1);
+    uint32_t* d_rcount = (uint32_t*)(d_resoff + (nq + 1));
+    uint32_t* d_next = d_rcount + (nq + 1);
+    uint32_t* pm = p.inputs.as<uint32_t>();
+    uint32_t* pef = pm + nq;
+    uint32_t* flag = pef + nq;
+    // scan scratch sized outside the capture (both scans take nq + 1 entries)
+    exclusive_scan_u64(d_total, d_resoff, nq + 1, s, p.tmp);
+    exclusive_scan_u32_to_u64(d_rcount, p.d_out_off, nq + 1, s, p.tmp);
+    auto ka = L.int8 ? k_phase_a<3> : L.mixed ? k_phase_a<2> : (L.fusedsimd ? k_phase_a<1> : k_phase_a<0>);
+    CUDA_CHECK(cudaFuncSetAttribute(ka, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem_a));
+    int per_sm = 1;
+    CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ka, L.wpb * 32, L.smem_a));
+    L.grid_a = (uint32_t)std::max<size_t>(1, std::min<size_t>((nq + L.wpb - 1) / L.wpb, (size_t)nsm * std::max(per_sm, 1)));
+    KCta kc = ix.wide ? pick_bc<uint64_t>(L.fusedsimd, L.counts, L.mixed) : pick_bc<uint32_t>(L.fusedsimd, L.counts, L.mixed);
+    CUDA_CHECK(cudaFuncSetAttribute(kc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem_bc));
+    per_sm = 1;
+    CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kc, 256, L.smem_bc));
+    L.grid_bc = (uint32_t)std::min<size_t>(nq, (size_t)nsm * std::max(per_sm, 1));
+    void (*kov)(DevView, const float*, uint32_t, uint32_t, const uint32_t*, const uint32_t*, const uint32_t*,
+                const uint64_t*, float, uint32_t, uint32_t, uint32_t*, uint32_t*, uint32_t*, size_t, uint64_t*,
+                uint32_t*, uint32_t*, const uint32_t*, SearchCounters*, const uint32_t*);
+    if (ix.wide) kov = L.fusedsimd ? k_phase_bc<uint64_t, true> : k_phase_bc<uint64_t, false>;
+    else kov = L.fusedsimd ? k_phase_bc<uint32_t, true> : k_phase_bc<uint32_t, false>;
+    CUDA_CHECK(cudaStreamSynchronize(s));
+
+    // ---- record ----
+    CUDA_CHECK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    try {
+    SearchCounters* ctr = p.ctr.as<SearchCounters>();
+    CUDA_CHECK(cudaMemsetAsync(ctr, 0, sizeof(SearchCounters), s));
+    CUDA_CHECK(cudaMemsetAsync(d_total, 0, (nq + 1) * 8, s));
+    CUDA_CHECK(cudaMemsetAsync(d_rcount, 0, (nq + 1) * 4 + 32, s));
+    CUDA_CHECK(cudaMemsetAsync(flag, 0, 4, s));
+    k_plan_inputs<<<(unsigned)((nq + 255) / 256), 256, 0, s>>>(p.d_m, p.d_ef, (uint32_t)nq, L.mmax, p.ef_max, pm, pef,
+                                                               flag);
+    ka<<<L.grid_a, L.wpb * 32, L.smem_a, s>>>(v, p.d_q, (uint32_t)nq, pm, pef, L.efc, L.vc, L.mmax,
+                                               p.prox.as<uint32_t>(), p.nprox.as<uint32_t>(), ctr, nullptr, 0, 0, 0,
+                                               nullptr, d_next + 4);
+    {
+        const size_t tot = nq * L.mmax;
+        auto kb = ix.wide ? k_phase_b_count<uint64_t> : k_phase_b_count<uint32_t>;
+        kb<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(v, (uint32_t)nq, p.d_kp, L.mmax, p.prox.as<uint32_t>(),
+                                                         p.nprox.as<uint32_t>(), p.plen.as<uint32_t>(), d_total);
+    }
+    exclusive_scan_u64(d_total, d_resoff, nq + 1, s, p.tmp);
+    k_kdist_column<<<(unsigned)((ix.cur + 255) / 256), 256, 0, s>>>(v, L.kidx, p.kcol.as<float>());
+    uint64_t* resbuf = p.res.as<uint64_t>();
+    uint32_t* ovl = flag + 4;  // the overflow list (nq entries) after the clamp flag
+    kc<<<L.grid_bc, 256, L.smem_bc, s>>>(v, p.d_q, (uint32_t)nq, L.mmax, p.prox.as<uint32_t>(), p.nprox.as<uint32_t>(),
+                                         p.plen.as<uint32_t>(), d_total, d_resoff, p.threshold, p.kcol.as<float>(),
+                                         L.kidx, resbuf, d_rcount, d_next, ovl, d_next + 1, ctr);
+    kov<<<(unsigned)(slots / 4), 128, L.smem_w, s>>>(v, p.d_q, 0, L.mmax, p.prox.as<uint32_t>(),
+                                                      p.nprox.as<uint32_t>(), p.plen.as<uint32_t>(), d_resoff,
+                                                      p.threshold, L.kidx, L.hcap, p.hkey.as<uint32_t>(),
+                                                      p.hcnt.as<uint32_t>(), p.lp.as<uint32_t>(), L.tmax, resbuf,
+                                                      d_rcount, d_next + 2, ovl, ctr, d_next + 1);
+    exclusive_scan_u32_to_u64(d_rcount, p.d_out_off, nq + 1, s, p.tmp);
+    k_pack_results_capped<<<(unsigned)nq, 128, 0, s>>>((uint32_t)nq, d_resoff, d_rcount, p.d_out_off, resbuf,
+                                                        p.d_out_lab, p.cap);
+    } catch (...) {
+        cudaGraph_t g = nullptr;
+        cudaStreamEndCapture(s, &g);  // leave the stream usable
+        if (g) cudaGraphDestroy(g);
+        throw;
+    }
+    const cudaError_t ce = cudaStreamEndCapture(s, &p.graph);
+    if (ce != cudaSuccess) fail(HRNN_ERR_CUDA, std::string("search plan: capture failed: ") + cudaGetErrorString(ce));
+    CUDA_CHECK(cudaGraphInstantiate(&p.exec, p.graph, 0));
+    p.generation = ix.generation;
+}
+
+void plan_run(SearchPlan& p, cudaStream_t s) {
+    if (p.generation != p.ix->generation)
+        fail(HRNN_ERR_STATE, "search plan: the index changed after the plan was made; make a new plan");
+    CUDA_CHECK(cudaGraphLaunch(p.exec, s));
+}
+
+uint64_t plan_result(SearchPlan& p, cudaStream_t s, int* clamped) {
+    CUDA_CHECK(cudaStreamSynchronize(s));
+    uint64_t total = 0;
+    uint32_t flag = 0;
+    CUDA_CHECK(cudaMemcpy(&total, p.d_out_off + p.nq, 8, cudaMemcpyDeviceToHost));
+    CUDA_CHECK(cudaMemcpy(&flag, p.inputs.as<uint32_t>() + 2 * p.nq, 4, cudaMemcpyDeviceToHost));
+    if (clamped) *clamped = flag ? 1 : 0;
+    return total;
 }
 
 }  // namespace hrnn

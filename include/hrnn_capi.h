@@ -74,6 +74,7 @@ typedef struct {
     uint64_t n_launches;    /* kernels this call launched                       */
     uint64_t n_budget[3];   /* learned budget: queries at level 0, 1, fallback */
     double phase_a_ms, phase_b_ms, phase_c_ms;   /* device time of each phase   */
+    uint32_t a_warps_per_block, a_visit_slots;   /* phase-A launch shape used (autotuned) */
 } hrnn_search_stats;
 
 /* Per-iteration counters of the last refineKNNG call (the reference prints the
@@ -173,6 +174,32 @@ hrnn_status hrnn_search_rknn_batch_device(hrnn_index* h, const float* d_queries,
                                           uint64_t* d_out_labels, size_t cap,
                                           uint64_t* out_total, void* stream);
 
+/* Captured search plan (new; the reference answers one query per call).  The batch
+ * search of hrnn_search_rknn_batch_device for one batch shape -- nq queries in
+ * d_queries, per-query m / K' / ef_search in d_m / d_K_prime / d_ef_search, results
+ * to d_out_offsets (nq + 1) and d_out_labels (cap) -- recorded once as a CUDA graph
+ * and replayed by hrnn_search_plan_run with no host synchronisation inside: fill
+ * the same input buffers, run, read the outputs.  The bounds a plan is made for:
+ * m <= m_max and ef_search <= ef_max (larger values run clamped to them and are
+ * reported by hrnn_search_plan_result), threshold and k fixed.  Staging is sized
+ * for nq * m_max * (the index's longest reverse list) postings (HRNN_ERR_NOMEM
+ * when that exceeds half the free device memory).  The precision form is the
+ * index's at creation; the learned budget must be disabled.  A plan is bound to
+ * the index as it was: any later call that changes the index (add, refine, build,
+ * insert, compact, set_knng, set_l2_order, set_precision, set_ef) makes run fail
+ * with HRNN_ERR_STATE.  Answers equal hrnn_search_rknn_batch_device's.
+ *   hrnn_search_plan_result: waits for `stream`; *total = out_offsets[nq];
+ *     *clamped = 1 if some query's m or ef_search was above the maxima;
+ *     HRNN_ERR_CAPACITY when total > cap (labels then not written). */
+typedef struct hrnn_search_plan hrnn_search_plan;
+hrnn_status hrnn_search_plan_create(hrnn_index* h, const float* d_queries, size_t nq, const uint32_t* d_m,
+                                    const uint32_t* d_K_prime, const uint32_t* d_ef_search, uint32_t m_max,
+                                    uint32_t ef_max, float threshold, uint32_t k, uint64_t* d_out_offsets,
+                                    uint64_t* d_out_labels, size_t cap, void* stream, hrnn_search_plan** out);
+hrnn_status hrnn_search_plan_run(hrnn_search_plan* plan, void* stream);
+hrnn_status hrnn_search_plan_result(hrnn_search_plan* plan, void* stream, uint64_t* total, int* clamped);
+void hrnn_search_plan_destroy(hrnn_search_plan* plan);
+
 /* compactForServing(max_k_serve) -- hrnn.h:299-364: dense kdist[n x max_k_serve]. */
 hrnn_status hrnn_compact_for_serving(hrnn_index* h, size_t max_k_serve);
 
@@ -213,6 +240,15 @@ hrnn_status hrnn_get_refine_stats(hrnn_index* h, hrnn_refine_stats* st);
 #define HRNN_PREC_BF16 1
 #define HRNN_PREC_INT8 2
 hrnn_status hrnn_set_precision(hrnn_index* h, int precision);
+
+/* Launch-shape autotuning of the beam search (new).  With it on (the default), the
+ * first batch of at least 1024 queries for a given distance mode and beam size
+ * times the beam-search kernel at warps-per-block {2, 4} x visited-cache slots
+ * {256, 512, 1024} on that batch and keeps the fastest for the index; answers do
+ * not depend on the shape (a visited-cache miss only re-scores a node, which the
+ * beam bound rejects again).  Off: 4 warps per block (fewer when the beam does not
+ * fit), 512 slots. */
+hrnn_status hrnn_set_autotune(hrnn_index* h, int enable);
 
 /* Local join of refineKNNG (new; the reference computes every sample pair's FP32
  * distance, hrnn.h:1823-1853).  Every mode yields the same proposals, hence the

@@ -1,0 +1,127 @@
+"""Captured search plans (hrnn_search_plan_*): the batch search recorded once as a
+CUDA graph over fixed device buffers and replayed per batch.  Every replay must
+answer exactly as the stream-ordered batch call does on the same inputs."""
+import numpy as np
+import pytest
+
+from oracle import data
+
+import hrnn_b200 as H
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def index(tmp_path_factory):
+    X = data.mixture(20000, 128, 32, 1.0, 7, 7)
+    h = H.HRNN(dim=128, max_elements=20000, M=16, ef_construction=100, random_seed=100, K_knng=100)
+    h.add_points(X)
+    h.refineKNNG(4, 30)
+    h.buildRKNNG()
+    return h
+
+
+def _batch(seed, nq, m_max, ef_max):
+    rng = np.random.default_rng(seed)
+    Q = data.mixture(nq, 128, 32, 1.0, 7, 100 + seed)
+    m = rng.integers(1, m_max + 1, nq).astype(np.uint32)
+    ef = rng.integers(10, ef_max + 1, nq).astype(np.uint32)
+    kp = rng.integers(20, 101, nq).astype(np.uint32)
+    return Q, m, kp, ef
+
+
+def _regular(h, torch, q, m, kp, ef, k, cap):
+    off = torch.zeros(q.shape[0] + 1, dtype=torch.int64, device="cuda")
+    lab = torch.zeros(cap, dtype=torch.int64, device="cuda")
+    tot = h.search_rknn_batch_device(q.data_ptr(), q.shape[0], m.data_ptr(), kp.data_ptr(), ef.data_ptr(), 1.0, k,
+                                     off.data_ptr(), lab.data_ptr(), cap)
+    torch.cuda.synchronize()
+    return off.cpu().numpy(), lab.cpu().numpy()[:tot]
+
+
+@pytest.mark.parametrize("precision", [H.PREC_FP32_EXACT, H.PREC_INT8])
+def test_plan_replays_equal_batch_calls(index, precision):
+    import torch
+    h = index
+    h.set_precision(precision)
+    nq, m_max, ef_max, k, cap = 3000, 8, 120, 10, 3000 * 64
+    q = torch.zeros((nq, 128), dtype=torch.float32, device="cuda")
+    m = torch.zeros(nq, dtype=torch.int32, device="cuda")
+    kp = torch.zeros(nq, dtype=torch.int32, device="cuda")
+    ef = torch.zeros(nq, dtype=torch.int32, device="cuda")
+    off = torch.zeros(nq + 1, dtype=torch.int64, device="cuda")
+    lab = torch.zeros(cap, dtype=torch.int64, device="cuda")
+    plan = h.search_plan(q.data_ptr(), nq, m.data_ptr(), kp.data_ptr(), ef.data_ptr(), m_max, ef_max, 1.0, k,
+                         off.data_ptr(), lab.data_ptr(), cap)
+    try:
+        for seed in (1, 2):  # two different batches through the same graph
+            Q, hm, hkp, hef = _batch(seed, nq, m_max, ef_max)
+            q.copy_(torch.from_numpy(Q))
+            m.copy_(torch.from_numpy(hm.astype(np.int32)))
+            kp.copy_(torch.from_numpy(hkp.astype(np.int32)))
+            ef.copy_(torch.from_numpy(hef.astype(np.int32)))
+            torch.cuda.synchronize()  # the plan runs on the index's stream
+            plan.run()
+            total, clamped = plan.result()
+            assert not clamped
+            got_off, got_lab = off.cpu().numpy(), lab.cpu().numpy()[:total]
+            exp_off, exp_lab = _regular(h, torch, q, m, kp, ef, k, cap)
+            assert total == exp_off[-1] and total > 0
+            assert np.array_equal(got_off, exp_off)
+            assert np.array_equal(got_lab, exp_lab)
+    finally:
+        plan.close()
+        h.set_precision(H.PREC_FP32_EXACT)
+
+
+def test_plan_clamps_capacity_and_index_changes(index):
+    import torch
+    h = index
+    nq, k = 500, 10
+    Q, hm, hkp, hef = _batch(3, nq, 6, 80)
+    hm[7] = 40  # above m_max: runs with m_max and is reported
+    q = torch.from_numpy(Q).cuda()
+    m = torch.from_numpy(hm.astype(np.int32)).cuda()
+    kp = torch.from_numpy(hkp.astype(np.int32)).cuda()
+    ef = torch.from_numpy(hef.astype(np.int32)).cuda()
+    off = torch.zeros(nq + 1, dtype=torch.int64, device="cuda")
+    lab = torch.zeros(4, dtype=torch.int64, device="cuda")
+    plan = h.search_plan(q.data_ptr(), nq, m.data_ptr(), kp.data_ptr(), ef.data_ptr(), 6, 80, 1.0, k,
+                         off.data_ptr(), lab.data_ptr(), 4)
+    try:
+        torch.cuda.synchronize()
+        plan.run()
+        with pytest.raises(H.HrnnError) as e:  # far more than 4 results
+            plan.result()
+        assert e.value.code == H.ERR_CAPACITY
+        assert int(off[-1].item()) > 4
+        # the clamped query equals a batch call with m = m_max
+        m_ref = m.clone()
+        m_ref[7] = 6
+        exp_off, _ = _regular(h, torch, q, m_ref, kp, ef, k, int(off[-1].item()) + 16)
+        assert np.array_equal(off.cpu().numpy(), exp_off)
+        h.setEf(50)  # any call that changes the index invalidates the plan
+        with pytest.raises(H.HrnnError) as e:
+            plan.run()
+        assert e.value.code == H.ERR_STATE
+    finally:
+        plan.close()
+
+
+def test_autotuned_launch_shape_keeps_answers(index):
+    h = index
+    Q, _, _, _ = _batch(4, 2048, 8, 120)
+    h.set_autotune(False)
+    plain = h.search_rknn_batch(Q, 5, 100, 150, threshold=1.0, k=10)
+    st0 = h.last_search_stats()
+    h.set_autotune(True)
+    tuned = h.search_rknn_batch(Q, 5, 100, 150, threshold=1.0, k=10)
+    st1 = h.last_search_stats()
+    again = h.search_rknn_batch(Q, 5, 100, 150, threshold=1.0, k=10)  # the cached shape
+    st2 = h.last_search_stats()
+    assert (st1["a_warps_per_block"], st1["a_visit_slots"]) in {(w, v) for w in (2, 4) for v in (256, 512, 1024)}
+    assert (st2["a_warps_per_block"], st2["a_visit_slots"]) == (st1["a_warps_per_block"], st1["a_visit_slots"])
+    assert (st0["a_warps_per_block"], st0["a_visit_slots"]) == (4, 512)  # the untuned shape at d = 128
+    for a, b, c in zip(plain, tuned, again):
+        assert np.array_equal(a, b) and np.array_equal(a, c)
+    assert st1["n_result"] == st0["n_result"]
