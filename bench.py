@@ -51,6 +51,11 @@ WORKLOADS = {
     "build-200k-d128-K500": dict(n=200_000, d=128, C=256, sigma=1.0, seed=2, dirichlet=True, nq=1_000,
                                  qseed=1002, M=16, efc=400, K=500, iters=2, S=50, k=10, Kp=500, ef=200,
                                  m_sweep=[5]),
+    # Join profiling case: 50k points of the same generator, K_knng=100, three
+    # NNDescent iterations (about 2 GB on the device; used with --build-only).
+    "build-50k-d128-K100": dict(n=50_000, d=128, C=256, sigma=1.0, seed=2, dirichlet=True, nq=1_000,
+                                qseed=1002, M=16, efc=100, K=100, iters=3, S=50, k=10, Kp=100, ef=200,
+                                m_sweep=[5]),
     # The reference's CPU-runnable case: 100k x 128, 64 equal Gaussians (seed 0), K_knng=100.
     "plain-100k-d128-K100": dict(n=100_000, d=128, C=64, sigma=1.0, seed=0, dirichlet=False, nq=1_000, qseed=1,
                                  M=16, efc=400, K=100, iters=10, S=50, k=10, Kp=100, ef=200,
@@ -210,13 +215,14 @@ class StdoutToStderr:
         os.close(self.saved)
 
 
-def build_index(H, W, X, dev_sync):
+def build_index(H, W, X, dev_sync, join="exact"):
     with StdoutToStderr():
-        return _build_index(H, W, X, dev_sync)
+        return _build_index(H, W, X, dev_sync, join)
 
 
-def _build_index(H, W, X, dev_sync):
+def _build_index(H, W, X, dev_sync, join):
     h = H.HRNN(W["d"], W["n"], W["M"], W["efc"], 100, W["K"])
+    h.set_join_mode({"exact": H.JOIN_EXACT, "tensor": H.JOIN_TENSOR, "audit": H.JOIN_AUDIT}[join])
     t0 = time.perf_counter()
     h.add_points(X)
     dev_sync()
@@ -244,6 +250,10 @@ def main():
     ap.add_argument("--build-only", action="store_true", help="build the index, print its build times, exit")
     ap.add_argument("--budget-train", type=int, default=200_000, help="training queries of the budget MLP")
     ap.add_argument("--queries", type=int, default=0, help="queries per step (default: the workload's)")
+    ap.add_argument("--learned-precision", default="auto", choices=["auto", "bf16", "int8"],
+                    help="reduced-precision form the learned budget runs on (auto: the faster one as timed)")
+    ap.add_argument("--join", default="exact", choices=["exact", "tensor", "audit"],
+                    help="refineKNNG local join: exact FP32 (default), tensor-core screened, or audited screen")
     args = ap.parse_args()
     W = dict(WORKLOADS[args.workload])
     if args.queries > 0:
@@ -272,7 +282,7 @@ def main():
     Q = replica_queries(W, rank)
     log(f"[bench] data {X.shape} queries {Q.shape} ({time.perf_counter() - t_gen:.1f}s)")
 
-    h, build = build_index(H, W, X, dev_sync)
+    h, build = build_index(H, W, X, dev_sync, args.join)
     rs = h.last_refine_stats()
     log(f"[bench] build: {json.dumps(build)}")
     build["knng_quality"] = knng_quality(torch, h, X, W["K"], dev)
@@ -399,7 +409,12 @@ def main():
     # pair reaching the recall target ----
     budget_info = None
     if not args.no_learned:
-        lp = max((f for f in forms if f != "plain"), key=lambda f: results[f]["qps"])
+        if args.learned_precision == "auto":
+            lp = max((f for f in forms if f != "plain"), key=lambda f: results[f]["qps"])
+        else:
+            lp = {"bf16": "mixed", "int8": "mixed_int8"}[args.learned_precision]
+            if lp not in forms:
+                lp = "mixed"
         lprec = forms[lp]
         budget_info = train_budget(H, h, W, args, dev_sync, lprec)
         budget_info["precision_form"] = lp
