@@ -499,6 +499,9 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(h, W, Q, params, args.cpu_sample)
+        del h
+        cpu["build"] = cpu_build_baseline(H, torch, dev, dev_sync)
+        log(f"[bench] build baseline: {json.dumps(cpu['build'])}")
 
     line = {
         "metric": "RkNN queries/s at recall>=0.95 (k=10)", "value": round(qps, 1), "unit": "queries/s",
@@ -623,6 +626,55 @@ def cpu_baseline(h, W, Q, params, sample):
                 "single_thread": {"value": round(n1 / secs1, 1), "sample": f"{n1} queries, 1 thread"}}
     finally:
         shutil.rmtree(td, ignore_errors=True)
+
+
+def cpu_build_baseline(H, torch, dev, dev_sync):
+    """The reference's own build (HNSW insertion with the KNN seeds, refineKNNG,
+    buildRKNNG; oracle/_ref) on its CPU-runnable case -- 100k x 128, 64 equal
+    Gaussians, K_knng=100, ef_construction=400, 10 iterations of S=50 -- with all
+    host cores, beside the GPU build of the same points, and the KNN-graph recall
+    of both against exact kNN (1000 seeded nodes, each index in its own id order)."""
+    from oracle import idx, ref
+    if not ref.available():
+        return {"kind": "reference", "sample": "oracle/_ref not built"}
+    import shutil
+    import tempfile
+    W1 = WORKLOADS["plain-100k-d128-K100"]
+    X1 = mixture(W1["n"], W1["d"], W1["C"], W1["sigma"], W1["seed"], W1["seed"], dirichlet=W1["dirichlet"])
+    cores = os.cpu_count() or 1
+    out = {"workload": "plain-100k-d128-K100", "kind": "reference", "cores": cores}
+    td = tempfile.mkdtemp(prefix="hrnn_build_ref_")
+    try:
+        with StdoutToStderr():
+            r = ref.RefIndex.create(W1["d"], W1["n"], W1["M"], W1["efc"], 100, W1["K"])
+            t0 = time.perf_counter()
+            r.add_points(X1, threads=cores)
+            t1 = time.perf_counter()
+            r.refine(W1["iters"], W1["S"], threads=cores)
+            t2 = time.perf_counter()
+            r.build_rknng()
+            t3 = time.perf_counter()
+            p = os.path.join(td, "ref.idx")
+            r.save(p)
+        Xr = idx.read_idx(p).vectors()  # the reference's internal order (parallel insertion)
+
+        class _RefLists:
+            def get_knng(self):
+                return r.knng(W1["K"])
+
+        out["reference"] = {"hnsw_insert_s": round(t1 - t0, 3), "nndescent_s": round(t2 - t1, 3),
+                            "rknng_csr_s": round(t3 - t2, 3), "knng_build_s": round(t3 - t1, 3),
+                            "knng_quality": knng_quality(torch, _RefLists(), Xr, W1["K"], dev)}
+        del r
+        g, b = build_index(H, W1, X1, dev_sync)
+        b = {k_: round(v, 3) for k_, v in b.items()}
+        b["knng_quality"] = knng_quality(torch, g, X1, W1["K"], dev)
+        out["gpu"] = b
+        out["speedup_knng_build"] = round(out["reference"]["knng_build_s"] / max(b["knng_build_s"], 1e-9), 1)
+        del g
+    finally:
+        shutil.rmtree(td, ignore_errors=True)
+    return out
 
 
 def run_reference_arm(args, W, h, Q, params, sweep, build):

@@ -923,6 +923,8 @@ void refine_knng(Index& ix, int iters, int sample) {
         CUDA_CHECK(cudaStreamSynchronize(s));
         t_sample = elapsed(e0, ev[2]);
         unsigned long long proposals = 0;
+        unsigned long long njoin_ok = 0;  // pair count after the last accepted chunk
+        JoinTcCounters jc_ok{};           // screen counts after the last accepted chunk
         // ---- phase 2, chunk by chunk ----
         for (uint32_t node0 = 0; node0 < n;) {
             uint32_t node1 = std::min<uint32_t>(n, node0 + chunk);
@@ -957,10 +959,14 @@ void refine_knng(Index& ix, int iters, int sample) {
             if (np > pcap) {
                 if (chunk == 1) fail(HRNN_ERR_NOMEM, "refineKNNG: proposal buffer too small for one node");
                 chunk = std::max<uint32_t>(1, chunk / 4);  // redo this chunk smaller (the join is pure)
-                unsigned long long z = 0;
-                CUDA_CHECK(cudaMemcpyAsync(d_njoin, &z, 8, cudaMemcpyHostToDevice, s));
+                // the pair and screen counts of the dropped attempt start over
+                CUDA_CHECK(cudaMemcpyAsync(d_njoin, &njoin_ok, 8, cudaMemcpyHostToDevice, s));
+                if (tcj) CUDA_CHECK(cudaMemcpyAsync(d_jc, &jc_ok, sizeof(jc_ok), cudaMemcpyHostToDevice, s));
+                CUDA_CHECK(cudaStreamSynchronize(s));
                 continue;
             }
+            CUDA_CHECK(cudaMemcpyAsync(&njoin_ok, d_njoin, 8, cudaMemcpyDeviceToHost, s));
+            if (tcj) CUDA_CHECK(cudaMemcpyAsync(&jc_ok, d_jc, sizeof(jc_ok), cudaMemcpyDeviceToHost, s));
             if (np) {
                 bucket_and_merge(n, K, prop.as<Prop>(), np, tcount, toff, tcur, bucket.as<uint64_t>(), tmp, hdr, ids,
                                  dist, isnew.as<uint8_t>(), d_nupd, d_nextt, merge_smem, merge_grid, nsm, s, ev[6]);
