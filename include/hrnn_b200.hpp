@@ -176,6 +176,10 @@ public:
     // Precision of the search (HRNN_PREC_FP32_EXACT: the reference's answers;
     // HRNN_PREC_BF16: the mixed-precision form with exact decisions).
     void setPrecision(int precision) { call([&] { return hrnn_set_precision(h_, precision); }); }
+    // Local join of refineKNNG (HRNN_JOIN_EXACT, HRNN_JOIN_TENSOR, HRNN_JOIN_AUDIT).
+    void setJoinMode(int mode) { call([&] { return hrnn_set_join_mode(h_, mode); }); }
+    // Launch-shape autotuning of the batch search (on by default).
+    void setAutotune(bool enable) { call([&] { return hrnn_set_autotune(h_, enable ? 1 : 0); }); }
 
     hrnn_index* handle() {
         std::lock_guard<std::mutex> lk(mu_);
