@@ -56,6 +56,11 @@ WORKLOADS = {
     "build-50k-d128-K100": dict(n=50_000, d=128, C=256, sigma=1.0, seed=2, dirichlet=True, nq=1_000,
                                 qseed=1002, M=16, efc=100, K=100, iters=3, S=50, k=10, Kp=100, ef=200,
                                 m_sweep=[5]),
+    # Large single-GPU case (build only): 10M x 96, 1024 equal Gaussians (sigma 1,
+    # seed 4), K_knng=200 (8 GB of ids + 8 GB of distances), reverse CSR of 2e9 entries.
+    "large-10M-d96-K200": dict(n=10_000_000, d=96, C=1024, sigma=1.0, seed=4, dirichlet=False, nq=100_000,
+                               qseed=1004, M=16, efc=200, K=200, iters=10, S=50, k=10, Kp=200, ef=200,
+                               m_sweep=[1, 2, 3, 4, 5, 6, 8, 10, 20, 50]),
     # The reference's CPU-runnable case: 100k x 128, 64 equal Gaussians (seed 0), K_knng=100.
     "plain-100k-d128-K100": dict(n=100_000, d=128, C=64, sigma=1.0, seed=0, dirichlet=False, nq=1_000, qseed=1,
                                  M=16, efc=400, K=100, iters=10, S=50, k=10, Kp=100, ef=200,
