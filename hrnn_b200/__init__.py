@@ -296,18 +296,34 @@ class HRNN:
         Q = np.ascontiguousarray(Q, np.float32)
         nq = Q.shape[0]
         mm, kp, ef = _u32(m, nq), _u32(K_prime, nq), _u32(ef_search, nq)
-        off = np.zeros(nq + 1, np.uint64)
+        off, lab = self.search_rknn_batch_csr(Q, mm, kp, ef, threshold, k)
+        return [lab[off[i]:off[i + 1]] for i in range(nq)]
+
+    def search_rknn_batch_csr(self, Q, m, K_prime, ef_search, threshold: float = 1.0, k: int = 10):
+        """Batch of searchRknn with host arrays; returns (offsets[nq + 1], labels):
+        query i's labels are labels[offsets[i]:offsets[i + 1]], ascending internal id."""
+        Q = np.ascontiguousarray(Q, np.float32)
+        nq = Q.shape[0]
+        mm, kp, ef = _u32(m, nq), _u32(K_prime, nq), _u32(ef_search, nq)
+        off = np.empty(nq + 1, np.uint64)
         cap = max(16, int(np.sum(mm.astype(np.int64)) * 64))
-        lab = np.zeros(cap, np.uint64)
+        lab = np.empty(cap, np.uint64)
         rc = _lib.hrnn_search_rknn_batch(self._h, _p(Q), nq, _p(mm), _p(kp), _p(ef), threshold, k, _p(off),
                                          _p(lab), cap)
         if rc == ERR_CAPACITY:
             cap = int(off[-1])
-            lab = np.zeros(max(cap, 1), np.uint64)
+            lab = np.empty(max(cap, 1), np.uint64)
             rc = _lib.hrnn_search_rknn_batch(self._h, _p(Q), nq, _p(mm), _p(kp), _p(ef), threshold, k,
                                              _p(off), _p(lab), cap)
         _check(rc)
-        return [lab[off[i]:off[i + 1]].copy() for i in range(nq)]
+        return off, lab[:int(off[-1])]
+
+    def search_rknn_batch_host(self, q_ptr, nq, m_ptr, kp_ptr, ef_ptr, threshold, k, off_ptr, lab_ptr, cap) -> int:
+        """hrnn_search_rknn_batch on raw HOST pointers (e.g. pinned buffers): copies
+        in, searches, copies out and waits; returns the total result count."""
+        _check(_lib.hrnn_search_rknn_batch(self._h, _vp(q_ptr), nq, _vp(m_ptr), _vp(kp_ptr), _vp(ef_ptr), threshold,
+                                           k, _vp(off_ptr), _vp(lab_ptr), cap))
+        return int(C.c_uint64.from_address(off_ptr + 8 * nq).value)
 
     def search_rknn_batch_device(self, q_ptr, nq, m_ptr, kp_ptr, ef_ptr, threshold, k, off_ptr, lab_ptr,
                                  cap, stream=0):
