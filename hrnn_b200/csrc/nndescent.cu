@@ -123,8 +123,123 @@ __global__ void k_sample_fill(const uint32_t* __restrict__ ids, const float* __r
 }
 
 // Appends the R smallest owners of each reverse segment, ascending, after the
-// forward samples (nn_old then stays within 2R = S + R, hrnn.h:1816-1817).
-// Also sums |new| + |old| over the nodes into *entries.
+// forward samples (nn_old then stays within 2R = S + R, hrnn.h:1816-1817), one
+// warp per node, for R <= kRevSel: the R-th smallest owner by four 8-bit radix
+// passes over the segment (owners are distinct within a segment), the owners at or
+// below it collected, then placed by rank.  Also sums |new| + |old| over the
+// nodes into *entries.
+constexpr uint32_t kRevSel = 128;
+
+__global__ void __launch_bounds__(256) k_sample_rev_sel(uint32_t n, uint32_t R, uint32_t cap,
+                                                        const uint64_t* __restrict__ roff,
+                                                        const uint32_t* __restrict__ rbuf,
+                                                        uint32_t* __restrict__ newl, uint32_t* __restrict__ newc,
+                                                        uint32_t* __restrict__ oldl, uint32_t* __restrict__ oldc,
+                                                        unsigned long long* __restrict__ entries) {
+    __shared__ uint32_t hist_all[8][256];
+    __shared__ uint32_t pick_all[8][kRevSel];
+    const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
+    uint32_t* hist = hist_all[wl];
+    uint32_t* pick = pick_all[wl];
+    unsigned long long my_entries = 0;
+    const size_t warp = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const size_t nw = ((size_t)gridDim.x * blockDim.x) >> 5;
+    for (size_t i = warp; i < n; i += nw) {
+        for (int type = 0; type < 2; ++type) {
+            const size_t seg = 2 * i + type;
+            const uint64_t b = roff[seg];
+            const uint32_t len = (uint32_t)(roff[seg + 1] - b);
+            uint32_t* L = type == 0 ? newl : oldl;
+            uint32_t* C = type == 0 ? newc : oldc;
+            const uint32_t base = C[i];
+            const uint32_t take = min(len, R);
+            if (take > 0) {
+                // threshold: the take-th smallest owner (all of them when len <= R)
+                uint32_t T = 0xFFFFFFFFu;
+                if (len > R) {
+                    uint32_t prefix = 0, mask = 0, rank = R;
+                    for (int shift = 24; shift >= 0; shift -= 8) {
+#pragma unroll
+                        for (int k = 0; k < 8; ++k) hist[8 * lane + k] = 0;
+                        __syncwarp();
+                        for (uint32_t x = lane; x < len; x += 32) {
+                            const uint32_t v = rbuf[b + x];
+                            if ((v & mask) == prefix) atomicAdd(&hist[(v >> shift) & 255u], 1u);
+                        }
+                        __syncwarp();
+                        uint32_t loc[8], sum = 0;
+#pragma unroll
+                        for (int k = 0; k < 8; ++k) {
+                            loc[k] = hist[8 * lane + k];
+                            sum += loc[k];
+                        }
+                        uint32_t incl = sum;
+                        for (int o = 1; o < 32; o <<= 1) {
+                            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+                            if (lane >= o) incl += y;
+                        }
+                        const uint32_t excl = incl - sum;
+                        uint32_t bin = 0, nrank = 0;
+                        const bool mine = excl < rank && rank <= incl;
+                        if (mine) {
+                            uint32_t r = rank - excl;
+#pragma unroll
+                            for (int k = 0; k < 8; ++k) {
+                                if (r <= loc[k]) {
+                                    bin = 8u * lane + (uint32_t)k;
+                                    nrank = r;
+                                    break;
+                                }
+                                r -= loc[k];
+                            }
+                        }
+                        const int src = __ffs(__ballot_sync(0xFFFFFFFFu, mine)) - 1;
+                        bin = __shfl_sync(0xFFFFFFFFu, bin, src);
+                        rank = __shfl_sync(0xFFFFFFFFu, nrank, src);
+                        prefix |= bin << shift;
+                        mask |= 0xFFu << shift;
+                        __syncwarp();
+                    }
+                    T = prefix;
+                }
+                // the owners at or below the threshold (exactly `take` of them)
+                uint32_t got = 0;
+                for (uint32_t x0 = 0; x0 < len; x0 += 32) {
+                    const uint32_t x = x0 + lane;
+                    const uint32_t v = x < len ? rbuf[b + x] : 0xFFFFFFFFu;
+                    const bool keep = x < len && v <= T;
+                    const uint32_t bal = __ballot_sync(0xFFFFFFFFu, keep);
+                    if (keep) pick[got + __popc(bal & lanemask_lt_())] = v;
+                    got += __popc(bal);
+                }
+                __syncwarp();
+                // ascending by rank (distinct values)
+                uint32_t v4[kRevSel / 32], r4[kRevSel / 32];
+#pragma unroll
+                for (int k = 0; k < (int)(kRevSel / 32); ++k) {
+                    const uint32_t x = lane + 32u * k;
+                    v4[k] = x < take ? pick[x] : 0xFFFFFFFFu;
+                    r4[k] = 0;
+                }
+                for (uint32_t y = 0; y < take; ++y) {
+                    const uint32_t w = pick[y];
+#pragma unroll
+                    for (int k = 0; k < (int)(kRevSel / 32); ++k) r4[k] += w < v4[k] ? 1u : 0u;
+                }
+#pragma unroll
+                for (int k = 0; k < (int)(kRevSel / 32); ++k) {
+                    const uint32_t x = lane + 32u * k;
+                    if (x < take) L[i * cap + base + r4[k]] = v4[k];
+                }
+                __syncwarp();
+            }
+            if (lane == 0) C[i] = base + take;
+            my_entries += base + take;
+        }
+    }
+    if (lane == 0 && my_entries) atomicAdd(entries, my_entries);
+}
+
 __global__ void k_sample_rev(uint32_t n, uint32_t R, uint32_t cap, const uint64_t* __restrict__ roff,
                              const uint32_t* __restrict__ rbuf, uint32_t* __restrict__ newl,
                              uint32_t* __restrict__ newc, uint32_t* __restrict__ oldl, uint32_t* __restrict__ oldc,
@@ -912,9 +1027,14 @@ void refine_knng(Index& ix, int iters, int sample) {
                                           newc.as<uint32_t>(), oldl.as<uint32_t>(), oldc.as<uint32_t>(),
                                           roff.as<uint64_t>(), rcur.as<uint32_t>(), rbuf.as<uint32_t>());
         CUDA_LAUNCH_CHECK();
-        k_sample_rev<<<g1, 256, 0, s>>>(n, R, cap, roff.as<uint64_t>(), rbuf.as<uint32_t>(), newl.as<uint32_t>(),
-                                         newc.as<uint32_t>(), oldl.as<uint32_t>(), oldc.as<uint32_t>(),
-                                         ctr.as<unsigned long long>() + 4);
+        if (R <= kRevSel)
+            k_sample_rev_sel<<<g1, 256, 0, s>>>(n, R, cap, roff.as<uint64_t>(), rbuf.as<uint32_t>(),
+                                                 newl.as<uint32_t>(), newc.as<uint32_t>(), oldl.as<uint32_t>(),
+                                                 oldc.as<uint32_t>(), ctr.as<unsigned long long>() + 4);
+        else
+            k_sample_rev<<<g1, 256, 0, s>>>(n, R, cap, roff.as<uint64_t>(), rbuf.as<uint32_t>(), newl.as<uint32_t>(),
+                                             newc.as<uint32_t>(), oldl.as<uint32_t>(), oldc.as<uint32_t>(),
+                                             ctr.as<unsigned long long>() + 4);
         CUDA_LAUNCH_CHECK();
         CUDA_CHECK(cudaEventRecord(ev[2], s));
         // |new| + |old| summed over nodes (gather bytes of the join)
