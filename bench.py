@@ -37,7 +37,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 WORKLOADS = {
-    # BASELINE configuration quoted for the metric: 1M x 128, Dirichlet(1) mixture of
+    # The configuration the metric is quoted on: 1M x 128, Dirichlet(1) mixture of
     # 256 Gaussians (centres ~ N(0, 4I), sigma 1, seed 2), K_knng=500.
     "mixed-1M-d128-K500": dict(n=1_000_000, d=128, C=256, sigma=1.0, seed=2, dirichlet=True, nq=10_000,
                                qseed=1002, M=16, efc=400, K=500, iters=10, S=50, k=10, Kp=500, ef=200,
