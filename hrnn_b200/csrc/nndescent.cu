@@ -432,16 +432,29 @@ __global__ void k_thresholds(const uint32_t* __restrict__ hdr, const float* __re
     if (u < n) thr[u] = worst_of(hdr, dist, K, u);
 }
 
+// The join emits a pair's proposals next to each other, so a warp's 32
+// consecutive proposals name few targets: lanes of the same target share one
+// atomic (leader adds the group's size, each lane takes its rank in the group).
 __global__ void k_bucket_count(const Prop* __restrict__ prop, unsigned long long np, uint32_t* __restrict__ tcount) {
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < np; i += (size_t)gridDim.x * blockDim.x)
-        atomicAdd(&tcount[prop[i].target], 1u);
+    const uint32_t lt = lanemask_lt_();
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < np; i += (size_t)gridDim.x * blockDim.x) {
+        const uint32_t t = prop[i].target;
+        const uint32_t peers = __match_any_sync(__activemask(), t);
+        if ((peers & lt) == 0) atomicAdd(&tcount[t], (uint32_t)__popc(peers));
+    }
 }
 
 __global__ void k_bucket_fill(const Prop* __restrict__ prop, unsigned long long np, const uint64_t* __restrict__ toff,
                               uint32_t* __restrict__ tcur, uint64_t* __restrict__ bucket) {
+    const uint32_t lt = lanemask_lt_();
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < np; i += (size_t)gridDim.x * blockDim.x) {
-        Prop p = prop[i];
-        uint64_t pos = toff[p.target] + atomicAdd(&tcur[p.target], 1u);
+        const Prop p = prop[i];
+        const uint32_t peers = __match_any_sync(__activemask(), p.target);
+        const int leader = __ffs(peers) - 1;
+        uint32_t base = 0;
+        if ((peers & lt) == 0) base = atomicAdd(&tcur[p.target], (uint32_t)__popc(peers));
+        base = __shfl_sync(peers, base, leader);
+        const uint64_t pos = toff[p.target] + base + (uint32_t)__popc(peers & lt);
         bucket[pos] = ((uint64_t)__float_as_uint(p.d) << 32) | p.source;  // d >= 0: bit order = value order
     }
 }
