@@ -15,6 +15,7 @@
 // rknng_reference_order() produces the reference's exact byte order on the host
 // for saveIndex by applying the same std::sort call to the owner-ordered array.
 #include <algorithm>
+#include <cstdlib>
 #include <cfloat>
 #include <vector>
 
@@ -244,6 +245,11 @@ void build_rknng(Index& ix) {
                                std::to_string(rb) + " bits)");
     ix.rank_bits = rb;
     ix.wide = (nb + rb) > 32;
+    // HRNN_RKNNG_WIDE=1 stores 64-bit entries even when 32 bits hold owner and
+    // rank: a valid wide CSR (the .idx records the entry width), which lets a
+    // small index exercise the path that n * K > 2^32 list slots would take.
+    if (const char* fw = std::getenv("HRNN_RKNNG_WIDE"))
+        if (fw[0] == '1') ix.wide = true;
     if (ix.wide) build_impl<uint64_t>(ix);
     else build_impl<uint32_t>(ix);
     ix.csr_in_reference_order = false;

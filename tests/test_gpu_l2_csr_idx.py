@@ -5,8 +5,8 @@ import os
 import numpy as np
 import pytest
 
-from conftest import golden_results
-from oracle import idx, port
+from conftest import golden_results, have_ref
+from oracle import data, idx, port
 
 import hrnn_b200 as H
 
@@ -79,3 +79,33 @@ def test_csr_large_random_graph_with_hubs(tmp_path):
     o_off, o_ent, _, _ = port.rknng(ids, cnt, n, K, canonical=True)
     assert np.array_equal(off, o_off) and np.array_equal(ent, o_ent)
     assert int(np.max(np.diff(off))) > 16384          # exercised the global-memory sort
+
+
+def test_wide_entries_match_narrow_and_reference(golden_idx, tmp_path, monkeypatch):
+    """64-bit reverse-CSR entries (forced on a small index with HRNN_RKNNG_WIDE=1,
+    the layout an index with node_bits + rank_bits > 32 gets): the same offsets and
+    (owner, rank) values as the 32-bit ones, the same search answers, and a saved
+    wide .idx that the reference loads and answers identically."""
+    h = H.HRNN.load(golden_idx, 32)
+    Q = data.mixture(64, 32, 12, 1.0, 11, 77)
+    monkeypatch.delenv("HRNN_RKNNG_WIDE", raising=False)
+    h.buildRKNNG()  # the loaded CSR is in the file's (reference) order; rebuild both in the device's
+    narrow = h.search_rknn_batch(Q, 10, 24, 40, threshold=1.0, k=10)
+    off_n, ent_n, rb_n, wide_n = h.get_rknng()
+    monkeypatch.setenv("HRNN_RKNNG_WIDE", "1")
+    h.buildRKNNG()
+    off_w, ent_w, rb_w, wide_w = h.get_rknng()
+    assert wide_w and not wide_n and rb_w == rb_n
+    assert ent_w.dtype == np.uint64 and ent_n.dtype == np.uint32
+    assert np.array_equal(off_w, off_n) and np.array_equal(ent_w, ent_n.astype(np.uint64))
+    wide = h.search_rknn_batch(Q, 10, 24, 40, threshold=1.0, k=10)
+    assert all(np.array_equal(a, b) for a, b in zip(narrow, wide))
+    exp = port.OracleIndex(idx.read_idx(golden_idx)).search_batch(Q, 10, 24, 40, threshold=1.0, k=10)
+    assert all(np.array_equal(a, b) for a, b in zip(wide, exp))
+    if have_ref():
+        from oracle import ref
+        p = str(tmp_path / "wide.idx")
+        h.saveIndex(p)
+        r = ref.RefIndex.load(p, 32)
+        a = r.search_batch(Q, 10, 24, 40, threshold=1.0, k=10)
+        assert all(np.array_equal(x, y) for x, y in zip(a, wide))
