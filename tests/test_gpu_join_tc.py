@@ -92,3 +92,15 @@ def test_join_mode_argument_checked(tmp_path):
     h = H.HRNN.load(p, 32)
     with pytest.raises(H.HrnnError):
         h.set_join_mode(7)
+
+
+def test_tensor_join_falls_back_beyond_one_tile(tmp_path):
+    """S = 80 gives sample lists of up to 160 new rows, more than one M = 128 tile:
+    the refinement runs the exact join (and says so) with the same lists."""
+    p = _pre_index(tmp_path, 6000, 64, 60, 6)
+    ht, he = H.HRNN.load(p, 64), H.HRNN.load(p, 64)
+    ht.set_join_mode(H.JOIN_TENSOR)
+    ht.refineKNNG(1, 80)
+    he.refineKNNG(1, 80)
+    assert ht.last_refine_stats()["join_mode"] == H.JOIN_EXACT
+    _same_up_to_ties(ht.get_knng(), he.get_knng(), 60)
