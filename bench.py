@@ -164,6 +164,29 @@ def rknn_gt_fp64(torch, X, Q, kth, dev):
     return [np.sort(ids) for ids, _ in groundtruth.rknn_fp64(X, Q, kth, dev)]
 
 
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch of the two
+# search kernels on the default workload, from one one-pass ncu capture of
+# `bench.py --steps 2 --warmup 3 --no-cpu-baseline --learned-precision int8`
+# (10,000 queries per launch), keyed by (precision form, phase, learned budget).
+NCU_TRAFFIC = {
+    "mixed-1M-d128-K500": {
+        ("fp32", "a", False): 17.287e9, ("fp32", "bc", False): 23.951e9,
+        ("bf16", "a", False): 6.415e9, ("bf16", "bc", False): 12.019e9,
+        ("int8", "a", False): 2.814e9, ("int8", "bc", False): 6.457e9,
+        # the learned budget at cutoff 0.99 with fallback m = 5 (its usual choice here)
+        ("int8", "a", True): 2.819e9, ("int8", "bc", True): 5.449e9,
+    },
+}
+NCU_TRAFFIC_QUERIES = 10_000
+
+
+def ncu_traffic(workload, form, phase, learned, nq):
+    """Measured DRAM bytes of one launch of that kernel, scaled from the capture's
+    10,000 queries to nq; None when the workload or form was not captured."""
+    v = NCU_TRAFFIC.get(workload, {}).get((form, phase, bool(learned)))
+    return None if v is None else int(v * nq / NCU_TRAFFIC_QUERIES)
+
+
 def knng_quality(torch, h, X, K, dev, sample=1000, seed=5):
     """Recall of the KNN graph against exact kNN, and the relative error of its
     stored FP32 distances against FP64 ones, on `sample` seeded nodes (FP64 on the
@@ -391,8 +414,13 @@ def main():
         dom = max(phases, key=lambda k_: phases[k_][0])
         tms, tb = phases[dom]
         achieved = tb / (tms / 1e3) / 1e9 if tms > 0 else 0.0
+        form = {H.PREC_FP32_EXACT: "fp32", H.PREC_BF16: "bf16", H.PREC_INT8: "int8"}[prec]
+        traffic = ncu_traffic(args.workload, form, "a" if dom.startswith("phase_a") else "bc", learned, nq)
         roof = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
-                "frac": round(achieved / hbm, 4), "peak_source": peak_kind, "traffic": None,
+                "frac": round(achieved / hbm, 4), "peak_source": peak_kind, "traffic": traffic,
+                "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of this kernel, one-pass "
+                                   "capture of this workload's timed steps, scaled by queries")
+                if traffic is not None else None,
                 "algorithmic_bytes_per_launch": int(tb), "launch_ms": round(tms, 3),
                 "per_query": {k_: round(st[k_] / nq, 3) for k_ in
                               ("n_dist", "n_expanded", "n_posting", "n_verified", "n_result", "n_lowp_decided",

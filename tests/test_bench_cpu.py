@@ -61,3 +61,12 @@ def test_workloads_are_well_formed():
         assert W["n"] > 0 and W["d"] % 16 == 0 and W["K"] > 0 and W["k"] <= W["K"], name
         assert W["m_sweep"] == sorted(W["m_sweep"]), name
     assert "mixed-1M-d128-K500" in b.WORKLOADS
+
+
+def test_ncu_traffic_table():
+    b = _bench()
+    assert b.ncu_traffic("mixed-1M-d128-K500", "int8", "a", True, 10_000) == 2_819_000_000
+    assert b.ncu_traffic("mixed-1M-d128-K500", "int8", "bc", False, 10_000) == 6_457_000_000
+    assert b.ncu_traffic("mixed-1M-d128-K500", "fp32", "bc", False, 5_000) == 11_975_500_000
+    assert b.ncu_traffic("mixed-500k-d128-K250", "int8", "a", False, 10_000) is None
+    assert b.ncu_traffic("mixed-1M-d128-K500", "fp64", "a", False, 10_000) is None
