@@ -165,26 +165,38 @@ def rknn_gt_fp64(torch, X, Q, kth, dev):
 
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch of the two
-# search kernels on the default workload, from one one-pass ncu capture of
-# `bench.py --steps 2 --warmup 3 --no-cpu-baseline --learned-precision int8`
-# (10,000 queries per launch), keyed by (precision form, phase, learned budget).
-NCU_TRAFFIC = {
-    "mixed-1M-d128-K500": {
-        ("fp32", "a", False): 17.287e9, ("fp32", "bc", False): 23.951e9,
-        ("bf16", "a", False): 6.415e9, ("bf16", "bc", False): 12.019e9,
-        ("int8", "a", False): 2.814e9, ("int8", "bc", False): 6.457e9,
-        # the learned budget at cutoff 0.99 with fallback m = 5 (its usual choice here)
-        ("int8", "a", True): 2.819e9, ("int8", "bc", True): 5.449e9,
-    },
-}
+# search kernels, from a one-pass ncu capture (a couple of launches of each kernel)
+# of the bench command on the named workload, keyed by (precision form, phase,
+# learned budget) and tied to the kernel sources it was captured on: when the
+# sources have changed since (SEARCH_SOURCES hash differs), no traffic figure is
+# reported rather than a stale one.
+NCU_TRAFFIC = {}
 NCU_TRAFFIC_QUERIES = 10_000
+SEARCH_SOURCES = ("common.cuh", "beam.cuh", "search_plain.cu", "search_bc.cu", "mixed.cu", "budget.cu")
+
+
+def search_src_hash() -> str:
+    import hashlib
+    hsh = hashlib.sha256()
+    for f in SEARCH_SOURCES:
+        with open(os.path.join(ROOT, "hrnn_b200", "csrc", f), "rb") as fh:
+            hsh.update(fh.read())
+    return hsh.hexdigest()[:16]
 
 
 def ncu_traffic(workload, form, phase, learned, nq):
-    """Measured DRAM bytes of one launch of that kernel, scaled from the capture's
-    10,000 queries to nq; None when the workload or form was not captured."""
-    v = NCU_TRAFFIC.get(workload, {}).get((form, phase, bool(learned)))
-    return None if v is None else int(v * nq / NCU_TRAFFIC_QUERIES)
+    """(DRAM bytes of one launch of that kernel scaled from the capture's queries to
+    nq, source note); (None, why) when not captured on the current kernels."""
+    cap = NCU_TRAFFIC.get(workload)
+    if not cap:
+        return None, "no capture of this workload"
+    if cap["src_hash"] != search_src_hash():
+        return None, f"capture {cap['src_hash']} predates the current kernel sources"
+    v = cap["bytes"].get((form, phase, bool(learned)))
+    if v is None:
+        return None, "form not captured"
+    return int(v * nq / cap["queries"]), (f"ncu dram__bytes_read.sum + dram__bytes_write.sum, one-pass capture of "
+                                          f"{cap['command']} on kernel sources {cap['src_hash']}, scaled by queries")
 
 
 def knng_quality(torch, h, X, K, dev, sample=1000, seed=5):
@@ -415,12 +427,11 @@ def main():
         tms, tb = phases[dom]
         achieved = tb / (tms / 1e3) / 1e9 if tms > 0 else 0.0
         form = {H.PREC_FP32_EXACT: "fp32", H.PREC_BF16: "bf16", H.PREC_INT8: "int8"}[prec]
-        traffic = ncu_traffic(args.workload, form, "a" if dom.startswith("phase_a") else "bc", learned, nq)
+        traffic, traffic_src = ncu_traffic(args.workload, form, "a" if dom.startswith("phase_a") else "bc", learned,
+                                           nq)
         roof = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
                 "frac": round(achieved / hbm, 4), "peak_source": peak_kind, "traffic": traffic,
-                "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of this kernel, one-pass "
-                                   "capture of this workload's timed steps, scaled by queries")
-                if traffic is not None else None,
+                "traffic_source": traffic_src,
                 "algorithmic_bytes_per_launch": int(tb), "launch_ms": round(tms, 3),
                 "per_query": {k_: round(st[k_] / nq, 3) for k_ in
                               ("n_dist", "n_expanded", "n_posting", "n_verified", "n_result", "n_lowp_decided",
@@ -547,9 +558,18 @@ def main():
                                    "join_mode": rs["join_mode"], "screen_survivors": rs["screen_survivors"],
                                    "screen_dense_nodes": rs["screen_dense_nodes"]}
 
-    cpu = None
+    cpu, parity = None, None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(h, W, Q, params, args.cpu_sample)
+        # Parity on this index: the plain form's answers for the CPU sample at the
+        # plain form's parameters, and the headline form's answers (from the e2e
+        # leg) whose every point the reference's own FP32 test must accept.
+        ns = min(args.cpu_sample, nq)
+        pparams = dict(params, m=mstars["plain"])
+        h.set_precision(H.PREC_FP32_EXACT)
+        plain_ans = h.search_rknn_batch(Q[:ns], pparams["m"], W["Kp"], W["ef"], threshold=1.0, k=W["k"])
+        _, kd_all, kc_all = h.get_knng_column(W["k"] - 1)
+        cpu, parity = cpu_baseline(h, W, Q, pparams, ns, gt=gt[:ns], plain_ans=plain_ans, head_ans=out[:ns],
+                                   head=head, X=X, kcol=(kd_all, kc_all))
         del h
         cpu["build"] = cpu_build_baseline(H, torch, dev, dev_sync)
         log(f"[bench] build baseline: {json.dumps(cpu['build'])}")
@@ -574,7 +594,7 @@ def main():
         "speedup_vs_plain": round(qps / results["plain"]["qps"], 3),
         "learned_budget": budget_info,
         "e2e": {k_: (round(v, 1) if isinstance(v, float) else v) for k_, v in e2e.items()},
-        "gpu_launches": int(launches), "roofline": roofline, "cpu_baseline": cpu, "clocks": ck,
+        "gpu_launches": int(launches), "roofline": roofline, "cpu_baseline": cpu, "parity": parity, "clocks": ck,
         "knng_build": {k_: (round(v, 3) if isinstance(v, float) else v) for k_, v in build.items()},
     }
     if rank == 0:
@@ -651,14 +671,19 @@ def _save_for_reference(h):
     return td, p
 
 
-def cpu_baseline(h, W, Q, params, sample):
+def cpu_baseline(h, W, Q, params, sample, gt=None, plain_ans=None, head_ans=None, head=None, X=None, kcol=None):
     """The reference's searchRknn (oracle/_ref) on the same index on this host's
     cores: all threads on `sample` queries, and one thread (the reference
-    protocol, src/hrnn_search.cpp:168-180) on a tenth of them."""
+    protocol, src/hrnn_search.cpp:168-180) on a tenth of them.  Returns
+    (baseline, parity): the reference's answers for the sample are compared query
+    by query with the GPU plain form's (`plain_ans`, same m, K', ef, k,
+    threshold), and every point the headline form returned (`head_ans`) is put
+    to the reference's own FP32 test d(q, p) <= kdist(p, k-1) (hrnn.h:2058-2069,
+    286-293) with the reference's L2 (space_l2.h)."""
     from oracle import ref
     if not ref.available():
-        return {"value": None, "unit": "queries/s", "cores": 0, "kind": "reference",
-                "sample": "oracle/_ref not built"}
+        return ({"value": None, "unit": "queries/s", "cores": 0, "kind": "reference",
+                 "sample": "oracle/_ref not built"}, None)
     import shutil
     td, p = _save_for_reference(h)
     try:
@@ -667,14 +692,40 @@ def cpu_baseline(h, W, Q, params, sample):
         log(f"[bench] reference loaded the index ({time.perf_counter() - t0:.1f}s)")
         cores = os.cpu_count() or 1
         Qs = Q[:sample]
-        _, secs = r.search_batch(Qs, params["m"], params["K_prime"], params["ef_search"], k=params["k"],
-                                 threads=cores, return_seconds=True)
+        res, secs = r.search_batch(Qs, params["m"], params["K_prime"], params["ef_search"], k=params["k"],
+                                   threads=cores, return_seconds=True)
         n1 = max(20, sample // 10)
         _, secs1 = r.search_batch(Q[:n1], params["m"], params["K_prime"], params["ef_search"], k=params["k"],
                                   threads=1, return_seconds=True)
-        return {"value": round(len(Qs) / secs, 1), "unit": "queries/s", "cores": cores, "kind": "reference",
+        base = {"value": round(len(Qs) / secs, 1), "unit": "queries/s", "cores": cores, "kind": "reference",
                 "sample": f"{len(Qs)} of the step's queries, {cores} threads (query-parallel searchRknn)",
                 "single_thread": {"value": round(n1 / secs1, 1), "sample": f"{n1} queries, 1 thread"}}
+        parity = None
+        if plain_ans is not None:
+            mism = [i for i in range(len(Qs)) if not np.array_equal(np.asarray(res[i], np.uint64),
+                                                                      np.asarray(plain_ans[i], np.uint64))]
+            parity = {"queries": len(Qs), "m": params["m"], "K_prime": params["K_prime"],
+                      "ef_search": params["ef_search"], "k": params["k"], "threshold": 1.0,
+                      "mismatches": len(mism), "first_mismatches": mism[:8],
+                      "answers": int(sum(len(x) for x in res))}
+            if gt is not None:
+                parity["recall_reference"] = round(macro_recall(gt, res), 4)
+                parity["recall_gpu_plain"] = round(macro_recall(gt, plain_ans), 4)
+        if head_ans is not None and X is not None and kcol is not None:
+            # labels are internal ids (the bench inserts in data order)
+            qi = np.concatenate([np.full(len(a), i, np.int64) for i, a in enumerate(head_ans)] + [np.zeros(0, np.int64)])
+            pi = np.concatenate([np.asarray(a, np.int64) for a in head_ans] + [np.zeros(0, np.int64)])
+            kd, kc = kcol
+            d_ref = ref.l2_batch(Qs[qi], X[pi]) if len(qi) else np.zeros(0, np.float32)
+            kdp = np.where(kc[pi] > params["k"] - 1, kd[pi], np.float32(np.finfo(np.float32).max)).astype(np.float32)
+            fail = d_ref > kdp
+            ulp = np.spacing(kdp).astype(np.float64)
+            band = np.abs(d_ref.astype(np.float64) - kdp.astype(np.float64)) <= 16.0 * ulp
+            parity = parity or {}
+            parity.update({"head_form": head, "head_answers": int(len(qi)),
+                           "lowp_false_accepts": int(np.sum(fail & ~band)),
+                           "fp64_band_accepts": int(np.sum(fail & band))})
+        return base, parity
     finally:
         shutil.rmtree(td, ignore_errors=True)
 
@@ -739,7 +790,7 @@ def run_reference_arm(args, W, h, Q, params, sweep, build):
     try:
         r = ref.RefIndex.load(p, W["d"])
         cores = os.cpu_count() or 1
-        per_step = min(W["nq"], 2000)
+        per_step = W["nq"]
         for i in range(args.warmup):
             r.search_batch(Q[:min(200, per_step)], params["m"], params["K_prime"], params["ef_search"],
                            k=params["k"], threads=cores)

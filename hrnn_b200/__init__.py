@@ -439,6 +439,13 @@ class HRNN:
         _check(_lib.hrnn_get_knng(self._h, _p(ids), _p(d), _p(cnt)))
         return ids, d, cnt
 
+    def get_knng_column(self, j: int):
+        """(ids[:, j], dists[:, j], cnt) of the KNN slot: e.g. j = k - 1 gives the
+        k-th neighbour distance the verification compares against (hrnn.h:286-293;
+        meaningful where cnt > j)."""
+        ids, d, cnt = self.get_knng()
+        return ids[:, j].copy(), d[:, j].copy(), cnt
+
     def set_knng(self, ids, dists, cnt):
         ids = np.ascontiguousarray(ids, np.uint32)
         dists = np.ascontiguousarray(dists, np.float32)

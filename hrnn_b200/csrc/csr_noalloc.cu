@@ -9,8 +9,9 @@
 //
 // Host code cannot use that array's name as a device address: the device
 // address is obtained once per device with cudaGetSymbolAddress, on the first
-// call with that device current.  Make that first call before any stream
-// capture.  All calls share the array, so calls that overlap on the GPU (two
+// call with that device current (and again if the device's context was
+// re-created since, e.g. by cudaDeviceReset).  Make that first call before any
+// stream capture.  All calls share the array, so calls that overlap on the GPU (two
 // streams, two threads) race; run them one after the other.  The array keeps the
 // last call's contents; every region that must start at zero is cleared here.
 //
@@ -38,30 +39,68 @@ constexpr int kScanT = 512, kScanPer = 8, kScanTile = kScanT * kScanPer;
 static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 
 std::mutex g_mu;
-void* g_addr[64] = {nullptr};
+struct ScratchSlot {
+    void* ctx = nullptr;   // the device context the address belongs to
+    void* addr = nullptr;
+};
+ScratchSlot g_slot[64];
+using CtxGetCurrent = int (*)(void**);  // cuCtxGetCurrent(CUcontext*), fetched through the runtime
 
+void* current_context() {
+    static CtxGetCurrent fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            f = nullptr;
+        return reinterpret_cast<CtxGetCurrent>(f);
+    }();
+    void* ctx = nullptr;
+    if (fn && fn(&ctx) != 0) ctx = nullptr;
+    return ctx;
+}
+
+// Device address of g_scratch on `dev` (current).  Looked up with
+// cudaGetSymbolAddress on the first call on a device, and again when the
+// device's context is not the one the cached address was taken in (after a
+// cudaDeviceReset the module is loaded anew and the array may move).
 void* scratch_address(int dev) {
     std::lock_guard<std::mutex> lk(g_mu);
     if (dev < 0 || dev >= 64) fail(HRNN_ERR_ARG, "build_rknng_noalloc: device ordinal out of range");
-    if (!g_addr[dev]) {
+    CUDA_CHECK(cudaSetDevice(dev));  // binds (and, after a reset, creates) the device's primary context
+    void* ctx = current_context();
+    ScratchSlot& sl = g_slot[dev];
+    if (!sl.addr || !ctx || ctx != sl.ctx) {
         void* p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
         if (e != cudaSuccess || !p)
             fail(HRNN_ERR_CUDA, std::string("build_rknng_noalloc: cudaGetSymbolAddress failed: ") +
                                     cudaGetErrorString(e));
-        g_addr[dev] = p;
+        sl.addr = p;
+        sl.ctx = ctx ? ctx : current_context();
     }
-    return g_addr[dev];
+    return sl.addr;
 }
 
+// In-degree histogram of the caller's graph, which is checked on the way: a count
+// above K or an id >= n is not followed but flagged in bad[0] / bad[1], and the
+// transpose stops with HRNN_ERR_ARG before anything is scattered.
 __global__ void na_degree(const uint32_t* __restrict__ ids, const uint32_t* __restrict__ cnt, size_t n, uint32_t K,
-                          uint32_t* __restrict__ deg) {
+                          uint32_t* __restrict__ deg, uint32_t* __restrict__ bad) {
     size_t warp = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     int lane = threadIdx.x & 31;
     size_t nw = ((size_t)gridDim.x * blockDim.x) >> 5;
     for (size_t i = warp; i < n; i += nw) {
         uint32_t c = cnt[i] & 0xFFFFu;
-        for (uint32_t j = lane; j < c; j += 32) atomicAdd(&deg[ids[i * K + j]], 1u);
+        if (c > K) {
+            if (lane == 0) atomicAdd(&bad[0], 1u);
+            continue;
+        }
+        for (uint32_t j = lane; j < c; j += 32) {
+            const uint32_t id = ids[i * K + j];
+            if (id < n) atomicAdd(&deg[id], 1u);
+            else atomicAdd(&bad[1], 1u);
+        }
     }
 }
 
@@ -224,15 +263,16 @@ uint64_t transpose(const uint32_t* ids, const uint32_t* cnt, size_t n, uint32_t 
     uint32_t* cursor = (uint32_t*)(base + al256((n + 1) * 4));
     uint32_t* big = (uint32_t*)((char*)cursor + al256((n + 1) * 4));
     uint64_t* part = (uint64_t*)((char*)big + al256((n + 1) * 4));
-    uint32_t* ctl = (uint32_t*)((char*)part + al256(tiles * 8));  // [0] n_big, [1] max P
+    // ctl: [0] n_big, [1] max P, [2] counts above K, [3] ids >= n
+    uint32_t* ctl = (uint32_t*)((char*)part + al256(tiles * 8));
     uint64_t* stage = (uint64_t*)((char*)ctl + 256);
     const size_t used = (size_t)((char*)stage - base);
     const size_t stage_words = (kScratchBytes - used) / 8;
     CUDA_CHECK(cudaMemsetAsync(deg, 0, (n + 1) * 4, s));
     CUDA_CHECK(cudaMemsetAsync(cursor, 0, (n + 1) * 4, s));
-    CUDA_CHECK(cudaMemsetAsync(ctl, 0, 8, s));
+    CUDA_CHECK(cudaMemsetAsync(ctl, 0, 16, s));
     const int grid = nsm * 8;
-    na_degree<<<grid, 256, 0, s>>>(ids, cnt, n, K, deg);
+    na_degree<<<grid, 256, 0, s>>>(ids, cnt, n, K, deg, ctl + 2);
     CUDA_LAUNCH_CHECK();
     na_scan_tiles<<<(unsigned)tiles, kScanT, 0, s>>>(deg, off, n + 1, part);
     CUDA_LAUNCH_CHECK();
@@ -241,8 +281,13 @@ uint64_t transpose(const uint32_t* ids, const uint32_t* cnt, size_t n, uint32_t 
     na_scan_add<<<(unsigned)tiles, kScanT, 0, s>>>(off, n + 1, part);
     CUDA_LAUNCH_CHECK();
     uint64_t total = 0;
+    uint32_t badc[2] = {0, 0};
     CUDA_CHECK(cudaMemcpyAsync(&total, off + n, 8, cudaMemcpyDeviceToHost, s));
+    CUDA_CHECK(cudaMemcpyAsync(badc, ctl + 2, 8, cudaMemcpyDeviceToHost, s));
     CUDA_CHECK(cudaStreamSynchronize(s));
+    if (badc[0] || badc[1])
+        fail(HRNN_ERR_ARG, "build_rknng_noalloc: the graph has " + std::to_string(badc[0]) +
+                               " count(s) above K and " + std::to_string(badc[1]) + " neighbour id(s) >= n");
     if (total > cap) return total;  // caller's entry buffer too small: report the need
     E* ent = static_cast<E*>(entries);
     na_scatter<E><<<grid, 256, 0, s>>>(ids, cnt, n, K, off, cursor, ent, rb);

@@ -159,8 +159,17 @@ void load_idx(Index& ix, const std::string& path, size_t dim, size_t max_element
     if (ix.label_offset < ix.offsetData || (ix.label_offset - ix.offsetData) != dim * 4)
         fail(HRNN_ERR_FORMAT, "loadIndex: vector size in file does not match dim");
     if (ix.size_data_per_element != ix.label_offset + 8 || ix.maxM0 > 4096 || ix.maxM > 4096 ||
-        (ix.K > 0 && ix.size_knng_slot != 4 + ix.K * 8))
+        (ix.K > 0 && ix.size_knng_slot != 4 + ix.K * 8) || ix.K > 0xFFFF ||
+        ix.offsetLevel0 + (1 + ix.maxM0) * 4 > ix.size_data_per_element ||
+        (ix.K > 0 && ix.offsetKNNG + ix.size_knng_slot > ix.size_data_per_element))
         fail(HRNN_ERR_FORMAT, "loadIndex: inconsistent element layout");
+    // Every id the device kernels follow is range-checked below before it is
+    // uploaded: a corrupt file is rejected here instead of becoming out-of-bounds
+    // device reads in the search and refinement kernels.
+    if (cur > 0xFFFFFFFEull) fail(HRNN_ERR_FORMAT, "loadIndex: element count beyond 32-bit ids");
+    if (cur > 0 && (ix.enterpoint >= cur || ix.maxlevel < 0))
+        fail(HRNN_ERR_FORMAT, "loadIndex: entry point out of range");
+    if (cur == 0 && ix.maxlevel >= 0) fail(HRNN_ERR_FORMAT, "loadIndex: entry point out of range");
     ix.dim = dim;
     ix.max_elements = max_elements;
     ix.cur = cur;
@@ -184,10 +193,16 @@ void load_idx(Index& ix, const std::string& path, size_t dim, size_t max_element
         kd.resize(c * std::max<size_t>(K, 1));
         vv.resize(c * dim);
         lb.resize(c);
-#pragma omp parallel for schedule(static)
+        int bad_links = 0, bad_knn = 0;
+#pragma omp parallel for schedule(static) reduction(| : bad_links, bad_knn)
         for (long long e = 0; e < (long long)c; ++e) {
             const char* rec = blob.data() + (size_t)e * S;
             std::memcpy(&a0[e * W], rec + ix.offsetLevel0, W * 4);
+            // level-0 links: count (low 16 bits) <= maxM0, ids < cur
+            const uint32_t lc = a0[e * W] & 0xFFFFu;
+            if (lc > ix.maxM0) bad_links = 1;
+            else
+                for (uint32_t j = 0; j < lc; ++j) bad_links |= a0[e * W + 1 + j] >= cur;
             if (K > 0) {
                 std::memcpy(&kh[e], rec + ix.offsetKNNG, 4);
                 const char* p = rec + ix.offsetKNNG + 4;
@@ -195,10 +210,17 @@ void load_idx(Index& ix, const std::string& path, size_t dim, size_t max_element
                     std::memcpy(&kid[e * K + j], p + j * 8, 4);
                     std::memcpy(&kd[e * K + j], p + j * 8 + 4, 4);
                 }
+                // KNN slot: count <= K, ids < cur
+                const uint32_t kc = kh[e] & 0xFFFFu;
+                if (kc > K) bad_knn = 1;
+                else
+                    for (uint32_t j = 0; j < kc; ++j) bad_knn |= kid[e * K + j] >= cur;
             }
             std::memcpy(&vv[e * dim], rec + ix.offsetData, dim * 4);
             std::memcpy(&lb[e], rec + ix.label_offset, 8);
         }
+        if (bad_links) fail(HRNN_ERR_FORMAT, "loadIndex: level-0 link count or id out of range");
+        if (bad_knn) fail(HRNN_ERR_FORMAT, "loadIndex: KNN-graph count or id out of range");
         CUDA_CHECK(cudaMemcpy(ix.adj0.as<uint32_t>() + base * W, a0.data(), c * W * 4, cudaMemcpyHostToDevice));
         if (K > 0) {
             CUDA_CHECK(cudaMemcpy(ix.knn_hdr.as<uint32_t>() + base, kh.data(), c * 4, cudaMemcpyHostToDevice));
@@ -226,6 +248,31 @@ void load_idx(Index& ix, const std::string& path, size_t dim, size_t max_element
         ix.upper.resize(w0 + sz / 4);
         r.bytes(ix.upper.data() + w0, sz);
     }
+    // Upper layers: the entry point reaches maxlevel, and a link at level l leads
+    // to an element that has level l (the descent then reads that element's
+    // level-l block, which must exist).
+    if (cur > 0 && ix.levels[ix.enterpoint] < ix.maxlevel)
+        fail(HRNN_ERR_FORMAT, "loadIndex: entry point below maxlevel");
+    {
+        const size_t WU = 1 + ix.maxM;
+        int bad = 0;
+#pragma omp parallel for schedule(static) reduction(| : bad)
+        for (long long i = 0; i < (long long)cur; ++i) {
+            for (int32_t l = 1; l <= ix.levels[i]; ++l) {
+                const uint32_t* blk = ix.upper.data() + ix.upper_off[i] + (size_t)(l - 1) * WU;
+                const uint32_t c = blk[0] & 0xFFFFu;
+                if (c > ix.maxM) {
+                    bad = 1;
+                    break;
+                }
+                for (uint32_t j = 0; j < c; ++j) {
+                    const uint32_t id = blk[1 + j];
+                    bad |= id >= cur || ix.levels[id] < l;
+                }
+            }
+        }
+        if (bad) fail(HRNN_ERR_FORMAT, "loadIndex: upper-layer link count or id out of range");
+    }
     ix.upper_dirty = true;
     ix.sync_upper_to_device();
     // Reverse CSR (hrnn.h:1024-1047).
@@ -251,6 +298,31 @@ void load_idx(Index& ix, const std::string& path, size_t dim, size_t max_element
         }
         if (no != cur + 1 || (no && off[no - 1] != ne))
             fail(HRNN_ERR_FORMAT, "loadIndex: inconsistent reverse CSR");
+        // Offsets ascend from 0; every entry's owner is an element and its rank a
+        // KNN-slot position (owner << rank_bits | rank, hrnn.h:1876-1880, 1910-1918).
+        const uint32_t eb_bits = ix.wide ? 64u : 32u;
+        if (ix.rank_bits >= eb_bits || (ix.K > 0 && ix.K > (1ull << ix.rank_bits)) || (no && off[0] != 0))
+            fail(HRNN_ERR_FORMAT, "loadIndex: inconsistent reverse CSR");
+        {
+            int bad = 0;
+            const uint64_t rmask = (1ull << ix.rank_bits) - 1;
+#pragma omp parallel for schedule(static) reduction(| : bad)
+            for (long long i = 1; i < (long long)no; ++i) bad |= off[i] < off[i - 1];
+            if (!bad) {
+#pragma omp parallel for schedule(static) reduction(| : bad)
+                for (long long e = 0; e < (long long)ne; ++e) {
+                    uint64_t x;
+                    if (ix.wide) std::memcpy(&x, ent.data() + (size_t)e * 8, 8);
+                    else {
+                        uint32_t x32;
+                        std::memcpy(&x32, ent.data() + (size_t)e * 4, 4);
+                        x = x32;
+                    }
+                    bad |= (x >> ix.rank_bits) >= cur || (x & rmask) >= std::max<size_t>(ix.K, 1);
+                }
+            }
+            if (bad) fail(HRNN_ERR_FORMAT, "loadIndex: reverse CSR offset, owner or rank out of range");
+        }
         ix.csr_off.alloc(no * 8);
         ix.csr_ent.alloc(ne * esz);
         CUDA_CHECK(cudaMemcpy(ix.csr_off.p, off.data(), no * 8, cudaMemcpyHostToDevice));

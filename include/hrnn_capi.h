@@ -340,11 +340,18 @@ hrnn_status hrnn_get_rknng(hrnn_index* h, uint64_t* n_offsets, uint64_t* n_entri
  *              node_bits + rank_bits <= 32 (*wide = 0), else u64;
  *   *n_entries receives the entry count (also on HRNN_ERR_CAPACITY).
  * Same output as hrnn_build_rknng + hrnn_get_rknng(..., reference_order = 0).
+ * The graph is checked on the device first: a count above K or a neighbour id
+ * >= n returns HRNN_ERR_ARG and nothing is scattered.
  * Its scratch is a fixed 32 MiB __device__ array in the library, held by every
- * GPU that loads it: n is limited to 2,097,152 (HRNN_ERR_LIMIT beyond), and one
- * reverse list to the scratch's staging size.  The first call on a device looks
- * up the array's address (make it before any stream capture).  Calls share the
- * array: calls that overlap on the GPU race; issue them one after another.
+ * GPU that loads it: n is limited to 2,097,152 (HRNN_ERR_LIMIT beyond).  The
+ * counters take 12 (n+1) bytes of it and the rest stages the sort of reverse
+ * lists longer than 16,384 entries, so one reverse list may hold at most the
+ * largest power of two <= (33,554,432 - 12 (n+1) - 8 ceil((n+1)/4096) - 1280) / 8
+ * entries: 524,288 at n = 2,097,152; every possible list (< n) at
+ * n <= 1,048,576.  A longer list returns HRNN_ERR_LIMIT.  The first call on a
+ * device looks up the array's address (again after the device's context was
+ * re-created); make it before any stream capture.  Calls share the array:
+ * calls that overlap on the GPU race; issue them one after another.
  * Runs on `stream` (cudaStream_t) on the current device and returns after it
  * finishes. */
 hrnn_status hrnn_build_rknng_noalloc(const uint32_t* d_knn_ids, const uint32_t* d_knn_cnt, size_t n,

@@ -95,7 +95,10 @@ class IdxFile:
 
 def read_idx(path: str) -> IdxFile:
     with open(path, "rb") as f:
-        raw = f.read()
+        return read_idx_bytes(f.read())
+
+
+def read_idx_bytes(raw: bytes) -> IdxFile:
     h = _HDR.unpack_from(raw, 0)
     if h[0] != MAGIC:
         raise ValueError("Not an HRNN index file (bad magic)")

@@ -63,10 +63,20 @@ def test_workloads_are_well_formed():
     assert "mixed-1M-d128-K500" in b.WORKLOADS
 
 
-def test_ncu_traffic_table():
+def test_ncu_traffic_is_tied_to_the_kernel_sources():
     b = _bench()
-    assert b.ncu_traffic("mixed-1M-d128-K500", "int8", "a", True, 10_000) == 2_819_000_000
-    assert b.ncu_traffic("mixed-1M-d128-K500", "int8", "bc", False, 10_000) == 6_457_000_000
-    assert b.ncu_traffic("mixed-1M-d128-K500", "fp32", "bc", False, 5_000) == 11_975_500_000
-    assert b.ncu_traffic("mixed-500k-d128-K250", "int8", "a", False, 10_000) is None
-    assert b.ncu_traffic("mixed-1M-d128-K500", "fp64", "a", False, 10_000) is None
+    saved = dict(b.NCU_TRAFFIC)
+    try:
+        b.NCU_TRAFFIC.clear()
+        b.NCU_TRAFFIC["w"] = {"src_hash": b.search_src_hash(), "queries": 10_000, "command": "c",
+                              "bytes": {("int8", "a", True): 2_819_000_000}}
+        v, src = b.ncu_traffic("w", "int8", "a", True, 5_000)
+        assert v == 1_409_500_000 and "c" in src
+        assert b.ncu_traffic("w", "int8", "bc", True, 5_000)[0] is None
+        assert b.ncu_traffic("other", "int8", "a", True, 5_000)[0] is None
+        b.NCU_TRAFFIC["w"]["src_hash"] = "0" * 16          # captured on other sources: not reported
+        v, src = b.ncu_traffic("w", "int8", "a", True, 5_000)
+        assert v is None and "predates" in src
+    finally:
+        b.NCU_TRAFFIC.clear()
+        b.NCU_TRAFFIC.update(saved)
