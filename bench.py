@@ -56,11 +56,36 @@ WORKLOADS = {
     "build-50k-d128-K100": dict(n=50_000, d=128, C=256, sigma=1.0, seed=2, dirichlet=True, nq=1_000,
                                 qseed=1002, M=16, efc=100, K=100, iters=3, S=50, k=10, Kp=100, ef=200,
                                 m_sweep=[5]),
-    # Large single-GPU case (build only): 10M x 96, 1024 equal Gaussians (sigma 1,
-    # seed 4), K_knng=200 (8 GB of ids + 8 GB of distances), reverse CSR of 2e9 entries.
+    # Large single-GPU case: 10M x 96, 1024 equal Gaussians (sigma 1, seed 4),
+    # K_knng=200 (8 GB of ids + 8 GB of distances), reverse CSR of 2e9 entries;
+    # 100,000 queries per step, recall against a float64 ground truth of the first
+    # 5,000 (radii computed only for the points the stored k-th distances let a
+    # query reach).
     "large-10M-d96-K200": dict(n=10_000_000, d=96, C=1024, sigma=1.0, seed=4, dirichlet=False, nq=100_000,
                                qseed=1004, M=16, efc=200, K=200, iters=10, S=50, k=10, Kp=200, ef=200,
-                               m_sweep=[1, 2, 3, 4, 5, 6, 8, 10, 20, 50]),
+                               m_sweep=[1, 2, 3, 4, 5, 6, 8, 10, 20, 50], gt_subset=5000, val_n=2000),
+    # Learned search budget: 1M x 256, 512 equal Gaussians (sigma 1.5, seed 3),
+    # K_knng=500; the MLP trained on 200,000 seeded queries (draw seed 1003) labelled
+    # by the method itself, evaluated on 20,000 held-out queries (draw seed 2003);
+    # the caller's m is 50 and the budget falls back to it below confidence 0.9.
+    "learned-1M-d256-K500": dict(n=1_000_000, d=256, C=512, sigma=1.5, seed=3, dirichlet=False, nq=20_000,
+                                 qseed=2003, tseed=1003, M=16, efc=400, K=500, iters=10, S=50, k=10, Kp=500,
+                                 ef=200, m_sweep=[50], fixed_m=50, fixed_conf=0.9, budget_levels=(3, 10, 0)),
+    # Batched uneven queries + dynamic inserts: the 1M mixture split 0.5 by the
+    # reference's permutation (std::shuffle, mt19937(42)); build on 500k, insert
+    # 500k in 10 batches of 50k (insertPointDynamic with m_update proxies), flat
+    # reverse CSR, then 10,000 queries per step with m ~ U{1..50}, ef_search ~
+    # U[50, 400] (parameter seed 7), K'=500, k=10, replayed from a captured plan.
+    "dynamic-1M-d128-K500": dict(n=1_000_000, d=128, C=256, sigma=1.0, seed=2, dirichlet=True, nq=10_000,
+                                 qseed=1002, M=16, efc=400, K=500, iters=10, S=50, k=10, Kp=500, ef=200,
+                                 m_sweep=[5], split=0.5, batches=10, m_update=10, bidirectional=False,
+                                 m_range=(1, 50), ef_range=(50, 400), pseed=7),
+    # The same protocol at the reference's CPU-runnable size (100k x 128, K_knng=100):
+    # the reference's own dynamic inserts run beside the GPU's on it.
+    "dynamic-100k-d128-K100": dict(n=100_000, d=128, C=64, sigma=1.0, seed=0, dirichlet=False, nq=1_000, qseed=1,
+                                   M=16, efc=400, K=100, iters=10, S=50, k=10, Kp=100, ef=200, m_sweep=[5],
+                                   split=0.5, batches=10, m_update=10, bidirectional=False,
+                                   m_range=(1, 50), ef_range=(50, 400), pseed=7),
     # The reference's CPU-runnable case: 100k x 128, 64 equal Gaussians (seed 0), K_knng=100.
     "plain-100k-d128-K100": dict(n=100_000, d=128, C=64, sigma=1.0, seed=0, dirichlet=False, nq=1_000, qseed=1,
                                  M=16, efc=400, K=100, iters=10, S=50, k=10, Kp=100, ef=200,
@@ -152,6 +177,16 @@ def max_over_ranks(torch, value: float, device, world: int) -> float:
 def replica_queries(W: dict, rank: int) -> np.ndarray:
     """Each replica answers its own query stream (draw seed offset by the rank)."""
     return mixture(W["nq"], W["d"], W["C"], W["sigma"], W["seed"], W["qseed"] + rank, dirichlet=W["dirichlet"])
+
+
+VALIDATION_SEED_OFFSET = 5003  # the validation stream: neither timed nor used for training
+
+
+def validation_queries(W: dict, n: int = 5000) -> np.ndarray:
+    """Queries on which the bench makes its parameter choices (the same mixture,
+    a draw seed of its own)."""
+    return mixture(min(n, W["nq"]), W["d"], W["C"], W["sigma"], W["seed"], W["qseed"] + VALIDATION_SEED_OFFSET,
+                   dirichlet=W["dirichlet"])
 
 
 def kth_radius_fp64(torch, X, k, dev):
@@ -289,6 +324,8 @@ def main():
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-budget form")
     ap.add_argument("--build-only", action="store_true", help="build the index, print its build times, exit")
     ap.add_argument("--budget-train", type=int, default=200_000, help="training queries of the budget MLP")
+    ap.add_argument("--budget-levels", default="", help="m0,m1,ef of the learned budget's levels "
+                                                         "(ef 0: the caller's beam; default: the workload's)")
     ap.add_argument("--queries", type=int, default=0, help="queries per step (default: the workload's)")
     ap.add_argument("--learned-precision", default="auto", choices=["auto", "bf16", "int8"],
                     help="reduced-precision form the learned budget runs on (auto: the faster one as timed)")
@@ -317,6 +354,13 @@ def main():
     def dev_sync():
         torch.cuda.synchronize(dev)
 
+    if args.workload.startswith("dynamic-"):
+        run_dynamic(args, W, H, torch, dev, dev_sync, rank, world, local)
+        if world > 1:
+            torch.distributed.barrier()
+            torch.distributed.destroy_process_group()
+        return
+
     t_gen = time.perf_counter()
     X = mixture(W["n"], W["d"], W["C"], W["sigma"], W["seed"], W["seed"], dirichlet=W["dirichlet"])
     Q = replica_queries(W, rank)
@@ -336,11 +380,27 @@ def main():
         return
 
     # ---- ground truth and the recall sweep (untimed) ----
+    # Every parameter choice (the smallest m reaching the recall target per form,
+    # the learned budget's confidence and fallback m) is made on a separate
+    # validation stream; recall is reported on the timed queries themselves.
     t_gt = time.perf_counter()
-    kth = kth_radius_fp64(torch, X, W["k"], dev)
-    gt = rknn_gt_fp64(torch, X, Q, kth, dev)
+    Qv = validation_queries(W, W.get("val_n", 5000))
+    if "gt_subset" in W:
+        # every point's radius is out of reach at this size: an upper bound of it
+        # (the stored k-th distance, widened past FP32 rounding) screens the points
+        # some query can reach, and only those get their exact float64 radius
+        from hrnn_b200 import groundtruth
+        up = h.get_kdist(W["k"]).astype(np.float64) * (1.0 + 1e-4)
+        ns = min(W["gt_subset"], len(Q))
+        g_, nr = groundtruth.rknn_fp64_bounded(X, np.concatenate([Q[:ns], Qv]), up, W["k"], dev)
+        gt, gtv = [np.sort(i) for i, _ in g_[:ns]], [np.sort(i) for i, _ in g_[ns:]]
+        build["ground_truth"] = {"queries_with_gt": ns, "validation_queries": len(Qv), "radii_computed": nr}
+    else:
+        kth = kth_radius_fp64(torch, X, W["k"], dev)
+        gt = rknn_gt_fp64(torch, X, Q, kth, dev)
+        gtv = rknn_gt_fp64(torch, X, Qv, kth, dev)
     log(f"[bench] fp64 ground truth ({time.perf_counter() - t_gt:.1f}s), mean |RkNN| "
-        f"{np.mean([len(g) for g in gt]):.2f}, empty {sum(len(g) == 0 for g in gt)}")
+        f"{np.mean([len(g) for g in gt]):.2f}, empty {sum(len(g) == 0 for g in gt)}; validation {len(Qv)} queries")
     # GT ids are data indices; index labels are data indices too.
     nq, d = Q.shape
     forms = {"plain": H.PREC_FP32_EXACT, "mixed": H.PREC_BF16}
@@ -348,11 +408,12 @@ def main():
         forms["mixed_int8"] = H.PREC_INT8
 
     def sweep_form(prec, stop=False):
+        """Recall on the validation stream per m; the smallest m reaching the target."""
         h.set_precision(prec)
         sw, mstar = {}, None
         for m in W["m_sweep"]:
-            res = h.search_rknn_batch(Q, m, W["Kp"], W["ef"], threshold=1.0, k=W["k"])
-            sw[m] = macro_recall(gt, res)
+            res = h.search_rknn_batch(Qv, m, W["Kp"], W["ef"], threshold=1.0, k=W["k"])
+            sw[m] = macro_recall(gtv, res)
             if mstar is None and sw[m] >= TARGET_RECALL:
                 mstar = m
                 if stop:
@@ -361,9 +422,12 @@ def main():
 
     sweeps, mstars = {}, {}
     for name, prec in forms.items():
+        if "fixed_m" in W:  # the workload states the caller's m
+            sweeps[name], mstars[name] = {}, W["fixed_m"]
+            continue
         sweeps[name], mstars[name] = sweep_form(prec)
-        log(f"[bench] {name}: recall sweep {json.dumps({k_: round(v_, 4) for k_, v_ in sweeps[name].items()})}"
-            f" -> m={mstars[name]}")
+        log(f"[bench] {name}: validation recall sweep "
+            f"{json.dumps({k_: round(v_, 4) for k_, v_ in sweeps[name].items()})} -> m={mstars[name]}")
     h.set_precision(H.PREC_FP32_EXACT)
     params = {"m": mstars["plain"], "K_prime": W["Kp"], "ef_search": W["ef"], "k": W["k"], "threshold": 1.0}
 
@@ -372,28 +436,34 @@ def main():
         return
 
     # ---- timed device steps, per form ----
-    q_dev = torch.from_numpy(Q).to(dev)
-    kp_dev = torch.full((nq,), W["Kp"], dtype=torch.int32, device=dev)
-    ef_dev = torch.full((nq,), W["ef"], dtype=torch.int32, device=dev)
-    cap = nq * 512
-    off_dev = torch.zeros(nq + 1, dtype=torch.int64, device=dev)
-    lab_dev = torch.zeros(cap, dtype=torch.int64, device=dev)
     stream = torch.cuda.current_stream(dev)
     hbm, bf16, peak_kind = load_peaks()
     maxM0 = 2 * W["M"]
+    qsets = {}
+    for qn, (QQ, GG) in {"timed": (Q, gt), "val": (Qv, gtv)}.items():
+        nn_ = QQ.shape[0]
+        qsets[qn] = {"n": nn_, "gt": GG, "q": torch.from_numpy(QQ).to(dev),
+                     "kp": torch.full((nn_,), W["Kp"], dtype=torch.int32, device=dev),
+                     "ef": torch.full((nn_,), W["ef"], dtype=torch.int32, device=dev),
+                     "off": torch.zeros(nn_ + 1, dtype=torch.int64, device=dev),
+                     "lab": torch.zeros(nn_ * 512, dtype=torch.int64, device=dev), "cap": nn_ * 512}
 
-    def timed(prec, m_star, learned=False, steps=None, name=None):
+    def timed(prec, m_star, learned=False, steps=None, name=None, qset="timed"):
+        """Times `steps` batch calls on the query set (after the warm-up calls);
+        the recall reported is that of the timed calls' answers."""
         steps = steps or args.steps
+        S = qsets[qset]
+        nq_ = S["n"]
         clocks = ClockSampler(local)
         h.set_precision(prec)
         if learned:
             h.set_budget(True, **BUDGET)
-        m_dev = torch.full((nq,), m_star, dtype=torch.int32, device=dev)
+        m_dev = torch.full((nq_,), m_star, dtype=torch.int32, device=dev)
 
         def step():
-            return h.search_rknn_batch_device(q_dev.data_ptr(), nq, m_dev.data_ptr(), kp_dev.data_ptr(),
-                                              ef_dev.data_ptr(), 1.0, W["k"], off_dev.data_ptr(),
-                                              lab_dev.data_ptr(), cap, stream.cuda_stream)
+            return h.search_rknn_batch_device(S["q"].data_ptr(), nq_, m_dev.data_ptr(), S["kp"].data_ptr(),
+                                              S["ef"].data_ptr(), 1.0, W["k"], S["off"].data_ptr(),
+                                              S["lab"].data_ptr(), S["cap"], stream.cuda_stream)
 
         for _ in range(args.warmup):
             step()
@@ -404,9 +474,9 @@ def main():
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.nvtx.range_push("timed")  # profilers select the timed steps with this range
         e0.record(stream)
-        launches = 0
+        launches, tot = 0, 0
         for _ in range(steps):
-            step()
+            tot = step()
             launches += h.last_search_stats()["n_launches"]
         e1.record(stream)
         dev_sync()
@@ -414,6 +484,9 @@ def main():
         ck = clocks.stop()
         ms = max_over_ranks(torch, e0.elapsed_time(e1), dev, world)
         st = h.last_search_stats()
+        offs = S["off"].cpu().numpy()
+        labs = S["lab"][:tot].cpu().numpy()
+        recall = macro_recall(S["gt"], [labs[offs[i]:offs[i + 1]] for i in range(nq_)])
         # algorithmic bytes of the two phases: rows of 4 bytes/element (FP32), 2 (BF16)
         # or 1 plus 16 bytes of scale / error terms (INT8); the k-distance of each
         # verified id; the FP32 rows of the screens' undecided ids
@@ -428,12 +501,12 @@ def main():
         achieved = tb / (tms / 1e3) / 1e9 if tms > 0 else 0.0
         form = {H.PREC_FP32_EXACT: "fp32", H.PREC_BF16: "bf16", H.PREC_INT8: "int8"}[prec]
         traffic, traffic_src = ncu_traffic(args.workload, form, "a" if dom.startswith("phase_a") else "bc", learned,
-                                           nq)
+                                           nq_)
         roof = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
                 "frac": round(achieved / hbm, 4), "peak_source": peak_kind, "traffic": traffic,
                 "traffic_source": traffic_src,
                 "algorithmic_bytes_per_launch": int(tb), "launch_ms": round(tms, 3),
-                "per_query": {k_: round(st[k_] / nq, 3) for k_ in
+                "per_query": {k_: round(st[k_] / nq_, 3) for k_ in
                               ("n_dist", "n_expanded", "n_posting", "n_verified", "n_result", "n_lowp_decided",
                                "n_fp32_decided", "n_fp64_decided", "n_fp64_flipped")},
                 "phase_ms": {"a": round(st["phase_a_ms"], 3), "b": round(st["phase_b_ms"], 3),
@@ -441,8 +514,9 @@ def main():
         if learned:
             roof["budget_levels"] = st["n_budget"]
             h.set_budget(False, **BUDGET)
-        return {"qps": world * nq * steps / (ms / 1e3), "ms_per_step": ms / steps, "launches": launches,
-                "roofline": roof, "clocks": ck, "m": m_star, "prec": prec, "recall_sweep": sweeps[name]}
+        return {"qps": world * nq_ * steps / (ms / 1e3), "ms_per_step": ms / steps, "launches": launches,
+                "roofline": roof, "clocks": ck, "m": m_star, "prec": prec, "recall_sweep": sweeps[name],
+                "recall": recall}
 
     results = {}
     for name, prec in forms.items():
@@ -460,10 +534,18 @@ def main():
             if lp not in forms:
                 lp = "mixed"
         lprec = forms[lp]
+        if args.budget_levels:
+            m0_, m1_, ef_ = (int(x) for x in args.budget_levels.split(","))
+            BUDGET.update(m0=m0_, m1=m1_, ef=ef_)
+        elif "budget_levels" in W:
+            BUDGET.update(dict(zip(("m0", "m1", "ef"), W["budget_levels"])))
         budget_info = train_budget(H, h, W, args, dev_sync, lprec)
         budget_info["precision_form"] = lp
         cands = []
-        for c in CONFIDENCES:
+        for c in ([W["fixed_conf"]] if "fixed_conf" in W else CONFIDENCES):
+            if "fixed_m" in W:  # the workload states the fallback m and the cutoff
+                cands.append((c, W["fixed_m"], {}))
+                continue
             BUDGET["confidence"] = c
             h.set_budget(True, **BUDGET)
             sw, mstar = sweep_form(lprec, stop=True)
@@ -474,14 +556,17 @@ def main():
         h.set_budget(False, **BUDGET)
         h.set_precision(H.PREC_FP32_EXACT)
         trial = []
-        for c, mstar, sw in cands:
+        for c, mstar, sw in cands:  # timed on the validation stream
             BUDGET["confidence"] = c
             sweeps["learned"] = sw
-            r = timed(lprec, mstar, learned=True, steps=3, name="learned")
-            trial.append({"confidence": c, "m": mstar, "recall": round(sw[mstar], 4), "value": round(r["qps"], 1)})
+            r = timed(lprec, mstar, learned=True, steps=3, name="learned", qset="val")
+            trial.append({"confidence": c, "m": mstar, "recall_val": round(r["recall"], 4),
+                          "value_val": round(r["qps"], 1)})
         budget_info["candidates"] = trial
+        if "fixed_conf" not in W:
+            trial = [t_ for t_ in trial if t_["recall_val"] >= TARGET_RECALL]
         if trial:
-            best = max(trial, key=lambda t_: t_["value"])
+            best = max(trial, key=lambda t_: t_["value_val"])
             BUDGET["confidence"] = best["confidence"]
             sweeps["learned"] = next(sw for c, _, sw in cands if c == best["confidence"])
             mstars["learned"] = best["m"]
@@ -585,11 +670,13 @@ def main():
         "config": {"workload": args.workload, "n": W["n"], "dim": d, "K_knng": W["K"], "M": W["M"],
                    "ef_construction": W["efc"], "queries_per_step": nq, "form": head,
                    **params, "recall_macro": round(recall_timed, 4),
-                   "recall_sweep": {str(k_): round(v, 4) for k_, v in sweep.items()},
+                   "recall_sweep_validation": {str(k_): round(v, 4) for k_, v in sweep.items()},
+                   "selection": "m (and the learned budget's confidence) chosen on a separate validation stream "
+                                "of seeded queries; recall_macro is that of the timed queries' answers",
                    "parallelism": f"replicas{world}", "l2_flush": "inputs larger than L2 (index 7 GB)"},
         "forms": {k_: {"value": round(r_["qps"], 1), "ms_per_step": round(r_["ms_per_step"], 3), "m": r_["m"],
-                       "clocks": r_["clocks"],
-                       "recall_sweep": {str(a_): round(b_, 4) for a_, b_ in r_["recall_sweep"].items()},
+                       "recall_macro": round(r_["recall"], 4), "clocks": r_["clocks"],
+                       "recall_sweep_validation": {str(a_): round(b_, 4) for a_, b_ in r_["recall_sweep"].items()},
                        "roofline": r_["roofline"]} for k_, r_ in results.items()},
         "speedup_vs_plain": round(qps / results["plain"]["qps"], 3),
         "learned_budget": budget_info,
@@ -602,6 +689,253 @@ def main():
     if world > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# Batched uneven queries after dynamic inserts (the dynamic-* workloads)
+# ---------------------------------------------------------------------------
+
+def uneven_params(W: dict, nq: int):
+    """Per-query m ~ U{m_range}, ef_search ~ U[ef_range] (seeded), K' and k fixed."""
+    r = np.random.default_rng(W["pseed"])
+    m = r.integers(W["m_range"][0], W["m_range"][1] + 1, nq).astype(np.uint32)
+    ef = r.integers(W["ef_range"][0], W["ef_range"][1] + 1, nq).astype(np.uint32)
+    return m, np.full(nq, W["Kp"], np.uint32), ef
+
+
+def dynamic_build(H, W, X, dev_sync, perm, ref=False, threads=1):
+    """The reference's dynamic protocol (src/hrnn_dynamic_test.cpp:200-203, 240-262,
+    268-288, 305-331, 368): build on the first split of the permutation (labels =
+    data indices), refineKNNG, buildRKNNG_mutable, insertPointDynamic for the rest
+    in batches, then the flat reverse CSR the search reads.  ref=True runs the
+    reference's own code (oracle/_ref) with `threads` host threads instead."""
+    n = W["n"]
+    split = int(n * W["split"])
+    base, ins = perm[:split].astype(np.uint64), perm[split:].astype(np.uint64)
+    t = {}
+    with StdoutToStderr():
+        if ref:
+            from oracle import ref as R
+            h = R.RefIndex.create(W["d"], n, W["M"], W["efc"], 100, W["K"])
+        else:
+            h = H.HRNN(W["d"], n, W["M"], W["efc"], 100, W["K"])
+        t0 = time.perf_counter()
+        if ref:
+            h.add_points(X[base.astype(np.int64)], labels=base, threads=threads)
+        else:
+            h.add_points(X[base.astype(np.int64)], labels=base)
+        dev_sync()
+        t1 = time.perf_counter()
+        if ref:
+            h.refine(W["iters"], W["S"], threads=threads)
+            h.build_mutable()
+        else:
+            h.refineKNNG(W["iters"], W["S"])
+            h.buildRKNNG_mutable()
+        dev_sync()
+        t2 = time.perf_counter()
+        nb = W["batches"]
+        per = (len(ins) + nb - 1) // nb
+        batch_ms, dyn = [], []
+        for b in range(nb):
+            sl = ins[b * per:(b + 1) * per]
+            if len(sl) == 0:
+                continue
+            tb = time.perf_counter()
+            if ref:
+                h.insert_dynamic(X[sl.astype(np.int64)], sl, m_update=W["m_update"],
+                                 bidirectional=W["bidirectional"], threads=threads)
+            else:
+                h.insertPointDynamic(X[sl.astype(np.int64)], sl, W["m_update"], W["bidirectional"])
+            dev_sync()
+            batch_ms.append(round((time.perf_counter() - tb) * 1e3, 2))
+            if not ref:
+                dyn.append({k_: (round(v_, 2) if isinstance(v_, float) else v_)
+                            for k_, v_ in h.last_dynamic_stats().items()})
+        t3 = time.perf_counter()
+        if ref:
+            h.build_rknng()
+        else:
+            h.buildRKNNG()
+        dev_sync()
+        t4 = time.perf_counter()
+    t = {"initial_points": int(split), "inserted_points": int(len(ins)), "batches": len(batch_ms),
+         "hnsw_insert_s": round(t1 - t0, 3), "refine_and_mutable_s": round(t2 - t1, 3),
+         "insert_total_s": round(t3 - t2, 3), "insert_batch_ms": batch_ms,
+         "insert_points_per_s": round(len(ins) / max(t3 - t2, 1e-9), 1), "flat_rknng_s": round(t4 - t3, 3),
+         "m_update": W["m_update"], "bidirectional": bool(W["bidirectional"])}
+    if dyn:
+        t["per_batch"] = dyn
+    return h, t
+
+
+def run_dynamic(args, W, H, torch, dev, dev_sync, rank, world, local):
+    X = mixture(W["n"], W["d"], W["C"], W["sigma"], W["seed"], W["seed"], dirichlet=W["dirichlet"])
+    Q = replica_queries(W, rank)
+    nq, d = Q.shape
+    perm = H.dynamic_split(W["n"], 42)
+    m_h, kp_h, ef_h = uneven_params(W, nq)
+    h, dyn = dynamic_build(H, W, X, dev_sync, perm)
+    log(f"[bench] dynamic build: {json.dumps({k_: v_ for k_, v_ in dyn.items() if k_ != 'per_batch'})}")
+    kth = kth_radius_fp64(torch, X, W["k"], dev)
+    gt = rknn_gt_fp64(torch, X, Q, kth, dev)
+    if args.impl == "reference":
+        run_reference_arm(args, W, h, Q, {"m": m_h, "K_prime": kp_h, "ef_search": ef_h, "k": W["k"],
+                                          "threshold": 1.0}, None, dyn)
+        return
+    stream = torch.cuda.current_stream(dev)
+    q_d = torch.from_numpy(Q).to(dev)
+    m_d = torch.from_numpy(m_h.view(np.int32)).to(dev)
+    kp_d = torch.from_numpy(kp_h.view(np.int32)).to(dev)
+    ef_d = torch.from_numpy(ef_h.view(np.int32)).to(dev)
+    cap = nq * 2048
+    off_d = torch.zeros(nq + 1, dtype=torch.int64, device=dev)
+    lab_d = torch.zeros(cap, dtype=torch.int64, device=dev)
+    hbm, _, peak_kind = load_peaks()
+    forms = {"plain": H.PREC_FP32_EXACT, "mixed_int8": H.PREC_INT8}
+    out = {}
+    answers = {}
+    for name, prec in forms.items():
+        h.set_precision(prec)
+        # stream-ordered batch calls
+        def step():
+            return h.search_rknn_batch_device(q_d.data_ptr(), nq, m_d.data_ptr(), kp_d.data_ptr(), ef_d.data_ptr(),
+                                              1.0, W["k"], off_d.data_ptr(), lab_d.data_ptr(), cap,
+                                              stream.cuda_stream)
+        for _ in range(args.warmup):
+            step()
+        dev_sync()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            tot = step()
+        e1.record(stream)
+        dev_sync()
+        ms_b = max_over_ranks(torch, e0.elapsed_time(e1), dev, world)
+        st = h.last_search_stats()
+        offs, labs = off_d.cpu().numpy(), lab_d[:tot].cpu().numpy()
+        ans_b = [labs[offs[i]:offs[i + 1]].copy() for i in range(nq)]
+        # the same batch replayed from a captured plan (one graph launch per batch)
+        plan = h.search_plan(q_d.data_ptr(), nq, m_d.data_ptr(), kp_d.data_ptr(), ef_d.data_ptr(),
+                             W["m_range"][1], W["ef_range"][1], 1.0, W["k"], off_d.data_ptr(), lab_d.data_ptr(), cap,
+                             stream.cuda_stream)
+        clocks = ClockSampler(local)
+        for _ in range(args.warmup):
+            plan.run(stream.cuda_stream)
+        dev_sync()
+        clocks.start()
+        e0.record(stream)
+        for _ in range(args.steps):
+            plan.run(stream.cuda_stream)
+        e1.record(stream)
+        dev_sync()
+        ck = clocks.stop()
+        ms_p = max_over_ranks(torch, e0.elapsed_time(e1), dev, world)
+        tot_p, clamped = plan.result(stream.cuda_stream)
+        plan.close()
+        offs, labs = off_d.cpu().numpy(), lab_d[:tot_p].cpu().numpy()
+        ans_p = [labs[offs[i]:offs[i + 1]].copy() for i in range(nq)]
+        same = sum(np.array_equal(a, b) for a, b in zip(ans_b, ans_p))
+        answers[name] = ans_p
+        rb, rm = {H.PREC_FP32_EXACT: (4, 0), H.PREC_INT8: (1, 16)}[prec]
+        bytes_bc = st["n_posting"] * 4 + st["n_verified"] * (d * rb + rm + 4) + st["n_fp32_decided"] * d * 4 + \
+            st["n_result"] * 8
+        bytes_a = st["n_dist"] * (d * rb + rm) + st["n_expanded"] * (4 + 4 * 2 * W["M"])
+        phases = {"phase_a_beam_search": (st["phase_a_ms"], bytes_a),
+                  "phase_bc_posting_verify": (st["phase_c_ms"], bytes_bc)}
+        dom = max(phases, key=lambda k_: phases[k_][0])
+        tms, tb = phases[dom]
+        achieved = tb / (tms / 1e3) / 1e9 if tms > 0 else 0.0
+        out[name] = {"value_plan": round(world * nq * args.steps / (ms_p / 1e3), 1),
+                     "value_batch_calls": round(world * nq * args.steps / (ms_b / 1e3), 1),
+                     "ms_per_step_plan": round(ms_p / args.steps, 3), "ms_per_step_batch": round(ms_b / args.steps, 3),
+                     "recall_macro": round(macro_recall(gt, ans_p), 4), "plan_equals_batch_calls": int(same),
+                     "clamped": bool(clamped), "clocks": ck,
+                     "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": hbm,
+                                  "unit": "GB/s", "frac": round(achieved / hbm, 4), "peak_source": peak_kind,
+                                  "traffic": None, "algorithmic_bytes_per_launch": int(tb),
+                                  "launch_ms": round(tms, 3),
+                                  "phase_ms": {"a": round(st["phase_a_ms"], 3), "b": round(st["phase_b_ms"], 3),
+                                               "c": round(st["phase_c_ms"], 3)},
+                                  "per_query": {k_: round(st[k_] / nq, 2) for k_ in
+                                                ("n_dist", "n_expanded", "n_posting", "n_verified", "n_result")}},
+                     "a_launch_shape": {"warps_per_block": st["a_warps_per_block"],
+                                        "visit_slots": st["a_visit_slots"]}}
+        log(f"[bench] {name}: {json.dumps({k_: v_ for k_, v_ in out[name].items() if k_ != 'roofline'})}")
+    h.set_precision(H.PREC_FP32_EXACT)
+    # end to end: the host-buffer entry point with the per-query arrays
+    q_pin = torch.from_numpy(np.ascontiguousarray(Q)).pin_memory()
+    pm, pk, pe = (torch.from_numpy(a.view(np.int32)).pin_memory() for a in (m_h, kp_h, ef_h))
+    p_off = torch.zeros(nq + 1, dtype=torch.int64).pin_memory()
+    p_lab = torch.zeros(cap, dtype=torch.int64).pin_memory()
+    for _ in range(max(1, args.warmup)):
+        h.search_rknn_batch_host(q_pin.data_ptr(), nq, pm.data_ptr(), pk.data_ptr(), pe.data_ptr(), 1.0, W["k"],
+                                 p_off.data_ptr(), p_lab.data_ptr(), cap)
+    dev_sync()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        tot = h.search_rknn_batch_host(q_pin.data_ptr(), nq, pm.data_ptr(), pk.data_ptr(), pe.data_ptr(), 1.0,
+                                       W["k"], p_off.data_ptr(), p_lab.data_ptr(), cap)
+    e2e_s = max_over_ranks(torch, time.perf_counter() - t0, dev, world)
+    e2e = {"value": round(world * nq * args.steps / e2e_s, 1), "unit": "queries/s",
+           "h2d_bytes_per_step": int(nq * d * 4 + 3 * nq * 4), "d2h_bytes_per_step": int((nq + 1) * 8 + tot * 8),
+           "host_buffers": "pinned", "form": "plain"}
+    # parity of the plain form's answers with the reference's searchRknn on this index
+    parity, cpu = None, None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import ref
+        if ref.available():
+            import shutil
+            td, pth = _save_for_reference(h)
+            try:
+                r = ref.RefIndex.load(pth, W["d"])
+                ns = min(args.cpu_sample, nq)
+                cores = os.cpu_count() or 1
+                res, secs = r.search_batch(Q[:ns], m_h[:ns], kp_h[:ns], ef_h[:ns], k=W["k"], threads=cores,
+                                           return_seconds=True)
+                mism = [i for i in range(ns) if not np.array_equal(np.asarray(res[i], np.uint64),
+                                                                     np.asarray(answers["plain"][i], np.uint64))]
+                parity = {"queries": ns, "mismatches": len(mism), "first_mismatches": mism[:8],
+                          "params": "per-query m, ef_search as timed"}
+                cpu = {"value": round(ns / secs, 1), "unit": "queries/s", "cores": cores, "kind": "reference",
+                       "sample": f"{ns} of the step's queries, {cores} threads"}
+                del r
+            finally:
+                shutil.rmtree(td, ignore_errors=True)
+    head = max(out, key=lambda k_: out[k_]["value_plan"])
+    line = {
+        "metric": "RkNN queries/s (k=10), uneven per-query m and ef_search after dynamic inserts",
+        "value": out[head]["value_plan"], "unit": "queries/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": out[head]["ms_per_step_plan"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32" if head == "plain" else "int8 beam/screen + f32/f64",
+        "data": "synthetic (seeded Gaussian mixture)",
+        "config": {"workload": args.workload, "n": W["n"], "dim": d, "K_knng": W["K"], "M": W["M"],
+                   "ef_construction": W["efc"], "queries_per_step": nq, "form": head, "K_prime": W["Kp"],
+                   "m": f"U{{{W['m_range'][0]}..{W['m_range'][1]}}}", "ef_search": f"U[{W['ef_range'][0]}, "
+                   f"{W['ef_range'][1]}]", "k": W["k"], "recall_macro": out[head]["recall_macro"],
+                   "l2_flush": "inputs larger than L2 (index > 3 GB)", "parallelism": f"replicas{world}"},
+        "forms": out, "dynamic": dyn, "e2e": e2e, "parity": parity, "cpu_baseline": cpu,
+        "roofline": out[head]["roofline"], "clocks": out[head]["clocks"],
+    }
+    if W["n"] <= 200_000 and rank == 0 and not args.no_cpu_baseline:
+        line["reference_dynamic"] = reference_dynamic(H, W, X, Q, gt, m_h, kp_h, ef_h)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def reference_dynamic(H, W, X, Q, gt, m_h, kp_h, ef_h):
+    """The reference's own dynamic protocol on the same points, permutation and
+    queries with all host threads: build, insert and recall beside the GPU's."""
+    from oracle import ref
+    if not ref.available():
+        return {"kind": "reference", "sample": "oracle/_ref not built"}
+    cores = os.cpu_count() or 1
+    perm = H.dynamic_split(W["n"], 42)
+    r, t = dynamic_build(H, W, X, lambda: None, perm, ref=True, threads=cores)
+    res, secs = r.search_batch(Q, m_h, kp_h, ef_h, k=W["k"], threads=cores, return_seconds=True)
+    t.update({"kind": "reference", "cores": cores, "recall_macro": round(macro_recall(gt, res), 4),
+              "search_queries_per_s": round(len(Q) / secs, 1)})
+    return t
 
 
 # Learned budget: level 0 = 1 proxy, level 1 = 3 proxies, taken from the caller's
@@ -624,7 +958,8 @@ def train_budget(H, h, W, args, dev_sync, prec):
     from the timed ones) in the serving precision `prec`, then MLP training on the GPU."""
     t0 = time.perf_counter()
     n = args.budget_train
-    Qtr = mixture(n, W["d"], W["C"], W["sigma"], W["seed"], W["qseed"] + 7919, dirichlet=W["dirichlet"])
+    Qtr = mixture(n, W["d"], W["C"], W["sigma"], W["seed"], W.get("tseed", W["qseed"] + 7919),
+                  dirichlet=W["dirichlet"])
     h.set_precision(prec)
     full = _search_sets(h, Qtr, LABEL_M, W["Kp"], LABEL_EF, W["k"])
     Y = np.zeros((n, 2), np.uint8)
@@ -791,16 +1126,21 @@ def run_reference_arm(args, W, h, Q, params, sweep, build):
         r = ref.RefIndex.load(p, W["d"])
         cores = os.cpu_count() or 1
         per_step = W["nq"]
+
+        def sel(v, a, b):  # per-query parameter arrays follow their queries
+            return v[a:b] if isinstance(v, np.ndarray) else v
+
+        def run(a, b, secs=False):
+            return r.search_batch(Q[a:b], sel(params["m"], a, b), sel(params["K_prime"], a, b),
+                                  sel(params["ef_search"], a, b), k=params["k"], threads=cores, return_seconds=secs)
+
         for i in range(args.warmup):
-            r.search_batch(Q[:min(200, per_step)], params["m"], params["K_prime"], params["ef_search"],
-                           k=params["k"], threads=cores)
+            run(0, min(200, per_step))
         tot_q, tot_s = 0, 0.0
-        res_all = []
         for i in range(args.steps):
-            Qs = Q[(i * per_step) % W["nq"]:][:per_step]
-            res, secs = r.search_batch(Qs, params["m"], params["K_prime"], params["ef_search"], k=params["k"],
-                                       threads=cores, return_seconds=True)
-            tot_q += len(Qs)
+            a = (i * per_step) % W["nq"]
+            res, secs = run(a, a + per_step, True)
+            tot_q += len(res)
             tot_s += secs
         v = tot_q / tot_s
         line = {"impl": "reference", "metric": "RkNN queries/s at recall>=0.95 (k=10)", "value": round(v, 1),
@@ -808,7 +1148,9 @@ def run_reference_arm(args, W, h, Q, params, sweep, build):
                 "ms_per_step": round(1e3 * tot_s / args.steps, 3), "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Gaussian mixture)",
                 "config": {"workload": args.workload, "n": W["n"], "dim": W["d"], "K_knng": W["K"],
-                           "queries_per_step": per_step, **params,
+                           "queries_per_step": per_step,
+                           **{k_: (v_ if not isinstance(v_, np.ndarray) else "per-query, as the GPU arm's")
+                              for k_, v_ in params.items()},
                            "index": "the same .idx file (built by the GPU builder; the reference loads it "
                                     "with HRNN(space, path))"},
                 "cpu_baseline": {"value": round(v, 1), "unit": "queries/s", "cores": cores, "kind": "reference",

@@ -36,6 +36,7 @@ EXPORTS = [
     "hrnn_set_knng", "hrnn_get_rknng", "hrnn_l2_batch", "hrnn_build_rknng_noalloc",
     "hrnn_set_budget", "hrnn_budget_features", "hrnn_budget_train", "hrnn_budget_predict",
     "hrnn_budget_gradients", "hrnn_budget_get_weights", "hrnn_budget_set_weights", "hrnn_get_dynamic_stats",
+    "hrnn_dynamic_split", "hrnn_get_kdist",
 ]
 
 # Learned-budget MLP: 256 -> 256 -> 256 -> 2; parameters W1 b1 W2 b2 W3 b3 (row-major
@@ -193,6 +194,14 @@ def build_rknng_noalloc(d_knn_ids: int, d_knn_cnt: int, n: int, K: int, d_offset
     _check(_lib.hrnn_build_rknng_noalloc(_vp(d_knn_ids), _vp(d_knn_cnt), n, K, _vp(d_offsets), _vp(d_entries),
                                          entries_cap, C.byref(rb), C.byref(wide), C.byref(ne), _vp(stream)))
     return rb.value, bool(wide.value), ne.value
+
+
+def dynamic_split(n: int, seed: int = 42) -> np.ndarray:
+    """0..n-1 shuffled by std::shuffle with std::mt19937(seed): the split of the
+    reference's src/hrnn_dynamic_test.cpp:200-203 (first split*n build, rest insert)."""
+    perm = np.empty(n, np.uint32)
+    _check(_lib.hrnn_dynamic_split(C.c_uint64(n), C.c_uint32(seed), _p(perm)))
+    return perm
 
 
 def _split_params(flat):
@@ -438,6 +447,13 @@ class HRNN:
         cnt = np.zeros(n, np.uint32)
         _check(_lib.hrnn_get_knng(self._h, _p(ids), _p(d), _p(cnt)))
         return ids, d, cnt
+
+    def get_kdist(self, k: int) -> np.ndarray:
+        """kdist(p, k-1) of every element (FLT_MAX where the list is shorter than
+        k): the radius the verification compares against (hrnn.h:286-293)."""
+        out = np.empty(self.getCurrentElementCount(), np.float32)
+        _check(_lib.hrnn_get_kdist(self._h, C.c_uint32(k), _p(out)))
+        return out
 
     def get_knng_column(self, j: int):
         """(ids[:, j], dists[:, j], cnt) of the KNN slot: e.g. j = k - 1 gives the

@@ -1,0 +1,270 @@
+// Two-parent best-first search of level 0 for the reduced-precision search forms
+// (INT8 / BF16 rows).  Their proxies only choose candidates -- every returned
+// point is decided exactly afterwards -- so this search is free to differ from
+// searchBaseLayerST's sequential order (hrnn.h:484-616), which the exact form's
+// beam.cuh keeps:
+//
+//   * each step expands the two best unexpanded beam entries together: both link
+//     rows are loaded at once and all their fresh neighbours (up to 64) are
+//     scored in one memory round trip (two INT8 rows per lane), so a step costs
+//     one dependent row-gather latency for two expansions;
+//   * a scored neighbour enters the beam when it is closer than a full beam's last
+//     entry (no per-neighbour sequential acceptance count), duplicates within a
+//     step are merged with __match_any_sync, duplicates of beam entries by the
+//     equal-distance check;
+//   * the beam can be saved after a search with a small beam and resumed later
+//     with a larger one (the learned budget's fallback continues the frontier
+//     search instead of starting over).
+// The search ends when no unexpanded entry is left in the beam, like the
+// reference's stop rule (cand_dist > lowerBound with a full result heap).
+#pragma once
+
+#include "beam.cuh"
+
+namespace hrnn {
+
+// Per-warp shared memory of the two-parent search:
+// q | q8 (dim bytes, padded to 16) | qm | td[efc+32] | ti[efc+32] | vis[vc] | nd[64] | ni[64] | apos[32]
+__host__ __device__ inline size_t fast_smem_bytes(uint32_t dim, uint32_t efc, uint32_t vc) {
+    return (size_t)dim * 4 + (((size_t)dim + 15) & ~(size_t)15) + 16 + (size_t)(efc + 32) * 8 + (size_t)vc * 4 +
+           64 * 8 + 32 * 4;
+}
+
+__device__ inline WarpSmem carve_fast(char* base, uint32_t dim, uint32_t efc, uint32_t vc) {
+    WarpSmem s;
+    s.q = (float*)base;
+    base += (size_t)dim * 4;
+    s.q8 = (int*)base;
+    base += ((size_t)dim + 15) & ~(size_t)15;
+    s.qm = (float4*)base;
+    base += 16;
+    s.td = (float*)base;
+    base += (size_t)(efc + 32) * 4;
+    s.ti = (uint32_t*)base;
+    base += (size_t)(efc + 32) * 4;
+    s.xd = nullptr;
+    s.xi = nullptr;
+    s.vis = (uint32_t*)base;
+    base += (size_t)vc * 4;
+    s.nd = (float*)base;
+    base += 64 * 4;
+    s.ni = (uint32_t*)base;
+    base += 64 * 4;
+    s.apos = (uint32_t*)base;
+    return s;
+}
+
+// Two INT8 rows per lane (rows t and t + 32 of ids[0..cnt)), all loads of both
+// issued before the dot products.
+template <int NW>
+__device__ __forceinline__ void warp_i8_rows2(const DevView& v, const int* q8, float4 qm, const uint32_t* ids,
+                                              uint32_t cnt, float* dout) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t t0 = lane, t1 = lane + 32;
+    const uint32_t id0 = ids[t0 < cnt ? t0 : 0], id1 = ids[t1 < cnt ? t1 : 0];
+    const int4* x0 = reinterpret_cast<const int4*>(v.vec_i8 + (size_t)id0 * v.dim);
+    const int4* x1 = reinterpret_cast<const int4*>(v.vec_i8 + (size_t)id1 * v.dim);
+    const bool two = cnt > 32;
+    int4 a[NW], b[NW];
+#pragma unroll
+    for (int c = 0; c < NW; ++c) a[c] = __ldg(x0 + c);
+    if (two) {
+#pragma unroll
+        for (int c = 0; c < NW; ++c) b[c] = __ldg(x1 + c);
+    }
+    const float4 m0 = __ldg(v.i8_meta + id0);
+    const float4 m1 = two ? __ldg(v.i8_meta + id1) : m0;
+    int d0 = 0, d1 = 0;
+#pragma unroll
+    for (int c = 0; c < NW; ++c) {
+        d0 = __dp4a(a[c].x, q8[4 * c + 0], d0);
+        d0 = __dp4a(a[c].y, q8[4 * c + 1], d0);
+        d0 = __dp4a(a[c].z, q8[4 * c + 2], d0);
+        d0 = __dp4a(a[c].w, q8[4 * c + 3], d0);
+    }
+    if (t0 < cnt) dout[t0] = qm.x + m0.x * m0.x * m0.z - 2.f * qm.y * m0.x * (float)d0;
+    if (two) {
+#pragma unroll
+        for (int c = 0; c < NW; ++c) {
+            d1 = __dp4a(b[c].x, q8[4 * c + 0], d1);
+            d1 = __dp4a(b[c].y, q8[4 * c + 1], d1);
+            d1 = __dp4a(b[c].z, q8[4 * c + 2], d1);
+            d1 = __dp4a(b[c].w, q8[4 * c + 3], d1);
+        }
+        if (t1 < cnt) dout[t1] = qm.x + m1.x * m1.x * m1.z - 2.f * qm.y * m1.x * (float)d1;
+    }
+}
+
+// Scores ids[0..cnt) (cnt <= 64) with the form's rows: DM 3 INT8, DM 2 BF16.
+template <int DM>
+__device__ __forceinline__ void warp_dist_list64(const DevView& v, const float* q, const uint32_t* ids,
+                                                 uint32_t cnt, float* dout) {
+    if constexpr (DM == 3) {
+        const int* q8 = i8_q_words(q, v.dim);
+        const float4 qm = *i8_q_meta(q, v.dim);
+        // two rows per lane up to dim 128 (16 loads of 16 bytes in flight per
+        // lane); wider rows one per lane, 32 at a time
+        switch (v.dim >> 4) {
+            case 6: warp_i8_rows2<6>(v, q8, qm, ids, cnt, dout); break;
+            case 8: warp_i8_rows2<8>(v, q8, qm, ids, cnt, dout); break;
+            default:
+                warp_i8_list(v, q8, qm, ids, min(cnt, 32u), dout);
+                if (cnt > 32) warp_i8_list(v, q8, qm, ids + 32, cnt - 32, dout + 32);
+                break;
+        }
+        __syncwarp();
+    } else {
+        warp_dist_list<DM>(v, q, ids, min(cnt, 32u), dout);
+        if (cnt > 32) warp_dist_list<DM>(v, q, ids + 32, cnt - 32, dout + 32);
+    }
+}
+
+// Inserts the scored neighbours nd/ni[0..cnt) (cnt <= 32, one per lane) whose
+// distance is below a full beam's last entry; the beam stays sorted and is cut to
+// EF.  cursor moves back to the first inserted position.
+__device__ __forceinline__ void beam_insert_fast(WarpSmem& s, const float* nd, const uint32_t* ni, uint32_t cnt,
+                                                 uint32_t EF, uint32_t& tsize, uint32_t& cursor) {
+    const int lane = threadIdx.x & 31;
+    float d = FLT_MAX;
+    uint32_t id = kInvalid, pos = 0;
+    bool ok = false;
+    if ((uint32_t)lane < cnt) {
+        d = nd[lane];
+        id = ni[lane];
+        ok = !(tsize >= EF && d >= s.td[EF - 1]);
+    }
+    uint32_t okb = __ballot_sync(0xFFFFFFFFu, ok);
+    if (!okb) return;
+    // the same id twice in this batch (two parents sharing a neighbour that the
+    // lossy visited cache did not catch): the lowest lane keeps it
+    const uint32_t same = __match_any_sync(0xFFFFFFFFu, ok ? id : kInvalid);
+    if (ok && (same & lanemask_lt() & okb)) ok = false;
+    if (ok) {
+        pos = upper_bound(s.td, tsize, d);
+        for (int k = (int)pos - 1; k >= 0 && s.td[k] == d; --k)
+            if ((s.ti[k] & kIdMask) == id) {
+                ok = false;
+                break;
+            }
+    }
+    const uint32_t ab = __ballot_sync(0xFFFFFFFFu, ok);
+    if (!ab) return;
+    const uint32_t na = __popc(ab);
+    uint32_t before = 0;
+    if (na > 1) {
+        for (uint32_t m = ab; m; m &= m - 1) {
+            const int i = __ffs(m) - 1;
+            const float di = __shfl_sync(0xFFFFFFFFu, d, i);
+            if (di < d || (di == d && i < lane)) before++;
+        }
+    }
+    if (ok) s.apos[before] = pos;
+    __syncwarp();
+    const uint32_t lo = s.apos[0], amax = s.apos[na - 1];
+    const uint32_t newsize = min(tsize + na, EF);
+    if (tsize > lo) {
+        for (int b = (int)lo + (int)(((tsize - lo - 1) / 32) * 32); b >= (int)lo; b -= 32) {
+            const uint32_t k = (uint32_t)b + lane;
+            float dk = 0.f;
+            uint32_t ik = 0, np = 0xFFFFFFFFu;
+            if (k < tsize) {
+                dk = s.td[k];
+                ik = s.ti[k];
+                uint32_t sh = na;
+                if (k < amax) {
+                    uint32_t a = 0, e = na - 1;
+                    while (a < e) {
+                        const uint32_t mid = (a + e) >> 1;
+                        if (s.apos[mid] <= k) a = mid + 1;
+                        else e = mid;
+                    }
+                    sh = a;
+                }
+                np = k + sh;
+            }
+            __syncwarp();
+            if (np < newsize) {
+                s.td[np] = dk;
+                s.ti[np] = ik;
+            }
+            __syncwarp();
+        }
+    }
+    const uint32_t npos = pos + before;
+    if (ok && npos < newsize) {
+        s.td[npos] = d;
+        s.ti[npos] = id;
+    }
+    tsize = newsize;
+    cursor = min(cursor, lo);
+    __syncwarp();
+}
+
+// Two-parent search of level 0 continuing from the beam s.td/s.ti[0..tsize)
+// (sorted; ids carry kExpanded).  The visited cache must hold (at least) the
+// beam's ids.  Returns the beam size (<= EF).
+template <int DM>
+__device__ uint32_t beam_search_fast(const DevView& v, WarpSmem& s, uint32_t tsize, uint32_t EF, uint32_t vc,
+                                     unsigned long long& c_dist, unsigned long long& c_exp) {
+    const int lane = threadIdx.x & 31;
+    uint32_t cursor = 0;
+    for (;;) {
+        // the (up to) two best unexpanded entries at or after cursor
+        uint32_t par0 = kInvalid, par1 = kInvalid;
+        for (uint32_t b = cursor; b < tsize; b += 32) {
+            const uint32_t idx = b + lane;
+            const bool u = idx < tsize && !(s.ti[idx] & kExpanded);
+            uint32_t bal = __ballot_sync(0xFFFFFFFFu, u);
+            if (!bal) continue;
+            if (par0 == kInvalid) {
+                par0 = b + __ffs(bal) - 1;
+                bal &= bal - 1;
+            }
+            if (bal) {
+                par1 = b + __ffs(bal) - 1;
+                break;
+            }
+        }
+        if (par0 == kInvalid) break;
+        const uint32_t c0 = s.ti[par0] & kIdMask;
+        const uint32_t c1 = par1 != kInvalid ? (s.ti[par1] & kIdMask) : kInvalid;
+        cursor = (par1 != kInvalid ? par1 : par0) + 1;
+        __syncwarp();
+        if (lane == 0) {
+            s.ti[par0] |= kExpanded;
+            if (par1 != kInvalid) s.ti[par1] |= kExpanded;
+        }
+        c_exp += par1 != kInvalid ? 2 : 1;
+        // both link rows in one go (rows of at most 33 words, maxM0 <= 32)
+        uint32_t ra0 = 0, ra1 = 0, rb0 = 0, rb1 = 0;
+        load_row(v, c0, 0, ra0, ra1);
+        if (c1 != kInvalid) load_row(v, c1, 0, rb0, rb1);
+        uint32_t cnt = 0;
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            const uint32_t w0 = r ? rb0 : ra0, w1 = r ? rb1 : ra1;
+            const uint32_t size = r && c1 == kInvalid ? 0u : (__shfl_sync(0xFFFFFFFFu, w0, 0) & 0xFFFFu);
+            const uint32_t a = __shfl_sync(0xFFFFFFFFu, w0, (lane + 1) & 31);
+            const uint32_t bw = __shfl_sync(0xFFFFFFFFu, w1, 0);
+            const uint32_t nid = (uint32_t)lane < size ? (lane < 31 ? a : bw) : kInvalid;
+            const uint32_t slot = hash32(nid) & (vc - 1);
+            const bool fresh = (uint32_t)lane < size && s.vis[slot] != nid;
+            __syncwarp();
+            const uint32_t fb = __ballot_sync(0xFFFFFFFFu, fresh);
+            if (fresh) {
+                s.ni[cnt + __popc(fb & lanemask_lt())] = nid;
+                s.vis[slot] = nid;
+            }
+            cnt += __popc(fb);
+            __syncwarp();
+        }
+        if (cnt == 0) continue;
+        warp_dist_list64<DM>(v, s.q, s.ni, cnt, s.nd);
+        c_dist += cnt;
+        beam_insert_fast(s, s.nd, s.ni, min(cnt, 32u), EF, tsize, cursor);
+        if (cnt > 32) beam_insert_fast(s, s.nd + 32, s.ni + 32, cnt - 32, EF, tsize, cursor);
+    }
+    return tsize;
+}
+
+}  // namespace hrnn

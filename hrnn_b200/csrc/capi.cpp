@@ -4,6 +4,9 @@
 #include <cuda_runtime.h>
 
 #include <cstring>
+#include <algorithm>
+#include <random>
+#include <numeric>
 #include <memory>
 #include <new>
 #include <string>
@@ -295,6 +298,15 @@ hrnn_status hrnn_compact_for_serving(hrnn_index* h, size_t mks) {
     });
 }
 
+hrnn_status hrnn_get_kdist(hrnn_index* h, uint32_t k, float* out) {
+    return guard([&] {
+        need(h, "index");
+        need(out, "out");
+        set_device(h);
+        hrnn::kdist_column(h->ix, k, out);
+    });
+}
+
 hrnn_status hrnn_insert_dynamic(hrnn_index* h, const float* data, const uint64_t* labels, size_t n,
                                 unsigned m_update, int bidirectional) {
     return guard([&] {
@@ -488,6 +500,16 @@ hrnn_status hrnn_set_l2_order(hrnn_index* h, int lanes, int fused) {
         if (fused < 0 || fused > 3) hrnn::fail(HRNN_ERR_ARG, "fused must be in [0, 3]");
         h->ix.order.lanes = lanes;
         h->ix.order.fused = fused;
+    });
+}
+
+hrnn_status hrnn_dynamic_split(uint64_t n, uint32_t seed, uint32_t* perm) {
+    return guard([&] {
+        need(perm, "perm");
+        if (n > 0xFFFFFFFFull) hrnn::fail(HRNN_ERR_ARG, "dynamic_split: n must fit 32-bit ids");
+        std::iota(perm, perm + n, 0u);
+        std::mt19937 rng(seed);
+        std::shuffle(perm, perm + n, rng);
     });
 }
 

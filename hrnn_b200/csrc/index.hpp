@@ -166,6 +166,7 @@ struct SearchArgs {
     cudaStream_t stream;
 };
 uint64_t search_batch(Index& ix, const SearchArgs& a);  // returns total results
+void kdist_column(Index& ix, uint32_t k, float* host_out);  // kdist(p, k-1) of every element
 void l2_batch_device(const float* a, const float* b, size_t n, size_t dim, L2Order o, float* out,
                      cudaStream_t s);
 

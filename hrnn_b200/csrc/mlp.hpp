@@ -43,6 +43,7 @@ struct Budget {
     DevMem proj;                  // [dim x 128] fixed random projection of the query
     uint32_t proj_dim = 0;
     DevMem feat, decided, fallback_list, proxd;  // per-call work buffers
+    DevMem saved;                 // two-pass mode: the frontier beams the fallback resumes
     unsigned long long n_level[3] = {0, 0, 0};  // queries served at level 0 / 1 / fallback (last call)
 };
 

@@ -15,10 +15,13 @@
 // FP32 verification against the stored kNN radius, results in ascending
 // internal-id order (hrnn.h:2021-2070).
 #include <algorithm>
+#include <cstdlib>
+#include <string>
 #include <cfloat>
 #include <vector>
 
 #include "beam.cuh"
+#include "beam_fast.cuh"
 #include "index.hpp"
 #include "mlp.hpp"
 #include "plan.hpp"
@@ -53,6 +56,31 @@ __global__ void k_budget_decide(const float* z, uint32_t nq, float conf, uint32_
 void ensure_projection(Index& ix, Budget& b);
 __global__ void k_kdist_column(DevView v, uint32_t kidx, float* kcol);
 size_t bc_cta_smem(uint32_t dim, bool counts, bool mixed);
+size_t stream_warp_smem(uint32_t dim);
+template <class E, bool FUSED, int NB>
+__global__ void k_verify_stream(DevView, const float*, uint32_t, uint32_t, const uint32_t*, const uint32_t*,
+                                const uint32_t*, const uint64_t*, const float*, uint32_t, uint64_t*, uint32_t*,
+                                uint32_t*, uint32_t*, uint32_t*, SearchCounters*);
+using KStream = void (*)(DevView, const float*, uint32_t, uint32_t, const uint32_t*, const uint32_t*,
+                         const uint32_t*, const uint64_t*, const float*, uint32_t, uint64_t*, uint32_t*, uint32_t*,
+                         uint32_t*, uint32_t*, SearchCounters*);
+// HRNN_VERIFY=table: the INT8 form verifies through the CTA table kernel as well
+// (for comparisons of the two verification paths).
+inline bool verify_table_forced() {
+    const char* e = std::getenv("HRNN_VERIFY");
+    return e && std::string(e) == "table";
+}
+// The streaming verification of the INT8 form, or null where it does not apply
+// (other dims or forms, counted thresholds): those take the CTA kernel.
+inline KStream pick_stream(bool wide, bool fused, uint32_t dim) {
+    if (dim != 128 && dim != 96) return nullptr;
+    if (wide) {
+        if (dim == 128) return fused ? k_verify_stream<uint64_t, true, 8> : k_verify_stream<uint64_t, false, 8>;
+        return fused ? k_verify_stream<uint64_t, true, 6> : k_verify_stream<uint64_t, false, 6>;
+    }
+    if (dim == 128) return fused ? k_verify_stream<uint32_t, true, 8> : k_verify_stream<uint32_t, false, 8>;
+    return fused ? k_verify_stream<uint32_t, true, 6> : k_verify_stream<uint32_t, false, 6>;
+}
 
 namespace {
 
@@ -99,6 +127,91 @@ __global__ void __launch_bounds__(128) k_phase_a(DevView v, const float* __restr
         c_dist++;  // the reference evaluates the entry point again (hrnn.h:505)
         uint32_t tsize = beam_search<DM>(v, s, cur, curd, EF, 0, vc, c_dist, c_exp);
         uint32_t np_ = min(min(max(m, m_keep), mmax), tsize);
+        for (uint32_t i = lane; i < np_; i += 32) {
+            prox[(size_t)qi * mmax + i] = s.ti[i] & kIdMask;
+            if (proxd) proxd[(size_t)qi * mmax + i] = s.td[i];
+        }
+        if (lane == 0) nprox[qi] = np_;
+        __syncwarp();
+    }
+    if (lane == 0) {
+        atomicAdd(&ctr->n_dist, c_dist);
+        atomicAdd(&ctr->n_expanded, c_exp);
+    }
+}
+
+// Reduced-precision forms (DM 2 BF16, 3 INT8): descent, then the two-parent beam
+// search of beam_fast.cuh.  Arguments as k_phase_a, plus:
+//   save_cap, st_cnt / st_d / st_i: after the search, the first save_cap beam
+//     entries (with their expanded flags) are stored per query (row stride
+//     save_cap) -- the learned budget's frontier pass, which a fallback can
+//     resume;
+//   resume: start from the stored beam instead of the descent (its ids seed the
+//     visited cache), continue with the query's own ef, store nothing.
+template <int DM>
+__global__ void __launch_bounds__(128) k_phase_a_fast(DevView v, const float* __restrict__ Q, uint32_t nq,
+                                                      const uint32_t* __restrict__ qm,
+                                                      const uint32_t* __restrict__ qef, uint32_t efc, uint32_t vc,
+                                                      uint32_t mmax, uint32_t* __restrict__ prox,
+                                                      uint32_t* __restrict__ nprox, SearchCounters* __restrict__ ctr,
+                                                      const uint32_t* __restrict__ qlist, uint32_t m_over,
+                                                      uint32_t ef_over, uint32_t m_keep, float* __restrict__ proxd,
+                                                      uint32_t* __restrict__ next_q, uint32_t save_cap,
+                                                      uint32_t* __restrict__ st_cnt, float* __restrict__ st_d,
+                                                      uint32_t* __restrict__ st_i, int resume) {
+    extern __shared__ char smem_raw[];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    WarpSmem s = carve_fast(smem_raw + (size_t)w * fast_smem_bytes(v.dim, efc, vc), v.dim, efc, vc);
+    unsigned long long c_dist = 0, c_exp = 0;
+    for (;;) {
+        uint32_t j = 0;
+        if (lane == 0) j = atomicAdd(next_q, 1u);
+        j = __shfl_sync(0xFFFFFFFFu, j, 0);
+        if (j >= nq) break;
+        const uint32_t qi = qlist ? qlist[j] : j;
+        const uint32_t m = m_over ? m_over : qm[qi];
+        const uint32_t EF = min(max(ef_over ? ef_over : qef[qi], m), efc);
+        if (v.n == 0 || m == 0) {
+            if (lane == 0) nprox[qi] = 0;
+            continue;
+        }
+        for (uint32_t i = lane; i < v.dim; i += 32) s.q[i] = Q[(size_t)qi * v.dim + i];
+        for (uint32_t i = lane; i < vc; i += 32) s.vis[i] = kInvalid;
+        __syncwarp();
+        if constexpr (DM == 3) i8_prep_query(s, v.dim);
+        uint32_t tsize;
+        if (resume) {
+            tsize = min(st_cnt[qi], EF);
+            for (uint32_t i = lane; i < tsize; i += 32) {
+                const uint32_t id = st_i[(size_t)qi * save_cap + i];
+                s.td[i] = st_d[(size_t)qi * save_cap + i];
+                s.ti[i] = id;
+                s.vis[hash32(id & kIdMask) & (vc - 1)] = id & kIdMask;
+            }
+            __syncwarp();
+        } else {
+            uint32_t cur = v.enterpoint;
+            float curd = warp_dist_one<DM>(v, s.q, cur);
+            c_dist++;
+            greedy_descent<DM>(v, s, v.maxlevel, 0, cur, curd, c_dist);
+            if (lane == 0) {
+                s.td[0] = curd;
+                s.ti[0] = cur;
+                s.vis[hash32(cur) & (vc - 1)] = cur;
+            }
+            __syncwarp();
+            tsize = 1;
+        }
+        tsize = beam_search_fast<DM>(v, s, tsize, EF, vc, c_dist, c_exp);
+        if (save_cap && !resume) {
+            const uint32_t ns = min(tsize, save_cap);
+            for (uint32_t i = lane; i < ns; i += 32) {
+                st_d[(size_t)qi * save_cap + i] = s.td[i];
+                st_i[(size_t)qi * save_cap + i] = s.ti[i];
+            }
+            if (lane == 0) st_cnt[qi] = ns;
+        }
+        const uint32_t np_ = min(min(max(m, m_keep), mmax), tsize);
         for (uint32_t i = lane; i < np_; i += 32) {
             prox[(size_t)qi * mmax + i] = s.ti[i] & kIdMask;
             if (proxd) proxd[(size_t)qi * mmax + i] = s.td[i];
@@ -407,10 +520,9 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
     // more: the smaller per-warp shared memory keeps more warps resident, which
     // pays for the ~10% extra rows at ef = 200.
     uint32_t vc = 512;
-    size_t wsm = warp_smem_bytes(v.dim, efc, vc);
+    size_t wsm = std::max(warp_smem_bytes(v.dim, efc, vc), fast_smem_bytes(v.dim, efc, vc));
     int wpb = (int)std::max<size_t>(1, std::min<size_t>(4, (200 * 1024) / wsm));
     size_t smem_a = wsm * wpb;
-    if (smem_a > 227 * 1024) fail(HRNN_ERR_ARG, "searchRknn: ef/dim too large for one warp's beam");
     DevMem& prox = ix.scratch[0];
     DevMem& nprox = ix.scratch[1];
     DevMem& plen = ix.scratch[2];
@@ -440,11 +552,56 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
     const int nsm = sms(ix.device);
     CUDA_CHECK(cudaEventRecord(ev[0], s));
     {
-        auto kern = int8 ? k_phase_a<3> : mixed ? k_phase_a<2> : (fusedsimd ? k_phase_a<1> : k_phase_a<0>);
+        // The exact form runs the reference-order beam (k_phase_a); the reduced-
+        // precision forms the two-parent search (k_phase_a_fast).
+        // (The two-parent search reads link rows of at most 33 words, maxM0 <= 32.)
+        const bool fast = (int8 || mixed) && v.W0 <= 33;
+        const int dm = int8 ? 3 : mixed ? 2 : fusedsimd ? 1 : 0;
+        const void* kfun = fast ? (dm == 3 ? (const void*)k_phase_a_fast<3> : (const void*)k_phase_a_fast<2>)
+                                : (dm == 3 ? (const void*)k_phase_a<3>
+                                           : dm == 2 ? (const void*)k_phase_a<2>
+                                                     : dm == 1 ? (const void*)k_phase_a<1> : (const void*)k_phase_a<0>);
+        auto smem_for = [&](uint32_t cv, int cw) {
+            return (fast ? fast_smem_bytes(v.dim, efc, cv) : warp_smem_bytes(v.dim, efc, cv)) * (size_t)cw;
+        };
+        // One launch of the form's phase-A kernel; qlist / ef_over / m_keep / proxd /
+        // save / resume as documented at k_phase_a_fast (the exact kernel takes no
+        // save or resume).
+        auto launch = [&](unsigned g, int cw, uint32_t cv, size_t sm, uint32_t nqq, const uint32_t* qlist,
+                          uint32_t m_over, uint32_t ef_over, uint32_t m_keep, float* proxd, uint32_t* ctrq,
+                          uint32_t save_cap, uint32_t* st_cnt, float* st_d, uint32_t* st_i, int resume) {
+            if (fast && dm == 3)
+                k_phase_a_fast<3><<<g, cw * 32, sm, s>>>(v, a.d_q, nqq, a.d_m, a.d_ef, efc, cv, mmax,
+                                                         prox.as<uint32_t>(), nprox.as<uint32_t>(), ctr, qlist,
+                                                         m_over, ef_over, m_keep, proxd, ctrq, save_cap, st_cnt, st_d,
+                                                         st_i, resume);
+            else if (fast)
+                k_phase_a_fast<2><<<g, cw * 32, sm, s>>>(v, a.d_q, nqq, a.d_m, a.d_ef, efc, cv, mmax,
+                                                         prox.as<uint32_t>(), nprox.as<uint32_t>(), ctr, qlist,
+                                                         m_over, ef_over, m_keep, proxd, ctrq, save_cap, st_cnt, st_d,
+                                                         st_i, resume);
+            else if (dm == 3)
+                k_phase_a<3><<<g, cw * 32, sm, s>>>(v, a.d_q, nqq, a.d_m, a.d_ef, efc, cv, mmax, prox.as<uint32_t>(),
+                                                    nprox.as<uint32_t>(), ctr, qlist, m_over, ef_over, m_keep, proxd,
+                                                    ctrq);
+            else if (dm == 2)
+                k_phase_a<2><<<g, cw * 32, sm, s>>>(v, a.d_q, nqq, a.d_m, a.d_ef, efc, cv, mmax, prox.as<uint32_t>(),
+                                                    nprox.as<uint32_t>(), ctr, qlist, m_over, ef_over, m_keep, proxd,
+                                                    ctrq);
+            else if (dm == 1)
+                k_phase_a<1><<<g, cw * 32, sm, s>>>(v, a.d_q, nqq, a.d_m, a.d_ef, efc, cv, mmax, prox.as<uint32_t>(),
+                                                    nprox.as<uint32_t>(), ctr, qlist, m_over, ef_over, m_keep, proxd,
+                                                    ctrq);
+            else
+                k_phase_a<0><<<g, cw * 32, sm, s>>>(v, a.d_q, nqq, a.d_m, a.d_ef, efc, cv, mmax, prox.as<uint32_t>(),
+                                                    nprox.as<uint32_t>(), ctr, qlist, m_over, ef_over, m_keep, proxd,
+                                                    ctrq);
+            CUDA_LAUNCH_CHECK();
+        };
         uint32_t* d_qa = d_next + 4;  // work counters of the phase-A launches (zeroed with d_rcount)
         // Launch shape: the tuned one of this (distance mode, beam size), else timed
         // now on this batch when autotuning is on and the batch is large enough.
-        const uint64_t shape_key = ((uint64_t)(int8 ? 3 : mixed ? 2 : fusedsimd ? 1 : 0) << 32) | efc;
+        const uint64_t shape_key = ((uint64_t)dm << 32) | efc;
         auto shape = ix.autotune ? ix.a_shape.find(shape_key) : ix.a_shape.end();
         if (shape != ix.a_shape.end()) {
             wpb = (int)shape->second.first;
@@ -458,19 +615,17 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
             CUDA_CHECK(cudaEventCreate(&t1));
             for (uint32_t cv : {256u, 512u, 1024u}) {
                 for (int cw : {2, 4}) {
-                    const size_t sm = warp_smem_bytes(v.dim, efc, cv) * (size_t)cw;
+                    const size_t sm = smem_for(cv, cw);
                     if (sm > 200 * 1024) continue;
-                    CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+                    CUDA_CHECK(cudaFuncSetAttribute(kfun, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
                     int ps = 1;
-                    CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ps, kern, cw * 32, sm));
+                    CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ps, kfun, cw * 32, sm));
                     const unsigned g = (unsigned)std::max<size_t>(
                         1, std::min<size_t>((nq + cw - 1) / cw, (size_t)nsm * std::max(ps, 1)));
                     CUDA_CHECK(cudaMemsetAsync(d_qa, 0, 4, s));
                     CUDA_CHECK(cudaEventRecord(t0, s));
-                    kern<<<g, cw * 32, sm, s>>>(v, a.d_q, (uint32_t)nq, a.d_m, a.d_ef, efc, cv, mmax,
-                                                 prox.as<uint32_t>(), nprox.as<uint32_t>(), ctr, nullptr, 0, 0, 0,
-                                                 nullptr, d_qa);
-                    CUDA_LAUNCH_CHECK();
+                    launch(g, cw, cv, sm, (uint32_t)nq, nullptr, 0, 0, 0, nullptr, d_qa, 0, nullptr, nullptr,
+                           nullptr, 0);
                     CUDA_CHECK(cudaEventRecord(t1, s));
                     CUDA_CHECK(cudaEventSynchronize(t1));
                     float ms = 0.f;
@@ -492,25 +647,25 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
             CUDA_CHECK(cudaMemsetAsync(d_qa, 0, 4, s));
             CUDA_CHECK(cudaEventRecord(ev[0], s));
         }
-        smem_a = warp_smem_bytes(v.dim, efc, vc) * (size_t)wpb;
-        CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_a));
+        smem_a = smem_for(vc, wpb);
+        if (smem_a > 227 * 1024) fail(HRNN_ERR_ARG, "searchRknn: ef/dim too large for one warp's beam");
+        CUDA_CHECK(cudaFuncSetAttribute(kfun, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_a));
         // Persistent grid (every resident block), queries handed out by counters.
         int per_sm = 1;
-        CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, wpb * 32, smem_a));
+        CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfun, wpb * 32, smem_a));
         auto grid_for = [&](size_t n) {
             return (unsigned)std::max<size_t>(1, std::min<size_t>((n + wpb - 1) / wpb, (size_t)nsm * std::max(per_sm, 1)));
         };
         if (!learned) {
-            kern<<<grid_for(nq), wpb * 32, smem_a, s>>>(v, a.d_q, (uint32_t)nq, a.d_m, a.d_ef, efc, vc, mmax,
-                                                        prox.as<uint32_t>(), nprox.as<uint32_t>(), ctr, nullptr, 0, 0,
-                                                        0, nullptr, d_qa);
-            CUDA_LAUNCH_CHECK();
+            launch(grid_for(nq), wpb, vc, smem_a, (uint32_t)nq, nullptr, 0, 0, 0, nullptr, d_qa, 0, nullptr, nullptr,
+                   nullptr, 0);
         } else {
             // Learned budget: frontier pass for every query, features, MLP,
             // decision.  Single-pass mode: the frontier is the caller's own beam,
             // levels only trim the proxies.  Two-pass mode: the frontier beam is
-            // the level ef, and the queries the MLP is not confident about are
-            // searched again with the caller's (m, ef).
+            // the level ef; the queries the MLP is not confident about continue
+            // that search with the caller's (m, ef) -- the two-parent search
+            // resumes from the stored beam (the exact form searches again).
             Budget& b = *ix.budget;
             ensure_projection(ix, b);
             ix.kcol.ensure((size_t)std::max<size_t>(ix.cur, 1) * 4);
@@ -523,11 +678,17 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
             uint32_t* fb_count = b.decided.as<uint32_t>();
             unsigned long long* levels = (unsigned long long*)(b.decided.as<char>() + 8);
             CUDA_CHECK(cudaMemsetAsync(b.decided.p, 0, 64, s));
-            kern<<<grid_for(nq), wpb * 32, smem_a, s>>>(v, a.d_q, (uint32_t)nq, a.d_m, a.d_ef, efc, vc, mmax,
-                                                        prox.as<uint32_t>(), nprox.as<uint32_t>(), ctr, nullptr,
-                                                        two_pass ? b.m[1] : 0, two_pass ? b.ef : 0, kFrontier,
-                                                        b.proxd.as<float>(), d_qa);
-            CUDA_LAUNCH_CHECK();
+            const uint32_t save_cap = (two_pass && fast) ? ((b.ef + 31) & ~31u) : 0;
+            uint32_t *st_cnt = nullptr, *st_i = nullptr;
+            float* st_d = nullptr;
+            if (save_cap) {
+                b.saved.ensure(nq * 4 + (size_t)nq * save_cap * 8 + 256);
+                st_cnt = b.saved.as<uint32_t>();
+                st_d = (float*)(b.saved.as<char>() + ((nq * 4 + 255) & ~(size_t)255));
+                st_i = (uint32_t*)(st_d + (size_t)nq * save_cap);
+            }
+            launch(grid_for(nq), wpb, vc, smem_a, (uint32_t)nq, nullptr, two_pass ? b.m[1] : 0, two_pass ? b.ef : 0,
+                   kFrontier, b.proxd.as<float>(), d_qa, save_cap, st_cnt, st_d, st_i, 0);
             k_budget_features<<<(unsigned)((nq * 32 + 255) / 256), 256, 0, s>>>(
                 v, a.d_q, (uint32_t)nq, prox.as<uint32_t>(), b.proxd.as<float>(), nprox.as<uint32_t>(), mmax,
                 ix.kcol.as<float>(), b.proj.as<float>(), b.feat.as<float>());
@@ -541,13 +702,9 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
                 uint32_t nfb = 0;
                 CUDA_CHECK(cudaMemcpyAsync(&nfb, fb_count, 4, cudaMemcpyDeviceToHost, s));
                 CUDA_CHECK(cudaStreamSynchronize(s));
-                if (nfb) {
-                    kern<<<grid_for(nfb), wpb * 32, smem_a, s>>>(v, a.d_q, nfb, a.d_m, a.d_ef, efc, vc, mmax,
-                                                                 prox.as<uint32_t>(), nprox.as<uint32_t>(), ctr,
-                                                                 b.fallback_list.as<uint32_t>(), 0, 0, 0, nullptr,
-                                                                 d_qa + 1);
-                    CUDA_LAUNCH_CHECK();
-                }
+                if (nfb)
+                    launch(grid_for(nfb), wpb, vc, smem_a, nfb, b.fallback_list.as<uint32_t>(), 0, 0, 0, nullptr,
+                           d_qa + 1, save_cap, st_cnt, st_d, st_i, save_cap ? 1 : 0);
             }
         }
     }
@@ -581,16 +738,31 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
         k_kdist_column<<<(unsigned)((ix.cur + 255) / 256), 256, 0, s>>>(v, kidx, ix.kcol.as<float>());
         CUDA_LAUNCH_CHECK();
         const bool counts = a.threshold > 1.0f;
-        const size_t smem = bc_cta_smem(v.dim, counts, mixed);
-        KCta kc = ix.wide ? pick_bc<uint64_t>(fusedsimd, counts, mixed) : pick_bc<uint32_t>(fusedsimd, counts, mixed);
-        CUDA_CHECK(cudaFuncSetAttribute(kc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        int per_sm = 1;
-        CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kc, 256, smem));
-        unsigned grid = (unsigned)std::min<size_t>(nq, (size_t)nsm * std::max(per_sm, 1));
-        kc<<<grid, 256, smem, s>>>(v, a.d_q, (uint32_t)nq, mmax, prox.as<uint32_t>(), nprox.as<uint32_t>(),
-                                   plen.as<uint32_t>(), d_total, d_resoff, a.threshold, ix.kcol.as<float>(), kidx,
-                                   resbuf, d_rcount, d_next, ovl, d_nov, ctr);
-        CUDA_LAUNCH_CHECK();
+        KStream ks = (int8 && mixed && v.i8_screen && !counts && v.lanes == 16 && !verify_table_forced())
+                         ? pick_stream(ix.wide, fusedsimd, v.dim) : nullptr;
+        if (ks) {
+            // INT8 form: one warp per query, postings verified as they are read
+            const size_t smem = 8 * stream_warp_smem(v.dim);
+            CUDA_CHECK(cudaFuncSetAttribute(ks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            int per_sm = 1;
+            CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ks, 256, smem));
+            unsigned grid = (unsigned)std::min<size_t>((nq + 7) / 8, (size_t)nsm * std::max(per_sm, 1));
+            ks<<<grid, 256, smem, s>>>(v, a.d_q, (uint32_t)nq, mmax, prox.as<uint32_t>(), nprox.as<uint32_t>(),
+                                       plen.as<uint32_t>(), d_resoff, ix.kcol.as<float>(), kidx, resbuf, d_rcount,
+                                       d_next, ovl, d_nov, ctr);
+            CUDA_LAUNCH_CHECK();
+        } else {
+            const size_t smem = bc_cta_smem(v.dim, counts, mixed);
+            KCta kc = ix.wide ? pick_bc<uint64_t>(fusedsimd, counts, mixed) : pick_bc<uint32_t>(fusedsimd, counts, mixed);
+            CUDA_CHECK(cudaFuncSetAttribute(kc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            int per_sm = 1;
+            CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kc, 256, smem));
+            unsigned grid = (unsigned)std::min<size_t>(nq, (size_t)nsm * std::max(per_sm, 1));
+            kc<<<grid, 256, smem, s>>>(v, a.d_q, (uint32_t)nq, mmax, prox.as<uint32_t>(), nprox.as<uint32_t>(),
+                                       plen.as<uint32_t>(), d_total, d_resoff, a.threshold, ix.kcol.as<float>(), kidx,
+                                       resbuf, d_rcount, d_next, ovl, d_nov, ctr);
+            CUDA_LAUNCH_CHECK();
+        }
         // Queries whose shared-memory table or accepted list overflowed: the
         // global-memory warp kernel, with a table sized for their posting count.
         uint32_t nov = 0;
@@ -685,6 +857,19 @@ void l2_batch_device(const float* a, const float* b, size_t n, size_t dim, L2Ord
     CUDA_LAUNCH_CHECK();
 }
 
+void kdist_column(Index& ix, uint32_t k, float* host_out) {
+    if (!ix.knng_built && !ix.serve_mode) fail(HRNN_ERR_STATE, "kdist: KNNG not built yet");
+    if (k == 0 || (ix.serve_mode ? k > ix.max_k_serve : k > ix.K)) fail(HRNN_ERR_ARG, "kdist: k out of range");
+    if (ix.cur == 0) return;
+    DevView v = make_view(ix);
+    cudaStream_t s = ix.stream;
+    ix.kcol.ensure(ix.cur * 4);
+    k_kdist_column<<<(unsigned)((ix.cur + 255) / 256), 256, 0, s>>>(v, k - 1, ix.kcol.as<float>());
+    CUDA_LAUNCH_CHECK();
+    CUDA_CHECK(cudaMemcpyAsync(host_out, ix.kcol.p, ix.cur * 4, cudaMemcpyDeviceToHost, s));
+    CUDA_CHECK(cudaStreamSynchronize(s));
+}
+
 Budget& budget_of(Index& ix) {
     if (!ix.budget) ix.budget.reset(new Budget());
     return *ix.budget;
@@ -713,7 +898,8 @@ void budget_features(Index& ix, const float* d_q, size_t nq, uint32_t k, uint32_
     DevView v = make_view(ix);
     ensure_projection(ix, b);
     const uint32_t mmax = std::max<uint32_t>(m, kFrontier), efc = (std::max(m, ef) + 31) & ~31u, vc = 1024;
-    const size_t wsm = warp_smem_bytes(v.dim, efc, vc);
+    const bool fast = (mixed || int8) && v.W0 <= 33;  // the search the learned form's frontier pass runs
+    const size_t wsm = fast ? fast_smem_bytes(v.dim, efc, vc) : warp_smem_bytes(v.dim, efc, vc);
     const int wpb = (int)std::max<size_t>(1, std::min<size_t>(4, (200 * 1024) / wsm));
     const size_t smem_a = wsm * wpb;
     if (smem_a > 227 * 1024) fail(HRNN_ERR_ARG, "budget: ef/dim too large for one warp's beam");
@@ -726,13 +912,23 @@ void budget_features(Index& ix, const float* d_q, size_t nq, uint32_t k, uint32_
     ix.kcol.ensure((size_t)std::max<size_t>(ix.cur, 1) * 4);
     k_kdist_column<<<(unsigned)((ix.cur + 255) / 256), 256, 0, s>>>(v, k - 1, ix.kcol.as<float>());
     CUDA_LAUNCH_CHECK();
-    auto kern = int8 ? k_phase_a<3> : mixed ? k_phase_a<2> : (((ix.order.fused & 1) != 0) ? k_phase_a<1> : k_phase_a<0>);
-    CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_a));
     const int nsm = sms(ix.device);
     unsigned grid = (unsigned)std::max<size_t>(1, std::min<size_t>((nq + wpb - 1) / wpb, (size_t)nsm * 16));
-    kern<<<grid, wpb * 32, smem_a, s>>>(v, d_q, (uint32_t)nq, nullptr, nullptr, efc, vc, mmax, prox.as<uint32_t>(),
-                                        nprox.as<uint32_t>(), ix.counters.as<SearchCounters>(), nullptr, m, ef,
-                                        kFrontier, proxd.as<float>(), next.as<uint32_t>());
+    if (fast) {
+        auto kern = int8 ? k_phase_a_fast<3> : k_phase_a_fast<2>;
+        CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_a));
+        kern<<<grid, wpb * 32, smem_a, s>>>(v, d_q, (uint32_t)nq, nullptr, nullptr, efc, vc, mmax,
+                                            prox.as<uint32_t>(), nprox.as<uint32_t>(),
+                                            ix.counters.as<SearchCounters>(), nullptr, m, ef, kFrontier,
+                                            proxd.as<float>(), next.as<uint32_t>(), 0, nullptr, nullptr, nullptr, 0);
+    } else {
+        auto kern = int8 ? k_phase_a<3> : mixed ? k_phase_a<2> : ((ix.order.fused & 1) != 0) ? k_phase_a<1> : k_phase_a<0>;
+        CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_a));
+        kern<<<grid, wpb * 32, smem_a, s>>>(v, d_q, (uint32_t)nq, nullptr, nullptr, efc, vc, mmax,
+                                            prox.as<uint32_t>(), nprox.as<uint32_t>(),
+                                            ix.counters.as<SearchCounters>(), nullptr, m, ef, kFrontier,
+                                            proxd.as<float>(), next.as<uint32_t>());
+    }
     CUDA_LAUNCH_CHECK();
     k_budget_features<<<(unsigned)((nq * 32 + 255) / 256), 256, 0, s>>>(v, d_q, (uint32_t)nq, prox.as<uint32_t>(),
                                                                        proxd.as<float>(), nprox.as<uint32_t>(), mmax,
@@ -761,7 +957,7 @@ namespace {
 struct PlanLaunch {
     uint32_t efc, vc, mmax, wpb, grid_a, grid_bc, kidx, slots, hcap;
     size_t smem_a, smem_bc, smem_w, tmax;
-    bool mixed, int8, fusedsimd, counts;
+    bool mixed, int8, fusedsimd, counts, fast;
 };
 
 PlanLaunch plan_launch_shape(Index& ix, const SearchPlan& p) {
@@ -771,19 +967,22 @@ PlanLaunch plan_launch_shape(Index& ix, const SearchPlan& p) {
     const uint32_t efmax = std::max(std::max<uint32_t>(1, p.ef_max), L.mmax);
     L.efc = (efmax + 31) & ~31u;
     L.vc = 512;
-    const size_t wsm = warp_smem_bytes(v.dim, L.efc, L.vc);
-    L.wpb = (uint32_t)std::max<size_t>(1, std::min<size_t>(4, (200 * 1024) / wsm));
-    L.smem_a = wsm * L.wpb;
     L.fusedsimd = (ix.order.fused & 1) != 0;
     L.mixed = (ix.precision == HRNN_PREC_BF16 || ix.precision == HRNN_PREC_INT8) &&
               (v.dim == 96 || v.dim == 128 || v.dim == 256) && v.lanes == 16;
     L.int8 = ix.precision == HRNN_PREC_INT8 && v.dim % 16 == 0 && v.dim <= 256;
+    L.fast = (L.mixed || L.int8) && v.W0 <= 33;  // the reduced-precision forms' two-parent search, as in search_batch
+    auto wsm_of = [&](uint32_t vc) {
+        return L.fast ? fast_smem_bytes(v.dim, L.efc, vc) : warp_smem_bytes(v.dim, L.efc, vc);
+    };
+    L.wpb = (uint32_t)std::max<size_t>(1, std::min<size_t>(4, (200 * 1024) / wsm_of(L.vc)));
+    L.smem_a = wsm_of(L.vc) * L.wpb;
     const uint64_t shape_key = ((uint64_t)(L.int8 ? 3 : L.mixed ? 2 : L.fusedsimd ? 1 : 0) << 32) | L.efc;
     auto shape = ix.autotune ? ix.a_shape.find(shape_key) : ix.a_shape.end();  // tuned by an earlier batch call
     if (shape != ix.a_shape.end()) {
         L.wpb = shape->second.first;
         L.vc = shape->second.second;
-        L.smem_a = warp_smem_bytes(v.dim, L.efc, L.vc) * L.wpb;
+        L.smem_a = wsm_of(L.vc) * L.wpb;
     }
     L.counts = p.threshold > 1.0f;
     L.kidx = p.k - 1;
@@ -856,16 +1055,29 @@ void plan_create(SearchPlan& p, cudaStream_t s) {
     // scan scratch sized outside the capture (both scans take nq + 1 entries)
     exclusive_scan_u64(d_total, d_resoff, nq + 1, s, p.tmp);
     exclusive_scan_u32_to_u64(d_rcount, p.d_out_off, nq + 1, s, p.tmp);
-    auto ka = L.int8 ? k_phase_a<3> : L.mixed ? k_phase_a<2> : (L.fusedsimd ? k_phase_a<1> : k_phase_a<0>);
-    CUDA_CHECK(cudaFuncSetAttribute(ka, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem_a));
+    auto ka = L.int8 ? k_phase_a<3> : L.mixed ? k_phase_a<2> : L.fusedsimd ? k_phase_a<1> : k_phase_a<0>;
+    auto kaf = L.int8 ? k_phase_a_fast<3> : k_phase_a_fast<2>;
+    const void* kaf_or_ka = L.fast ? (const void*)kaf : (const void*)ka;
+    CUDA_CHECK(cudaFuncSetAttribute(kaf_or_ka, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem_a));
     int per_sm = 1;
-    CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ka, L.wpb * 32, L.smem_a));
+    CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kaf_or_ka, L.wpb * 32, L.smem_a));
     L.grid_a = (uint32_t)std::max<size_t>(1, std::min<size_t>((nq + L.wpb - 1) / L.wpb, (size_t)nsm * std::max(per_sm, 1)));
+    // verification: the streaming kernel of the INT8 form where search_batch takes it, else the CTA kernel
+    KStream ks = (L.int8 && L.mixed && !L.counts && v.lanes == 16 && !verify_table_forced())
+                     ? pick_stream(ix.wide, L.fusedsimd, v.dim) : nullptr;
     KCta kc = ix.wide ? pick_bc<uint64_t>(L.fusedsimd, L.counts, L.mixed) : pick_bc<uint32_t>(L.fusedsimd, L.counts, L.mixed);
-    CUDA_CHECK(cudaFuncSetAttribute(kc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem_bc));
-    per_sm = 1;
-    CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kc, 256, L.smem_bc));
-    L.grid_bc = (uint32_t)std::min<size_t>(nq, (size_t)nsm * std::max(per_sm, 1));
+    if (ks) {
+        L.smem_bc = 8 * stream_warp_smem(v.dim);
+        CUDA_CHECK(cudaFuncSetAttribute(ks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem_bc));
+        per_sm = 1;
+        CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ks, 256, L.smem_bc));
+        L.grid_bc = (uint32_t)std::min<size_t>((nq + 7) / 8, (size_t)nsm * std::max(per_sm, 1));
+    } else {
+        CUDA_CHECK(cudaFuncSetAttribute(kc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem_bc));
+        per_sm = 1;
+        CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kc, 256, L.smem_bc));
+        L.grid_bc = (uint32_t)std::min<size_t>(nq, (size_t)nsm * std::max(per_sm, 1));
+    }
     void (*kov)(DevView, const float*, uint32_t, uint32_t, const uint32_t*, const uint32_t*, const uint32_t*,
                 const uint64_t*, float, uint32_t, uint32_t, uint32_t*, uint32_t*, uint32_t*, size_t, uint64_t*,
                 uint32_t*, uint32_t*, const uint32_t*, SearchCounters*, const uint32_t*);
@@ -883,9 +1095,14 @@ void plan_create(SearchPlan& p, cudaStream_t s) {
     CUDA_CHECK(cudaMemsetAsync(flag, 0, 4, s));
     k_plan_inputs<<<(unsigned)((nq + 255) / 256), 256, 0, s>>>(p.d_m, p.d_ef, (uint32_t)nq, L.mmax, p.ef_max, pm, pef,
                                                                flag);
-    ka<<<L.grid_a, L.wpb * 32, L.smem_a, s>>>(v, p.d_q, (uint32_t)nq, pm, pef, L.efc, L.vc, L.mmax,
-                                               p.prox.as<uint32_t>(), p.nprox.as<uint32_t>(), ctr, nullptr, 0, 0, 0,
-                                               nullptr, d_next + 4);
+    if (L.fast)
+        kaf<<<L.grid_a, L.wpb * 32, L.smem_a, s>>>(v, p.d_q, (uint32_t)nq, pm, pef, L.efc, L.vc, L.mmax,
+                                                    p.prox.as<uint32_t>(), p.nprox.as<uint32_t>(), ctr, nullptr, 0, 0,
+                                                    0, nullptr, d_next + 4, 0, nullptr, nullptr, nullptr, 0);
+    else
+        ka<<<L.grid_a, L.wpb * 32, L.smem_a, s>>>(v, p.d_q, (uint32_t)nq, pm, pef, L.efc, L.vc, L.mmax,
+                                                   p.prox.as<uint32_t>(), p.nprox.as<uint32_t>(), ctr, nullptr, 0, 0,
+                                                   0, nullptr, d_next + 4);
     {
         const size_t tot = nq * L.mmax;
         auto kb = ix.wide ? k_phase_b_count<uint64_t> : k_phase_b_count<uint32_t>;
@@ -896,9 +1113,16 @@ void plan_create(SearchPlan& p, cudaStream_t s) {
     k_kdist_column<<<(unsigned)((ix.cur + 255) / 256), 256, 0, s>>>(v, L.kidx, p.kcol.as<float>());
     uint64_t* resbuf = p.res.as<uint64_t>();
     uint32_t* ovl = flag + 4;  // the overflow list (nq entries) after the clamp flag
-    kc<<<L.grid_bc, 256, L.smem_bc, s>>>(v, p.d_q, (uint32_t)nq, L.mmax, p.prox.as<uint32_t>(), p.nprox.as<uint32_t>(),
-                                         p.plen.as<uint32_t>(), d_total, d_resoff, p.threshold, p.kcol.as<float>(),
-                                         L.kidx, resbuf, d_rcount, d_next, ovl, d_next + 1, ctr);
+    if (ks)
+        ks<<<L.grid_bc, 256, L.smem_bc, s>>>(v, p.d_q, (uint32_t)nq, L.mmax, p.prox.as<uint32_t>(),
+                                             p.nprox.as<uint32_t>(), p.plen.as<uint32_t>(), d_resoff,
+                                             p.kcol.as<float>(), L.kidx, resbuf, d_rcount, d_next, ovl, d_next + 1,
+                                             ctr);
+    else
+        kc<<<L.grid_bc, 256, L.smem_bc, s>>>(v, p.d_q, (uint32_t)nq, L.mmax, p.prox.as<uint32_t>(),
+                                             p.nprox.as<uint32_t>(), p.plen.as<uint32_t>(), d_total, d_resoff,
+                                             p.threshold, p.kcol.as<float>(), L.kidx, resbuf, d_rcount, d_next, ovl,
+                                             d_next + 1, ctr);
     kov<<<(unsigned)(slots / 4), 128, L.smem_w, s>>>(v, p.d_q, 0, L.mmax, p.prox.as<uint32_t>(),
                                                       p.nprox.as<uint32_t>(), p.plen.as<uint32_t>(), d_resoff,
                                                       p.threshold, L.kidx, L.hcap, p.hkey.as<uint32_t>(),

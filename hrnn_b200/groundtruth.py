@@ -43,8 +43,9 @@ def _margin(na, nb):
     return 1e-4 * (na + nb) + 1e-3
 
 
-def kth_radius_fp64(X: np.ndarray, k: int, device=None, chunk: int = 2048) -> np.ndarray:
-    """Float64 squared distance of every point to its k-th nearest other point."""
+def kth_radius_fp64(X: np.ndarray, k: int, device=None, chunk: int = 2048, rows=None) -> np.ndarray:
+    """Float64 squared distance of every point (or of the points `rows`) to its
+    k-th nearest other point."""
     import torch
     device = device or torch.device("cuda", torch.cuda.current_device())
     torch.backends.cuda.matmul.allow_tf32 = False
@@ -56,27 +57,64 @@ def kth_radius_fp64(X: np.ndarray, k: int, device=None, chunk: int = 2048) -> np
     nx64 = (X64 ** 2).sum(1)
     nx = nx64.float()
     nxmax = nx64.max()
-    out = torch.empty(n, dtype=torch.float64, device=device)
+    R = torch.arange(n, device=device) if rows is None else torch.from_numpy(np.asarray(rows, np.int64)).to(device)
+    chunk = max(1, min(chunk, (1 << 31) // n))  # a chunk's float32 distance rows stay within 8 GB
+    out = torch.empty(len(R), dtype=torch.float64, device=device)
     pad = min(n - 1, k + 16)
     exact_rows = []
-    for s in range(0, n, chunk):
-        e = min(n, s + chunk)
-        D = nx[s:e, None] - 2.0 * (Xt[s:e] @ Xt.T) + nx[None, :]
-        D[torch.arange(e - s, device=device), torch.arange(s, e, device=device)] = float("inf")
+    for s in range(0, len(R), chunk):
+        e = min(len(R), s + chunk)
+        r = R[s:e]
+        D = nx[r, None] - 2.0 * (Xt[r] @ Xt.T) + nx[None, :]
+        D[torch.arange(e - s, device=device), r] = float("inf")
         vals, idx = torch.topk(D, pad, dim=1, largest=False, sorted=True)
-        ex = ((X64[s:e, None, :] - X64[idx]) ** 2).sum(2)
+        ex = ((X64[r, None, :] - X64[idx]) ** 2).sum(2)
         kth = torch.sort(ex, dim=1).values[:, k - 1]
         out[s:e] = kth
         # every point outside the pad candidates has a float32 distance >= the last
         # candidate's: if that minus the margin still exceeds kth, kth is exact
-        ok = (vals[:, -1].double() - _margin(nx64[s:e], nxmax)) > kth
+        ok = (vals[:, -1].double() - _margin(nx64[r], nxmax)) > kth
         if not bool(ok.all()):
             exact_rows.extend((torch.nonzero(~ok).flatten() + s).tolist())
-    for r in exact_rows:  # the whole row in float64
-        d = ((X64 - X64[r]) ** 2).sum(1)
-        d[r] = float("inf")
-        out[r] = torch.kthvalue(d, k).values
+    for j in exact_rows:  # the whole row in float64
+        i = int(R[j])
+        d = ((X64 - X64[i]) ** 2).sum(1)
+        d[i] = float("inf")
+        out[j] = torch.kthvalue(d, k).values
     return out.cpu().numpy()
+
+
+def rknn_fp64_bounded(X: np.ndarray, Q: np.ndarray, kth_upper: np.ndarray, k: int, device=None,
+                      q_chunk: int = 64, x_chunk: int = 1 << 21):
+    """RkNN ground truth of a query subset without every point's k-th radius:
+    kth_upper[x] >= x's true k-th radius (e.g. the k-th distance of an approximate
+    KNN list -- the k-th smallest of any k other points' distances is at least
+    the true one) screens the points, the exact float64 radius is computed only
+    for the points some query may reach, and every decision is float64.
+    Returns what rknn_fp64 returns, and the number of radii computed."""
+    import torch
+    device = device or torch.device("cuda", torch.cuda.current_device())
+    torch.backends.cuda.matmul.allow_tf32 = False
+    n = X.shape[0]
+    Xt = torch.from_numpy(np.ascontiguousarray(X, np.float32)).to(device)
+    nx64 = (Xt.double() ** 2).sum(1)
+    up = torch.from_numpy(np.asarray(kth_upper, np.float64)).to(device)
+    cand = []
+    for s in range(0, Q.shape[0], q_chunk):
+        q = torch.from_numpy(np.ascontiguousarray(Q[s:s + q_chunk], np.float32)).to(device)
+        nq = (q.double() ** 2).sum(1)
+        for x0 in range(0, n, x_chunk):
+            x1 = min(n, x0 + x_chunk)
+            D = nq[:, None] - 2.0 * (q @ Xt[x0:x1].T).double() + nx64[None, x0:x1]
+            hit = torch.nonzero(D <= up[None, x0:x1] + _margin(nq[:, None], nx64[None, x0:x1]))
+            if len(hit):
+                cand.append(hit[:, 1] + x0)
+            del D
+    rows = torch.unique(torch.cat(cand)).cpu().numpy() if cand else np.zeros(0, np.int64)
+    kth = np.full(n, -1.0)  # radius unknown = unreachable: -1 admits nothing
+    if len(rows):
+        kth[rows] = kth_radius_fp64(X, k, device, rows=rows)
+    return rknn_fp64(X, Q, kth, device, chunk=q_chunk), int(len(rows))
 
 
 def rknn_fp64(X: np.ndarray, Q: np.ndarray, kth: np.ndarray, device=None, chunk: int = 256):

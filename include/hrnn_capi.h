@@ -98,6 +98,13 @@ typedef struct {
     int32_t join_mode;                           /* join mode the last call ran          */
 } hrnn_refine_stats;
 
+/* The split of src/hrnn_dynamic_test.cpp:200-203: perm[0..n) = 0..n-1 shuffled by
+ * std::shuffle with std::mt19937(seed) (seed 42 there) -- the first split*n
+ * entries build the index, the rest are inserted.  std::shuffle's draw sequence
+ * belongs to the C++ standard library, so the permutation is made by this
+ * library's own libstdc++ rather than restated. */
+hrnn_status hrnn_dynamic_split(uint64_t n, uint32_t seed, uint32_t* perm);
+
 /* Counters of the last hrnn_insert_dynamic call. */
 typedef struct {
     uint64_t n_inserted;     /* points added                                    */
@@ -202,6 +209,11 @@ void hrnn_search_plan_destroy(hrnn_search_plan* plan);
 
 /* compactForServing(max_k_serve) -- hrnn.h:299-364: dense kdist[n x max_k_serve]. */
 hrnn_status hrnn_compact_for_serving(hrnn_index* h, size_t max_k_serve);
+
+/* The radius every verification compares against, kdist(p, k-1) of
+ * hrnn.h:286-293 (FLT_MAX where the KNN list is shorter than k; the serve-mode
+ * matrix after compactForServing), for every element: out[cur_element_count]. */
+hrnn_status hrnn_get_kdist(hrnn_index* h, uint32_t k, float* out);
 
 /* insertPointDynamic(x, label, m_update, bidirectional) for n points --
  * hrnn.h:2360-2534, as the insert loop of src/hrnn_dynamic_test.cpp:310-331. */

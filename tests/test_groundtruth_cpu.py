@@ -43,3 +43,20 @@ def test_fbin_roundtrip(tmp_path):
     G.write_fbin(p, X)
     assert np.array_equal(G.read_fbin(p), X)
     assert np.array_equal(data.read_fbin(p), X)
+
+
+def test_bounded_groundtruth_equals_full():
+    """Radii only for the points an upper bound of their k-th radius lets some
+    query reach: the same ground truth as with every radius, fewer radii."""
+    torch = pytest.importorskip("torch")
+    from hrnn_b200 import groundtruth as G
+    X = data.mixture(3000, 24, 6, 1.0, 5, 5)
+    Q = data.mixture(50, 24, 6, 1.0, 5, 6)
+    cpu = torch.device("cpu")
+    kth = G.kth_radius_fp64(X, 7, cpu, chunk=256)
+    rows = np.array([5, 17, 2999])
+    assert np.array_equal(G.kth_radius_fp64(X, 7, cpu, chunk=100, rows=rows), kth[rows])
+    full = G.rknn_fp64(X, Q, kth, cpu, chunk=16)
+    got, nr = G.rknn_fp64_bounded(X, Q, kth * 1.3 + 0.1, 7, cpu, q_chunk=16, x_chunk=1000)
+    assert nr < len(X)
+    assert all(np.array_equal(a[0], b[0]) for a, b in zip(full, got))
