@@ -36,7 +36,7 @@ EXPORTS = [
     "hrnn_set_knng", "hrnn_get_rknng", "hrnn_l2_batch", "hrnn_build_rknng_noalloc",
     "hrnn_set_budget", "hrnn_budget_features", "hrnn_budget_train", "hrnn_budget_predict",
     "hrnn_budget_gradients", "hrnn_budget_get_weights", "hrnn_budget_set_weights", "hrnn_get_dynamic_stats",
-    "hrnn_dynamic_split", "hrnn_get_kdist",
+    "hrnn_dynamic_split", "hrnn_get_kdist", "hrnn_get_rknng_mutable",
 ]
 
 # Learned-budget MLP: 256 -> 256 -> 256 -> 2; parameters W1 b1 W2 b2 W3 b3 (row-major
@@ -447,6 +447,18 @@ class HRNN:
         cnt = np.zeros(n, np.uint32)
         _check(_lib.hrnn_get_knng(self._h, _p(ids), _p(d), _p(cnt)))
         return ids, d, cnt
+
+    def get_rknng_mutable(self):
+        """The mutable reverse lists (rknng_lists_ of hrnn.h:1942-1959) as one owner
+        array per element, in the device's order."""
+        n = self.getCurrentElementCount()
+        lens = np.zeros(n, np.uint64)
+        _check(_lib.hrnn_get_rknng_mutable(self._h, _p(lens), None))
+        flat = np.zeros(max(int(lens.sum()), 1), np.uint32)
+        _check(_lib.hrnn_get_rknng_mutable(self._h, _p(lens), _p(flat)))
+        off = np.zeros(n + 1, np.int64)
+        off[1:] = np.cumsum(lens.astype(np.int64))
+        return [flat[off[i]:off[i + 1]] for i in range(n)]
 
     def get_kdist(self, k: int) -> np.ndarray:
         """kdist(p, k-1) of every element (FLT_MAX where the list is shorter than

@@ -298,6 +298,14 @@ hrnn_status hrnn_compact_for_serving(hrnn_index* h, size_t mks) {
     });
 }
 
+hrnn_status hrnn_get_rknng_mutable(hrnn_index* h, uint64_t* lens, uint32_t* flat) {
+    return guard([&] {
+        need(h, "index");
+        set_device(h);
+        hrnn::mutable_get(h->ix, lens, flat);
+    });
+}
+
 hrnn_status hrnn_get_kdist(hrnn_index* h, uint32_t k, float* out) {
     return guard([&] {
         need(h, "index");
@@ -552,6 +560,7 @@ hrnn_status hrnn_get_rknng(hrnn_index* h, uint64_t* n_offsets, uint64_t* n_entri
         hrnn::Index& ix = h->ix;
         if (!ix.rknng_built) hrnn::fail(HRNN_ERR_STATE, "searchRknn: RKNNG not built");
         set_device(h);
+        hrnn::ensure_flat_rknng(ix);
         if (n_offsets) *n_offsets = ix.cur + 1;
         if (n_entries) *n_entries = ix.csr_entries;
         if (entry_bytes) *entry_bytes = ix.wide ? 8 : 4;

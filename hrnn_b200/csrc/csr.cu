@@ -254,6 +254,7 @@ void build_rknng(Index& ix) {
     else build_impl<uint32_t>(ix);
     ix.csr_in_reference_order = false;
     ix.rknng_built = true;
+    ix.csr_stale = false;
 }
 
 void rknng_reference_order(Index& ix, uint64_t* offsets, void* entries) {
@@ -272,6 +273,7 @@ void compact_for_serving(Index& ix, size_t mks) {
     if (ix.serve_mode) return;                            // hrnn.h:300
     if (ix.K == 0 || !ix.knng_built) fail(HRNN_ERR_STATE, "compactForServing: KNNG not built");
     if (mks == 0 || mks > ix.K) fail(HRNN_ERR_ARG, "compactForServing: max_k_serve must be in [1, K_knng]");
+    if (ix.rknng_built) ensure_flat_rknng(ix);
     size_t n = ix.cur;
     ix.kdist_serve.alloc(std::max<size_t>(n * mks, 1) * 4);
     size_t tot = n * mks;

@@ -338,6 +338,7 @@ void load_idx(Index& ix, const std::string& path, size_t dim, size_t max_element
 
 void save_idx(Index& ix, const std::string& path) {
     if (ix.serve_mode) fail(HRNN_ERR_STATE, "saveIndex: index is in serve mode");
+    ensure_flat_rknng(ix);
     CUDA_CHECK(cudaStreamSynchronize(ix.stream));
     Writer w;
     w.out.open(path, std::ios::binary);

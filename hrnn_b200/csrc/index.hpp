@@ -54,6 +54,18 @@ struct SearchCounters {
     unsigned long long n_lowp, n_fp32, n_fp64, n_flip, overflow;
 };
 
+// Device mutable reverse lists (rknng_mutable.cu): element i's owners in
+// ent[off[i] .. off[i] + len[i]), cap[i] slots.
+struct MutableLists {
+    DevMem off, len, cap, ent;
+    DevMem ops, ctl;                          // pending edits; ctl: edit count (u64), flags
+    DevMem ocnt, ocur, ooff, grouped, tmp;    // grouping work space
+    unsigned long long ops_cap = 0;
+    uint32_t slack_shift = 0;                 // capacities doubled after an overflow
+    bool valid = false;
+    uint64_t rebuilds = 0, applied = 0;
+};
+
 struct Index {
     // ---- device / stream -------------------------------------------------
     int device = 0;
@@ -111,6 +123,8 @@ struct Index {
     // ---- buildRKNNG_mutable / insertPointDynamic: the reverse lists are the
     // CSR above, rebuilt after each batch of inserts (so they are exact).
     bool rknng_mutable = false;
+    MutableLists mr;          // the reverse lists insertPointDynamic reads and edits
+    bool csr_stale = false;   // the flat CSR predates inserts: rebuilt before its next use
     hrnn_dynamic_stats dyn_stats{};
 
     // ---- serve mode (compactForServing, hrnn.h:299-364) -------------------
@@ -150,6 +164,14 @@ L2Order detect_l2_order();
 void build_rknng(Index& ix);
 void rknng_reference_order(Index& ix, uint64_t* offsets, void* entries);
 void build_rknng_mutable(Index& ix);
+void ensure_flat_rknng(Index& ix);  // rebuilds the flat CSR when inserts made it stale
+
+// rknng_mutable.cu
+void mutable_build(Index& ix);
+void mutable_ops_reserve(Index& ix, unsigned long long cap);
+void mutable_register(Index& ix, uint32_t x0, uint32_t nx);
+void mutable_apply(Index& ix);
+void mutable_get(Index& ix, uint64_t* lens, uint32_t* flat);
 
 // search.cu
 struct SearchArgs {

@@ -462,6 +462,7 @@ __global__ void k_bucket_fill(const Prop* __restrict__ prop, unsigned long long 
 // ---- phase 2: merge ----------------------------------------------------------
 
 constexpr int kMT = 256;          // merge CTA threads
+constexpr uint64_t kOpRemove = 0x80000000ull;  // reverse-list edit: remove (else add) the owner
 constexpr uint32_t kMH = 8192;    // source-id hash slots
 constexpr uint32_t kMS = 4096;    // survivor keys
 
@@ -545,11 +546,18 @@ __device__ uint32_t block_select(const float* Ld, uint32_t cnt, const uint64_t* 
 // (list U survivors) by radix selection; sort the survivors at or below tau by
 // (d, source) and merge them into the list, list entries first among equal
 // distances, keeping K.  Inserted entries are marked new (isnew may be null).
+//
+// ops (may be null): the list changes as reverse-list edits for the mutable
+// reverse lists -- an inserted entry v of u's list is (v << 32 | u), an entry w it
+// pushed out (w << 32 | u | kOpRemove); at most ops_cap are written, *nops counts
+// them all.
 __global__ void __launch_bounds__(kMT) k_merge_cta(uint32_t n, uint32_t K, const uint64_t* __restrict__ toff,
                                                    const uint64_t* __restrict__ bucket, uint32_t* __restrict__ hdr,
                                                    uint32_t* __restrict__ ids, float* __restrict__ dist,
                                                    uint8_t* __restrict__ isnew, unsigned long long* __restrict__ nupd,
-                                                   uint32_t* __restrict__ next_t) {
+                                                   uint32_t* __restrict__ next_t, uint64_t* __restrict__ ops,
+                                                   unsigned long long* __restrict__ nops,
+                                                   unsigned long long ops_cap) {
     extern __shared__ __align__(16) char smraw[];
     uint64_t* surv = (uint64_t*)smraw;
     uint32_t* hk = (uint32_t*)(surv + kMS);
@@ -579,10 +587,12 @@ __global__ void __launch_bounds__(kMT) k_merge_cta(uint32_t n, uint32_t K, const
         uint32_t* Li2 = LiB;
         uint8_t* Lf2 = LfB;
         uint32_t cnt = hdr[u] & 0xFFFFu;
+        const uint32_t cnt0 = cnt;
+        // Lf: bit 0 the entry's new flag, bit 1 "was in the list before this merge"
         for (uint32_t j = tid; j < cnt; j += kMT) {
             Ld[j] = dist[(size_t)u * K + j];
             Li[j] = ids[(size_t)u * K + j];
-            Lf[j] = isnew ? isnew[(size_t)u * K + j] : 0;
+            Lf[j] = (uint8_t)((isnew ? isnew[(size_t)u * K + j] : 0) | 2);
         }
         if (tid == 0) ctl[5] = cnt;
         for (uint64_t w0 = pb; w0 < pe; w0 += W) {
@@ -703,10 +713,31 @@ __global__ void __launch_bounds__(kMT) k_merge_cta(uint32_t n, uint32_t K, const
         }
         __syncthreads();
         const uint32_t lo = ctl[5];
+        if (ops) {
+            // entries kept from before form a prefix of the old list (the merge keeps
+            // list order); the old entries after it were pushed out
+            if (tid == 0) ctl[6] = 0;
+            __syncthreads();
+            uint32_t kept_l = 0;
+            for (uint32_t j = tid; j < cnt; j += kMT) kept_l += (Lf[j] >> 1) & 1u;
+            if (kept_l) atomicAdd(&ctl[6], kept_l);
+            __syncthreads();
+            const uint32_t kept = ctl[6];
+            for (uint32_t j = lo + tid; j < cnt; j += kMT)
+                if (!(Lf[j] & 2u)) {
+                    const unsigned long long o = atomicAdd(nops, 1ull);
+                    if (o < ops_cap) ops[o] = ((uint64_t)Li[j] << 32) | u;
+                }
+            for (uint32_t j = kept + tid; j < cnt0; j += kMT) {
+                const unsigned long long o = atomicAdd(nops, 1ull);
+                if (o < ops_cap) ops[o] = ((uint64_t)ids[(size_t)u * K + j] << 32) | u | kOpRemove;
+            }
+            __syncthreads();
+        }
         for (uint32_t j = lo + tid; j < cnt; j += kMT) {
             dist[(size_t)u * K + j] = Ld[j];
             ids[(size_t)u * K + j] = Li[j];
-            if (isnew) isnew[(size_t)u * K + j] = Lf[j];
+            if (isnew) isnew[(size_t)u * K + j] = Lf[j] & 1u;
         }
         if (tid == 0) hdr[u] = (hdr[u] & 0xFFFF0000u) | cnt;
     }
@@ -720,7 +751,8 @@ __global__ void __launch_bounds__(kMT) k_merge_cta(uint32_t n, uint32_t K, const
 void bucket_and_merge(uint32_t n, uint32_t K, const Prop* prop, unsigned long long np, DevMem& tcount, DevMem& toff,
                       DevMem& tcur, uint64_t* bucket, DevMem& tmp, uint32_t* hdr, uint32_t* ids, float* dist,
                       uint8_t* isnew, unsigned long long* d_nupd, uint32_t* d_nextt, size_t merge_smem,
-                      unsigned merge_grid, int nsm, cudaStream_t s, cudaEvent_t mid) {
+                      unsigned merge_grid, int nsm, cudaStream_t s, cudaEvent_t mid, uint64_t* ops = nullptr,
+                      unsigned long long* nops = nullptr, unsigned long long ops_cap = 0) {
     CUDA_CHECK(cudaMemsetAsync(tcount.p, 0, ((size_t)n + 1) * 4, s));
     CUDA_CHECK(cudaMemsetAsync(tcur.p, 0, ((size_t)n + 1) * 4, s));
     const unsigned gb = (unsigned)std::min<unsigned long long>((np + 255) / 256, (unsigned long long)nsm * 32);
@@ -732,7 +764,7 @@ void bucket_and_merge(uint32_t n, uint32_t K, const Prop* prop, unsigned long lo
     if (mid) CUDA_CHECK(cudaEventRecord(mid, s));
     CUDA_CHECK(cudaMemsetAsync(d_nextt, 0, 4, s));
     k_merge_cta<<<merge_grid, kMT, merge_smem, s>>>(n, K, toff.as<uint64_t>(), bucket, hdr, ids, dist, isnew, d_nupd,
-                                                    d_nextt);
+                                                    d_nextt, ops, nops, ops_cap);
     CUDA_LAUNCH_CHECK();
 }
 
@@ -827,7 +859,10 @@ __global__ void __launch_bounds__(256) k_dyn_self_query(
     const uint32_t* __restrict__ hdr, const uint32_t* __restrict__ ids, uint32_t K,
     const uint64_t* __restrict__ csr_off, const void* __restrict__ csr_ent_v, uint32_t rb, uint32_t m_update, int bidir,
     const float* __restrict__ thr, Prop* __restrict__ prop, unsigned long long* __restrict__ pcount,
-    unsigned long long pcap, unsigned long long* __restrict__ ndist, uint32_t* __restrict__ next) {
+    unsigned long long pcap, unsigned long long* __restrict__ ndist, uint32_t* __restrict__ next,
+    const uint32_t* __restrict__ mlen) {
+    // mlen non-null: the reverse lists are the mutable ones (owner ids from
+    // csr_off[y], mlen[y] of them) instead of the flat CSR
     extern __shared__ __align__(16) char smraw[];
     const E* __restrict__ csr_ent = static_cast<const E*>(csr_ent_v);
     float* q = (float*)smraw;
@@ -904,12 +939,13 @@ __global__ void __launch_bounds__(256) k_dyn_self_query(
         };
         for (uint32_t pi = 0; pi < P; ++pi) {
             const uint32_t y = ids[(size_t)x * K + pi];
-            const uint64_t b = csr_off[y], e = csr_off[y + 1];
+            const uint64_t b = csr_off[y], e = mlen ? b + mlen[y] : csr_off[y + 1];
             for (uint64_t e0 = b; e0 < e; e0 += 256) {
                 if (ctl[1] + 256 > kDB || ctl[2] + 256 > kDC * 3 / 5) flush();
                 const uint64_t idx = e0 + tid;
                 if (idx < e) {
-                    const uint32_t o = (uint32_t)(csr_ent[idx] >> rb);
+                    const uint32_t o = mlen ? static_cast<const uint32_t*>(csr_ent_v)[idx]
+                                            : (uint32_t)(csr_ent[idx] >> rb);
                     if (!hset_contains(xh, kDX, o) && hset_insert(ch, kDC, o)) {
                         buf[atomicAdd(&ctl[1], 1u)] = o;
                         atomicAdd(&ctl[2], 1u);
@@ -1150,10 +1186,24 @@ void refine_knng(Index& ix, int iters, int sample) {
 
 void build_rknng_mutable(Index& ix) {
     if (!ix.knng_built) fail(HRNN_ERR_STATE, "buildRKNNG_mutable: KNNG not built yet");  // hrnn.h:1943-1944
-    build_rknng(ix);
+    ix.mr.slack_shift = 0;
+    mutable_build(ix);
     ix.rknng_mutable = true;
-    std::printf("    buildRKNNG_mutable: n=%zu total_entries=%zu\n", ix.cur, ix.csr_entries);
+    uint64_t total = 0;
+    if (ix.cur) {
+        std::vector<uint32_t> ln(ix.cur);
+        CUDA_CHECK(cudaMemcpy(ln.data(), ix.mr.len.p, ix.cur * 4, cudaMemcpyDeviceToHost));
+        for (uint32_t x : ln) total += x;
+    }
+    std::printf("    buildRKNNG_mutable: n=%zu total_entries=%llu\n", ix.cur, (unsigned long long)total);
     std::fflush(stdout);
+}
+
+void ensure_flat_rknng(Index& ix) {
+    if (ix.csr_stale) {
+        build_rknng(ix);
+        ix.csr_stale = false;
+    }
 }
 
 void insert_dynamic(Index& ix, const float* data, const uint64_t* labels, size_t n, unsigned m_update,
@@ -1184,6 +1234,8 @@ void insert_dynamic(Index& ix, const float* data, const uint64_t* labels, size_t
                                                (unsigned long long)(free_b * 0.3 / 20)}));
     prop.alloc(pcap * sizeof(Prop));
     bucket.alloc(pcap * 8);
+    if (!ix.mr.valid) mutable_build(ix);
+    mutable_ops_reserve(ix, std::min<unsigned long long>(2 * pcap, 1ull << 26));
     unsigned long long* d_pcount = ctr.as<unsigned long long>();
     unsigned long long* d_ndist = d_pcount + 1;
     unsigned long long* d_nupd = d_pcount + 2;
@@ -1214,7 +1266,7 @@ void insert_dynamic(Index& ix, const float* data, const uint64_t* labels, size_t
         CUDA_CHECK(cudaEventRecord(ev[0], s));
         add_points(ix, data + done * ix.dim, labels ? labels + done : nullptr, sb);
         CUDA_CHECK(cudaEventRecord(ev[1], s));
-        build_rknng(ix);  // the batch joins its neighbours' reverse lists
+        mutable_register(ix, x0, (uint32_t)sb);  // the batch joins its neighbours' reverse lists
         CUDA_CHECK(cudaEventRecord(ev[2], s));
         const uint32_t nall = (uint32_t)ix.cur;
         auto kq = ix.wide ? (fusedsimd ? k_dyn_self_query<true, uint64_t> : k_dyn_self_query<false, uint64_t>)
@@ -1232,9 +1284,9 @@ void insert_dynamic(Index& ix, const float* data, const uint64_t* labels, size_t
             const unsigned grid = (unsigned)std::min<size_t>(na, (size_t)nsm * std::max(sq_per_sm, 1));
             kq<<<grid, 256, sq_smem, s>>>(ix.vec.as<float>(), (uint32_t)ix.dim, ix.order.lanes, ix.order.fused,
                                           x0 + a, na, ix.knn_hdr.as<uint32_t>(), ix.knn_ids.as<uint32_t>(), K,
-                                          ix.csr_off.as<uint64_t>(), ix.csr_ent.p, ix.rank_bits, m_update,
+                                          ix.mr.off.as<uint64_t>(), ix.mr.ent.p, 0, m_update,
                                           bidirectional ? 1 : 0, thr.as<float>(), prop.as<Prop>(), d_pcount, pcap,
-                                          d_ndist, d_next);
+                                          d_ndist, d_next, ix.mr.len.as<uint32_t>());
             CUDA_LAUNCH_CHECK();
             unsigned long long np = 0;
             CUDA_CHECK(cudaMemcpyAsync(&np, d_pcount, 8, cudaMemcpyDeviceToHost, s));
@@ -1244,10 +1296,14 @@ void insert_dynamic(Index& ix, const float* data, const uint64_t* labels, size_t
                 chunk = std::max<uint32_t>(1, chunk / 4);
                 continue;
             }
-            if (np)
+            if (np) {
+                // the merge's list changes are edited into the mutable reverse lists
                 bucket_and_merge(nall, K, prop.as<Prop>(), np, tcount, toff, tcur, bucket.as<uint64_t>(), tmp,
                                  ix.knn_hdr.as<uint32_t>(), ix.knn_ids.as<uint32_t>(), ix.knn_dist.as<float>(), nullptr,
-                                 d_nupd, d_nextt, merge_smem, merge_grid, nsm, s, nullptr);
+                                 d_nupd, d_nextt, merge_smem, merge_grid, nsm, s, nullptr, ix.mr.ops.as<uint64_t>(),
+                                 ix.mr.ctl.as<unsigned long long>(), ix.mr.ops_cap);
+                mutable_apply(ix);
+            }
             st.n_proposals += np;
             a += na;
             if (np < pcap / 4) chunk = std::min<uint32_t>(chunk * 2, 1u << 20);
@@ -1261,13 +1317,14 @@ void insert_dynamic(Index& ix, const float* data, const uint64_t* labels, size_t
         st.n_batches++;
         done += sb;
     }
-    CUDA_CHECK(cudaEventRecord(ev[0], s));
-    build_rknng(ix);  // reverse lists of the final graph
-    CUDA_CHECK(cudaEventRecord(ev[1], s));
+    // The flat CSR the search reads (sorted by rank) is rebuilt once, before its
+    // next use (the reference's driver calls buildRKNNG after its inserts,
+    // src/hrnn_dynamic_test.cpp:368).
+    ix.csr_stale = true;
+    ix.rknng_built = true;
     unsigned long long hc[3] = {0, 0, 0};
     CUDA_CHECK(cudaMemcpyAsync(hc, ctr.p, 24, cudaMemcpyDeviceToHost, s));
     CUDA_CHECK(cudaStreamSynchronize(s));
-    st.rknng_ms += elapsed(ev[0], ev[1]);
     for (auto& e : ev) cudaEventDestroy(e);
     st.n_inserted = n;
     st.n_dist = hc[1];

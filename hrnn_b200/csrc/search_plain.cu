@@ -481,6 +481,7 @@ DevView make_view(Index& ix) {
 
 uint64_t search_batch(Index& ix, const SearchArgs& a) {
     if (!ix.rknng_built) fail(HRNN_ERR_STATE, "searchRknn: RKNNG not built");
+    ensure_flat_rknng(ix);
     cudaStream_t s = a.stream ? a.stream : ix.stream;
     const size_t nq = a.nq;
     if (ix.serve_mode && (a.k == 0 || a.k > ix.max_k_serve))
@@ -880,6 +881,7 @@ Budget& budget_of(Index& ix) {
 // and k_budget_features, in the index's precision mode.
 void budget_features(Index& ix, const float* d_q, size_t nq, uint32_t k, uint32_t m, uint32_t ef, float* d_feat) {
     if (!ix.rknng_built) fail(HRNN_ERR_STATE, "searchRknn: RKNNG not built");
+    ensure_flat_rknng(ix);
     if (ix.dim % 4 != 0) fail(HRNN_ERR_ARG, "budget: dim must be a multiple of 4");
     if (nq == 0) return;
     Budget& b = budget_of(ix);
@@ -996,6 +998,7 @@ PlanLaunch plan_launch_shape(Index& ix, const SearchPlan& p) {
 void plan_create(SearchPlan& p, cudaStream_t s) {
     Index& ix = *p.ix;
     if (!ix.rknng_built) fail(HRNN_ERR_STATE, "searchRknn: RKNNG not built");
+    ensure_flat_rknng(ix);
     if (ix.budget && ix.budget->enabled)
         fail(HRNN_ERR_STATE, "search plan: the learned budget is not captured; disable it first");
     if (p.nq == 0 || p.nq > (1u << 30)) fail(HRNN_ERR_ARG, "search plan: nq must be in [1, 2^30]");

@@ -105,6 +105,12 @@ typedef struct {
  * library's own libstdc++ rather than restated. */
 hrnn_status hrnn_dynamic_split(uint64_t n, uint32_t seed, uint32_t* perm);
 
+/* The mutable reverse lists of buildRKNNG_mutable (rknng_lists_, hrnn.h:1942-1959),
+ * as insertPointDynamic maintains them on the device: lens[cur_element_count]
+ * receives each list's length, flat the lists one after another (owner ids, in
+ * no particular order, as the reference's per-node vectors).  Either may be NULL. */
+hrnn_status hrnn_get_rknng_mutable(hrnn_index* h, uint64_t* lens, uint32_t* flat);
+
 /* Counters of the last hrnn_insert_dynamic call. */
 typedef struct {
     uint64_t n_inserted;     /* points added                                    */

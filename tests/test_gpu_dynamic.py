@@ -108,3 +108,29 @@ def test_dynamic_insert_errors():
         h.insertPointDynamic(X[N0:N0 + 20], np.arange(N0, N0 + 20, dtype=np.uint64))
     h.insertPointDynamic(X[N0:N0 + 10], np.arange(N0, N0 + 10, dtype=np.uint64))
     assert h.getCurrentElementCount() == N0 + 10
+
+
+@pytest.mark.parametrize("m_update,bidir", [(4, False), (0, True)])
+def test_mutable_reverse_lists_follow_the_graph(m_update, bidir):
+    """The device's mutable reverse lists (buildRKNNG_mutable, edited in place by
+    every insert batch: the new points join their neighbours' lists, accepted and
+    pushed-out entries move) equal the transpose of the KNN graph after each call,
+    as sets, for every element."""
+    X, _ = _data()
+    h = _build(X)
+
+    def check():
+        ids, _, cnt = h.get_knng()
+        lists = h.get_rknng_mutable()
+        n = h.getCurrentElementCount()
+        exp = [[] for _ in range(n)]
+        for i in range(n):
+            for y in ids[i, :cnt[i]]:
+                exp[int(y)].append(i)
+        bad = [y for y in range(n) if sorted(lists[y].tolist()) != sorted(exp[y])]
+        assert not bad, bad[:5]
+
+    check()
+    for a, b in ((N0, N0 + 700), (N0 + 700, N0 + N1)):
+        h.insertPointDynamic(X[a:b], np.arange(a, b, dtype=np.uint64), m_update, bidir)
+        check()
