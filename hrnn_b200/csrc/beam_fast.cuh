@@ -202,18 +202,22 @@ __device__ __forceinline__ void beam_insert_fast(WarpSmem& s, const float* nd, c
 
 // Two-parent search of level 0 continuing from the beam s.td/s.ti[0..tsize)
 // (sorted; ids carry kExpanded).  The visited cache must hold (at least) the
-// beam's ids.  Returns the beam size (<= EF).
+// beam's ids.  The beam keeps the EF nearest scored points; only its first EX
+// (<= EF) are expanded, the rest is a reserve a later search with a larger beam
+// can resume from (the first EX entries evolve exactly as in a search with
+// EF = EX).  Returns the beam size (<= EF).
 template <int DM>
-__device__ uint32_t beam_search_fast(const DevView& v, WarpSmem& s, uint32_t tsize, uint32_t EF, uint32_t vc,
-                                     unsigned long long& c_dist, unsigned long long& c_exp) {
+__device__ uint32_t beam_search_fast(const DevView& v, WarpSmem& s, uint32_t tsize, uint32_t EF, uint32_t EX,
+                                     uint32_t vc, unsigned long long& c_dist, unsigned long long& c_exp) {
     const int lane = threadIdx.x & 31;
     uint32_t cursor = 0;
     for (;;) {
-        // the (up to) two best unexpanded entries at or after cursor
+        // the (up to) two best unexpanded entries at or after cursor, among the first EX
         uint32_t par0 = kInvalid, par1 = kInvalid;
-        for (uint32_t b = cursor; b < tsize; b += 32) {
+        const uint32_t lim = min(tsize, EX);
+        for (uint32_t b = cursor; b < lim; b += 32) {
             const uint32_t idx = b + lane;
-            const bool u = idx < tsize && !(s.ti[idx] & kExpanded);
+            const bool u = idx < lim && !(s.ti[idx] & kExpanded);
             uint32_t bal = __ballot_sync(0xFFFFFFFFu, u);
             if (!bal) continue;
             if (par0 == kInvalid) {

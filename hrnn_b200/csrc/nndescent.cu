@@ -283,13 +283,16 @@ __global__ void k_sample_rev(uint32_t n, uint32_t R, uint32_t cap, const uint64_
 // One block per node of the chunk: exact FP32 distances of all sample pairs.
 // The node's rows are staged in shared memory (stride dim + 4 floats: 16-byte
 // aligned and free of bank conflicts for float4 reads).  A warp takes a tile of
-// 4 rows i x 32 columns j (lane = column): the 4 row vectors are read by every
+// kJR rows i x 32 columns j (lane = column): the row vectors are read by every
 // lane at the same address (broadcast) and the lane's column vector once for all
-// 4 pairs.  Each pair keeps the reference's 16 accumulators (element e into
-// accumulator e mod 16, then summed left to right), so the tiling leaves every
-// distance bit-identical.  Proposals are appended with one atomic per warp tile.
+// kJR pairs, so a 16-byte shared-memory read feeds 4 kJR elementwise steps.
+// Each pair keeps the reference's 16 accumulators (element e into accumulator
+// e mod 16, then summed left to right), so the tiling leaves every distance
+// bit-identical.  Proposals are appended with one atomic per warp tile.
+constexpr int kJR = 8;
+
 template <bool FUSED>
-__global__ void __launch_bounds__(256) k_join(const float* __restrict__ vec, uint32_t dim, uint32_t node0,
+__global__ void __launch_bounds__(256, 1) k_join(const float* __restrict__ vec, uint32_t dim, uint32_t node0,
                                               uint32_t node1, uint32_t cap, const uint32_t* __restrict__ newl,
                                               const uint32_t* __restrict__ newc, const uint32_t* __restrict__ oldl,
                                               const uint32_t* __restrict__ oldc, const float* __restrict__ thr,
@@ -297,7 +300,7 @@ __global__ void __launch_bounds__(256) k_join(const float* __restrict__ vec, uin
                                               unsigned long long pcap, unsigned long long* __restrict__ njoin) {
     extern __shared__ __align__(16) float sm[];
     const uint32_t SP = dim + 4;
-    uint32_t* sid = (uint32_t*)(sm + (size_t)2 * cap * SP);
+    uint32_t* sid = (uint32_t*)(sm + (size_t)(2 * cap + kJR) * SP);
     float* sthr = (float*)(sid + 2 * cap);
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const uint32_t d4 = dim >> 2;
@@ -319,17 +322,19 @@ __global__ void __launch_bounds__(256) k_join(const float* __restrict__ vec, uin
             for (uint32_t c = lane; c < d4; c += 32) dst[c] = __ldg(src + c);
         }
         __syncthreads();
-        const uint32_t ti_n = (nn + 3) >> 2, tj_n = (tot + 31) >> 5;
+        const uint32_t ti_n = (nn + kJR - 1) / kJR, tj_n = (tot + 31) >> 5;
         for (uint32_t t = w; t < ti_n * tj_n; t += nw) {
-            const uint32_t i0 = (t / tj_n) << 2, jb = (t % tj_n) << 5;
+            const uint32_t i0 = (t / tj_n) * kJR, jb = (t % tj_n) << 5;
             if (jb + 31 <= i0) continue;  // no j > i in this tile (uniform over the warp)
             const uint32_t j = jb + lane;
             const uint32_t jr = j < tot ? j : tot - 1;
-            float acc[4][16];
+            float acc[kJR][16];
 #pragma unroll
-            for (int r = 0; r < 4; ++r)
+            for (int r = 0; r < kJR; ++r)
 #pragma unroll
                 for (int l = 0; l < 16; ++l) acc[r][l] = 0.f;
+            // rows past the staged ones (i0 + r >= tot) read the spare rows at the
+            // end of the stage; their sums are never used
             const float4* xb = reinterpret_cast<const float4*>(sm + (size_t)jr * SP);
             const float4* xa = reinterpret_cast<const float4*>(sm + (size_t)i0 * SP);
             const uint32_t sp4 = SP >> 2;
@@ -338,7 +343,7 @@ __global__ void __launch_bounds__(256) k_join(const float* __restrict__ vec, uin
                 for (int c = 0; c < 4; ++c) {
                     const float4 b = xb[e4 + c];
 #pragma unroll
-                    for (int r = 0; r < 4; ++r) {
+                    for (int r = 0; r < kJR; ++r) {
                         const float4 a = xa[(size_t)r * sp4 + e4 + c];
                         acc[r][4 * c + 0] = sq_step(acc[r][4 * c + 0], a.x - b.x, FUSED);
                         acc[r][4 * c + 1] = sq_step(acc[r][4 * c + 1], a.y - b.y, FUSED);
@@ -347,12 +352,12 @@ __global__ void __launch_bounds__(256) k_join(const float* __restrict__ vec, uin
                     }
                 }
             }
-            float dd[4];
+            float dd[kJR];
             uint32_t emit = 0;  // bit 2r: i -> j proposal, bit 2r+1: j -> i
             const uint32_t bj = sid[jr];
             const float tj = sthr[jr];
 #pragma unroll
-            for (int r = 0; r < 4; ++r) {
+            for (int r = 0; r < kJR; ++r) {
                 float dv = acc[r][0];
 #pragma unroll
                 for (int l = 1; l < 16; ++l) dv = __fadd_rn(dv, acc[r][l]);
@@ -377,7 +382,7 @@ __global__ void __launch_bounds__(256) k_join(const float* __restrict__ vec, uin
                 basep = __shfl_sync(0xFFFFFFFFu, basep, 0);
                 unsigned long long p = basep + (incl - ne);
 #pragma unroll
-                for (int r = 0; r < 4; ++r) {
+                for (int r = 0; r < kJR; ++r) {
                     const uint32_t ai = sid[(i0 + r) < tot ? i0 + r : 0];
                     if ((emit >> (2 * r)) & 1u) {
                         if (p < pcap) prop[p] = Prop{ai, bj, dd[r]};
@@ -1029,7 +1034,7 @@ void refine_knng(Index& ix, int iters, int sample) {
     // Tensor-core screened join where the dims and sample sizes allow it.
     const bool tcj = fast && ix.join_mode != kJoinExact && join_tc_supported((uint32_t)ix.dim, cap);
     JoinTcCounters* d_jc = reinterpret_cast<JoinTcCounters*>(ctr.as<char>() + 64);
-    const size_t join_smem = (size_t)2 * cap * (ix.dim + 4) * 4 + (size_t)2 * cap * 8;
+    const size_t join_smem = (size_t)(2 * cap + kJR) * (ix.dim + 4) * 4 + (size_t)2 * cap * 8;
     if (fast) {
         auto kj = (ix.order.fused & 1) ? k_join<true> : k_join<false>;
         if (join_smem > 227 * 1024) fail(HRNN_ERR_ARG, "refineKNNG: sample size too large for dim");

@@ -202,7 +202,10 @@ __global__ void __launch_bounds__(128) k_phase_a_fast(DevView v, const float* __
             __syncwarp();
             tsize = 1;
         }
-        tsize = beam_search_fast<DM>(v, s, tsize, EF, vc, c_dist, c_exp);
+        // a frontier pass that stores its beam keeps a reserve beyond EF for the
+        // resumed search (expanding only the first EF entries)
+        const uint32_t cap_beam = (save_cap && !resume) ? max(EF, min(save_cap, efc)) : EF;
+        tsize = beam_search_fast<DM>(v, s, tsize, cap_beam, EF, vc, c_dist, c_exp);
         if (save_cap && !resume) {
             const uint32_t ns = min(tsize, save_cap);
             for (uint32_t i = lane; i < ns; i += 32) {
@@ -679,7 +682,10 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
             uint32_t* fb_count = b.decided.as<uint32_t>();
             unsigned long long* levels = (unsigned long long*)(b.decided.as<char>() + 8);
             CUDA_CHECK(cudaMemsetAsync(b.decided.p, 0, 64, s));
-            const uint32_t save_cap = (two_pass && fast) ? ((b.ef + 31) & ~31u) : 0;
+            // the stored frontier beam: the level beam plus a reserve (up to twice
+            // the level ef, within the batch's largest beam) that the fallback resumes
+            const uint32_t save_cap =
+                (two_pass && fast) ? std::min<uint32_t>(efc, (std::max(2 * b.ef, b.ef + 32) + 31) & ~31u) : 0;
             uint32_t *st_cnt = nullptr, *st_i = nullptr;
             float* st_d = nullptr;
             if (save_cap) {
