@@ -652,9 +652,9 @@ def main():
         pparams = dict(params, m=mstars["plain"])
         h.set_precision(H.PREC_FP32_EXACT)
         plain_ans = h.search_rknn_batch(Q[:ns], pparams["m"], W["Kp"], W["ef"], threshold=1.0, k=W["k"])
-        _, kd_all, kc_all = h.get_knng_column(W["k"] - 1)
+        kd_all = h.get_kdist(W["k"])  # kdist(p, k-1), FLT_MAX where the list is shorter (hrnn.h:286-293)
         cpu, parity = cpu_baseline(h, W, Q, pparams, ns, gt=gt[:ns], plain_ans=plain_ans, head_ans=out[:ns],
-                                   head=head, X=X, kcol=(kd_all, kc_all))
+                                   head=head, X=X, kcol=kd_all)
         del h
         cpu["build"] = cpu_build_baseline(H, torch, dev, dev_sync)
         log(f"[bench] build baseline: {json.dumps(cpu['build'])}")
@@ -1050,9 +1050,8 @@ def cpu_baseline(h, W, Q, params, sample, gt=None, plain_ans=None, head_ans=None
             # labels are internal ids (the bench inserts in data order)
             qi = np.concatenate([np.full(len(a), i, np.int64) for i, a in enumerate(head_ans)] + [np.zeros(0, np.int64)])
             pi = np.concatenate([np.asarray(a, np.int64) for a in head_ans] + [np.zeros(0, np.int64)])
-            kd, kc = kcol
             d_ref = ref.l2_batch(Qs[qi], X[pi]) if len(qi) else np.zeros(0, np.float32)
-            kdp = np.where(kc[pi] > params["k"] - 1, kd[pi], np.float32(np.finfo(np.float32).max)).astype(np.float32)
+            kdp = kcol[pi].astype(np.float32)
             fail = d_ref > kdp
             ulp = np.spacing(kdp).astype(np.float64)
             band = np.abs(d_ref.astype(np.float64) - kdp.astype(np.float64)) <= 16.0 * ulp

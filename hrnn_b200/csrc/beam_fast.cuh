@@ -96,7 +96,10 @@ __device__ __forceinline__ void warp_i8_rows2(const DevView& v, const int* q8, f
 }
 
 // Scores ids[0..cnt) (cnt <= 64) with the form's rows: DM 3 INT8, DM 2 BF16.
-template <int DM>
+// R2: INT8 rows two per lane (all 64 in one round trip, at twice the registers
+// and so fewer resident warps) or one per lane in two rounds; the launch-shape
+// autotuner picks.
+template <int DM, bool R2>
 __device__ __forceinline__ void warp_dist_list64(const DevView& v, const float* q, const uint32_t* ids,
                                                  uint32_t cnt, float* dout) {
     if constexpr (DM == 3) {
@@ -104,13 +107,12 @@ __device__ __forceinline__ void warp_dist_list64(const DevView& v, const float* 
         const float4 qm = *i8_q_meta(q, v.dim);
         // two rows per lane up to dim 128 (16 loads of 16 bytes in flight per
         // lane); wider rows one per lane, 32 at a time
-        switch (v.dim >> 4) {
-            case 6: warp_i8_rows2<6>(v, q8, qm, ids, cnt, dout); break;
-            case 8: warp_i8_rows2<8>(v, q8, qm, ids, cnt, dout); break;
-            default:
-                warp_i8_list(v, q8, qm, ids, min(cnt, 32u), dout);
-                if (cnt > 32) warp_i8_list(v, q8, qm, ids + 32, cnt - 32, dout + 32);
-                break;
+        const uint32_t nw = v.dim >> 4;
+        if (R2 && nw == 6) warp_i8_rows2<6>(v, q8, qm, ids, cnt, dout);
+        else if (R2 && nw == 8) warp_i8_rows2<8>(v, q8, qm, ids, cnt, dout);
+        else {
+            warp_i8_list(v, q8, qm, ids, min(cnt, 32u), dout);
+            if (cnt > 32) warp_i8_list(v, q8, qm, ids + 32, cnt - 32, dout + 32);
         }
         __syncwarp();
     } else {
@@ -206,7 +208,7 @@ __device__ __forceinline__ void beam_insert_fast(WarpSmem& s, const float* nd, c
 // (<= EF) are expanded, the rest is a reserve a later search with a larger beam
 // can resume from (the first EX entries evolve exactly as in a search with
 // EF = EX).  Returns the beam size (<= EF).
-template <int DM>
+template <int DM, bool R2>
 __device__ uint32_t beam_search_fast(const DevView& v, WarpSmem& s, uint32_t tsize, uint32_t EF, uint32_t EX,
                                      uint32_t vc, unsigned long long& c_dist, unsigned long long& c_exp) {
     const int lane = threadIdx.x & 31;
@@ -263,7 +265,7 @@ __device__ uint32_t beam_search_fast(const DevView& v, WarpSmem& s, uint32_t tsi
             __syncwarp();
         }
         if (cnt == 0) continue;
-        warp_dist_list64<DM>(v, s.q, s.ni, cnt, s.nd);
+        warp_dist_list64<DM, R2>(v, s.q, s.ni, cnt, s.nd);
         c_dist += cnt;
         beam_insert_fast(s, s.nd, s.ni, min(cnt, 32u), EF, tsize, cursor);
         if (cnt > 32) beam_insert_fast(s, s.nd + 32, s.ni + 32, cnt - 32, EF, tsize, cursor);

@@ -205,6 +205,10 @@ hrnn_status hrnn_search_rknn_batch(hrnn_index* h, const float* q, size_t nq, con
             CUDA_CHECK(cudaMemcpyAsync(def, ef, ib, cudaMemcpyHostToDevice, s));
         }
         hrnn::SearchArgs a{dq, nq, dm, dkp, def, threshold, k, doff, dlab, cap, s};
+        for (size_t i = 0; i < nq; ++i) {  // the maxima from the host arrays: no read-back
+            a.h_mmax = std::max(a.h_mmax, m[i]);
+            a.h_efmax = std::max(a.h_efmax, std::max(ef[i], m[i]));
+        }
         uint64_t total = hrnn::search_batch(ix, a);
         CUDA_CHECK(cudaMemcpyAsync(out_offsets, doff, ob, cudaMemcpyDeviceToHost, s));
         if (total <= cap && total && out_labels)

@@ -66,6 +66,19 @@ struct MutableLists {
     uint64_t rebuilds = 0, applied = 0;
 };
 
+// Work space of the streaming INT8 verification (verify_stream.cu), reserved
+// for a batch shape.
+struct StreamBufs {
+    DevMem qq, qmeta;      // the queries' INT8 copies and their scalars
+    DevMem cnt, coff;      // chunks per (query, proxy) pair and their prefix sum
+    DevMem chunks;         // work items
+    DevMem acc_cnt;        // acceptances per query
+    DevMem ctl;            // work counter
+    DevMem tmp;            // scan scratch
+    size_t npairs = 0;
+    void reserve(uint32_t nq, uint32_t dim, size_t npairs, size_t max_chunks);
+};
+
 struct Index {
     // ---- device / stream -------------------------------------------------
     int device = 0;
@@ -137,6 +150,7 @@ struct Index {
     DevMem io;           // host-buffer entry points stage their inputs/outputs here
     DevMem counters;     // SearchCounters
     DevMem kcol;         // f32 [n]: kdist(p, k-1) of the current search call
+    StreamBufs sb;       // streaming verification of the INT8 form
     hrnn_search_stats last_stats{};
     hrnn_refine_stats refine_stats{};
     std::unique_ptr<Budget> budget;  // learned search budget (hrnn_set_budget)
@@ -186,6 +200,9 @@ struct SearchArgs {
     uint64_t* d_out_labels;
     size_t cap;
     cudaStream_t stream;
+    // the batch's largest m and max(ef, m) when the caller knows them (host
+    // inputs); 0: read back from d_m / d_ef
+    uint32_t h_mmax = 0, h_efmax = 0;
 };
 uint64_t search_batch(Index& ix, const SearchArgs& a);  // returns total results
 void kdist_column(Index& ix, uint32_t k, float* host_out);  // kdist(p, k-1) of every element

@@ -24,6 +24,7 @@ struct SearchPlan {
     // plan-owned device state (addresses fixed for the graph's lifetime)
     DevMem inputs;    // m and ef clamped to the maxima; clamp flag
     DevMem prox, nprox, plen, qtot, res, kcol, hkey, hcnt, lp, tmp, ctr;
+    StreamBufs sb;    // streaming verification (INT8 form)
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     ~SearchPlan() {

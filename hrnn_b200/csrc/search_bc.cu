@@ -459,236 +459,6 @@ __global__ void __launch_bounds__(kBCThreads) k_phase_bc_cta(
     }
 }
 
-// ---------------------------------------------------------------------------
-// Streaming verification of the INT8 form (threshold <= 1, dims 96 / 128): one
-// warp per query, no candidate table.  Every posting of the proxies' prefixes is
-// verified where it is read -- 32 postings per step, one candidate row per lane,
-// the INT8 screen first, the few rows it cannot decide in exact FP32 (two lanes
-// per row, the reference's order) and inside kTieUlps of the radius in FP64.
-// An owner listed by several proxies is verified once per listing (the same
-// decision each time); the accepted ids are sorted and deduplicated at the end,
-// which also gives the ascending internal-id order of hrnn.h:2055.  With every
-// count >= 1 passing the threshold (hrnn.h:2043-2052), the candidate set, the
-// decisions and so the answers are the CTA kernel's.  A query with more than
-// kStreamAcc acceptances (duplicates included) is flagged for the overflow pass.
-// ---------------------------------------------------------------------------
-
-constexpr uint32_t kStreamAcc = 512;
-
-__host__ __device__ size_t stream_warp_smem(uint32_t dim) {
-    return (size_t)dim * 4 + (((size_t)dim + 15) & ~(size_t)15) + 16 + 32 * 4 + (size_t)kStreamAcc * 4;
-}
-
-// The INT8 screen of one row: 1 accept, 0 reject, -1 undecided.
-// |sqrt(d) - sqrt(D)| <= e_q + e_x with D = ||s_q q8 - s c||^2 evaluated in FP32
-// within 8 ulps of (sqrt(s_q^2 sum q8^2) + s sqrt(sum c^2))^2; rho covers the
-// reference's own FP32 sum and this bound's roundings.
-__device__ __forceinline__ int i8_decide(float D, float kd, float4 qv, float4 xm, uint32_t dim) {
-    if (kd == FLT_MAX) return 1;
-    const float rq = sqrtf(qv.x), rx = xm.x * sqrtf(xm.z);
-    const float ef = 8.f * 5.9604645e-8f * (rq + rx) * (rq + rx);
-    const float e = qv.z + xm.y;
-    const float rho = (4.f * dim + 64.f) * 5.9604645e-8f;
-    const float hi = sqrtf(D + ef) * (1.f + rho) + e;
-    const float lo = fmaxf(0.f, sqrtf(fmaxf(0.f, D - ef)) * (1.f - rho) - e);
-    const float U = hi * hi * (1.f + rho), L = lo * lo * (1.f - rho);
-    return U < kd ? 1 : (L > kd ? 0 : -1);
-}
-
-// Appends the ids of the lanes with a set to acc[na..]; sets ovf instead when
-// they do not fit (warp-uniform).
-__device__ __forceinline__ void stream_append(bool a, uint32_t id, uint32_t* acc, uint32_t& na, bool& ovf) {
-    const uint32_t ab = __ballot_sync(0xFFFFFFFFu, a);
-    if (!ab) return;
-    if (na + __popc(ab) > kStreamAcc) {
-        ovf = true;
-        return;
-    }
-    if (a) acc[na + __popc(ab & lanemask_lt())] = id;
-    na += __popc(ab);
-}
-
-template <class E, bool FUSED, int NB>
-__global__ void __launch_bounds__(256, 3) k_verify_stream(
-    DevView v, const float* __restrict__ Q, uint32_t nq, uint32_t mmax, const uint32_t* __restrict__ prox,
-    const uint32_t* __restrict__ nprox, const uint32_t* __restrict__ plen, const uint64_t* __restrict__ res_off,
-    const float* __restrict__ kcol, uint32_t kidx, uint64_t* __restrict__ resbuf, uint32_t* __restrict__ res_count,
-    uint32_t* __restrict__ next_q, uint32_t* __restrict__ overflow_list, uint32_t* __restrict__ n_overflow,
-    SearchCounters* __restrict__ ctr) {
-    extern __shared__ char smraw[];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const uint32_t dim = v.dim;
-    char* base = smraw + (size_t)w * stream_warp_smem(dim);
-    float* q = (float*)base;
-    int* q8 = (int*)(q + dim);
-    float4* qmp = (float4*)((char*)q8 + ((dim + 15) & ~15u));
-    uint32_t* st = (uint32_t*)(qmp + 1);
-    uint32_t* acc = st + 32;
-    unsigned long long c_post = 0, c_res = 0, c_lowp = 0, c_fp32 = 0, c_fp64 = 0, c_flip = 0;
-    for (;;) {
-        uint32_t qi = 0;
-        if (lane == 0) qi = atomicAdd(next_q, 1u);
-        qi = __shfl_sync(0xFFFFFFFFu, qi, 0);
-        if (qi >= nq) break;
-        const uint32_t np_ = nprox[qi];
-        for (uint32_t i = lane; i < dim; i += 32) q[i] = Q[(size_t)qi * dim + i];
-        __syncwarp();
-        {   // the query's INT8 copy (as i8_prep_query)
-            float mx = 0.f;
-            for (uint32_t j = lane; j < dim; j += 32) mx = fmaxf(mx, fabsf(q[j]));
-            for (int o = 16; o; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, o));
-            const float sc = mx > 0.f ? mx / 127.f : 1.f;
-            int8_t* qb = reinterpret_cast<int8_t*>(q8);
-            double e2 = 0.0;
-            int c2 = 0;
-            for (uint32_t j = lane; j < dim; j += 32) {
-                const int c = max(-127, min(127, __float2int_rn(q[j] / sc)));
-                qb[j] = (int8_t)c;
-                const double dlt = (double)q[j] - (double)sc * (double)c;
-                e2 += dlt * dlt;
-                c2 += c * c;
-            }
-            for (int o = 16; o; o >>= 1) {
-                e2 += __shfl_xor_sync(0xFFFFFFFFu, e2, o);
-                c2 += __shfl_xor_sync(0xFFFFFFFFu, c2, o);
-            }
-            if (lane == 0) *qmp = make_float4(sc * sc * (float)c2, sc, __double2float_ru(sqrt(e2)), 0.f);
-            __syncwarp();
-        }
-        const float4 qv = *qmp;
-        uint32_t na = 0;
-        bool ovf = false;
-        for (uint32_t pi = 0; pi < np_ && !ovf; ++pi) {
-            const uint32_t p = prox[(size_t)qi * mmax + pi];
-            const uint32_t len = plen[(size_t)qi * mmax + pi];
-            const uint64_t b = v.csr_off[p];
-            c_post += len;
-            for (uint32_t e0 = 0; e0 < len && !ovf; e0 += 32) {
-                const uint32_t e = e0 + lane;
-                const bool live = e < len;
-                const uint32_t id = live ? (uint32_t)(((const E*)v.csr_ent)[b + e] >> v.rank_bits) : p;
-                const float kd = __ldg(kcol + id);
-                const float4 xm = __ldg(v.i8_meta + id);
-                const float D = i8_row<NB>(q8, qv, v.vec_i8 + (size_t)id * dim, xm);
-                const int dec = live ? i8_decide(D, kd, qv, xm, dim) : 0;
-                if (dec >= 0 && live) c_lowp++;
-                stream_append(dec == 1, id, acc, na, ovf);
-                const uint32_t und = __ballot_sync(0xFFFFFFFFu, dec < 0);
-                if (!und) continue;
-                // exact FP32 (and FP64 in the tie band) for the undecided rows
-                __syncwarp();
-                if (dec < 0) st[__popc(und & lanemask_lt())] = id;
-                __syncwarp();
-                const uint32_t nu = __popc(und);
-                // one row per half-warp (few rows, few registers): lane l of a half
-                // owns the reference's accumulator l
-                const int hh = lane >> 4, l16 = lane & 15;
-                for (uint32_t r = 0; r < nu; r += 2) {
-                    const uint32_t t = r + hh;
-                    const bool lv = t < nu;
-                    const uint32_t x = st[lv ? t : r];
-                    const float kx = __ldg(kcol + x);
-                    const float d32 = l2_half16<FUSED>(q, v.vec + (size_t)x * dim, NB, l16);
-                    int decision = d32 <= kx;
-                    if (lv && l16 == 0) c_fp32++;
-                    const bool tie = lv && kx != FLT_MAX && v.knn_ids && kidx < (v.knn_hdr[x] & 0xFFFFu) &&
-                                     fabsf(d32 - kx) <= kTieUlps * (nextafterf(kx, FLT_MAX) - kx);
-                    if (__any_sync(0xFFFFFFFFu, tie)) {
-                        // FP64: d(q, x) against d(x, x_k), x_k the k-th neighbour of x
-                        double a = 0.0, bb = 0.0;
-                        if (tie) {
-                            const uint32_t nk = v.knn_ids[(size_t)x * v.K + kidx];
-                            const float* xr = v.vec + (size_t)x * dim;
-                            const float* yr = v.vec + (size_t)nk * dim;
-                            for (uint32_t e2 = l16; e2 < dim; e2 += 16) {
-                                const double tq = (double)q[e2] - (double)xr[e2];
-                                const double ty = (double)xr[e2] - (double)yr[e2];
-                                a += tq * tq;
-                                bb += ty * ty;
-                            }
-                        }
-                        for (int o = 8; o; o >>= 1) {
-                            a += __shfl_xor_sync(0xFFFFFFFFu, a, o);
-                            bb += __shfl_xor_sync(0xFFFFFFFFu, bb, o);
-                        }
-                        if (tie) {
-                            const int d64 = a <= bb;
-                            if (l16 == 0) {
-                                c_fp64++;
-                                if (d64 != decision) c_flip++;
-                            }
-                            decision = d64;
-                        }
-                    }
-                    stream_append(lv && l16 == 0 && decision == 1, x, acc, na, ovf);
-                }
-                __syncwarp();
-            }
-        }
-        if (ovf) {
-            if (lane == 0) overflow_list[atomicAdd(n_overflow, 1u)] = qi;
-            __syncwarp();
-            continue;
-        }
-        // sort the accepted ids (bitonic, shared memory), drop repeats, write labels
-        uint32_t P = 32;
-        while (P < na) P <<= 1;
-        for (uint32_t i = na + lane; i < P; i += 32) acc[i] = kInvalid;
-        __syncwarp();
-        for (uint32_t k = 2; k <= P; k <<= 1)
-            for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-                for (uint32_t i = lane; i < P; i += 32) {
-                    const uint32_t y = i ^ j;
-                    if (y > i) {
-                        const uint32_t a0 = acc[i], a1 = acc[y];
-                        if ((a0 > a1) == ((i & k) == 0)) {
-                            acc[i] = a1;
-                            acc[y] = a0;
-                        }
-                    }
-                }
-                __syncwarp();
-            }
-        const uint64_t ro = res_off[qi];
-        uint32_t nu = 0;
-        for (uint32_t b0 = 0; b0 < na; b0 += 32) {
-            const uint32_t i = b0 + lane;
-            const bool keep = i < na && (i == 0 || acc[i] != acc[i - 1]);
-            const uint32_t kb = __ballot_sync(0xFFFFFFFFu, keep);
-            if (keep) resbuf[ro + nu + __popc(kb & lanemask_lt())] = v.labels[acc[i]];
-            nu += __popc(kb);
-        }
-        if (lane == 0) res_count[qi] = nu;
-        c_res += nu;
-        __syncwarp();
-    }
-    for (int o = 16; o; o >>= 1) {
-        c_lowp += __shfl_xor_sync(0xFFFFFFFFu, c_lowp, o);
-        c_fp32 += __shfl_xor_sync(0xFFFFFFFFu, c_fp32, o);
-        c_fp64 += __shfl_xor_sync(0xFFFFFFFFu, c_fp64, o);
-        c_flip += __shfl_xor_sync(0xFFFFFFFFu, c_flip, o);
-    }
-    if (lane == 0) {
-        atomicAdd(&ctr->n_posting, c_post);
-        atomicAdd(&ctr->n_cand, c_post);
-        atomicAdd(&ctr->n_verified, c_post);
-        atomicAdd(&ctr->n_result, c_res);
-        atomicAdd(&ctr->n_lowp, c_lowp);
-        atomicAdd(&ctr->n_fp32, c_fp32);
-        atomicAdd(&ctr->n_fp64, c_fp64);
-        atomicAdd(&ctr->n_flip, c_flip);
-    }
-}
-
-#define INST_S(E, F, NB)                                                                                             \
-    template __global__ void k_verify_stream<E, F, NB>(DevView, const float*, uint32_t, uint32_t, const uint32_t*,  \
-                                                       const uint32_t*, const uint32_t*, const uint64_t*,           \
-                                                       const float*, uint32_t, uint64_t*, uint32_t*, uint32_t*,     \
-                                                       uint32_t*, uint32_t*, SearchCounters*);
-INST_S(uint32_t, false, 8) INST_S(uint32_t, true, 8) INST_S(uint32_t, false, 6) INST_S(uint32_t, true, 6)
-INST_S(uint64_t, false, 8) INST_S(uint64_t, true, 8) INST_S(uint64_t, false, 6) INST_S(uint64_t, true, 6)
-#undef INST_S
-
 // explicit instantiations used by search_plain.cu
 #define INST(E, F, C, X)                                                                                            \
     template __global__ void k_phase_bc_cta<E, F, C, X>(DevView, const float*, uint32_t, uint32_t, const uint32_t*, \

@@ -25,6 +25,7 @@
 #include "index.hpp"
 #include "mlp.hpp"
 #include "plan.hpp"
+#include "verify_stream.hpp"
 
 namespace hrnn {
 
@@ -56,30 +57,11 @@ __global__ void k_budget_decide(const float* z, uint32_t nq, float conf, uint32_
 void ensure_projection(Index& ix, Budget& b);
 __global__ void k_kdist_column(DevView v, uint32_t kidx, float* kcol);
 size_t bc_cta_smem(uint32_t dim, bool counts, bool mixed);
-size_t stream_warp_smem(uint32_t dim);
-template <class E, bool FUSED, int NB>
-__global__ void k_verify_stream(DevView, const float*, uint32_t, uint32_t, const uint32_t*, const uint32_t*,
-                                const uint32_t*, const uint64_t*, const float*, uint32_t, uint64_t*, uint32_t*,
-                                uint32_t*, uint32_t*, uint32_t*, SearchCounters*);
-using KStream = void (*)(DevView, const float*, uint32_t, uint32_t, const uint32_t*, const uint32_t*,
-                         const uint32_t*, const uint64_t*, const float*, uint32_t, uint64_t*, uint32_t*, uint32_t*,
-                         uint32_t*, uint32_t*, SearchCounters*);
 // HRNN_VERIFY=table: the INT8 form verifies through the CTA table kernel as well
 // (for comparisons of the two verification paths).
 inline bool verify_table_forced() {
     const char* e = std::getenv("HRNN_VERIFY");
     return e && std::string(e) == "table";
-}
-// The streaming verification of the INT8 form, or null where it does not apply
-// (other dims or forms, counted thresholds): those take the CTA kernel.
-inline KStream pick_stream(bool wide, bool fused, uint32_t dim) {
-    if (dim != 128 && dim != 96) return nullptr;
-    if (wide) {
-        if (dim == 128) return fused ? k_verify_stream<uint64_t, true, 8> : k_verify_stream<uint64_t, false, 8>;
-        return fused ? k_verify_stream<uint64_t, true, 6> : k_verify_stream<uint64_t, false, 6>;
-    }
-    if (dim == 128) return fused ? k_verify_stream<uint32_t, true, 8> : k_verify_stream<uint32_t, false, 8>;
-    return fused ? k_verify_stream<uint32_t, true, 6> : k_verify_stream<uint32_t, false, 6>;
 }
 
 namespace {
@@ -148,7 +130,7 @@ __global__ void __launch_bounds__(128) k_phase_a(DevView v, const float* __restr
 //     resume;
 //   resume: start from the stored beam instead of the descent (its ids seed the
 //     visited cache), continue with the query's own ef, store nothing.
-template <int DM>
+template <int DM, bool R2>
 __global__ void __launch_bounds__(128) k_phase_a_fast(DevView v, const float* __restrict__ Q, uint32_t nq,
                                                       const uint32_t* __restrict__ qm,
                                                       const uint32_t* __restrict__ qef, uint32_t efc, uint32_t vc,
@@ -205,7 +187,7 @@ __global__ void __launch_bounds__(128) k_phase_a_fast(DevView v, const float* __
         // a frontier pass that stores its beam keeps a reserve beyond EF for the
         // resumed search (expanding only the first EF entries)
         const uint32_t cap_beam = (save_cap && !resume) ? max(EF, min(save_cap, efc)) : EF;
-        tsize = beam_search_fast<DM>(v, s, tsize, cap_beam, EF, vc, c_dist, c_exp);
+        tsize = beam_search_fast<DM, R2>(v, s, tsize, cap_beam, EF, vc, c_dist, c_exp);
         if (save_cap && !resume) {
             const uint32_t ns = min(tsize, save_cap);
             for (uint32_t i = lane; i < ns; i += 32) {
@@ -502,14 +484,19 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
         return 0;
     }
     // Per-batch maxima of m and ef (sizes the proxy table and the beam).
-    std::vector<uint32_t> hm(nq), hef(nq);
-    CUDA_CHECK(cudaMemcpyAsync(hm.data(), a.d_m, nq * 4, cudaMemcpyDeviceToHost, s));
-    CUDA_CHECK(cudaMemcpyAsync(hef.data(), a.d_ef, nq * 4, cudaMemcpyDeviceToHost, s));
-    CUDA_CHECK(cudaStreamSynchronize(s));
     uint32_t mmax = 1, efmax = 1;
-    for (size_t i = 0; i < nq; ++i) {
-        mmax = std::max(mmax, hm[i]);
-        efmax = std::max(efmax, std::max(hef[i], hm[i]));
+    if (a.h_mmax) {
+        mmax = std::max<uint32_t>(1, a.h_mmax);
+        efmax = std::max<uint32_t>(1, std::max(a.h_efmax, a.h_mmax));
+    } else {
+        std::vector<uint32_t> hm(nq), hef(nq);
+        CUDA_CHECK(cudaMemcpyAsync(hm.data(), a.d_m, nq * 4, cudaMemcpyDeviceToHost, s));
+        CUDA_CHECK(cudaMemcpyAsync(hef.data(), a.d_ef, nq * 4, cudaMemcpyDeviceToHost, s));
+        CUDA_CHECK(cudaStreamSynchronize(s));
+        for (size_t i = 0; i < nq; ++i) {
+            mmax = std::max(mmax, hm[i]);
+            efmax = std::max(efmax, std::max(hef[i], hm[i]));
+        }
     }
     if (efmax > (1u << 16)) fail(HRNN_ERR_ARG, "searchRknn: ef_search/m too large (max 65536)");
     const bool learned = ix.budget && ix.budget->enabled && ix.budget->mlp.ready && ix.dim % 4 == 0;
@@ -561,10 +548,15 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
         // (The two-parent search reads link rows of at most 33 words, maxM0 <= 32.)
         const bool fast = (int8 || mixed) && v.W0 <= 33;
         const int dm = int8 ? 3 : mixed ? 2 : fusedsimd ? 1 : 0;
-        const void* kfun = fast ? (dm == 3 ? (const void*)k_phase_a_fast<3> : (const void*)k_phase_a_fast<2>)
-                                : (dm == 3 ? (const void*)k_phase_a<3>
-                                           : dm == 2 ? (const void*)k_phase_a<2>
-                                                     : dm == 1 ? (const void*)k_phase_a<1> : (const void*)k_phase_a<0>);
+        // r2: the INT8 two-parent search scores two rows per lane (a launch-shape choice)
+        bool r2 = false;
+        auto kfun_of = [&](bool two) {
+            return fast ? (dm == 3 ? (two ? (const void*)k_phase_a_fast<3, true> : (const void*)k_phase_a_fast<3, false>)
+                                   : (const void*)k_phase_a_fast<2, false>)
+                        : (dm == 3 ? (const void*)k_phase_a<3>
+                                   : dm == 2 ? (const void*)k_phase_a<2>
+                                             : dm == 1 ? (const void*)k_phase_a<1> : (const void*)k_phase_a<0>);
+        };
         auto smem_for = [&](uint32_t cv, int cw) {
             return (fast ? fast_smem_bytes(v.dim, efc, cv) : warp_smem_bytes(v.dim, efc, cv)) * (size_t)cw;
         };
@@ -574,13 +566,18 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
         auto launch = [&](unsigned g, int cw, uint32_t cv, size_t sm, uint32_t nqq, const uint32_t* qlist,
                           uint32_t m_over, uint32_t ef_over, uint32_t m_keep, float* proxd, uint32_t* ctrq,
                           uint32_t save_cap, uint32_t* st_cnt, float* st_d, uint32_t* st_i, int resume) {
-            if (fast && dm == 3)
-                k_phase_a_fast<3><<<g, cw * 32, sm, s>>>(v, a.d_q, nqq, a.d_m, a.d_ef, efc, cv, mmax,
-                                                         prox.as<uint32_t>(), nprox.as<uint32_t>(), ctr, qlist,
-                                                         m_over, ef_over, m_keep, proxd, ctrq, save_cap, st_cnt, st_d,
-                                                         st_i, resume);
+            if (fast && dm == 3 && r2)
+                k_phase_a_fast<3, true><<<g, cw * 32, sm, s>>>(v, a.d_q, nqq, a.d_m, a.d_ef, efc, cv, mmax,
+                                                               prox.as<uint32_t>(), nprox.as<uint32_t>(), ctr, qlist,
+                                                               m_over, ef_over, m_keep, proxd, ctrq, save_cap, st_cnt,
+                                                               st_d, st_i, resume);
+            else if (fast && dm == 3)
+                k_phase_a_fast<3, false><<<g, cw * 32, sm, s>>>(v, a.d_q, nqq, a.d_m, a.d_ef, efc, cv, mmax,
+                                                                prox.as<uint32_t>(), nprox.as<uint32_t>(), ctr, qlist,
+                                                                m_over, ef_over, m_keep, proxd, ctrq, save_cap, st_cnt,
+                                                                st_d, st_i, resume);
             else if (fast)
-                k_phase_a_fast<2><<<g, cw * 32, sm, s>>>(v, a.d_q, nqq, a.d_m, a.d_ef, efc, cv, mmax,
+                k_phase_a_fast<2, false><<<g, cw * 32, sm, s>>>(v, a.d_q, nqq, a.d_m, a.d_ef, efc, cv, mmax,
                                                          prox.as<uint32_t>(), nprox.as<uint32_t>(), ctr, qlist,
                                                          m_over, ef_over, m_keep, proxd, ctrq, save_cap, st_cnt, st_d,
                                                          st_i, resume);
@@ -608,19 +605,24 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
         const uint64_t shape_key = ((uint64_t)dm << 32) | efc;
         auto shape = ix.autotune ? ix.a_shape.find(shape_key) : ix.a_shape.end();
         if (shape != ix.a_shape.end()) {
-            wpb = (int)shape->second.first;
+            wpb = (int)(shape->second.first & 0xFF);
+            r2 = (shape->second.first & 0x100) != 0;
             vc = shape->second.second;
         } else if (ix.autotune && !learned && nq >= 1024) {
             float best = FLT_MAX;
             int bw = wpb;
             uint32_t bv = vc;
+            bool br2 = false;
             cudaEvent_t t0, t1;
             CUDA_CHECK(cudaEventCreate(&t0));
             CUDA_CHECK(cudaEventCreate(&t1));
+            for (int two = 0; two < ((fast && dm == 3) ? 2 : 1); ++two)
             for (uint32_t cv : {256u, 512u, 1024u}) {
                 for (int cw : {2, 4}) {
                     const size_t sm = smem_for(cv, cw);
                     if (sm > 200 * 1024) continue;
+                    r2 = two != 0;
+                    const void* kfun = kfun_of(r2);
                     CUDA_CHECK(cudaFuncSetAttribute(kfun, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
                     int ps = 1;
                     CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ps, kfun, cw * 32, sm));
@@ -638,6 +640,7 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
                         best = ms;
                         bw = cw;
                         bv = cv;
+                        br2 = r2;
                     }
                 }
             }
@@ -645,7 +648,8 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
             cudaEventDestroy(t1);
             wpb = bw;
             vc = bv;
-            ix.a_shape[shape_key] = {(uint32_t)wpb, vc};
+            r2 = br2;
+            ix.a_shape[shape_key] = {(uint32_t)wpb | (r2 ? 0x100u : 0u), vc};
             // the trials' counts and work counter start over
             CUDA_CHECK(cudaMemsetAsync(ctr, 0, sizeof(SearchCounters), s));
             CUDA_CHECK(cudaMemsetAsync(d_qa, 0, 4, s));
@@ -653,6 +657,7 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
         }
         smem_a = smem_for(vc, wpb);
         if (smem_a > 227 * 1024) fail(HRNN_ERR_ARG, "searchRknn: ef/dim too large for one warp's beam");
+        const void* kfun = kfun_of(r2);
         CUDA_CHECK(cudaFuncSetAttribute(kfun, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_a));
         // Persistent grid (every resident block), queries handed out by counters.
         int per_sm = 1;
@@ -745,19 +750,13 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
         k_kdist_column<<<(unsigned)((ix.cur + 255) / 256), 256, 0, s>>>(v, kidx, ix.kcol.as<float>());
         CUDA_LAUNCH_CHECK();
         const bool counts = a.threshold > 1.0f;
-        KStream ks = (int8 && mixed && v.i8_screen && !counts && v.lanes == 16 && !verify_table_forced())
-                         ? pick_stream(ix.wide, fusedsimd, v.dim) : nullptr;
-        if (ks) {
-            // INT8 form: one warp per query, postings verified as they are read
-            const size_t smem = 8 * stream_warp_smem(v.dim);
-            CUDA_CHECK(cudaFuncSetAttribute(ks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            int per_sm = 1;
-            CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ks, 256, smem));
-            unsigned grid = (unsigned)std::min<size_t>((nq + 7) / 8, (size_t)nsm * std::max(per_sm, 1));
-            ks<<<grid, 256, smem, s>>>(v, a.d_q, (uint32_t)nq, mmax, prox.as<uint32_t>(), nprox.as<uint32_t>(),
-                                       plen.as<uint32_t>(), d_resoff, ix.kcol.as<float>(), kidx, resbuf, d_rcount,
-                                       d_next, ovl, d_nov, ctr);
-            CUDA_LAUNCH_CHECK();
+        if (int8 && mixed && !counts && stream_supported(v) && !verify_table_forced()) {
+            // INT8 form: postings verified as they are read, in chunks spread over
+            // persistent warps
+            const size_t npairs = nq * mmax;
+            ix.sb.reserve((uint32_t)nq, v.dim, npairs, stream_max_chunks(sum_total, npairs));
+            stream_verify(v, ix.wide, fusedsimd, a.d_q, (uint32_t)nq, mmax, prox.as<uint32_t>(), plen.as<uint32_t>(),
+                          d_resoff, ix.kcol.as<float>(), kidx, resbuf, d_rcount, ovl, d_nov, ctr, ix.sb, nsm, s);
         } else {
             const size_t smem = bc_cta_smem(v.dim, counts, mixed);
             KCta kc = ix.wide ? pick_bc<uint64_t>(fusedsimd, counts, mixed) : pick_bc<uint32_t>(fusedsimd, counts, mixed);
@@ -923,7 +922,7 @@ void budget_features(Index& ix, const float* d_q, size_t nq, uint32_t k, uint32_
     const int nsm = sms(ix.device);
     unsigned grid = (unsigned)std::max<size_t>(1, std::min<size_t>((nq + wpb - 1) / wpb, (size_t)nsm * 16));
     if (fast) {
-        auto kern = int8 ? k_phase_a_fast<3> : k_phase_a_fast<2>;
+        auto kern = int8 ? k_phase_a_fast<3, false> : k_phase_a_fast<2, false>;
         CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_a));
         kern<<<grid, wpb * 32, smem_a, s>>>(v, d_q, (uint32_t)nq, nullptr, nullptr, efc, vc, mmax,
                                             prox.as<uint32_t>(), nprox.as<uint32_t>(),
@@ -965,7 +964,7 @@ namespace {
 struct PlanLaunch {
     uint32_t efc, vc, mmax, wpb, grid_a, grid_bc, kidx, slots, hcap;
     size_t smem_a, smem_bc, smem_w, tmax;
-    bool mixed, int8, fusedsimd, counts, fast;
+    bool mixed, int8, fusedsimd, counts, fast, r2;
 };
 
 PlanLaunch plan_launch_shape(Index& ix, const SearchPlan& p) {
@@ -988,7 +987,8 @@ PlanLaunch plan_launch_shape(Index& ix, const SearchPlan& p) {
     const uint64_t shape_key = ((uint64_t)(L.int8 ? 3 : L.mixed ? 2 : L.fusedsimd ? 1 : 0) << 32) | L.efc;
     auto shape = ix.autotune ? ix.a_shape.find(shape_key) : ix.a_shape.end();  // tuned by an earlier batch call
     if (shape != ix.a_shape.end()) {
-        L.wpb = shape->second.first;
+        L.wpb = shape->second.first & 0xFF;
+        L.r2 = (shape->second.first & 0x100) != 0;
         L.vc = shape->second.second;
         L.smem_a = wsm_of(L.vc) * L.wpb;
     }
@@ -1065,22 +1065,21 @@ void plan_create(SearchPlan& p, cudaStream_t s) {
     exclusive_scan_u64(d_total, d_resoff, nq + 1, s, p.tmp);
     exclusive_scan_u32_to_u64(d_rcount, p.d_out_off, nq + 1, s, p.tmp);
     auto ka = L.int8 ? k_phase_a<3> : L.mixed ? k_phase_a<2> : L.fusedsimd ? k_phase_a<1> : k_phase_a<0>;
-    auto kaf = L.int8 ? k_phase_a_fast<3> : k_phase_a_fast<2>;
+    auto kaf = L.int8 ? (L.r2 ? k_phase_a_fast<3, true> : k_phase_a_fast<3, false>) : k_phase_a_fast<2, false>;
     const void* kaf_or_ka = L.fast ? (const void*)kaf : (const void*)ka;
     CUDA_CHECK(cudaFuncSetAttribute(kaf_or_ka, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem_a));
     int per_sm = 1;
     CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kaf_or_ka, L.wpb * 32, L.smem_a));
     L.grid_a = (uint32_t)std::max<size_t>(1, std::min<size_t>((nq + L.wpb - 1) / L.wpb, (size_t)nsm * std::max(per_sm, 1)));
     // verification: the streaming kernel of the INT8 form where search_batch takes it, else the CTA kernel
-    KStream ks = (L.int8 && L.mixed && !L.counts && v.lanes == 16 && !verify_table_forced())
-                     ? pick_stream(ix.wide, L.fusedsimd, v.dim) : nullptr;
+    // verification: the streaming kernel of the INT8 form where search_batch takes it, else the CTA kernel
+    const bool stream = L.int8 && L.mixed && !L.counts && stream_supported(v) && !verify_table_forced();
     KCta kc = ix.wide ? pick_bc<uint64_t>(L.fusedsimd, L.counts, L.mixed) : pick_bc<uint32_t>(L.fusedsimd, L.counts, L.mixed);
-    if (ks) {
-        L.smem_bc = 8 * stream_warp_smem(v.dim);
-        CUDA_CHECK(cudaFuncSetAttribute(ks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem_bc));
-        per_sm = 1;
-        CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ks, 256, L.smem_bc));
-        L.grid_bc = (uint32_t)std::min<size_t>((nq + 7) / 8, (size_t)nsm * std::max(per_sm, 1));
+    if (stream) {
+        p.sb.reserve((uint32_t)nq, v.dim, nq * L.mmax, stream_max_chunks(res_entries, nq * L.mmax));
+        stream_prepare(v, ix.wide, L.fusedsimd);
+        // the scan's scratch sized outside the capture
+        exclusive_scan_u32_to_u64(p.sb.cnt.as<uint32_t>(), p.sb.coff.as<uint64_t>(), nq * L.mmax + 1, s, p.sb.tmp);
     } else {
         CUDA_CHECK(cudaFuncSetAttribute(kc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem_bc));
         per_sm = 1;
@@ -1122,11 +1121,10 @@ void plan_create(SearchPlan& p, cudaStream_t s) {
     k_kdist_column<<<(unsigned)((ix.cur + 255) / 256), 256, 0, s>>>(v, L.kidx, p.kcol.as<float>());
     uint64_t* resbuf = p.res.as<uint64_t>();
     uint32_t* ovl = flag + 4;  // the overflow list (nq entries) after the clamp flag
-    if (ks)
-        ks<<<L.grid_bc, 256, L.smem_bc, s>>>(v, p.d_q, (uint32_t)nq, L.mmax, p.prox.as<uint32_t>(),
-                                             p.nprox.as<uint32_t>(), p.plen.as<uint32_t>(), d_resoff,
-                                             p.kcol.as<float>(), L.kidx, resbuf, d_rcount, d_next, ovl, d_next + 1,
-                                             ctr);
+    if (stream)
+        stream_verify(v, ix.wide, L.fusedsimd, p.d_q, (uint32_t)nq, L.mmax, p.prox.as<uint32_t>(),
+                      p.plen.as<uint32_t>(), d_resoff, p.kcol.as<float>(), L.kidx, resbuf, d_rcount, ovl,
+                      d_next + 1, ctr, p.sb, nsm, s);
     else
         kc<<<L.grid_bc, 256, L.smem_bc, s>>>(v, p.d_q, (uint32_t)nq, L.mmax, p.prox.as<uint32_t>(),
                                              p.nprox.as<uint32_t>(), p.plen.as<uint32_t>(), d_total, d_resoff,
