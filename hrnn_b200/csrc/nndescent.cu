@@ -289,10 +289,10 @@ __global__ void k_sample_rev(uint32_t n, uint32_t R, uint32_t cap, const uint64_
 // Each pair keeps the reference's 16 accumulators (element e into accumulator
 // e mod 16, then summed left to right), so the tiling leaves every distance
 // bit-identical.  Proposals are appended with one atomic per warp tile.
-constexpr int kJR = 8;
+constexpr int kJR = 4;  // 8 rows (207 registers, one block per SM) measured 1.4x slower
 
 template <bool FUSED>
-__global__ void __launch_bounds__(256, 1) k_join(const float* __restrict__ vec, uint32_t dim, uint32_t node0,
+__global__ void __launch_bounds__(256) k_join(const float* __restrict__ vec, uint32_t dim, uint32_t node0,
                                               uint32_t node1, uint32_t cap, const uint32_t* __restrict__ newl,
                                               const uint32_t* __restrict__ newc, const uint32_t* __restrict__ oldl,
                                               const uint32_t* __restrict__ oldc, const float* __restrict__ thr,
@@ -316,11 +316,18 @@ __global__ void __launch_bounds__(256, 1) k_join(const float* __restrict__ vec, 
             sthr[r] = thr[id];
         }
         __syncthreads();
-        for (uint32_t r = w; r < tot; r += nw) {  // a warp per row, float4 per lane
+        // the node's rows, a warp per row and 16 bytes per lane, as asynchronous
+        // copies: every row of the stage is in flight at once
+        for (uint32_t r = w; r < tot; r += nw) {
             const float4* src = reinterpret_cast<const float4*>(vec + (size_t)sid[r] * dim);
             float4* dst = reinterpret_cast<float4*>(sm + (size_t)r * SP);
-            for (uint32_t c = lane; c < d4; c += 32) dst[c] = __ldg(src + c);
+            for (uint32_t c = lane; c < d4; c += 32) {
+                const uint32_t sa = (uint32_t)__cvta_generic_to_shared(dst + c);
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(src + c) : "memory");
+            }
         }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
         __syncthreads();
         const uint32_t ti_n = (nn + kJR - 1) / kJR, tj_n = (tot + 31) >> 5;
         for (uint32_t t = w; t < ti_n * tj_n; t += nw) {

@@ -151,6 +151,7 @@ __global__ void __launch_bounds__(256, 3) k_verify_chunks(
             const float D = i8_row<NB>(q8, qv, v.vec_i8 + (size_t)id * dim, xm);
             const int dec = live ? i8_decide(D, kd, qv, xm, dim) : 0;
             if (dec >= 0 && live) c_lowp++;
+            // (the screens below need the FP32 query in shared memory)
             stream_accept(dec == 1, id, qi, res_off, acc_cnt, resbuf);
             const uint32_t und = __ballot_sync(0xFFFFFFFFu, dec < 0);
             if (!und) continue;
@@ -163,7 +164,30 @@ __global__ void __launch_bounds__(256, 3) k_verify_chunks(
             __syncwarp();
             if (dec < 0) st[__popc(und & ((1u << lane) - 1u))] = id;
             __syncwarp();
-            const uint32_t nu = __popc(und);
+            // the BF16 screen (two lanes per row) decides most of what INT8 could not
+            uint32_t nu = 0;
+            const uint32_t nu8 = __popc(und);
+            for (uint32_t r = 0; r < nu8; r += 16) {
+                const int pp = lane & 1;
+                const uint32_t tt = r + (lane >> 1);
+                const bool lv = tt < nu8;
+                const uint32_t x = st[lv ? tt : r];
+                const float kx = __ldg(kcol + x);
+                const float D = bf16_pair<NB>(q, v.vec_bf16 + (size_t)x * dim, pp);
+                const float ex = __ldg(v.vec_err + x);
+                const float rho = (4.f * dim + 64.f) * 5.9604645e-8f;
+                const float sD = sqrtf(D);
+                const float hi = sD * (1.f + rho) + ex, lo = fmaxf(0.f, sD * (1.f - rho) - ex);
+                const float U = hi * hi * (1.f + rho), L = lo * lo * (1.f - rho);
+                const int db = kx == FLT_MAX ? 1 : (U < kx ? 1 : (L > kx ? 0 : -1));
+                if (lv && pp == 0 && db >= 0) c_lowp++;
+                stream_accept(lv && pp == 0 && db == 1, x, qi, res_off, acc_cnt, resbuf);
+                const uint32_t u2 = __ballot_sync(0xFFFFFFFFu, lv && pp == 0 && db < 0);
+                __syncwarp();  // every lane has read its row of this round
+                if (lv && pp == 0 && db < 0) st[nu + __popc(u2 & ((1u << lane) - 1u))] = x;
+                nu += __popc(u2);
+                __syncwarp();
+            }
             const int hh = lane >> 4, l16 = lane & 15;  // one row per half-warp
             for (uint32_t r = 0; r < nu; r += 2) {
                 const uint32_t tt = r + hh;
