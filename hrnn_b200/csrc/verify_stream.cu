@@ -105,6 +105,110 @@ __device__ __forceinline__ void stream_accept(bool a, uint32_t id, uint32_t qi, 
     if (a) resbuf[res_off[qi] + base + __popc(ab & ((1u << lane) - 1u))] = id;
 }
 
+// Counters of one warp (summed into SearchCounters at the end).
+struct StreamCount {
+    unsigned long long lowp = 0, fp32 = 0, fp64 = 0, flip = 0;
+};
+
+// The rows the INT8 screen left undecided (lanes with dec < 0): the BF16 screen
+// (two lanes per row), then exact FP32 in the reference's order (a half-warp per
+// row) and FP64 inside the tie band.  Kept out of line: it is rare, and its
+// registers would otherwise weigh on the streaming loop.
+template <bool FUSED, int NB>
+__device__ __noinline__ void stream_undecided(const DevView& v, const float* __restrict__ Q, uint32_t qi, int dec,
+                                              uint32_t id, float* q, uint32_t* st, uint32_t& f32_q,
+                                              const float* __restrict__ kcol, uint32_t kidx,
+                                              const uint64_t* __restrict__ res_off, uint32_t* __restrict__ acc_cnt,
+                                              uint64_t* __restrict__ resbuf, StreamCount& cn) {
+    constexpr uint32_t dim = NB * 16;
+    const int lane = threadIdx.x & 31;
+    const uint32_t und = __ballot_sync(0xFFFFFFFFu, dec < 0);
+    if (f32_q != qi) {
+        __syncwarp();
+        for (uint32_t i = lane; i < dim; i += 32) q[i] = Q[(size_t)qi * dim + i];
+        f32_q = qi;
+    }
+    __syncwarp();
+    if (dec < 0) st[__popc(und & ((1u << lane) - 1u))] = id;
+    __syncwarp();
+    uint32_t nu = 0;
+    const uint32_t nu8 = __popc(und);
+    for (uint32_t r = 0; r < nu8; r += 16) {
+        const int pp = lane & 1;
+        const uint32_t tt = r + (lane >> 1);
+        const bool lv = tt < nu8;
+        const uint32_t x = st[lv ? tt : r];
+        const float kx = __ldg(kcol + x);
+        const float D = bf16_pair<NB>(q, v.vec_bf16 + (size_t)x * dim, pp);
+        const float ex = __ldg(v.vec_err + x);
+        const float rho = (4.f * dim + 64.f) * 5.9604645e-8f;
+        const float sD = sqrtf(D);
+        const float hi = sD * (1.f + rho) + ex, lo = fmaxf(0.f, sD * (1.f - rho) - ex);
+        const float U = hi * hi * (1.f + rho), L = lo * lo * (1.f - rho);
+        const int db = kx == FLT_MAX ? 1 : (U < kx ? 1 : (L > kx ? 0 : -1));
+        if (lv && pp == 0 && db >= 0) cn.lowp++;
+        stream_accept(lv && pp == 0 && db == 1, x, qi, res_off, acc_cnt, resbuf);
+        const uint32_t u2 = __ballot_sync(0xFFFFFFFFu, lv && pp == 0 && db < 0);
+        __syncwarp();  // every lane has read its row of this round
+        if (lv && pp == 0 && db < 0) st[nu + __popc(u2 & ((1u << lane) - 1u))] = x;
+        nu += __popc(u2);
+        __syncwarp();
+    }
+    const int hh = lane >> 4, l16 = lane & 15;  // one row per half-warp
+    for (uint32_t r = 0; r < nu; r += 2) {
+        const uint32_t tt = r + hh;
+        const bool lv = tt < nu;
+        const uint32_t x = st[lv ? tt : r];
+        const float kx = __ldg(kcol + x);
+        const float d32 = l2_half16<FUSED>(q, v.vec + (size_t)x * dim, NB, l16);
+        int decision = d32 <= kx;
+        if (lv && l16 == 0) cn.fp32++;
+        const bool tie = lv && kx != FLT_MAX && v.knn_ids && kidx < (v.knn_hdr[x] & 0xFFFFu) &&
+                         fabsf(d32 - kx) <= kTieUlpsS * (nextafterf(kx, FLT_MAX) - kx);
+        if (__any_sync(0xFFFFFFFFu, tie)) {
+            // FP64: d(q, x) against d(x, x_k), x_k the k-th neighbour of x
+            double a = 0.0, bb = 0.0;
+            if (tie) {
+                const uint32_t nk = v.knn_ids[(size_t)x * v.K + kidx];
+                const float* xr = v.vec + (size_t)x * dim;
+                const float* yr = v.vec + (size_t)nk * dim;
+                for (uint32_t e2 = l16; e2 < dim; e2 += 16) {
+                    const double tq = (double)q[e2] - (double)xr[e2];
+                    const double ty = (double)xr[e2] - (double)yr[e2];
+                    a += tq * tq;
+                    bb += ty * ty;
+                }
+            }
+            for (int o = 8; o; o >>= 1) {
+                a += __shfl_xor_sync(0xFFFFFFFFu, a, o);
+                bb += __shfl_xor_sync(0xFFFFFFFFu, bb, o);
+            }
+            if (tie) {
+                const int d64 = a <= bb;
+                if (l16 == 0) {
+                    cn.fp64++;
+                    if (d64 != decision) cn.flip++;
+                }
+                decision = d64;
+            }
+        }
+        stream_accept(lv && l16 == 0 && decision == 1, x, qi, res_off, acc_cnt, resbuf);
+    }
+    __syncwarp();
+}
+
+// One step of 32 postings already resolved to owner ids: the INT8 screen.
+template <int NB>
+__device__ __forceinline__ int stream_screen(const DevView& v, const int* q8, float4 qv, uint32_t id, bool live,
+                                             const float* __restrict__ kcol, float& kd_out) {
+    constexpr uint32_t dim = NB * 16;
+    const float kd = __ldg(kcol + id);
+    const float4 xm = __ldg(v.i8_meta + id);
+    const float D = i8_row<NB>(q8, qv, v.vec_i8 + (size_t)id * dim, xm);
+    kd_out = kd;
+    return live ? i8_decide(D, kd, qv, xm, dim) : 0;
+}
+
 template <class E, bool FUSED, int NB>
 __global__ void __launch_bounds__(256, 3) k_verify_chunks(
     DevView v, const float* __restrict__ Q, uint32_t mmax, const uint32_t* __restrict__ prox,
@@ -115,6 +219,7 @@ __global__ void __launch_bounds__(256, 3) k_verify_chunks(
     extern __shared__ __align__(16) char smraw[];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     constexpr uint32_t dim = NB * 16;
+    constexpr int kSteps = kChunk / 32;
     char* base = smraw + (size_t)w * (dim * 4 + dim + 32 * 4);
     float* q = (float*)base;                  // FP32 query (loaded when a row needs the exact test)
     int* q8 = (int*)(q + dim);                // INT8 query words
@@ -122,7 +227,8 @@ __global__ void __launch_bounds__(256, 3) k_verify_chunks(
     const uint64_t nch = *nchunks;
     uint32_t cur_q = kInvalid, f32_q = kInvalid;
     float4 qv = make_float4(0.f, 0.f, 0.f, 0.f);
-    unsigned long long c_post = 0, c_lowp = 0, c_fp32 = 0, c_fp64 = 0, c_flip = 0;
+    unsigned long long c_post = 0, c_lowp8 = 0;  // the streaming loop's own counters stay in registers
+    StreamCount cn;                              // the undecided path's
     for (;;) {
         uint64_t c = 0;
         if (lane == 0) c = atomicAdd((unsigned long long*)next, 1ull);
@@ -135,6 +241,13 @@ __global__ void __launch_bounds__(256, 3) k_verify_chunks(
         const uint32_t e1 = min(e0 + kChunk, len);
         const uint32_t p = prox[t];
         const uint64_t b = v.csr_off[p];
+        // every owner id of the chunk in one round trip (kSteps per lane)
+        uint32_t ids[kSteps];
+#pragma unroll
+        for (int j = 0; j < kSteps; ++j) {
+            const uint32_t e = e0 + lane + 32 * j;
+            ids[j] = e < e1 ? (uint32_t)(((const E*)v.csr_ent)[b + e] >> v.rank_bits) : p;
+        }
         if (qi != cur_q) {
             __syncwarp();
             if ((uint32_t)lane < dim / 4) q8[lane] = reinterpret_cast<const int*>(qq + (size_t)qi * dim)[lane];
@@ -143,94 +256,21 @@ __global__ void __launch_bounds__(256, 3) k_verify_chunks(
             __syncwarp();
         }
         if (lane == 0) c_post += e1 - e0;
-        for (uint32_t e = e0 + lane; e - lane < e1; e += 32) {
-            const bool live = e < e1;
-            const uint32_t id = live ? (uint32_t)(((const E*)v.csr_ent)[b + e] >> v.rank_bits) : p;
-            const float kd = __ldg(kcol + id);
-            const float4 xm = __ldg(v.i8_meta + id);
-            const float D = i8_row<NB>(q8, qv, v.vec_i8 + (size_t)id * dim, xm);
-            const int dec = live ? i8_decide(D, kd, qv, xm, dim) : 0;
-            if (dec >= 0 && live) c_lowp++;
-            // (the screens below need the FP32 query in shared memory)
-            stream_accept(dec == 1, id, qi, res_off, acc_cnt, resbuf);
-            const uint32_t und = __ballot_sync(0xFFFFFFFFu, dec < 0);
-            if (!und) continue;
-            // exact FP32 (and FP64 in the tie band) for the undecided rows
-            if (f32_q != qi) {
-                __syncwarp();
-                for (uint32_t i = lane; i < dim; i += 32) q[i] = Q[(size_t)qi * dim + i];
-                f32_q = qi;
-            }
-            __syncwarp();
-            if (dec < 0) st[__popc(und & ((1u << lane) - 1u))] = id;
-            __syncwarp();
-            // the BF16 screen (two lanes per row) decides most of what INT8 could not
-            uint32_t nu = 0;
-            const uint32_t nu8 = __popc(und);
-            for (uint32_t r = 0; r < nu8; r += 16) {
-                const int pp = lane & 1;
-                const uint32_t tt = r + (lane >> 1);
-                const bool lv = tt < nu8;
-                const uint32_t x = st[lv ? tt : r];
-                const float kx = __ldg(kcol + x);
-                const float D = bf16_pair<NB>(q, v.vec_bf16 + (size_t)x * dim, pp);
-                const float ex = __ldg(v.vec_err + x);
-                const float rho = (4.f * dim + 64.f) * 5.9604645e-8f;
-                const float sD = sqrtf(D);
-                const float hi = sD * (1.f + rho) + ex, lo = fmaxf(0.f, sD * (1.f - rho) - ex);
-                const float U = hi * hi * (1.f + rho), L = lo * lo * (1.f - rho);
-                const int db = kx == FLT_MAX ? 1 : (U < kx ? 1 : (L > kx ? 0 : -1));
-                if (lv && pp == 0 && db >= 0) c_lowp++;
-                stream_accept(lv && pp == 0 && db == 1, x, qi, res_off, acc_cnt, resbuf);
-                const uint32_t u2 = __ballot_sync(0xFFFFFFFFu, lv && pp == 0 && db < 0);
-                __syncwarp();  // every lane has read its row of this round
-                if (lv && pp == 0 && db < 0) st[nu + __popc(u2 & ((1u << lane) - 1u))] = x;
-                nu += __popc(u2);
-                __syncwarp();
-            }
-            const int hh = lane >> 4, l16 = lane & 15;  // one row per half-warp
-            for (uint32_t r = 0; r < nu; r += 2) {
-                const uint32_t tt = r + hh;
-                const bool lv = tt < nu;
-                const uint32_t x = st[lv ? tt : r];
-                const float kx = __ldg(kcol + x);
-                const float d32 = l2_half16<FUSED>(q, v.vec + (size_t)x * dim, NB, l16);
-                int decision = d32 <= kx;
-                if (lv && l16 == 0) c_fp32++;
-                const bool tie = lv && kx != FLT_MAX && v.knn_ids && kidx < (v.knn_hdr[x] & 0xFFFFu) &&
-                                 fabsf(d32 - kx) <= kTieUlpsS * (nextafterf(kx, FLT_MAX) - kx);
-                if (__any_sync(0xFFFFFFFFu, tie)) {
-                    // FP64: d(q, x) against d(x, x_k), x_k the k-th neighbour of x
-                    double a = 0.0, bb = 0.0;
-                    if (tie) {
-                        const uint32_t nk = v.knn_ids[(size_t)x * v.K + kidx];
-                        const float* xr = v.vec + (size_t)x * dim;
-                        const float* yr = v.vec + (size_t)nk * dim;
-                        for (uint32_t e2 = l16; e2 < dim; e2 += 16) {
-                            const double tq = (double)q[e2] - (double)xr[e2];
-                            const double ty = (double)xr[e2] - (double)yr[e2];
-                            a += tq * tq;
-                            bb += ty * ty;
-                        }
-                    }
-                    for (int o = 8; o; o >>= 1) {
-                        a += __shfl_xor_sync(0xFFFFFFFFu, a, o);
-                        bb += __shfl_xor_sync(0xFFFFFFFFu, bb, o);
-                    }
-                    if (tie) {
-                        const int d64 = a <= bb;
-                        if (l16 == 0) {
-                            c_fp64++;
-                            if (d64 != decision) c_flip++;
-                        }
-                        decision = d64;
-                    }
-                }
-                stream_accept(lv && l16 == 0 && decision == 1, x, qi, res_off, acc_cnt, resbuf);
-            }
-            __syncwarp();
+        const uint32_t nsteps = (e1 - e0 + 31) / 32;
+#pragma unroll
+        for (int j = 0; j < kSteps; ++j) {
+            if ((uint32_t)j >= nsteps) break;
+            const bool live = e0 + lane + 32 * j < e1;
+            float kd;
+            const int dec = stream_screen<NB>(v, q8, qv, ids[j], live, kcol, kd);
+            if (dec >= 0 && live) c_lowp8++;
+            stream_accept(dec == 1, ids[j], qi, res_off, acc_cnt, resbuf);
+            if (__any_sync(0xFFFFFFFFu, dec < 0))
+                stream_undecided<FUSED, NB>(v, Q, qi, dec, ids[j], q, st, f32_q, kcol, kidx, res_off, acc_cnt,
+                                            resbuf, cn);
         }
     }
+    unsigned long long c_lowp = c_lowp8 + cn.lowp, c_fp32 = cn.fp32, c_fp64 = cn.fp64, c_flip = cn.flip;
     for (int o = 16; o; o >>= 1) {
         c_lowp += __shfl_xor_sync(0xFFFFFFFFu, c_lowp, o);
         c_fp32 += __shfl_xor_sync(0xFFFFFFFFu, c_fp32, o);

@@ -1,11 +1,11 @@
 """What the trained budget network gains over the method without it, on queries
 it never saw.  An MLP trained by the library's own kernels on (query, "is the
 answer with m_l proxies complete") labels of a training stream serves a
-held-out stream: against the plain search at the caller's m it must scan far
-fewer postings per query (the work of phase B/C) at the same recall, and
-against a plain search whose uniform m costs at least as many postings it must
-reach at least that search's recall -- the budget spends the work where a query
-needs it."""
+held-out stream.  Against a plain search with a uniform m that scans at least
+as many postings per query (the work of phase B/C), the budget must reach at
+least that search's recall -- it spends the work where a query needs it -- and
+at one confidence cutoff it must scan far fewer postings than the caller's m at
+nearly its recall."""
 import numpy as np
 import pytest
 
