@@ -31,6 +31,7 @@ namespace {
 
 constexpr uint32_t kChunk = 256;     // postings per work item
 constexpr uint32_t kFinCap = 1024;   // acceptances a query's finishing warp sorts in shared memory
+constexpr uint32_t kBigCap = 16384;  // ... and a finishing block (64 KB of shared memory)
 constexpr float kTieUlpsS = 16.f;    // FP64 re-decision band around the radius, in ulps of kd
 
 // The INT8 screen of one row: 1 accept, 0 reject, -1 undecided.
@@ -289,12 +290,12 @@ __global__ void __launch_bounds__(256, 3) k_verify_chunks(
 }
 
 // One warp per query: sort the accepted ids (bitonic, shared memory), drop
-// repeats, write the labels over the query's slice; more than kFinCap
-// acceptances go to the overflow list.
+// repeats, write the labels over the query's slice; queries with more than
+// kFinCap acceptances are listed for k_stream_finish_big.
 __global__ void __launch_bounds__(256) k_stream_finish(DevView v, uint32_t nq, const uint64_t* __restrict__ res_off,
                                                        const uint32_t* __restrict__ acc_cnt,
                                                        uint64_t* __restrict__ resbuf, uint32_t* __restrict__ res_count,
-                                                       uint32_t* __restrict__ ovl, uint32_t* __restrict__ n_ovl,
+                                                       uint32_t* __restrict__ big, uint32_t* __restrict__ n_big,
                                                        SearchCounters* __restrict__ ctr) {
     __shared__ uint32_t sm[8][kFinCap];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -302,8 +303,8 @@ __global__ void __launch_bounds__(256) k_stream_finish(DevView v, uint32_t nq, c
     if (qi >= nq) return;
     uint32_t* acc = sm[w];
     const uint32_t na = acc_cnt[qi];
-    if (na > kFinCap) {
-        if (lane == 0) ovl[atomicAdd(n_ovl, 1u)] = qi;
+    if (na > kFinCap) {  // left to the block-wide pass
+        if (lane == 0) big[atomicAdd(n_big, 1u)] = qi;
         return;
     }
     const uint64_t ro = res_off[qi];
@@ -341,6 +342,69 @@ __global__ void __launch_bounds__(256) k_stream_finish(DevView v, uint32_t nq, c
 
 // Blocks per SM of one instantiation; its shared-memory attribute is set on the
 // first call (outside any stream capture: stream_prepare).
+// One block per listed query (blocks take them from a counter): the same with up
+// to kBigCap acceptances sorted by the block in shared memory; more than that go
+// to the overflow list (answered from scratch by the overflow pass).
+__global__ void __launch_bounds__(1024) k_stream_finish_big(DevView v, const uint64_t* __restrict__ res_off,
+                                                            const uint32_t* __restrict__ acc_cnt,
+                                                            const uint32_t* __restrict__ big,
+                                                            const uint32_t* __restrict__ n_big,
+                                                            uint32_t* __restrict__ next, uint64_t* __restrict__ resbuf,
+                                                            uint32_t* __restrict__ res_count,
+                                                            uint32_t* __restrict__ ovl, uint32_t* __restrict__ n_ovl,
+                                                            SearchCounters* __restrict__ ctr) {
+    extern __shared__ uint32_t acc[];  // kBigCap
+    __shared__ uint32_t ctl[2];
+    const int tid = threadIdx.x, lane = tid & 31;
+    const uint32_t nb = *n_big;
+    for (;;) {
+        __syncthreads();
+        if (tid == 0) ctl[0] = atomicAdd(next, 1u);
+        __syncthreads();
+        const uint32_t b = ctl[0];
+        if (b >= nb) break;
+        const uint32_t qi = big[b];
+        const uint32_t na = acc_cnt[qi];
+        if (na > kBigCap) {
+            if (tid == 0) ovl[atomicAdd(n_ovl, 1u)] = qi;
+            continue;
+        }
+        const uint64_t ro = res_off[qi];
+        uint32_t P = 32;
+        while (P < na) P <<= 1;
+        for (uint32_t i = tid; i < P; i += blockDim.x) acc[i] = i < na ? (uint32_t)resbuf[ro + i] : kInvalid;
+        __syncthreads();
+        for (uint32_t k = 2; k <= P; k <<= 1)
+            for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+                for (uint32_t i = tid; i < P; i += blockDim.x) {
+                    const uint32_t y = i ^ j;
+                    if (y > i) {
+                        const uint32_t a0 = acc[i], a1 = acc[y];
+                        if ((a0 > a1) == ((i & k) == 0)) {
+                            acc[i] = a1;
+                            acc[y] = a0;
+                        }
+                    }
+                }
+                __syncthreads();
+            }
+        if (tid < 32) {  // one warp compacts the sorted ids
+            uint32_t nu = 0;
+            for (uint32_t b0 = 0; b0 < na; b0 += 32) {
+                const uint32_t i = b0 + lane;
+                const bool keep = i < na && (i == 0 || acc[i] != acc[i - 1]);
+                const uint32_t kb = __ballot_sync(0xFFFFFFFFu, keep);
+                if (keep) resbuf[ro + nu + __popc(kb & ((1u << lane) - 1u))] = v.labels[acc[i]];
+                nu += __popc(kb);
+            }
+            if (lane == 0) {
+                res_count[qi] = nu;
+                if (nu) atomicAdd(&ctr->n_result, (unsigned long long)nu);
+            }
+        }
+    }
+}
+
 template <class E, bool F, int NB>
 int chunks_per_sm() {
     static int per_sm = 0;
@@ -372,6 +436,12 @@ void launch_chunks(const DevView& v, const float* Q, uint32_t mmax, const uint32
 }  // namespace
 
 void stream_prepare(const DevView& v, bool wide, bool fused) {
+    static bool big_set = false;
+    if (!big_set) {
+        CUDA_CHECK(cudaFuncSetAttribute(k_stream_finish_big, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)(kBigCap * 4)));
+        big_set = true;
+    }
     if (v.dim == 128) {
         if (wide) fused ? chunks_per_sm<uint64_t, true, 8>() : chunks_per_sm<uint64_t, false, 8>();
         else fused ? chunks_per_sm<uint32_t, true, 8>() : chunks_per_sm<uint32_t, false, 8>();
@@ -391,7 +461,7 @@ void StreamBufs::reserve(uint32_t nq_, uint32_t dim, size_t npairs_, size_t max_
     cnt.ensure((npairs_ + 1) * 4);
     coff.ensure((npairs_ + 1) * 8);
     chunks.ensure(std::max<size_t>(max_chunks, 1) * 8);
-    acc_cnt.ensure((size_t)nq_ * 4 + 16);
+    acc_cnt.ensure((size_t)nq_ * 8 + 16);  // counts, then the list of queries for the block-wide pass
     ctl.ensure(64);
     npairs = npairs_;
 }
@@ -406,8 +476,9 @@ void stream_verify(const DevView& v, bool wide, bool fused, const float* Q, uint
                    SearchCounters* ctr, StreamBufs& B, int nsm, cudaStream_t s) {
     const size_t npairs = (size_t)nq * mmax;
     if (B.npairs != npairs) fail(HRNN_ERR_STATE, "stream_verify: buffers reserved for another shape");
+    stream_prepare(v, wide, fused);
     CUDA_CHECK(cudaMemsetAsync(B.acc_cnt.p, 0, (size_t)nq * 4, s));
-    CUDA_CHECK(cudaMemsetAsync(B.ctl.p, 0, 8, s));
+    CUDA_CHECK(cudaMemsetAsync(B.ctl.p, 0, 16, s));
     k_quantize_queries<<<(unsigned)(((size_t)nq * 32 + 255) / 256), 256, 0, s>>>(Q, nq, v.dim, B.qq.as<int8_t>(),
                                                                                   B.qmeta.as<float4>());
     CUDA_LAUNCH_CHECK();
@@ -429,8 +500,13 @@ void stream_verify(const DevView& v, bool wide, bool fused, const float* Q, uint
         else fused ? launch_chunks<uint32_t, true, 6>(v, Q, mmax, prox, plen, res_off, kcol, kidx, B, resbuf, ctr, nsm, s)
                    : launch_chunks<uint32_t, false, 6>(v, Q, mmax, prox, plen, res_off, kcol, kidx, B, resbuf, ctr, nsm, s);
     }
-    k_stream_finish<<<(nq + 7) / 8, 256, 0, s>>>(v, nq, res_off, B.acc_cnt.as<uint32_t>(), resbuf, res_count, ovl,
-                                                 n_ovl, ctr);
+    uint32_t* big_n = B.ctl.as<uint32_t>() + 2;  // [2] big queries, [3] their work counter
+    uint32_t* big = B.acc_cnt.as<uint32_t>() + nq;
+    k_stream_finish<<<(nq + 7) / 8, 256, 0, s>>>(v, nq, res_off, B.acc_cnt.as<uint32_t>(), resbuf, res_count, big,
+                                                 big_n, ctr);
+    CUDA_LAUNCH_CHECK();
+    k_stream_finish_big<<<nsm, 1024, kBigCap * 4, s>>>(v, res_off, B.acc_cnt.as<uint32_t>(), big, big_n, big_n + 1,
+                                                       resbuf, res_count, ovl, n_ovl, ctr);
     CUDA_LAUNCH_CHECK();
 }
 
