@@ -78,6 +78,13 @@ __global__ void k_quantize_queries(const float* __restrict__ Q, uint32_t nq, uin
     if (lane == 0) qmeta[qi] = make_float4(sc * sc * (float)c2, sc, __double2float_ru(sqrt(e2)), 0.f);
 }
 
+// meta[i].w = kdist(i, k-1) of this call, next to the row's scale and error
+// terms, so the screen reads one 16-byte record per candidate.
+__global__ void k_meta_radius(const float* __restrict__ kcol, uint32_t n, float4* __restrict__ meta) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) meta[i].w = kcol[i];
+}
+
 // Chunks per (query, proxy) prefix.
 __global__ void k_chunk_count(const uint32_t* __restrict__ plen, size_t npairs, uint32_t* __restrict__ cnt) {
     const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -198,20 +205,41 @@ __device__ __noinline__ void stream_undecided(const DevView& v, const float* __r
     __syncwarp();
 }
 
-// One step of 32 postings already resolved to owner ids: the INT8 screen.
+// Two steps of 32 postings (owner ids a and b of this lane) through the INT8
+// screen with the loads of both rows issued before either dot product: 1 accept,
+// 0 reject, -1 undecided for each.  meta.w holds kdist(p, k-1) of this call.
 template <int NB>
-__device__ __forceinline__ int stream_screen(const DevView& v, const int* q8, float4 qv, uint32_t id, bool live,
-                                             const float* __restrict__ kcol, float& kd_out) {
+__device__ __forceinline__ void stream_screen2(const DevView& v, const int* q8, float4 qv, uint32_t ida, bool la,
+                                               uint32_t idb, bool lb, int& da, int& db) {
     constexpr uint32_t dim = NB * 16;
-    const float kd = __ldg(kcol + id);
-    const float4 xm = __ldg(v.i8_meta + id);
-    const float D = i8_row<NB>(q8, qv, v.vec_i8 + (size_t)id * dim, xm);
-    kd_out = kd;
-    return live ? i8_decide(D, kd, qv, xm, dim) : 0;
+    const int4* xa = reinterpret_cast<const int4*>(v.vec_i8 + (size_t)ida * dim);
+    const int4* xb = reinterpret_cast<const int4*>(v.vec_i8 + (size_t)idb * dim);
+    int4 ra[NB], rb[NB];
+#pragma unroll
+    for (int c = 0; c < NB; ++c) ra[c] = __ldg(xa + c);
+#pragma unroll
+    for (int c = 0; c < NB; ++c) rb[c] = __ldg(xb + c);
+    const float4 ma = __ldg(v.i8_meta + ida), mb = __ldg(v.i8_meta + idb);
+    int sa = 0, sb = 0;
+#pragma unroll
+    for (int c = 0; c < NB; ++c) {
+        sa = __dp4a(ra[c].x, q8[4 * c + 0], sa);
+        sa = __dp4a(ra[c].y, q8[4 * c + 1], sa);
+        sa = __dp4a(ra[c].z, q8[4 * c + 2], sa);
+        sa = __dp4a(ra[c].w, q8[4 * c + 3], sa);
+        sb = __dp4a(rb[c].x, q8[4 * c + 0], sb);
+        sb = __dp4a(rb[c].y, q8[4 * c + 1], sb);
+        sb = __dp4a(rb[c].z, q8[4 * c + 2], sb);
+        sb = __dp4a(rb[c].w, q8[4 * c + 3], sb);
+    }
+    const float Da = qv.x + ma.x * ma.x * ma.z - 2.f * qv.y * ma.x * (float)sa;
+    const float Db = qv.x + mb.x * mb.x * mb.z - 2.f * qv.y * mb.x * (float)sb;
+    da = la ? i8_decide(Da, ma.w, qv, ma, dim) : 0;
+    db = lb ? i8_decide(Db, mb.w, qv, mb, dim) : 0;
 }
 
 template <class E, bool FUSED, int NB>
-__global__ void __launch_bounds__(256, 3) k_verify_chunks(
+__global__ void __launch_bounds__(256, 2) k_verify_chunks(
     DevView v, const float* __restrict__ Q, uint32_t mmax, const uint32_t* __restrict__ prox,
     const uint32_t* __restrict__ plen, const uint64_t* __restrict__ res_off, const float* __restrict__ kcol,
     uint32_t kidx, const int8_t* __restrict__ qq, const float4* __restrict__ qmeta,
@@ -259,15 +287,19 @@ __global__ void __launch_bounds__(256, 3) k_verify_chunks(
         if (lane == 0) c_post += e1 - e0;
         const uint32_t nsteps = (e1 - e0 + 31) / 32;
 #pragma unroll
-        for (int j = 0; j < kSteps; ++j) {
+        for (int j = 0; j < kSteps; j += 2) {
             if ((uint32_t)j >= nsteps) break;
-            const bool live = e0 + lane + 32 * j < e1;
-            float kd;
-            const int dec = stream_screen<NB>(v, q8, qv, ids[j], live, kcol, kd);
-            if (dec >= 0 && live) c_lowp8++;
-            stream_accept(dec == 1, ids[j], qi, res_off, acc_cnt, resbuf);
-            if (__any_sync(0xFFFFFFFFu, dec < 0))
-                stream_undecided<FUSED, NB>(v, Q, qi, dec, ids[j], q, st, f32_q, kcol, kidx, res_off, acc_cnt,
+            const bool la = e0 + lane + 32 * j < e1, lb = e0 + lane + 32 * (j + 1) < e1;
+            int da, db;
+            stream_screen2<NB>(v, q8, qv, ids[j], la, ids[j + 1], lb, da, db);
+            c_lowp8 += (uint32_t)(da >= 0 && la) + (uint32_t)(db >= 0 && lb);
+            stream_accept(da == 1, ids[j], qi, res_off, acc_cnt, resbuf);
+            stream_accept(db == 1, ids[j + 1], qi, res_off, acc_cnt, resbuf);
+            if (__any_sync(0xFFFFFFFFu, da < 0))
+                stream_undecided<FUSED, NB>(v, Q, qi, da, ids[j], q, st, f32_q, kcol, kidx, res_off, acc_cnt,
+                                            resbuf, cn);
+            if (__any_sync(0xFFFFFFFFu, db < 0))
+                stream_undecided<FUSED, NB>(v, Q, qi, db, ids[j + 1], q, st, f32_q, kcol, kidx, res_off, acc_cnt,
                                             resbuf, cn);
         }
     }
@@ -479,6 +511,8 @@ void stream_verify(const DevView& v, bool wide, bool fused, const float* Q, uint
     stream_prepare(v, wide, fused);
     CUDA_CHECK(cudaMemsetAsync(B.acc_cnt.p, 0, (size_t)nq * 4, s));
     CUDA_CHECK(cudaMemsetAsync(B.ctl.p, 0, 16, s));
+    k_meta_radius<<<(v.n + 255) / 256, 256, 0, s>>>(kcol, v.n, const_cast<float4*>(v.i8_meta));
+    CUDA_LAUNCH_CHECK();
     k_quantize_queries<<<(unsigned)(((size_t)nq * 32 + 255) / 256), 256, 0, s>>>(Q, nq, v.dim, B.qq.as<int8_t>(),
                                                                                   B.qmeta.as<float4>());
     CUDA_LAUNCH_CHECK();

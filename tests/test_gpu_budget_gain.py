@@ -16,7 +16,7 @@ import hrnn_b200 as H
 pytestmark = pytest.mark.gpu
 
 N, D, K, KP, EF, KK = 40000, 64, 64, 64, 96, 10
-M_USER, M0, M1 = 12, 1, 3
+M_USER, M0, M1 = 5, 1, 3
 
 
 @pytest.fixture(scope="module")
