@@ -539,7 +539,7 @@ def main():
             BUDGET.update(m0=m0_, m1=m1_, ef=ef_)
         elif "budget_levels" in W:
             BUDGET.update(dict(zip(("m0", "m1", "ef"), W["budget_levels"])))
-        budget_info = train_budget(H, h, W, args, dev_sync, lprec)
+        budget_info = train_budget(H, h, W, args, dev_sync, lprec, mstars["plain"])
         budget_info["precision_form"] = lp
         cands = []
         for c in ([W["fixed_conf"]] if "fixed_conf" in W else CONFIDENCES):
@@ -938,12 +938,15 @@ def reference_dynamic(H, W, X, Q, gt, m_h, kp_h, ef_h):
     return t
 
 
-# Learned budget: level 0 = 1 proxy, level 1 = 3 proxies, taken from the caller's
-# own beam (single pass); a query takes a level when the MLP gives that level's
-# answer being complete a probability >= 0.9, else the caller's m.
-BUDGET = dict(m0=1, m1=3, ef=0, confidence=0.9)
+# Learned budget: level 0 = 3 proxies, level 1 = 5 proxies, both from a beam of 64
+# (two-pass mode); a query takes a level when the MLP gives that level's answer
+# being complete a probability >= the cutoff, else it continues the search with
+# the caller's (m, ef_search).
+BUDGET = dict(m0=3, m1=5, ef=64, confidence=0.9)
 CONFIDENCES = (0.95, 0.98, 0.99, 0.995, 0.998)
-LABEL_M, LABEL_EF = 50, 200  # the "complete" answer the labels compare against
+# The labels compare a level's answer with the caller's own answer (m, ef_search):
+# a level is "complete" for a query when it returns every point the caller's
+# search returns, so taking it changes the work and not the answer.
 
 
 def _search_sets(h, Q, m, kp, ef, k, chunk=10_000):
@@ -953,22 +956,24 @@ def _search_sets(h, Q, m, kp, ef, k, chunk=10_000):
     return out
 
 
-def train_budget(H, h, W, args, dev_sync, prec):
+def train_budget(H, h, W, args, dev_sync, prec, label_m):
     """Features and labels of `args.budget_train` seeded queries (a stream separate
-    from the timed ones) in the serving precision `prec`, then MLP training on the GPU."""
+    from the timed ones) in the serving precision `prec`, then MLP training on the
+    GPU.  A label says whether a level's answer contains the answer of the caller's
+    search (label_m proxies, the workload's ef_search)."""
     t0 = time.perf_counter()
     n = args.budget_train
     Qtr = mixture(n, W["d"], W["C"], W["sigma"], W["seed"], W.get("tseed", W["qseed"] + 7919),
                   dirichlet=W["dirichlet"])
     h.set_precision(prec)
-    full = _search_sets(h, Qtr, LABEL_M, W["Kp"], LABEL_EF, W["k"])
+    full = _search_sets(h, Qtr, label_m, W["Kp"], W["ef"], W["k"])
     Y = np.zeros((n, 2), np.uint8)
     for j, ml in enumerate((BUDGET["m0"], BUDGET["m1"])):
         got = _search_sets(h, Qtr, ml, W["Kp"], BUDGET["ef"] or W["ef"], W["k"])
         Y[:, j] = [np.isin(f, g, assume_unique=True).all() for f, g in zip(full, got)]
     t1 = time.perf_counter()
     h.set_budget(False, **BUDGET)
-    feat = np.concatenate([h.budget_features(Qtr[s:s + 50_000], W["k"], LABEL_M, W["ef"])
+    feat = np.concatenate([h.budget_features(Qtr[s:s + 50_000], W["k"], label_m, W["ef"])
                            for s in range(0, n, 50_000)])
     dev_sync()
     t2 = time.perf_counter()
@@ -988,7 +993,7 @@ def train_budget(H, h, W, args, dev_sync, prec):
                         "wrong_level_rate": round(float(wrong.mean()), 5)})
     h.set_precision(H.PREC_FP32_EXACT)
     info = {"train_queries": n, "levels": {"m0": BUDGET["m0"], "m1": BUDGET["m1"], "ef": BUDGET["ef"] or W["ef"]},
-            "label_ref": {"m": LABEL_M, "ef": LABEL_EF},
+            "label_ref": {"m": label_m, "ef": W["ef"]},
             "label_rate": [round(float(Y[:, 0].mean()), 4), round(float(Y[:, 1].mean()), 4)],
             "final_loss": round(loss, 4), "heldout_queries": ho, "heldout": heldout,
             "labels_s": round(t1 - t0, 1), "features_s": round(t2 - t1, 1), "train_s": round(t3 - t2, 1)}

@@ -400,6 +400,53 @@ __device__ __forceinline__ void warp_i8_list(const DevView& v, const int* q8, fl
     __syncwarp();
 }
 
+// Cooperative INT8 row reads.  In round i of a block of eight rounds, lane
+// (g, s) = (lane >> 3, lane & 7) reads bytes 16 s .. 16 s + 15 of row 4 i + g of a
+// block of 32 rows, so one 16-byte load per lane covers four whole rows (one
+// 128-byte line each) instead of 32 scattered ones; lanes with s >= NB (rows
+// narrower than 128 bytes) read nothing.
+template <int NB>
+__device__ __forceinline__ int4 coop_i8_load(const int8_t* vec, uint32_t id) {
+    const int s = threadIdx.x & 7;
+    return s < NB ? __ldg(reinterpret_cast<const int4*>(vec + (size_t)id * (NB * 16)) + s) : make_int4(0, 0, 0, 0);
+}
+
+__device__ __forceinline__ int dp4a4(int4 a, int4 b) {
+    return __dp4a(a.x, b.x, __dp4a(a.y, b.y, __dp4a(a.z, b.z, __dp4a(a.w, b.w, 0))));
+}
+
+// The row of a block whose whole dot product coop_sum8 leaves in this lane.
+__device__ __forceinline__ uint32_t coop_row() { return 4 * (threadIdx.x & 7) + ((threadIdx.x >> 3) & 3); }
+
+// Folds the eight partial dot products p[i] (round i) of the lanes of a group of
+// eight so that lane (g, s) ends with the sum over the group of p[s] -- the whole
+// dot product of row 4 s + g.  Three butterfly steps, each swapping half of the
+// values still held: 4 + 2 + 1 shuffles for eight rows.
+__device__ __forceinline__ int coop_sum8(const int (&p)[8]) {
+    const int s = threadIdx.x & 7;
+    const bool b2 = s & 4, b1 = s & 2, b0 = s & 1;
+    int w[4], x[2];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int send = b2 ? p[k] : p[k + 4], keep = b2 ? p[k + 4] : p[k];
+        w[k] = keep + __shfl_xor_sync(0xFFFFFFFFu, send, 4);
+    }
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const int send = b1 ? w[k] : w[k + 2], keep = b1 ? w[k + 2] : w[k];
+        x[k] = keep + __shfl_xor_sync(0xFFFFFFFFu, send, 2);
+    }
+    const int send = b0 ? x[0] : x[1], keep = b0 ? x[1] : x[0];
+    return keep + __shfl_xor_sync(0xFFFFFFFFu, send, 1);
+}
+
+// This lane's INT8 query words for the cooperative reads (bytes 16 s .. 16 s + 15).
+template <int NB>
+__device__ __forceinline__ int4 coop_q_words(const int* q8) {
+    const int s = threadIdx.x & 7;
+    return s < NB ? make_int4(q8[4 * s], q8[4 * s + 1], q8[4 * s + 2], q8[4 * s + 3]) : make_int4(0, 0, 0, 0);
+}
+
 // One row scored by every lane (the entry point of a search).
 __device__ __forceinline__ float i8_one(const DevView& v, const float* q, uint32_t id) {
     const int* q8 = i8_q_words(q, v.dim);

@@ -6,7 +6,7 @@
 //
 //   * each step expands the two best unexpanded beam entries together: both link
 //     rows are loaded at once and all their fresh neighbours (up to 64) are
-//     scored in one memory round trip (two INT8 rows per lane), so a step costs
+//     scored in one memory round trip (INT8 rows read by eight lanes each), so a step costs
 //     one dependent row-gather latency for two expansions;
 //   * a scored neighbour enters the beam when it is closer than a full beam's last
 //     entry (no per-neighbour sequential acceptance count), duplicates within a
@@ -54,62 +54,71 @@ __device__ inline WarpSmem carve_fast(char* base, uint32_t dim, uint32_t efc, ui
     return s;
 }
 
-// Two INT8 rows per lane (rows t and t + 32 of ids[0..cnt)), all loads of both
-// issued before the dot products.
-template <int NW>
-__device__ __forceinline__ void warp_i8_rows2(const DevView& v, const int* q8, float4 qm, const uint32_t* ids,
-                                              uint32_t cnt, float* dout) {
-    const int lane = threadIdx.x & 31;
-    const uint32_t t0 = lane, t1 = lane + 32;
-    const uint32_t id0 = ids[t0 < cnt ? t0 : 0], id1 = ids[t1 < cnt ? t1 : 0];
-    const int4* x0 = reinterpret_cast<const int4*>(v.vec_i8 + (size_t)id0 * v.dim);
-    const int4* x1 = reinterpret_cast<const int4*>(v.vec_i8 + (size_t)id1 * v.dim);
-    const bool two = cnt > 32;
-    int4 a[NW], b[NW];
+// ids[0..cnt) (cnt <= 64) scored with cooperative row reads (coop_i8_load): a
+// block of 32 rows in eight load rounds, four whole rows per load instruction.
+// R2: both blocks' loads issued before either is scored (one memory round trip
+// for 64 rows, twice the registers); otherwise block by block.
+template <int NB, bool R2>
+__device__ __forceinline__ void warp_i8_coop(const DevView& v, const int* q8, float4 qm, const uint32_t* ids,
+                                             uint32_t cnt, float* dout) {
+    const int g = (threadIdx.x >> 3) & 3;
+    const int4 qw = coop_q_words<NB>(q8);
+    const uint32_t r = coop_row();
+    const uint32_t nb = cnt > 32 ? 2 : 1;
+    auto finish = [&](const int4 (&x)[8], float4 m, uint32_t b0) {
+        int p[8];
 #pragma unroll
-    for (int c = 0; c < NW; ++c) a[c] = __ldg(x0 + c);
-    if (two) {
+        for (int i = 0; i < 8; ++i) p[i] = dp4a4(x[i], qw);
+        const int d = coop_sum8(p);
+        if (b0 + r < cnt) dout[b0 + r] = qm.x + m.x * m.x * m.z - 2.f * qm.y * m.x * (float)d;
+    };
+    if constexpr (R2) {
+        int4 x0[8], x1[8];
+        float4 m0, m1 = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
-        for (int c = 0; c < NW; ++c) b[c] = __ldg(x1 + c);
-    }
-    const float4 m0 = __ldg(v.i8_meta + id0);
-    const float4 m1 = two ? __ldg(v.i8_meta + id1) : m0;
-    int d0 = 0, d1 = 0;
-#pragma unroll
-    for (int c = 0; c < NW; ++c) {
-        d0 = __dp4a(a[c].x, q8[4 * c + 0], d0);
-        d0 = __dp4a(a[c].y, q8[4 * c + 1], d0);
-        d0 = __dp4a(a[c].z, q8[4 * c + 2], d0);
-        d0 = __dp4a(a[c].w, q8[4 * c + 3], d0);
-    }
-    if (t0 < cnt) dout[t0] = qm.x + m0.x * m0.x * m0.z - 2.f * qm.y * m0.x * (float)d0;
-    if (two) {
-#pragma unroll
-        for (int c = 0; c < NW; ++c) {
-            d1 = __dp4a(b[c].x, q8[4 * c + 0], d1);
-            d1 = __dp4a(b[c].y, q8[4 * c + 1], d1);
-            d1 = __dp4a(b[c].z, q8[4 * c + 2], d1);
-            d1 = __dp4a(b[c].w, q8[4 * c + 3], d1);
+        for (int i = 0; i < 8; ++i) {
+            const uint32_t t = 4 * i + g;
+            x0[i] = coop_i8_load<NB>(v.vec_i8, ids[t < cnt ? t : 0]);
         }
-        if (t1 < cnt) dout[t1] = qm.x + m1.x * m1.x * m1.z - 2.f * qm.y * m1.x * (float)d1;
+        m0 = __ldg(v.i8_meta + ids[r < cnt ? r : 0]);
+        if (nb > 1) {
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const uint32_t t = 32 + 4 * i + g;
+                x1[i] = coop_i8_load<NB>(v.vec_i8, ids[t < cnt ? t : 0]);
+            }
+            m1 = __ldg(v.i8_meta + ids[32 + r < cnt ? 32 + r : 0]);
+        }
+        finish(x0, m0, 0);
+        if (nb > 1) finish(x1, m1, 32);
+    } else {
+        for (uint32_t b0 = 0; b0 < 32 * nb; b0 += 32) {
+            int4 x[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const uint32_t t = b0 + 4 * i + g;
+                x[i] = coop_i8_load<NB>(v.vec_i8, ids[t < cnt ? t : 0]);
+            }
+            const float4 m = __ldg(v.i8_meta + ids[b0 + r < cnt ? b0 + r : 0]);
+            finish(x, m, b0);
+        }
     }
 }
 
 // Scores ids[0..cnt) (cnt <= 64) with the form's rows: DM 3 INT8, DM 2 BF16.
-// R2: INT8 rows two per lane (all 64 in one round trip, at twice the registers
-// and so fewer resident warps) or one per lane in two rounds; the launch-shape
-// autotuner picks.
+// R2: all 64 INT8 rows in one memory round trip (at twice the registers and so
+// fewer resident warps) or 32 at a time; the launch-shape autotuner picks.
 template <int DM, bool R2>
 __device__ __forceinline__ void warp_dist_list64(const DevView& v, const float* q, const uint32_t* ids,
                                                  uint32_t cnt, float* dout) {
     if constexpr (DM == 3) {
         const int* q8 = i8_q_words(q, v.dim);
         const float4 qm = *i8_q_meta(q, v.dim);
-        // two rows per lane up to dim 128 (16 loads of 16 bytes in flight per
-        // lane); wider rows one per lane, 32 at a time
+        // rows of 96 and 128 bytes read cooperatively; other widths one row per
+        // lane, 32 at a time
         const uint32_t nw = v.dim >> 4;
-        if (R2 && nw == 6) warp_i8_rows2<6>(v, q8, qm, ids, cnt, dout);
-        else if (R2 && nw == 8) warp_i8_rows2<8>(v, q8, qm, ids, cnt, dout);
+        if (nw == 6) warp_i8_coop<6, R2>(v, q8, qm, ids, cnt, dout);
+        else if (nw == 8) warp_i8_coop<8, R2>(v, q8, qm, ids, cnt, dout);
         else {
             warp_i8_list(v, q8, qm, ids, min(cnt, 32u), dout);
             if (cnt > 32) warp_i8_list(v, q8, qm, ids + 32, cnt - 32, dout + 32);

@@ -136,15 +136,19 @@ __global__ void __launch_bounds__(256) k_sample_rev_sel(uint32_t n, uint32_t R, 
                                                         uint32_t* __restrict__ newl, uint32_t* __restrict__ newc,
                                                         uint32_t* __restrict__ oldl, uint32_t* __restrict__ oldc,
                                                         unsigned long long* __restrict__ entries) {
+    // entries[0]: |new| + |old| summed over the nodes; entries[2]: the join's
+    // pairs |new| (|new| - 1) / 2 + |new| |old| summed (an upper bound: pairs of
+    // equal ids are skipped by the join)
     __shared__ uint32_t hist_all[8][256];
     __shared__ uint32_t pick_all[8][kRevSel];
     const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
     uint32_t* hist = hist_all[wl];
     uint32_t* pick = pick_all[wl];
-    unsigned long long my_entries = 0;
+    unsigned long long my_entries = 0, my_pairs = 0;
     const size_t warp = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const size_t nw = ((size_t)gridDim.x * blockDim.x) >> 5;
     for (size_t i = warp; i < n; i += nw) {
+        uint32_t fin[2] = {0, 0};
         for (int type = 0; type < 2; ++type) {
             const size_t seg = 2 * i + type;
             const uint64_t b = roff[seg];
@@ -235,20 +239,24 @@ __global__ void __launch_bounds__(256) k_sample_rev_sel(uint32_t n, uint32_t R, 
             }
             if (lane == 0) C[i] = base + take;
             my_entries += base + take;
+            fin[type] = base + take;
         }
+        my_pairs += (unsigned long long)fin[0] * (fin[0] - (fin[0] > 0)) / 2 + (unsigned long long)fin[0] * fin[1];
     }
     if (lane == 0 && my_entries) atomicAdd(entries, my_entries);
+    if (lane == 0 && my_pairs) atomicAdd(entries + 2, my_pairs);
 }
 
 __global__ void k_sample_rev(uint32_t n, uint32_t R, uint32_t cap, const uint64_t* __restrict__ roff,
                              const uint32_t* __restrict__ rbuf, uint32_t* __restrict__ newl,
                              uint32_t* __restrict__ newc, uint32_t* __restrict__ oldl, uint32_t* __restrict__ oldc,
                              unsigned long long* __restrict__ entries) {
-    unsigned long long my_entries = 0;
+    unsigned long long my_entries = 0, my_pairs = 0;  // as k_sample_rev_sel
     size_t warp = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     int lane = threadIdx.x & 31;
     size_t nw = ((size_t)gridDim.x * blockDim.x) >> 5;
     for (size_t i = warp; i < n; i += nw) {
+        uint32_t fin[2] = {0, 0};
         for (int type = 0; type < 2; ++type) {
             size_t seg = 2 * i + type;
             uint64_t b = roff[seg], e = roff[seg + 1];
@@ -273,68 +281,140 @@ __global__ void k_sample_rev(uint32_t n, uint32_t R, uint32_t cap, const uint64_
             __syncwarp();
             if (lane == 0) C[i] = base + take;
             my_entries += base + take;
+            fin[type] = base + take;
         }
+        my_pairs += (unsigned long long)fin[0] * (fin[0] - (fin[0] > 0)) / 2 + (unsigned long long)fin[0] * fin[1];
     }
     if (lane == 0 && my_entries) atomicAdd(entries, my_entries);
+    if (lane == 0 && my_pairs) atomicAdd(entries + 2, my_pairs);
 }
 
 // ---- phase 2: join -----------------------------------------------------------
 
-// One block per node of the chunk: exact FP32 distances of all sample pairs.
-// The node's rows are staged in shared memory (stride dim + 4 floats: 16-byte
-// aligned and free of bank conflicts for float4 reads).  A warp takes a tile of
-// kJR rows i x 32 columns j (lane = column): the row vectors are read by every
-// lane at the same address (broadcast) and the lane's column vector once for all
-// kJR pairs, so a 16-byte shared-memory read feeds 4 kJR elementwise steps.
-// Each pair keeps the reference's 16 accumulators (element e into accumulator
-// e mod 16, then summed left to right), so the tiling leaves every distance
-// bit-identical.  Proposals are appended with one atomic per warp tile.
+// One block (16 warps) per node of the chunk at a time: exact FP32 distances of
+// all sample pairs.  The node's rows are staged in shared memory (stride dim + 4
+// floats: 16-byte aligned and free of bank conflicts for float4 reads).  Work
+// unit: kJR rows i0 .. i0 + 3 (a row tile of the new list) x one column j > i0;
+// a tile's columns run from i0 + 1 to the last row, and the units of all tiles
+// are numbered consecutively, so a warp takes 32 consecutive units (lane = unit)
+// and no lane computes a pair below the diagonal or past the last row.  The row
+// vectors are mostly read by the whole warp at one address (broadcast) and the
+// lane's column vector once for all kJR pairs, so a 16-byte shared-memory read
+// feeds 4 kJR elementwise steps.  Each pair keeps the reference's 16
+// accumulators (element e into accumulator e mod 16, then summed left to right),
+// so the tiling leaves every distance bit-identical.
+//
+// NBUF 2 (512 threads, one block per SM): two stages, the next node's rows
+// copied asynchronously while the current node is computed -- for iterations
+// with many pairs per node.  NBUF 1 (256 threads, two blocks per SM): one stage,
+// for iterations with few pairs per node (and dims whose two stages do not fit).
+// Nodes without new entries have no pairs and are skipped.  Proposals go to
+// ranges of the buffer a warp reserves kReserve slots at a time (one atomic per
+// range instead of one per tile; a tile's proposals continue in a new range when
+// the current one is full); the unused end of a warp's last range is filled with
+// target kNoTarget, which the grouping skips.
 constexpr int kJR = 4;  // 8 rows (207 registers, one block per SM) measured 1.4x slower
+constexpr uint32_t kReserve = 128;
+constexpr uint32_t kNoTarget = 0xFFFFFFFFu;
 
-template <bool FUSED>
-__global__ void __launch_bounds__(256) k_join(const float* __restrict__ vec, uint32_t dim, uint32_t node0,
-                                              uint32_t node1, uint32_t cap, const uint32_t* __restrict__ newl,
-                                              const uint32_t* __restrict__ newc, const uint32_t* __restrict__ oldl,
-                                              const uint32_t* __restrict__ oldc, const float* __restrict__ thr,
-                                              Prop* __restrict__ prop, unsigned long long* __restrict__ pcount,
-                                              unsigned long long pcap, unsigned long long* __restrict__ njoin) {
+// Units of row tiles 0 .. a-1 (tile t has tot - 1 - kJR t columns).
+__device__ __forceinline__ uint32_t join_units_before(uint32_t a, uint32_t tot) {
+    return a * (tot - 1) - (kJR / 2) * a * (a - 1);
+}
+
+__host__ __device__ inline size_t join_stage_floats(uint32_t dim, uint32_t cap) {
+    return (size_t)(2 * cap + kJR) * (dim + 4);
+}
+
+__host__ __device__ inline size_t join_smem_bytes(uint32_t dim, uint32_t cap, int nbuf) {
+    return (size_t)nbuf * (join_stage_floats(dim, cap) * 4 + (size_t)2 * cap * 8);
+}
+
+template <int NBUF>
+constexpr int join_threads() {
+    return NBUF == 2 ? 512 : 256;
+}
+
+template <bool FUSED, int NBUF>
+__global__ void __launch_bounds__(join_threads<NBUF>(), NBUF == 2 ? 1 : 2) k_join(const float* __restrict__ vec, uint32_t dim, uint32_t node0,
+                                                 uint32_t node1, uint32_t cap, const uint32_t* __restrict__ newl,
+                                                 const uint32_t* __restrict__ newc, const uint32_t* __restrict__ oldl,
+                                                 const uint32_t* __restrict__ oldc, const float* __restrict__ thr,
+                                                 Prop* __restrict__ prop, unsigned long long* __restrict__ pcount,
+                                                 unsigned long long pcap, unsigned long long* __restrict__ njoin) {
     extern __shared__ __align__(16) float sm[];
     const uint32_t SP = dim + 4;
-    uint32_t* sid = (uint32_t*)(sm + (size_t)(2 * cap + kJR) * SP);
-    float* sthr = (float*)(sid + 2 * cap);
+    const size_t stage = join_stage_floats(dim, cap);
+    // stage b: rows at sm + b stage, then (after all stages) ids and thresholds
+    uint32_t* const ids0 = (uint32_t*)(sm + NBUF * stage);
+    auto rows_of = [&](int b) { return sm + b * stage; };
+    auto ids_of = [&](int b) { return ids0 + (size_t)b * 4 * cap; };
+    auto thr_of = [&](int b) { return (float*)(ids0 + (size_t)b * 4 * cap + 2 * cap); };
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const uint32_t d4 = dim >> 2;
     unsigned long long local_pairs = 0;
-    for (uint32_t node = node0 + blockIdx.x; node < node1; node += gridDim.x) {
-        const uint32_t nn = newc[node], no = oldc[node];
-        if (nn == 0) continue;  // no pairs (uniform over the block)
-        const uint32_t tot = nn + no;
-        __syncthreads();
+    unsigned long long rbase = 0, rend = 0;  // this warp's reserved proposal range (uniform over the warp)
+
+    // ids and thresholds of a node's rows (new first, then old) into stage b
+    auto load_ids = [&](uint32_t node, int b, uint32_t nn, uint32_t tot) {
         for (uint32_t r = threadIdx.x; r < tot; r += blockDim.x) {
             const uint32_t id = r < nn ? newl[(size_t)node * cap + r] : oldl[(size_t)node * cap + (r - nn)];
-            sid[r] = id;
-            sthr[r] = thr[id];
+            ids_of(b)[r] = id;
+            thr_of(b)[r] = thr[id];
         }
-        __syncthreads();
-        // the node's rows, a warp per row and 16 bytes per lane, as asynchronous
-        // copies: every row of the stage is in flight at once
+    };
+    // the rows themselves, a warp per row and 16 bytes per lane, as asynchronous copies
+    auto issue_rows = [&](int b, uint32_t tot) {
         for (uint32_t r = w; r < tot; r += nw) {
-            const float4* src = reinterpret_cast<const float4*>(vec + (size_t)sid[r] * dim);
-            float4* dst = reinterpret_cast<float4*>(sm + (size_t)r * SP);
+            const float4* src = reinterpret_cast<const float4*>(vec + (size_t)ids_of(b)[r] * dim);
+            float4* dst = reinterpret_cast<float4*>(rows_of(b) + (size_t)r * SP);
             for (uint32_t c = lane; c < d4; c += 32) {
                 const uint32_t sa = (uint32_t)__cvta_generic_to_shared(dst + c);
                 asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(src + c) : "memory");
             }
         }
         asm volatile("cp.async.commit_group;\n" ::: "memory");
-        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-        __syncthreads();
-        const uint32_t ti_n = (nn + kJR - 1) / kJR, tj_n = (tot + 31) >> 5;
-        for (uint32_t t = w; t < ti_n * tj_n; t += nw) {
-            const uint32_t i0 = (t / tj_n) * kJR, jb = (t % tj_n) << 5;
-            if (jb + 31 <= i0) continue;  // no j > i in this tile (uniform over the warp)
-            const uint32_t j = jb + lane;
-            const uint32_t jr = j < tot ? j : tot - 1;
+    };
+    // `cnt` slots for this warp's proposals (warp-uniform call): the rest of the
+    // current range first (rem slots from *b1), then a new range from *b2; the
+    // proposal at position v of the tile goes to v < rem ? b1 + v : b2 + v - rem,
+    // so only the end of the last range is left unused
+    auto reserve = [&](uint32_t cnt, unsigned long long& b1, uint32_t& rem, unsigned long long& b2) {
+        b1 = rbase;
+        rem = (uint32_t)min((unsigned long long)cnt, rend - rbase);
+        b2 = 0;
+        if (rem < cnt) {
+            const uint32_t need = cnt - rem, take = max(need, kReserve);
+            unsigned long long t0 = 0;
+            if (lane == 0) t0 = atomicAdd(pcount, (unsigned long long)take);
+            b2 = __shfl_sync(0xFFFFFFFFu, t0, 0);
+            rbase = b2 + need;
+            rend = b2 + take;
+        } else {
+            rbase += cnt;
+        }
+    };
+
+    auto compute = [&](int b, uint32_t nn, uint32_t tot) {
+        const float* R = rows_of(b);
+        const uint32_t* ids = ids_of(b);
+        const float* th = thr_of(b);
+        const uint32_t ntile = (nn + kJR - 1) / kJR;
+        const uint32_t F = join_units_before(ntile, tot);
+        const uint32_t sp4 = SP >> 2;
+        for (uint32_t f0 = 32u * w; f0 < F; f0 += 32u * nw) {
+            const uint32_t f = f0 + lane;
+            const bool live = f < F;
+            // row tile of unit f: the largest a with join_units_before(a) <= f
+            uint32_t lo = 0, hi = ntile - 1;
+            const uint32_t fc = live ? f : F - 1;
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi + 1) >> 1;
+                if (join_units_before(mid, tot) <= fc) lo = mid;
+                else hi = mid - 1;
+            }
+            const uint32_t i0 = lo * kJR;
+            const uint32_t j = i0 + 1 + (fc - join_units_before(lo, tot));
             float acc[kJR][16];
 #pragma unroll
             for (int r = 0; r < kJR; ++r)
@@ -342,27 +422,26 @@ __global__ void __launch_bounds__(256) k_join(const float* __restrict__ vec, uin
                 for (int l = 0; l < 16; ++l) acc[r][l] = 0.f;
             // rows past the staged ones (i0 + r >= tot) read the spare rows at the
             // end of the stage; their sums are never used
-            const float4* xb = reinterpret_cast<const float4*>(sm + (size_t)jr * SP);
-            const float4* xa = reinterpret_cast<const float4*>(sm + (size_t)i0 * SP);
-            const uint32_t sp4 = SP >> 2;
+            const float4* xb = reinterpret_cast<const float4*>(R + (size_t)j * SP);
+            const float4* xa = reinterpret_cast<const float4*>(R + (size_t)i0 * SP);
             for (uint32_t e4 = 0; e4 < d4; e4 += 4) {
 #pragma unroll
                 for (int c = 0; c < 4; ++c) {
-                    const float4 b = xb[e4 + c];
+                    const float4 bb = xb[e4 + c];
 #pragma unroll
                     for (int r = 0; r < kJR; ++r) {
-                        const float4 a = xa[(size_t)r * sp4 + e4 + c];
-                        acc[r][4 * c + 0] = sq_step(acc[r][4 * c + 0], a.x - b.x, FUSED);
-                        acc[r][4 * c + 1] = sq_step(acc[r][4 * c + 1], a.y - b.y, FUSED);
-                        acc[r][4 * c + 2] = sq_step(acc[r][4 * c + 2], a.z - b.z, FUSED);
-                        acc[r][4 * c + 3] = sq_step(acc[r][4 * c + 3], a.w - b.w, FUSED);
+                        const float4 aa = xa[(size_t)r * sp4 + e4 + c];
+                        acc[r][4 * c + 0] = sq_step(acc[r][4 * c + 0], aa.x - bb.x, FUSED);
+                        acc[r][4 * c + 1] = sq_step(acc[r][4 * c + 1], aa.y - bb.y, FUSED);
+                        acc[r][4 * c + 2] = sq_step(acc[r][4 * c + 2], aa.z - bb.z, FUSED);
+                        acc[r][4 * c + 3] = sq_step(acc[r][4 * c + 3], aa.w - bb.w, FUSED);
                     }
                 }
             }
             float dd[kJR];
             uint32_t emit = 0;  // bit 2r: i -> j proposal, bit 2r+1: j -> i
-            const uint32_t bj = sid[jr];
-            const float tj = sthr[jr];
+            const uint32_t bj = ids[j];
+            const float tj = th[j];
 #pragma unroll
             for (int r = 0; r < kJR; ++r) {
                 float dv = acc[r][0];
@@ -370,9 +449,9 @@ __global__ void __launch_bounds__(256) k_join(const float* __restrict__ vec, uin
                 for (int l = 1; l < 16; ++l) dv = __fadd_rn(dv, acc[r][l]);
                 dd[r] = dv;
                 const uint32_t i = i0 + r;
-                if (i < nn && j > i && j < tot && sid[i] != bj) {
+                if (live && i < nn && j > i && ids[i] != bj) {
                     local_pairs++;
-                    if (dv < sthr[i]) emit |= 1u << (2 * r);
+                    if (dv < th[i]) emit |= 1u << (2 * r);
                     if (dv < tj) emit |= 2u << (2 * r);
                 }
             }
@@ -384,25 +463,82 @@ __global__ void __launch_bounds__(256) k_join(const float* __restrict__ vec, uin
             }
             const uint32_t wt = __shfl_sync(0xFFFFFFFFu, incl, 31);
             if (wt) {
-                unsigned long long basep = 0;
-                if (lane == 0) basep = atomicAdd(pcount, (unsigned long long)wt);
-                basep = __shfl_sync(0xFFFFFFFFu, basep, 0);
-                unsigned long long p = basep + (incl - ne);
+                unsigned long long b1, b2;
+                uint32_t rem;
+                reserve(wt, b1, rem, b2);
+                uint32_t v = incl - ne;  // this lane's first position in the tile
+                auto slot = [&](uint32_t x) { return x < rem ? b1 + x : b2 + (x - rem); };
 #pragma unroll
                 for (int r = 0; r < kJR; ++r) {
-                    const uint32_t ai = sid[(i0 + r) < tot ? i0 + r : 0];
+                    const uint32_t ai = ids[(i0 + r) < tot ? i0 + r : 0];
                     if ((emit >> (2 * r)) & 1u) {
-                        if (p < pcap) prop[p] = Prop{ai, bj, dd[r]};
-                        p++;
+                        const unsigned long long q = slot(v++);
+                        if (q < pcap) prop[q] = Prop{ai, bj, dd[r]};
                     }
                     if ((emit >> (2 * r + 1)) & 1u) {
-                        if (p < pcap) prop[p] = Prop{bj, ai, dd[r]};
-                        p++;
+                        const unsigned long long q = slot(v++);
+                        if (q < pcap) prop[q] = Prop{bj, ai, dd[r]};
                     }
                 }
             }
         }
+    };
+
+    uint32_t node = node0 + blockIdx.x;
+    if constexpr (NBUF == 2) {
+        // this block's next node with new entries at or after x (uniform over the block)
+        auto next_active = [&](uint32_t x) {
+            while (x < node1 && newc[x] == 0) x += gridDim.x;
+            return x;
+        };
+        // the first node's stage, then per node: the next node's ids, wait for this
+        // node's rows, start the next node's rows, compute
+        node = next_active(node);
+        uint32_t nn = 0, tot = 0;
+        if (node < node1) {
+            nn = newc[node];
+            tot = nn + oldc[node];
+            load_ids(node, 0, nn, tot);
+        }
+        __syncthreads();
+        issue_rows(0, tot);
+        int b = 0;
+        while (node < node1) {
+            const uint32_t nxt = next_active(node + gridDim.x);
+            uint32_t nn2 = 0, tot2 = 0;
+            if (nxt < node1) {
+                nn2 = newc[nxt];
+                tot2 = nn2 + oldc[nxt];
+                load_ids(nxt, b ^ 1, nn2, tot2);
+            }
+            asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+            __syncthreads();  // this node's rows and the next node's ids are in place
+            issue_rows(b ^ 1, tot2);
+            compute(b, nn, tot);
+            __syncthreads();  // stage b is free for the node after next
+            b ^= 1;
+            node = nxt;
+            nn = nn2;
+            tot = tot2;
+        }
+        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    } else {
+        for (; node < node1; node += gridDim.x) {
+            const uint32_t nn = newc[node];
+            if (nn == 0) continue;  // no pairs (uniform over the block)
+            const uint32_t tot = nn + oldc[node];
+            __syncthreads();
+            load_ids(node, 0, nn, tot);
+            __syncthreads();
+            issue_rows(0, tot);
+            asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+            __syncthreads();
+            compute(0, nn, tot);
+        }
     }
+    // the unused end of this warp's range
+    for (unsigned long long q = rbase + lane; q < rend; q += 32)
+        if (q < pcap) prop[q].target = kNoTarget;
     atomicAdd(njoin, local_pairs);
 }
 
@@ -447,12 +583,23 @@ __global__ void k_thresholds(const uint32_t* __restrict__ hdr, const float* __re
 // The join emits a pair's proposals next to each other, so a warp's 32
 // consecutive proposals name few targets: lanes of the same target share one
 // atomic (leader adds the group's size, each lane takes its rank in the group).
-__global__ void k_bucket_count(const Prop* __restrict__ prop, unsigned long long np, uint32_t* __restrict__ tcount) {
+// Slots with target kNoTarget (the unused ends of the join's reserved ranges) are
+// skipped; `nvalid` (optional) counts the others.
+__global__ void k_bucket_count(const Prop* __restrict__ prop, unsigned long long np, uint32_t* __restrict__ tcount,
+                               unsigned long long* __restrict__ nvalid) {
     const uint32_t lt = lanemask_lt_();
+    uint32_t mine = 0;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < np; i += (size_t)gridDim.x * blockDim.x) {
         const uint32_t t = prop[i].target;
         const uint32_t peers = __match_any_sync(__activemask(), t);
-        if ((peers & lt) == 0) atomicAdd(&tcount[t], (uint32_t)__popc(peers));
+        if ((peers & lt) == 0 && t != kNoTarget) {
+            atomicAdd(&tcount[t], (uint32_t)__popc(peers));
+            mine += __popc(peers);
+        }
+    }
+    if (nvalid) {
+        for (int o = 16; o; o >>= 1) mine += __shfl_xor_sync(0xFFFFFFFFu, mine, o);
+        if ((threadIdx.x & 31) == 0 && mine) atomicAdd(nvalid, (unsigned long long)mine);
     }
 }
 
@@ -464,8 +611,10 @@ __global__ void k_bucket_fill(const Prop* __restrict__ prop, unsigned long long 
         const uint32_t peers = __match_any_sync(__activemask(), p.target);
         const int leader = __ffs(peers) - 1;
         uint32_t base = 0;
-        if ((peers & lt) == 0) base = atomicAdd(&tcur[p.target], (uint32_t)__popc(peers));
+        const bool real = p.target != kNoTarget;
+        if ((peers & lt) == 0 && real) base = atomicAdd(&tcur[p.target], (uint32_t)__popc(peers));
         base = __shfl_sync(peers, base, leader);
+        if (!real) continue;
         const uint64_t pos = toff[p.target] + base + (uint32_t)__popc(peers & lt);
         bucket[pos] = ((uint64_t)__float_as_uint(p.d) << 32) | p.source;  // d >= 0: bit order = value order
     }
@@ -563,13 +712,17 @@ __device__ uint32_t block_select(const float* Ld, uint32_t cnt, const uint64_t* 
 // reverse lists -- an inserted entry v of u's list is (v << 32 | u), an entry w it
 // pushed out (w << 32 | u | kOpRemove); at most ops_cap are written, *nops counts
 // them all.
+//
+// tlist (may be null): merge only the targets tlist[0 .. *tlist_n) (those the
+// warp merge left), instead of every target.
 __global__ void __launch_bounds__(kMT) k_merge_cta(uint32_t n, uint32_t K, const uint64_t* __restrict__ toff,
                                                    const uint64_t* __restrict__ bucket, uint32_t* __restrict__ hdr,
                                                    uint32_t* __restrict__ ids, float* __restrict__ dist,
                                                    uint8_t* __restrict__ isnew, unsigned long long* __restrict__ nupd,
                                                    uint32_t* __restrict__ next_t, uint64_t* __restrict__ ops,
                                                    unsigned long long* __restrict__ nops,
-                                                   unsigned long long ops_cap) {
+                                                   unsigned long long ops_cap, const uint32_t* __restrict__ tlist,
+                                                   const uint32_t* __restrict__ tlist_n) {
     extern __shared__ __align__(16) char smraw[];
     uint64_t* surv = (uint64_t*)smraw;
     uint32_t* hk = (uint32_t*)(surv + kMS);
@@ -584,12 +737,13 @@ __global__ void __launch_bounds__(kMT) k_merge_cta(uint32_t n, uint32_t K, const
     const int tid = threadIdx.x;
     const uint32_t W = merge_window(K);
     unsigned long long upd = 0;
+    const uint32_t nt = tlist ? *tlist_n : n;
     for (;;) {
         __syncthreads();
         if (tid == 0) ctl[0] = atomicAdd(next_t, 1u);
         __syncthreads();
-        const uint32_t u = ctl[0];
-        if (u >= n) break;
+        if (ctl[0] >= nt) break;
+        const uint32_t u = tlist ? tlist[ctl[0]] : ctl[0];
         const uint64_t pb = toff[u], pe = toff[u + 1];
         if (pb == pe) continue;
         float* Ld = LdA;
@@ -757,6 +911,174 @@ __global__ void __launch_bounds__(kMT) k_merge_cta(uint32_t n, uint32_t K, const
     if ((tid & 31) == 0 && upd) atomicAdd(nupd, upd);
 }
 
+// One warp per target with proposals (targets handed out by *next_t): the
+// CTA merge's result without block-wide steps, for targets whose proposals below
+// the farthest entry (after the first filter) number at most kWS -- the common
+// case once lists are full.  Survivors (d < farthest entry of a full list) are
+// sorted by (d, source) in shared memory (bitonic, warp-synchronous); repeats are
+// adjacent, and a listed source is found among the list entries of exactly its
+// distance (a pair's distance is a pure function of the pair, so a listed
+// source carries the same distance); each survivor goes after the list entries
+// of distance <= its own, each list entry after the survivors below it, and the
+// first K are kept.  Targets with more survivors are listed in ovl for the CTA
+// merge, their lists untouched.
+constexpr uint32_t kWS = 1024;  // survivors a warp merge holds
+constexpr int kWW = 8;          // warps per block of the warp merge
+
+__host__ __device__ inline size_t merge_warp_bytes(uint32_t K) {
+    return (size_t)kWS * 8 + (((size_t)K * 9 + 15) & ~(size_t)15);
+}
+
+__global__ void __launch_bounds__(kWW * 32) k_merge_warp(uint32_t n, uint32_t K, const uint64_t* __restrict__ toff,
+                                                         const uint64_t* __restrict__ bucket,
+                                                         uint32_t* __restrict__ hdr, uint32_t* __restrict__ ids,
+                                                         float* __restrict__ dist, uint8_t* __restrict__ isnew,
+                                                         unsigned long long* __restrict__ nupd,
+                                                         uint32_t* __restrict__ next_t, uint32_t* __restrict__ ovl,
+                                                         uint32_t* __restrict__ n_ovl) {
+    extern __shared__ __align__(16) char smraw[];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    char* base = smraw + (size_t)w * merge_warp_bytes(K);
+    uint64_t* sk = (uint64_t*)base;  // survivor keys: d bits << 32 | source
+    float* Ld = (float*)(base + (size_t)kWS * 8);
+    uint32_t* Li = (uint32_t*)(Ld + K);
+    uint8_t* Lf = (uint8_t*)(Li + K);
+    const uint32_t lt = lanemask_lt_();
+    unsigned long long upd = 0;
+    for (;;) {
+        uint32_t u = 0;
+        if (lane == 0) u = atomicAdd(next_t, 1u);
+        u = __shfl_sync(0xFFFFFFFFu, u, 0);
+        if (u >= n) break;
+        const uint64_t pb = toff[u], pe = toff[u + 1];
+        if (pb == pe) continue;
+        const uint32_t cnt = hdr[u] & 0xFFFFu;
+        const float worst = cnt >= K ? dist[(size_t)u * K + cnt - 1] : FLT_MAX;
+        __syncwarp();  // the previous target's reads of sk / Ld are done
+        // survivors: proposals below the farthest entry of a full list
+        uint32_t S = 0;
+        bool over = false;
+        for (uint64_t x0 = pb; x0 < pe; x0 += 32) {
+            const uint64_t x = x0 + lane;
+            uint64_t key = 0;
+            bool keep = false;
+            if (x < pe) {
+                key = bucket[x];
+                keep = __uint_as_float((uint32_t)(key >> 32)) < worst;
+            }
+            const uint32_t bal = __ballot_sync(0xFFFFFFFFu, keep);
+            if (S + __popc(bal) > kWS) {
+                over = true;
+                break;
+            }
+            if (keep) sk[S + __popc(bal & lt)] = key;
+            S += __popc(bal);
+        }
+        if (over) {
+            if (lane == 0) ovl[atomicAdd(n_ovl, 1u)] = u;
+            continue;
+        }
+        if (S == 0) continue;
+        // sort the survivors (bitonic over PP >= S slots, padding ~0)
+        uint32_t PP = 32;
+        while (PP < S) PP <<= 1;
+        for (uint32_t i = S + lane; i < PP; i += 32) sk[i] = ~0ull;
+        for (uint32_t j = lane; j < cnt; j += 32) {
+            Ld[j] = dist[(size_t)u * K + j];
+            Li[j] = ids[(size_t)u * K + j];
+            Lf[j] = isnew ? isnew[(size_t)u * K + j] : 0;
+        }
+        __syncwarp();
+        for (uint32_t k = 2; k <= PP; k <<= 1)
+            for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+                for (uint32_t t = lane; t < PP / 2; t += 32) {
+                    const uint32_t i = ((t & ~(j - 1)) << 1) | (t & (j - 1)), y = i | j;
+                    const uint64_t a = sk[i], b = sk[y];
+                    if ((a > b) == ((i & k) == 0)) {
+                        sk[i] = b;
+                        sk[y] = a;
+                    }
+                }
+                __syncwarp();
+            }
+        // drop repeats (adjacent after the sort) and listed sources, compacting in
+        // place (a write never passes the read position of a later round: the key
+        // before a round's first is carried in a register)
+        uint32_t C = 0;
+        uint64_t carry = ~0ull;
+        for (uint32_t i0 = 0; i0 < S; i0 += 32) {
+            const uint32_t i = i0 + lane;
+            const uint64_t key = i < S ? sk[i] : ~0ull;
+            uint64_t prev = __shfl_up_sync(0xFFFFFFFFu, key, 1);
+            if (lane == 0) prev = carry;
+            carry = __shfl_sync(0xFFFFFFFFu, key, 31);
+            bool keep = i < S && key != prev;
+            if (keep) {
+                const float d = __uint_as_float((uint32_t)(key >> 32));
+                uint32_t lo = 0, hi = cnt;  // list entries with distance <= d
+                while (lo < hi) {
+                    const uint32_t mid = (lo + hi) >> 1;
+                    if (Ld[mid] <= d) lo = mid + 1;
+                    else hi = mid;
+                }
+                for (int k2 = (int)lo - 1; k2 >= 0 && Ld[k2] == d; --k2)
+                    if (Li[k2] == (uint32_t)key) {
+                        keep = false;
+                        break;
+                    }
+            }
+            const uint32_t bal = __ballot_sync(0xFFFFFFFFu, keep);
+            __syncwarp();
+            if (keep) sk[C + __popc(bal & lt)] = key;
+            C += __popc(bal);
+            __syncwarp();
+        }
+        if (C == 0) continue;
+        const uint32_t ncnt = min(cnt + C, K);
+        // survivor x goes to x + (list entries with distance <= its own)
+        uint32_t first = K;  // the first position that changes
+        for (uint32_t x = lane; x < C; x += 32) {
+            const uint64_t key = sk[x];
+            const float d = __uint_as_float((uint32_t)(key >> 32));
+            uint32_t lo = 0, hi = cnt;
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (Ld[mid] <= d) lo = mid + 1;
+                else hi = mid;
+            }
+            const uint32_t pos = x + lo;
+            first = min(first, pos);
+            if (pos < ncnt) {
+                dist[(size_t)u * K + pos] = d;
+                ids[(size_t)u * K + pos] = (uint32_t)key;
+                if (isnew) isnew[(size_t)u * K + pos] = 1;
+                upd++;
+            }
+        }
+        for (int o = 16; o; o >>= 1) first = min(first, __shfl_xor_sync(0xFFFFFFFFu, first, o));
+        // list entry j (at or after the first change) goes to j + (survivors below it)
+        for (uint32_t j = first + lane; j < cnt; j += 32) {
+            const float d = Ld[j];
+            const uint64_t bound = (uint64_t)__float_as_uint(d) << 32;
+            uint32_t lo = 0, hi = C;
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (sk[mid] < bound) lo = mid + 1;
+                else hi = mid;
+            }
+            const uint32_t pos = j + lo;
+            if (pos < ncnt) {
+                dist[(size_t)u * K + pos] = d;
+                ids[(size_t)u * K + pos] = Li[j];
+                if (isnew) isnew[(size_t)u * K + pos] = Lf[j];
+            }
+        }
+        if (lane == 0) hdr[u] = (hdr[u] & 0xFFFF0000u) | ncnt;
+    }
+    for (int o = 16; o; o >>= 1) upd += __shfl_xor_sync(0xFFFFFFFFu, upd, o);
+    if (lane == 0 && upd) atomicAdd(nupd, upd);
+}
+
 // Groups np proposals by target (count, scan, scatter of (d, source) keys) and
 // merges each target's group into its list (k_merge_cta).  tcount / toff / tcur
 // hold n + 1 entries; `mid` is recorded between the grouping and the merge.
@@ -764,19 +1086,38 @@ void bucket_and_merge(uint32_t n, uint32_t K, const Prop* prop, unsigned long lo
                       DevMem& tcur, uint64_t* bucket, DevMem& tmp, uint32_t* hdr, uint32_t* ids, float* dist,
                       uint8_t* isnew, unsigned long long* d_nupd, uint32_t* d_nextt, size_t merge_smem,
                       unsigned merge_grid, int nsm, cudaStream_t s, cudaEvent_t mid, uint64_t* ops = nullptr,
-                      unsigned long long* nops = nullptr, unsigned long long ops_cap = 0) {
+                      unsigned long long* nops = nullptr, unsigned long long ops_cap = 0,
+                      unsigned long long* nvalid = nullptr) {
     CUDA_CHECK(cudaMemsetAsync(tcount.p, 0, ((size_t)n + 1) * 4, s));
     CUDA_CHECK(cudaMemsetAsync(tcur.p, 0, ((size_t)n + 1) * 4, s));
     const unsigned gb = (unsigned)std::min<unsigned long long>((np + 255) / 256, (unsigned long long)nsm * 32);
-    k_bucket_count<<<gb, 256, 0, s>>>(prop, np, tcount.as<uint32_t>());
+    k_bucket_count<<<gb, 256, 0, s>>>(prop, np, tcount.as<uint32_t>(), nvalid);
     CUDA_LAUNCH_CHECK();
     exclusive_scan_u32_to_u64(tcount.as<uint32_t>(), toff.as<uint64_t>(), (size_t)n + 1, s, tmp);
     k_bucket_fill<<<gb, 256, 0, s>>>(prop, np, toff.as<uint64_t>(), tcur.as<uint32_t>(), bucket);
     CUDA_LAUNCH_CHECK();
     if (mid) CUDA_CHECK(cudaEventRecord(mid, s));
     CUDA_CHECK(cudaMemsetAsync(d_nextt, 0, 4, s));
-    k_merge_cta<<<merge_grid, kMT, merge_smem, s>>>(n, K, toff.as<uint64_t>(), bucket, hdr, ids, dist, isnew, d_nupd,
-                                                    d_nextt, ops, nops, ops_cap);
+    if (!ops && merge_warp_bytes(K) * kWW <= 227 * 1024) {
+        // warp merge for every target, then the CTA merge for the targets it left
+        // (tcur and tcount are free after the scatter: the left targets and their count)
+        static int per_sm = 0;
+        const size_t wsm = merge_warp_bytes(K) * kWW;
+        CUDA_CHECK(cudaFuncSetAttribute(k_merge_warp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm));
+        if (!per_sm) CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_merge_warp, kWW * 32, wsm));
+        uint32_t* left = tcur.as<uint32_t>();
+        uint32_t* n_left = tcount.as<uint32_t>();
+        CUDA_CHECK(cudaMemsetAsync(n_left, 0, 4, s));
+        k_merge_warp<<<(unsigned)(nsm * std::max(per_sm, 1)), kWW * 32, wsm, s>>>(
+            n, K, toff.as<uint64_t>(), bucket, hdr, ids, dist, isnew, d_nupd, d_nextt, left, n_left);
+        CUDA_LAUNCH_CHECK();
+        CUDA_CHECK(cudaMemsetAsync(d_nextt, 0, 4, s));
+        k_merge_cta<<<merge_grid, kMT, merge_smem, s>>>(n, K, toff.as<uint64_t>(), bucket, hdr, ids, dist, isnew,
+                                                        d_nupd, d_nextt, nullptr, nullptr, 0, left, n_left);
+    } else {
+        k_merge_cta<<<merge_grid, kMT, merge_smem, s>>>(n, K, toff.as<uint64_t>(), bucket, hdr, ids, dist, isnew,
+                                                        d_nupd, d_nextt, ops, nops, ops_cap, nullptr, nullptr);
+    }
     CUDA_LAUNCH_CHECK();
 }
 
@@ -1036,17 +1377,41 @@ void refine_knng(Index& ix, int iters, int sample) {
     unsigned long long* d_njoin = ctr.as<unsigned long long>() + 1;
     unsigned long long* d_nupd = ctr.as<unsigned long long>() + 2;
     uint32_t* d_nextt = (uint32_t*)(ctr.as<unsigned long long>() + 3);  // merge work counter
-    unsigned long long* d_pcount = ctr.as<unsigned long long>();  // proposal count of a chunk
+    unsigned long long* d_pcount = ctr.as<unsigned long long>();  // proposal slots of a chunk
+    unsigned long long* d_nprop = ctr.as<unsigned long long>() + 5;  // proposals of the iteration
     const bool fast = ix.order.lanes == 16 && ix.dim % 16 == 0;
     // Tensor-core screened join where the dims and sample sizes allow it.
     const bool tcj = fast && ix.join_mode != kJoinExact && join_tc_supported((uint32_t)ix.dim, cap);
     JoinTcCounters* d_jc = reinterpret_cast<JoinTcCounters*>(ctr.as<char>() + 64);
-    const size_t join_smem = (size_t)(2 * cap + kJR) * (ix.dim + 4) * 4 + (size_t)2 * cap * 8;
+    // The exact join's two forms: two stages (the next node's rows copied during
+    // the current node's pairs) for iterations with many pairs per node, where two
+    // stages fit in shared memory; one stage otherwise.  Both persistent (every
+    // block resident).
+    const bool jf = (ix.order.fused & 1) != 0;
+    const bool join2_fits = join_smem_bytes((uint32_t)ix.dim, cap, 2) <= 227 * 1024;
+    const size_t join_smem1 = join_smem_bytes((uint32_t)ix.dim, cap, 1);
+    const size_t join_smem2 = join_smem_bytes((uint32_t)ix.dim, cap, 2);
+    auto kj1 = jf ? k_join<true, 1> : k_join<false, 1>;
+    auto kj2 = jf ? k_join<true, 2> : k_join<false, 2>;
+    unsigned join_grid1 = (unsigned)nsm, join_grid2 = (unsigned)nsm;
     if (fast) {
-        auto kj = (ix.order.fused & 1) ? k_join<true> : k_join<false>;
-        if (join_smem > 227 * 1024) fail(HRNN_ERR_ARG, "refineKNNG: sample size too large for dim");
-        CUDA_CHECK(cudaFuncSetAttribute(kj, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)join_smem));
+        if (join_smem1 > 227 * 1024) fail(HRNN_ERR_ARG, "refineKNNG: sample size too large for dim");
+        int per_sm = 1;
+        CUDA_CHECK(cudaFuncSetAttribute(kj1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)join_smem1));
+        CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kj1, join_threads<1>(), join_smem1));
+        join_grid1 = (unsigned)(nsm * std::max(per_sm, 1));
+        if (join2_fits) {
+            CUDA_CHECK(cudaFuncSetAttribute(kj2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)join_smem2));
+            CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kj2, join_threads<2>(), join_smem2));
+            join_grid2 = (unsigned)(nsm * std::max(per_sm, 1));
+        }
     }
+    // Chunk sizing: proposals per join pair of the last accepted chunk (0 until
+    // one is known), so a chunk aims at 70 % of the target even when the pairs per
+    // node jump between iterations (a chunk over the buffer is computed twice).
+    // Fewer, larger chunks are cheaper: every merge pass reads and writes the
+    // lists of all targets it touches.
+    double prop_per_pair = 0.0;
     const size_t merge_smem = merge_cta_bytes(K);
     if (merge_smem > 227 * 1024 || merge_window(K) < 256)
         fail(HRNN_ERR_ARG, "refineKNNG: K_knng too large for the merge kernel");
@@ -1098,16 +1463,22 @@ void refine_knng(Index& ix, int iters, int sample) {
                                              ctr.as<unsigned long long>() + 4);
         CUDA_LAUNCH_CHECK();
         CUDA_CHECK(cudaEventRecord(ev[2], s));
-        // |new| + |old| summed over nodes (gather bytes of the join)
-        unsigned long long sample_entries = 0;
-        CUDA_CHECK(cudaMemcpyAsync(&sample_entries, ctr.as<unsigned long long>() + 4, 8, cudaMemcpyDeviceToHost, s));
+        // |new| + |old| summed over nodes (gather bytes of the join) and the join's pairs
+        unsigned long long sc[3] = {0, 0, 0};
+        CUDA_CHECK(cudaMemcpyAsync(sc, ctr.as<unsigned long long>() + 4, 24, cudaMemcpyDeviceToHost, s));
         CUDA_CHECK(cudaStreamSynchronize(s));
+        const unsigned long long sample_entries = sc[0];
+        const double pairs_per_node = (double)sc[2] / (double)n;
         t_sample = elapsed(e0, ev[2]);
-        unsigned long long proposals = 0;
         unsigned long long njoin_ok = 0;  // pair count after the last accepted chunk
+        unsigned long long nprop_ok = 0;  // proposal count after the last accepted chunk
         JoinTcCounters jc_ok{};           // screen counts after the last accepted chunk
+        const bool join2 = join2_fits && pairs_per_node >= 1000.0;
         // ---- phase 2, chunk by chunk ----
         for (uint32_t node0 = 0; node0 < n;) {
+            if (prop_per_pair > 0.0 && pairs_per_node > 0.0)
+                chunk = (uint32_t)std::max(1.0, std::min((double)n, 0.7 * (double)ptarget /
+                                                                       (prop_per_pair * pairs_per_node)));
             uint32_t node1 = std::min<uint32_t>(n, node0 + chunk);
             k_thresholds<<<(n + 255) / 256, 256, 0, s>>>(hdr, dist, n, K, thr.as<float>());
             CUDA_LAUNCH_CHECK();
@@ -1120,11 +1491,16 @@ void refine_knng(Index& ix, int iters, int sample) {
                         prop.as<Prop>(), d_pcount, pcap, d_njoin, d_jc, (ix.order.fused & 1) != 0, ix.join_mode, nsm,
                         s);
             } else if (fast) {
-                auto kj = (ix.order.fused & 1) ? k_join<true> : k_join<false>;
-                kj<<<grid, 256, join_smem, s>>>(ix.vec.as<float>(), (uint32_t)ix.dim, node0, node1, cap,
-                                                newl.as<uint32_t>(), newc.as<uint32_t>(), oldl.as<uint32_t>(),
-                                                oldc.as<uint32_t>(), thr.as<float>(), prop.as<Prop>(), d_pcount, pcap,
-                                                d_njoin);
+                if (join2)
+                    kj2<<<std::min<unsigned>(node1 - node0, join_grid2), join_threads<2>(), join_smem2, s>>>(
+                        ix.vec.as<float>(), (uint32_t)ix.dim, node0, node1, cap, newl.as<uint32_t>(),
+                        newc.as<uint32_t>(), oldl.as<uint32_t>(), oldc.as<uint32_t>(), thr.as<float>(),
+                        prop.as<Prop>(), d_pcount, pcap, d_njoin);
+                else
+                    kj1<<<std::min<unsigned>(node1 - node0, join_grid1), join_threads<1>(), join_smem1, s>>>(
+                        ix.vec.as<float>(), (uint32_t)ix.dim, node0, node1, cap, newl.as<uint32_t>(),
+                        newc.as<uint32_t>(), oldl.as<uint32_t>(), oldc.as<uint32_t>(), thr.as<float>(),
+                        prop.as<Prop>(), d_pcount, pcap, d_njoin);
             } else {
                 k_join_generic<<<grid, 128, 0, s>>>(ix.vec.as<float>(), (uint32_t)ix.dim, ix.order.lanes,
                                                     ix.order.fused, node0, node1, cap, newl.as<uint32_t>(),
@@ -1146,27 +1522,35 @@ void refine_knng(Index& ix, int iters, int sample) {
                 CUDA_CHECK(cudaStreamSynchronize(s));
                 continue;
             }
+            const unsigned long long njoin_prev = njoin_ok, nprop_prev = nprop_ok;
             CUDA_CHECK(cudaMemcpyAsync(&njoin_ok, d_njoin, 8, cudaMemcpyDeviceToHost, s));
             if (tcj) CUDA_CHECK(cudaMemcpyAsync(&jc_ok, d_jc, sizeof(jc_ok), cudaMemcpyDeviceToHost, s));
             if (np) {
                 bucket_and_merge(n, K, prop.as<Prop>(), np, tcount, toff, tcur, bucket.as<uint64_t>(), tmp, hdr, ids,
-                                 dist, isnew.as<uint8_t>(), d_nupd, d_nextt, merge_smem, merge_grid, nsm, s, ev[6]);
+                                 dist, isnew.as<uint8_t>(), d_nupd, d_nextt, merge_smem, merge_grid, nsm, s, ev[6],
+                                 nullptr, nullptr, 0, d_nprop);
                 CUDA_CHECK(cudaEventRecord(ev[5], s));
                 CUDA_CHECK(cudaEventSynchronize(ev[5]));
                 t_bucket += elapsed(ev[4], ev[6]);
                 t_merge += elapsed(ev[6], ev[5]);
             }
-            proposals += np;
             node0 = node1;
-            // Keep the chunk's proposals between a quarter and three quarters of
-            // the buffer (the size carries over to the next iteration).
-            if (np < ptarget / 4 && chunk < n) chunk = std::min<uint32_t>(n, chunk * 2);
-            else if (np > ptarget / 4 * 3 && chunk > 1) chunk /= 2;
+            CUDA_CHECK(cudaMemcpyAsync(&nprop_ok, d_nprop, 8, cudaMemcpyDeviceToHost, s));
+            CUDA_CHECK(cudaStreamSynchronize(s));
+            const unsigned long long chunk_props = nprop_ok - nprop_prev, chunk_pairs = njoin_ok - njoin_prev;
+            if (chunk_props && chunk_pairs) {
+                prop_per_pair = (double)chunk_props / (double)chunk_pairs;
+            } else if (prop_per_pair == 0.0) {
+                // no rate yet: keep the chunk's proposals between a quarter and three
+                // quarters of the target
+                if (chunk_props < ptarget / 4 && chunk < n) chunk = std::min<uint32_t>(n, chunk * 2);
+                else if (chunk_props > ptarget / 4 * 3 && chunk > 1) chunk /= 2;
+            }
         }
-        unsigned long long hc[3] = {0, 0, 0};
+        unsigned long long hc[6] = {0, 0, 0, 0, 0, 0};
         JoinTcCounters hj{};
         CUDA_CHECK(cudaEventRecord(e1, s));
-        CUDA_CHECK(cudaMemcpyAsync(hc, ctr.p, 24, cudaMemcpyDeviceToHost, s));
+        CUDA_CHECK(cudaMemcpyAsync(hc, ctr.p, 48, cudaMemcpyDeviceToHost, s));
         CUDA_CHECK(cudaMemcpyAsync(&hj, d_jc, sizeof(hj), cudaMemcpyDeviceToHost, s));
         CUDA_CHECK(cudaStreamSynchronize(s));
         if (hj.err) fail(HRNN_ERR_TIMEOUT, "refineKNNG: tensor-core join: wait on the MMA commit expired");
@@ -1179,7 +1563,7 @@ void refine_knng(Index& ix, int iters, int sample) {
             rs.iters = it + 1;
             rs.join_dists[it] = hc[1];
             rs.updates[it] = hc[2];
-            rs.proposals[it] = proposals;
+            rs.proposals[it] = hc[5];
             rs.sample_entries[it] = sample_entries;
             rs.ms[it] = ms;
             rs.sample_ms[it] = t_sample;

@@ -131,7 +131,7 @@ __global__ void __launch_bounds__(128) k_phase_a(DevView v, const float* __restr
 //   resume: start from the stored beam instead of the descent (its ids seed the
 //     visited cache), continue with the query's own ef, store nothing.
 template <int DM, bool R2>
-__global__ void __launch_bounds__(128) k_phase_a_fast(DevView v, const float* __restrict__ Q, uint32_t nq,
+__global__ void __launch_bounds__(128, R2 ? 4 : 1) k_phase_a_fast(DevView v, const float* __restrict__ Q, uint32_t nq,
                                                       const uint32_t* __restrict__ qm,
                                                       const uint32_t* __restrict__ qef, uint32_t efc, uint32_t vc,
                                                       uint32_t mmax, uint32_t* __restrict__ prox,
@@ -548,7 +548,7 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
         // (The two-parent search reads link rows of at most 33 words, maxM0 <= 32.)
         const bool fast = (int8 || mixed) && v.W0 <= 33;
         const int dm = int8 ? 3 : mixed ? 2 : fusedsimd ? 1 : 0;
-        // r2: the INT8 two-parent search scores two rows per lane (a launch-shape choice)
+        // r2: the INT8 two-parent search loads all 64 rows of a step at once (a launch-shape choice)
         bool r2 = false;
         auto kfun_of = [&](bool two) {
             return fast ? (dm == 3 ? (two ? (const void*)k_phase_a_fast<3, true> : (const void*)k_phase_a_fast<3, false>)

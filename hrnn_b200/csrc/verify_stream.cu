@@ -5,8 +5,8 @@
 // where it is read.  The postings are cut into chunks of kChunk (a proxy's prefix
 // into several when it is long), and persistent warps take chunks from a counter,
 // so one query with a proxy of a very long reverse list is spread over many warps
-// instead of holding one.  Per posting, one candidate row per lane: the INT8
-// screen first (the query's INT8 copy in shared memory, dp4a against the row); the
+// instead of holding one.  Per posting the INT8 screen first (rows read by eight
+// lanes each, four rows per load instruction, dp4a against the query); the
 // few rows it cannot decide in exact FP32 (the reference's order, a half-warp per
 // row) and, inside kTieUlps of the radius, in FP64.  An owner listed by several
 // proxies is verified once per listing -- the same decision each time.
@@ -20,6 +20,8 @@
 // listed for the overflow pass, which answers it from scratch.
 #include <algorithm>
 #include <cfloat>
+#include <cstdlib>
+#include <type_traits>
 
 #include "beam.cuh"
 #include "index.hpp"
@@ -205,41 +207,57 @@ __device__ __noinline__ void stream_undecided(const DevView& v, const float* __r
     __syncwarp();
 }
 
-// Two steps of 32 postings (owner ids a and b of this lane) through the INT8
-// screen with the loads of both rows issued before either dot product: 1 accept,
-// 0 reject, -1 undecided for each.  meta.w holds kdist(p, k-1) of this call.
-template <int NB>
-__device__ __forceinline__ void stream_screen2(const DevView& v, const int* q8, float4 qv, uint32_t ida, bool la,
-                                               uint32_t idb, bool lb, int& da, int& db) {
+// S steps of 32 postings through the INT8 screen, the loads of all S steps' rows
+// issued before any dot product: 1 accept, 0 reject, -1 undecided each; meta.w
+// holds kdist(p, k-1) of this call.  The rows are read cooperatively
+// (coop_i8_load): eight rounds of four whole rows per load instruction per step
+// instead of 32 rows touched per instruction -- the one-row-per-lane form kept
+// the L1 saturated with line lookups.  cid: the owner ids of the steps (32 per
+// step, shared memory); out: the id this lane decides in each step, posting
+// coop_row() of the step (live[s]: whether that posting exists).  qw: this lane's
+// query words (coop_q_words).
+template <int NB, int S>
+__device__ __forceinline__ void stream_screen_coop(const DevView& v, int4 qw, float4 qv, const uint32_t* cid,
+                                                   const bool (&live)[S], uint32_t (&out)[S], int (&dec)[S]) {
     constexpr uint32_t dim = NB * 16;
-    const int4* xa = reinterpret_cast<const int4*>(v.vec_i8 + (size_t)ida * dim);
-    const int4* xb = reinterpret_cast<const int4*>(v.vec_i8 + (size_t)idb * dim);
-    int4 ra[NB], rb[NB];
+    const int g = (threadIdx.x >> 3) & 3;
+    const uint32_t r = coop_row();
+    int4 x[S][8];
 #pragma unroll
-    for (int c = 0; c < NB; ++c) ra[c] = __ldg(xa + c);
+    for (int k = 0; k < S; ++k) {
+        out[k] = cid[32 * k + r];
 #pragma unroll
-    for (int c = 0; c < NB; ++c) rb[c] = __ldg(xb + c);
-    const float4 ma = __ldg(v.i8_meta + ida), mb = __ldg(v.i8_meta + idb);
-    int sa = 0, sb = 0;
-#pragma unroll
-    for (int c = 0; c < NB; ++c) {
-        sa = __dp4a(ra[c].x, q8[4 * c + 0], sa);
-        sa = __dp4a(ra[c].y, q8[4 * c + 1], sa);
-        sa = __dp4a(ra[c].z, q8[4 * c + 2], sa);
-        sa = __dp4a(ra[c].w, q8[4 * c + 3], sa);
-        sb = __dp4a(rb[c].x, q8[4 * c + 0], sb);
-        sb = __dp4a(rb[c].y, q8[4 * c + 1], sb);
-        sb = __dp4a(rb[c].z, q8[4 * c + 2], sb);
-        sb = __dp4a(rb[c].w, q8[4 * c + 3], sb);
+        for (int i = 0; i < 8; ++i) x[k][i] = coop_i8_load<NB>(v.vec_i8, cid[32 * k + 4 * i + g]);
     }
-    const float Da = qv.x + ma.x * ma.x * ma.z - 2.f * qv.y * ma.x * (float)sa;
-    const float Db = qv.x + mb.x * mb.x * mb.z - 2.f * qv.y * mb.x * (float)sb;
-    da = la ? i8_decide(Da, ma.w, qv, ma, dim) : 0;
-    db = lb ? i8_decide(Db, mb.w, qv, mb, dim) : 0;
+    float4 m[S];
+#pragma unroll
+    for (int k = 0; k < S; ++k) m[k] = __ldg(v.i8_meta + out[k]);
+#pragma unroll
+    for (int k = 0; k < S; ++k) {
+        int pp[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) pp[i] = dp4a4(x[k][i], qw);
+        const int dot = coop_sum8(pp);
+        const float D = qv.x + m[k].x * m[k].x * m[k].z - 2.f * qv.y * m[k].x * (float)dot;
+        dec[k] = live[k] ? i8_decide(D, m[k].w, qv, m[k], dim) : 0;
+    }
 }
 
-template <class E, bool FUSED, int NB>
-__global__ void __launch_bounds__(256, 2) k_verify_chunks(
+// S: steps of 32 postings in flight per warp (2: more loads in flight per warp;
+// 1: fewer registers, more resident warps -- the default).
+template <int S>
+constexpr int verify_min_blocks() {
+    return S == 2 ? 2 : 4;
+}
+
+// Per-warp shared memory: FP32 query | undecided ids of a step (32) | the
+// chunk's owner ids (kChunk).
+__host__ __device__ constexpr size_t verify_warp_smem(uint32_t dim) {
+    return (size_t)dim * 4 + 32 * 4 + kChunk * 4;
+}
+
+template <class E, bool FUSED, int NB, int S>
+__global__ void __launch_bounds__(256, verify_min_blocks<S>()) k_verify_chunks(
     DevView v, const float* __restrict__ Q, uint32_t mmax, const uint32_t* __restrict__ prox,
     const uint32_t* __restrict__ plen, const uint64_t* __restrict__ res_off, const float* __restrict__ kcol,
     uint32_t kidx, const int8_t* __restrict__ qq, const float4* __restrict__ qmeta,
@@ -249,13 +267,14 @@ __global__ void __launch_bounds__(256, 2) k_verify_chunks(
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     constexpr uint32_t dim = NB * 16;
     constexpr int kSteps = kChunk / 32;
-    char* base = smraw + (size_t)w * (dim * 4 + dim + 32 * 4);
+    char* base = smraw + (size_t)w * verify_warp_smem(dim);
     float* q = (float*)base;                  // FP32 query (loaded when a row needs the exact test)
-    int* q8 = (int*)(q + dim);                // INT8 query words
-    uint32_t* st = (uint32_t*)(q8 + dim / 4);  // undecided ids of a step
+    uint32_t* st = (uint32_t*)(q + dim);      // undecided ids of a step
+    uint32_t* cid = st + 32;                  // owner ids of the chunk
     const uint64_t nch = *nchunks;
     uint32_t cur_q = kInvalid, f32_q = kInvalid;
     float4 qv = make_float4(0.f, 0.f, 0.f, 0.f);
+    int4 qw = make_int4(0, 0, 0, 0);  // this lane's INT8 query words (the cooperative row reads)
     unsigned long long c_post = 0, c_lowp8 = 0;  // the streaming loop's own counters stay in registers
     StreamCount cn;                              // the undecided path's
     for (;;) {
@@ -270,37 +289,43 @@ __global__ void __launch_bounds__(256, 2) k_verify_chunks(
         const uint32_t e1 = min(e0 + kChunk, len);
         const uint32_t p = prox[t];
         const uint64_t b = v.csr_off[p];
-        // every owner id of the chunk in one round trip (kSteps per lane)
-        uint32_t ids[kSteps];
+        const uint32_t nsteps = (e1 - e0 + 31) / 32;
+        __syncwarp();  // the previous chunk's ids are no longer read
+        // every owner id of the chunk in one round trip; postings past the end read
+        // the proxy's own row (valid, never decided)
 #pragma unroll
         for (int j = 0; j < kSteps; ++j) {
             const uint32_t e = e0 + lane + 32 * j;
-            ids[j] = e < e1 ? (uint32_t)(((const E*)v.csr_ent)[b + e] >> v.rank_bits) : p;
+            if ((uint32_t)j < ((nsteps + S - 1) / S) * S)
+                cid[lane + 32 * j] = e < e1 ? (uint32_t)(((const E*)v.csr_ent)[b + e] >> v.rank_bits) : p;
         }
         if (qi != cur_q) {
-            __syncwarp();
-            if ((uint32_t)lane < dim / 4) q8[lane] = reinterpret_cast<const int*>(qq + (size_t)qi * dim)[lane];
             qv = qmeta[qi];
+            qw = (lane & 7) < NB ? reinterpret_cast<const int4*>(qq + (size_t)qi * dim)[lane & 7]
+                                 : make_int4(0, 0, 0, 0);
             cur_q = qi;
-            __syncwarp();
         }
+        __syncwarp();
         if (lane == 0) c_post += e1 - e0;
-        const uint32_t nsteps = (e1 - e0 + 31) / 32;
+#pragma unroll 1
+        for (uint32_t j = 0; j < nsteps; j += S) {
+            // this lane decides posting coop_row() of each step
+            bool live[S];
+            uint32_t id[S];
+            int dec[S];
 #pragma unroll
-        for (int j = 0; j < kSteps; j += 2) {
-            if ((uint32_t)j >= nsteps) break;
-            const bool la = e0 + lane + 32 * j < e1, lb = e0 + lane + 32 * (j + 1) < e1;
-            int da, db;
-            stream_screen2<NB>(v, q8, qv, ids[j], la, ids[j + 1], lb, da, db);
-            c_lowp8 += (uint32_t)(da >= 0 && la) + (uint32_t)(db >= 0 && lb);
-            stream_accept(da == 1, ids[j], qi, res_off, acc_cnt, resbuf);
-            stream_accept(db == 1, ids[j + 1], qi, res_off, acc_cnt, resbuf);
-            if (__any_sync(0xFFFFFFFFu, da < 0))
-                stream_undecided<FUSED, NB>(v, Q, qi, da, ids[j], q, st, f32_q, kcol, kidx, res_off, acc_cnt,
-                                            resbuf, cn);
-            if (__any_sync(0xFFFFFFFFu, db < 0))
-                stream_undecided<FUSED, NB>(v, Q, qi, db, ids[j + 1], q, st, f32_q, kcol, kidx, res_off, acc_cnt,
-                                            resbuf, cn);
+            for (int k = 0; k < S; ++k) live[k] = e0 + coop_row() + 32 * (j + k) < e1;
+            stream_screen_coop<NB, S>(v, qw, qv, cid + 32 * j, live, id, dec);
+#pragma unroll
+            for (int k = 0; k < S; ++k) {
+                c_lowp8 += (uint32_t)(dec[k] >= 0 && live[k]);
+                stream_accept(dec[k] == 1, id[k], qi, res_off, acc_cnt, resbuf);
+            }
+#pragma unroll
+            for (int k = 0; k < S; ++k)
+                if (__any_sync(0xFFFFFFFFu, dec[k] < 0))
+                    stream_undecided<FUSED, NB>(v, Q, qi, dec[k], id[k], q, st, f32_q, kcol, kidx, res_off, acc_cnt,
+                                                resbuf, cn);
         }
     }
     unsigned long long c_lowp = c_lowp8 + cn.lowp, c_fp32 = cn.fp32, c_fp64 = cn.fp64, c_flip = cn.flip;
@@ -437,13 +462,25 @@ __global__ void __launch_bounds__(1024) k_stream_finish_big(DevView v, const uin
     }
 }
 
-template <class E, bool F, int NB>
+// Steps in flight per warp of the streaming kernel: 1 (64 registers, four blocks
+// per SM) by default -- measured 13 % faster at 1M x 128 than 2 (two blocks per
+// SM); HRNN_STREAM_STEPS=2 selects the other form.
+int stream_steps() {
+    static int s = 0;
+    if (!s) {
+        const char* e = std::getenv("HRNN_STREAM_STEPS");
+        s = (e && e[0] == '2') ? 2 : 1;
+    }
+    return s;
+}
+
+template <class E, bool F, int NB, int S>
 int chunks_per_sm() {
     static int per_sm = 0;
     if (!per_sm) {
         constexpr uint32_t dim = NB * 16;
-        const size_t smem = 8 * (dim * 4 + dim + 32 * 4);
-        auto k = k_verify_chunks<E, F, NB>;
+        const size_t smem = 8 * verify_warp_smem(dim);
+        auto k = k_verify_chunks<E, F, NB, S>;
         CUDA_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         int ps = 1;
         CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ps, k, 256, smem));
@@ -452,14 +489,14 @@ int chunks_per_sm() {
     return per_sm;
 }
 
-template <class E, bool F, int NB>
+template <class E, bool F, int NB, int S>
 void launch_chunks(const DevView& v, const float* Q, uint32_t mmax, const uint32_t* prox, const uint32_t* plen,
                    const uint64_t* res_off, const float* kcol, uint32_t kidx, StreamBufs& B, uint64_t* resbuf,
                    SearchCounters* ctr, int nsm, cudaStream_t s) {
     constexpr uint32_t dim = NB * 16;
-    const size_t smem = 8 * (dim * 4 + dim + 32 * 4);
-    auto k = k_verify_chunks<E, F, NB>;
-    k<<<(unsigned)(nsm * chunks_per_sm<E, F, NB>()), 256, smem, s>>>(
+    const size_t smem = 8 * verify_warp_smem(dim);
+    auto k = k_verify_chunks<E, F, NB, S>;
+    k<<<(unsigned)(nsm * chunks_per_sm<E, F, NB, S>()), 256, smem, s>>>(
         v, Q, mmax, prox, plen, res_off, kcol, kidx, B.qq.as<int8_t>(), B.qmeta.as<float4>(), B.chunks.as<uint64_t>(),
         B.coff.as<uint64_t>() + B.npairs, B.ctl.as<uint32_t>(), B.acc_cnt.as<uint32_t>(), resbuf, ctr);
     CUDA_LAUNCH_CHECK();
@@ -474,13 +511,18 @@ void stream_prepare(const DevView& v, bool wide, bool fused) {
                                         (int)(kBigCap * 4)));
         big_set = true;
     }
-    if (v.dim == 128) {
-        if (wide) fused ? chunks_per_sm<uint64_t, true, 8>() : chunks_per_sm<uint64_t, false, 8>();
-        else fused ? chunks_per_sm<uint32_t, true, 8>() : chunks_per_sm<uint32_t, false, 8>();
-    } else {
-        if (wide) fused ? chunks_per_sm<uint64_t, true, 6>() : chunks_per_sm<uint64_t, false, 6>();
-        else fused ? chunks_per_sm<uint32_t, true, 6>() : chunks_per_sm<uint32_t, false, 6>();
-    }
+    auto prep = [&](auto steps) {
+        constexpr int S = decltype(steps)::value;
+        if (v.dim == 128) {
+            if (wide) fused ? chunks_per_sm<uint64_t, true, 8, S>() : chunks_per_sm<uint64_t, false, 8, S>();
+            else fused ? chunks_per_sm<uint32_t, true, 8, S>() : chunks_per_sm<uint32_t, false, 8, S>();
+        } else {
+            if (wide) fused ? chunks_per_sm<uint64_t, true, 6, S>() : chunks_per_sm<uint64_t, false, 6, S>();
+            else fused ? chunks_per_sm<uint32_t, true, 6, S>() : chunks_per_sm<uint32_t, false, 6, S>();
+        }
+    };
+    if (stream_steps() == 1) prep(std::integral_constant<int, 1>{});
+    else prep(std::integral_constant<int, 2>{});
 }
 
 bool stream_supported(const DevView& v) {
@@ -523,17 +565,26 @@ void stream_verify(const DevView& v, bool wide, bool fused, const float* Q, uint
     k_chunk_fill<<<(unsigned)((npairs + 255) / 256), 256, 0, s>>>(B.cnt.as<uint32_t>(), B.coff.as<uint64_t>(), npairs,
                                                                   B.chunks.as<uint64_t>());
     CUDA_LAUNCH_CHECK();
-    if (v.dim == 128) {
-        if (wide) fused ? launch_chunks<uint64_t, true, 8>(v, Q, mmax, prox, plen, res_off, kcol, kidx, B, resbuf, ctr, nsm, s)
-                        : launch_chunks<uint64_t, false, 8>(v, Q, mmax, prox, plen, res_off, kcol, kidx, B, resbuf, ctr, nsm, s);
-        else fused ? launch_chunks<uint32_t, true, 8>(v, Q, mmax, prox, plen, res_off, kcol, kidx, B, resbuf, ctr, nsm, s)
-                   : launch_chunks<uint32_t, false, 8>(v, Q, mmax, prox, plen, res_off, kcol, kidx, B, resbuf, ctr, nsm, s);
-    } else {
-        if (wide) fused ? launch_chunks<uint64_t, true, 6>(v, Q, mmax, prox, plen, res_off, kcol, kidx, B, resbuf, ctr, nsm, s)
-                        : launch_chunks<uint64_t, false, 6>(v, Q, mmax, prox, plen, res_off, kcol, kidx, B, resbuf, ctr, nsm, s);
-        else fused ? launch_chunks<uint32_t, true, 6>(v, Q, mmax, prox, plen, res_off, kcol, kidx, B, resbuf, ctr, nsm, s)
-                   : launch_chunks<uint32_t, false, 6>(v, Q, mmax, prox, plen, res_off, kcol, kidx, B, resbuf, ctr, nsm, s);
-    }
+    auto go = [&](auto steps) {
+        constexpr int S = decltype(steps)::value;
+        auto run = [&](auto e, auto f, auto nb) {
+            launch_chunks<decltype(e), decltype(f)::value, decltype(nb)::value, S>(v, Q, mmax, prox, plen, res_off,
+                                                                                kcol, kidx, B, resbuf, ctr, nsm, s);
+        };
+        using T = std::true_type;
+        using Fa = std::false_type;
+        using N8 = std::integral_constant<int, 8>;
+        using N6 = std::integral_constant<int, 6>;
+        if (v.dim == 128) {
+            if (wide) fused ? run(uint64_t{}, T{}, N8{}) : run(uint64_t{}, Fa{}, N8{});
+            else fused ? run(uint32_t{}, T{}, N8{}) : run(uint32_t{}, Fa{}, N8{});
+        } else {
+            if (wide) fused ? run(uint64_t{}, T{}, N6{}) : run(uint64_t{}, Fa{}, N6{});
+            else fused ? run(uint32_t{}, T{}, N6{}) : run(uint32_t{}, Fa{}, N6{});
+        }
+    };
+    if (stream_steps() == 1) go(std::integral_constant<int, 1>{});
+    else go(std::integral_constant<int, 2>{});
     uint32_t* big_n = B.ctl.as<uint32_t>() + 2;  // [2] big queries, [3] their work counter
     uint32_t* big = B.acc_cnt.as<uint32_t>() + nq;
     k_stream_finish<<<(nq + 7) / 8, 256, 0, s>>>(v, nq, res_off, B.acc_cnt.as<uint32_t>(), resbuf, res_count, big,
