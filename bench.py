@@ -783,7 +783,10 @@ def run_dynamic(args, W, H, torch, dev, dev_sync, rank, world, local):
         run_reference_arm(args, W, h, Q, {"m": m_h, "K_prime": kp_h, "ef_search": ef_h, "k": W["k"],
                                           "threshold": 1.0}, None, dyn)
         return
-    stream = torch.cuda.current_stream(dev)
+    # A stream of its own: the captured plan is an asynchronous graph launch, so
+    # the timing events must sit on the stream it runs on (a null handle would
+    # send the library's calls to the index's own stream).
+    stream = torch.cuda.Stream(dev)
     q_d = torch.from_numpy(Q).to(dev)
     m_d = torch.from_numpy(m_h.view(np.int32)).to(dev)
     kp_d = torch.from_numpy(kp_h.view(np.int32)).to(dev)
@@ -791,6 +794,7 @@ def run_dynamic(args, W, H, torch, dev, dev_sync, rank, world, local):
     cap = nq * 2048
     off_d = torch.zeros(nq + 1, dtype=torch.int64, device=dev)
     lab_d = torch.zeros(cap, dtype=torch.int64, device=dev)
+    dev_sync()  # made on the default stream, read on `stream`
     hbm, _, peak_kind = load_peaks()
     forms = {"plain": H.PREC_FP32_EXACT, "mixed_int8": H.PREC_INT8}
     out = {}
@@ -815,6 +819,9 @@ def run_dynamic(args, W, H, torch, dev, dev_sync, rank, world, local):
         st = h.last_search_stats()
         offs, labs = off_d.cpu().numpy(), lab_d[:tot].cpu().numpy()
         ans_b = [labs[offs[i]:offs[i + 1]].copy() for i in range(nq)]
+        off_d.zero_()  # the plan's replays must write the answers themselves
+        lab_d.zero_()
+        dev_sync()
         # the same batch replayed from a captured plan (one graph launch per batch)
         plan = h.search_plan(q_d.data_ptr(), nq, m_d.data_ptr(), kp_d.data_ptr(), ef_d.data_ptr(),
                              W["m_range"][1], W["ef_range"][1], 1.0, W["k"], off_d.data_ptr(), lab_d.data_ptr(), cap,

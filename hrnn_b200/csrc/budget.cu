@@ -63,13 +63,16 @@ __global__ void k_budget_features(DevView v, const float* __restrict__ Q, uint32
 // Per query: budget level from the logits; nprox trimmed for levels 0/1.
 // Fallback queries keep the caller's m (single pass) or are listed for a second
 // search (rerun).
+// grp (may be null): 1 for the queries listed for the second search, else 0.
 __global__ void k_budget_decide(const float* __restrict__ z, uint32_t nq, float conf, uint32_t m0, uint32_t m1,
                                 const uint32_t* __restrict__ qm, int rerun, uint32_t* __restrict__ nprox,
                                 uint32_t* __restrict__ fb_list,
-                                uint32_t* __restrict__ fb_count, unsigned long long* __restrict__ levels) {
+                                uint32_t* __restrict__ fb_count, unsigned long long* __restrict__ levels,
+                                uint8_t* __restrict__ grp) {
     const uint32_t qi = blockIdx.x * blockDim.x + threadIdx.x;
     if (qi >= nq) return;
     const float p0 = 1.f / (1.f + expf(-z[2 * qi])), p1 = 1.f / (1.f + expf(-z[2 * qi + 1]));
+    uint8_t g = 0;
     if (p0 >= conf) {
         nprox[qi] = min(nprox[qi], min(m0, qm[qi]));
         atomicAdd(&levels[0], 1ull);
@@ -77,10 +80,15 @@ __global__ void k_budget_decide(const float* __restrict__ z, uint32_t nq, float 
         nprox[qi] = min(nprox[qi], min(m1, qm[qi]));
         atomicAdd(&levels[1], 1ull);
     } else {
-        if (rerun) fb_list[atomicAdd(fb_count, 1u)] = qi;
-        else nprox[qi] = min(nprox[qi], qm[qi]);
+        if (rerun) {
+            fb_list[atomicAdd(fb_count, 1u)] = qi;
+            g = 1;
+        } else {
+            nprox[qi] = min(nprox[qi], qm[qi]);
+        }
         atomicAdd(&levels[2], 1ull);
     }
+    if (grp) grp[qi] = g;
 }
 
 void ensure_projection(Index& ix, Budget& b) {

@@ -17,6 +17,9 @@ namespace hrnn {
 Index::Index() = default;
 
 Index::~Index() {
+    for (auto& e : aux_ev)
+        if (e) cudaEventDestroy(e);
+    if (aux) cudaStreamDestroy(aux);
     if (stream) cudaStreamDestroy(stream);
 }
 

@@ -146,7 +146,11 @@ struct Index {
     DevMem kdist_serve;  // f32 [n][max_k_serve]
 
     // ---- scratch reused across calls ---------------------------------------
-    DevMem scratch[8];
+    DevMem scratch[10];
+    // a second stream and two events: the learned budget's second search runs
+    // beside the verification of the queries it does not concern
+    cudaStream_t aux = nullptr;
+    cudaEvent_t aux_ev[2] = {nullptr, nullptr};
     DevMem io;           // host-buffer entry points stage their inputs/outputs here
     DevMem counters;     // SearchCounters
     DevMem kcol;         // f32 [n]: kdist(p, k-1) of the current search call

@@ -455,24 +455,36 @@ __global__ void __launch_bounds__(join_threads<NBUF>(), NBUF == 2 ? 1 : 2) k_joi
                     if (dv < tj) emit |= 2u << (2 * r);
                 }
             }
-            const uint32_t ne = __popc(emit);
-            uint32_t incl = ne;
+            // The tile's proposals grouped by target, so the grouping pass meets
+            // long runs of one target: row r's proposals (target ids[i0 + r], the
+            // same for most lanes) in block r, then each lane's proposals to its
+            // column (target bj) together.
+            const uint32_t lt = (1u << lane) - 1u;
+            uint32_t rowpos[kJR], nrow = 0;
+#pragma unroll
+            for (int r = 0; r < kJR; ++r) {
+                const uint32_t bal = __ballot_sync(0xFFFFFFFFu, (emit >> (2 * r)) & 1u);
+                rowpos[r] = nrow + __popc(bal & lt);
+                nrow += __popc(bal);
+            }
+            const uint32_t nc = __popc(emit & 0xAAu);
+            uint32_t incl = nc;
             for (int o = 1; o < 32; o <<= 1) {
                 const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
                 if (lane >= o) incl += y;
             }
-            const uint32_t wt = __shfl_sync(0xFFFFFFFFu, incl, 31);
+            const uint32_t wt = nrow + __shfl_sync(0xFFFFFFFFu, incl, 31);
             if (wt) {
                 unsigned long long b1, b2;
                 uint32_t rem;
                 reserve(wt, b1, rem, b2);
-                uint32_t v = incl - ne;  // this lane's first position in the tile
                 auto slot = [&](uint32_t x) { return x < rem ? b1 + x : b2 + (x - rem); };
+                uint32_t v = nrow + incl - nc;  // this lane's first column-block position
 #pragma unroll
                 for (int r = 0; r < kJR; ++r) {
                     const uint32_t ai = ids[(i0 + r) < tot ? i0 + r : 0];
                     if ((emit >> (2 * r)) & 1u) {
-                        const unsigned long long q = slot(v++);
+                        const unsigned long long q = slot(rowpos[r]);
                         if (q < pcap) prop[q] = Prop{ai, bj, dd[r]};
                     }
                     if ((emit >> (2 * r + 1)) & 1u) {

@@ -401,7 +401,7 @@ __global__ void __launch_bounds__(kBCThreads) k_phase_bc_cta(
             verify(ns);
             __syncthreads();
             const uint32_t na = ctl[1];
-            if (na > kACap) {
+            if (na > kACap || ro + written + na > res_off[qi + 1]) {  // (or past a bounded slice)
                 overflow = true;
                 break;
             }

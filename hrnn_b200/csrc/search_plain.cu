@@ -53,7 +53,7 @@ __global__ void k_budget_features(DevView v, const float* Q, uint32_t nq, const 
                                   float* feat);
 __global__ void k_budget_decide(const float* z, uint32_t nq, float conf, uint32_t m0, uint32_t m1, const uint32_t* qm,
                                 int rerun, uint32_t* nprox,
-                                uint32_t* fb_list, uint32_t* fb_count, unsigned long long* levels);
+                                uint32_t* fb_list, uint32_t* fb_count, unsigned long long* levels, uint8_t* grp);
 void ensure_projection(Index& ix, Budget& b);
 __global__ void k_kdist_column(DevView v, uint32_t kidx, float* kcol);
 size_t bc_cta_smem(uint32_t dim, bool counts, bool mixed);
@@ -62,6 +62,12 @@ size_t bc_cta_smem(uint32_t dim, bool counts, bool mixed);
 inline bool verify_table_forced() {
     const char* e = std::getenv("HRNN_VERIFY");
     return e && std::string(e) == "table";
+}
+// HRNN_LEARNED_SERIAL=1: the learned budget's second search and the verification
+// run one after the other (for comparisons with the overlapped order).
+inline bool learned_serial() {
+    const char* e = std::getenv("HRNN_LEARNED_SERIAL");
+    return e && e[0] == '1';
 }
 
 namespace {
@@ -221,14 +227,17 @@ __device__ __forceinline__ uint32_t entry_owner(const void* ent, uint64_t i, uin
 
 // Prefix length (rank < K') of every proxy's reverse list and the per-query total.
 template <class E>
+// grp (may be null): the queries with grp[q] != want get no postings (a batch
+// verified in two groups).
 __global__ void k_phase_b_count(DevView v, uint32_t nq, const uint32_t* __restrict__ Kp, uint32_t mmax,
                                 const uint32_t* __restrict__ prox, const uint32_t* __restrict__ nprox,
-                                uint32_t* __restrict__ plen, uint64_t* __restrict__ total) {
+                                uint32_t* __restrict__ plen, uint64_t* __restrict__ total,
+                                const uint8_t* __restrict__ grp = nullptr, uint8_t want = 0) {
     size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t qi = (uint32_t)(t / mmax), pi = (uint32_t)(t % mmax);
     if (qi >= nq) return;
     uint32_t len = 0;
-    if (pi < nprox[qi]) {
+    if (pi < nprox[qi] && (!grp || grp[qi] == want)) {
         uint32_t p = prox[(size_t)qi * mmax + pi];
         uint64_t b = v.csr_off[p], e = v.csr_off[p + 1];
         uint32_t kp = Kp[qi];
@@ -264,8 +273,10 @@ __global__ void __launch_bounds__(128) k_phase_bc(DevView v, const float* __rest
                                                   uint32_t* __restrict__ res_count, uint32_t* __restrict__ next_q,
                                                   const uint32_t* __restrict__ qlist,
                                                   SearchCounters* __restrict__ ctr,
-                                                  const uint32_t* __restrict__ nq_dev) {
+                                                  const uint32_t* __restrict__ nq_dev,
+                                                  uint32_t* __restrict__ clamp) {
     // nq_dev: the query count in device memory (a captured plan), else nq.
+    // clamp (may be null): raised when a bounded result slice truncated an answer.
     extern __shared__ char smem_raw[];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, wpb = blockDim.x >> 5;
     const int half = lane >> 4, l = lane & 15;
@@ -366,15 +377,22 @@ __global__ void __launch_bounds__(128) k_phase_bc(DevView v, const float* __rest
                 __syncwarp();
             }
         }
-        c_res += na;
-        // Results in ascending internal-id order (hrnn.h:2055): rank sort.
-        uint64_t ro = res_off[qi];
+        // Results in ascending internal-id order (hrnn.h:2055): rank sort.  A
+        // bounded slice (a captured plan's staging) keeps its first entries and
+        // raises *clamp.
+        const uint64_t ro = res_off[qi];
+        const uint64_t slice = res_off[qi + 1] - ro;
+        const uint32_t room = (uint64_t)na < slice ? na : (uint32_t)slice;
         for (uint32_t i = lane; i < na; i += 32) {
             uint32_t x = list[i], rk = 0;
             for (uint32_t j = 0; j < na; ++j) rk += list[j] < x;
-            resbuf[ro + rk] = v.labels[x];
+            if (rk < room) resbuf[ro + rk] = v.labels[x];
         }
-        if (lane == 0) res_count[qi] = na;
+        c_res += room;
+        if (lane == 0) {
+            res_count[qi] = room;
+            if (room < na && clamp) atomicOr(clamp, 1u);
+        }
         __syncwarp();
     }
     if (lane == 0) {
@@ -385,11 +403,14 @@ __global__ void __launch_bounds__(128) k_phase_bc(DevView v, const float* __rest
     }
 }
 
+// grp (may be null): only the queries with grp[q] == want (a batch verified in two
+// groups, each with its own staging).
 __global__ void k_pack_results(uint32_t nq, const uint64_t* __restrict__ res_off,
                                const uint32_t* __restrict__ res_count, const uint64_t* __restrict__ out_off,
-                               const uint64_t* __restrict__ resbuf, uint64_t* __restrict__ out) {
+                               const uint64_t* __restrict__ resbuf, uint64_t* __restrict__ out,
+                               const uint8_t* __restrict__ grp = nullptr, uint8_t want = 0) {
     uint32_t qi = blockIdx.x;
-    if (qi >= nq) return;
+    if (qi >= nq || (grp && grp[qi] != want)) return;
     uint32_t c = res_count[qi];
     for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) out[out_off[qi] + i] = resbuf[res_off[qi] + i];
 }
@@ -522,7 +543,7 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
     prox.ensure(nq * mmax * 4);
     nprox.ensure(nq * 4);
     plen.ensure(nq * mmax * 4);
-    qtot.ensure((nq + 1) * 8 * 2 + (nq + 1) * 4 * 2 + 64);
+    qtot.ensure((nq + 1) * 8 * 4 + (nq + 1) * 4 * 2 + 128);  // d_total2 / d_resoff2 after d_next
     uint64_t* d_total = qtot.as<uint64_t>();
     uint64_t* d_resoff = d_total + (nq + 1);
     uint32_t* d_rcount = (uint32_t*)(d_resoff + (nq + 1));
@@ -541,6 +562,14 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
     if (mixed || int8) v = make_view(ix);
     v.i8_screen = (mixed && int8) ? 1 : 0;
     const int nsm = sms(ix.device);
+    // Learned budget, two-pass, INT8 streaming verification: the second search (the
+    // queries the MLP is not confident about) runs on a second stream beside the
+    // verification of the other queries, which verify as group 0; the second
+    // search's queries verify afterwards as group 1.  grp[q] is the query's group.
+    const bool counts_mode = a.threshold > 1.0f;
+    const bool stream_bc = int8 && mixed && !counts_mode && stream_supported(v) && !verify_table_forced();
+    bool split = false;
+    uint8_t* grp = nullptr;
     CUDA_CHECK(cudaEventRecord(ev[0], s));
     {
         // The exact form runs the reference-order beam (k_phase_a); the reduced-
@@ -563,38 +592,39 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
         // One launch of the form's phase-A kernel; qlist / ef_over / m_keep / proxd /
         // save / resume as documented at k_phase_a_fast (the exact kernel takes no
         // save or resume).
+        cudaStream_t ls = s;  // the stream of `launch` (the second search may run beside the first group's verification)
         auto launch = [&](unsigned g, int cw, uint32_t cv, size_t sm, uint32_t nqq, const uint32_t* qlist,
                           uint32_t m_over, uint32_t ef_over, uint32_t m_keep, float* proxd, uint32_t* ctrq,
                           uint32_t save_cap, uint32_t* st_cnt, float* st_d, uint32_t* st_i, int resume) {
             if (fast && dm == 3 && r2)
-                k_phase_a_fast<3, true><<<g, cw * 32, sm, s>>>(v, a.d_q, nqq, a.d_m, a.d_ef, efc, cv, mmax,
+                k_phase_a_fast<3, true><<<g, cw * 32, sm, ls>>>(v, a.d_q, nqq, a.d_m, a.d_ef, efc, cv, mmax,
                                                                prox.as<uint32_t>(), nprox.as<uint32_t>(), ctr, qlist,
                                                                m_over, ef_over, m_keep, proxd, ctrq, save_cap, st_cnt,
                                                                st_d, st_i, resume);
             else if (fast && dm == 3)
-                k_phase_a_fast<3, false><<<g, cw * 32, sm, s>>>(v, a.d_q, nqq, a.d_m, a.d_ef, efc, cv, mmax,
+                k_phase_a_fast<3, false><<<g, cw * 32, sm, ls>>>(v, a.d_q, nqq, a.d_m, a.d_ef, efc, cv, mmax,
                                                                 prox.as<uint32_t>(), nprox.as<uint32_t>(), ctr, qlist,
                                                                 m_over, ef_over, m_keep, proxd, ctrq, save_cap, st_cnt,
                                                                 st_d, st_i, resume);
             else if (fast)
-                k_phase_a_fast<2, false><<<g, cw * 32, sm, s>>>(v, a.d_q, nqq, a.d_m, a.d_ef, efc, cv, mmax,
+                k_phase_a_fast<2, false><<<g, cw * 32, sm, ls>>>(v, a.d_q, nqq, a.d_m, a.d_ef, efc, cv, mmax,
                                                          prox.as<uint32_t>(), nprox.as<uint32_t>(), ctr, qlist,
                                                          m_over, ef_over, m_keep, proxd, ctrq, save_cap, st_cnt, st_d,
                                                          st_i, resume);
             else if (dm == 3)
-                k_phase_a<3><<<g, cw * 32, sm, s>>>(v, a.d_q, nqq, a.d_m, a.d_ef, efc, cv, mmax, prox.as<uint32_t>(),
+                k_phase_a<3><<<g, cw * 32, sm, ls>>>(v, a.d_q, nqq, a.d_m, a.d_ef, efc, cv, mmax, prox.as<uint32_t>(),
                                                     nprox.as<uint32_t>(), ctr, qlist, m_over, ef_over, m_keep, proxd,
                                                     ctrq);
             else if (dm == 2)
-                k_phase_a<2><<<g, cw * 32, sm, s>>>(v, a.d_q, nqq, a.d_m, a.d_ef, efc, cv, mmax, prox.as<uint32_t>(),
+                k_phase_a<2><<<g, cw * 32, sm, ls>>>(v, a.d_q, nqq, a.d_m, a.d_ef, efc, cv, mmax, prox.as<uint32_t>(),
                                                     nprox.as<uint32_t>(), ctr, qlist, m_over, ef_over, m_keep, proxd,
                                                     ctrq);
             else if (dm == 1)
-                k_phase_a<1><<<g, cw * 32, sm, s>>>(v, a.d_q, nqq, a.d_m, a.d_ef, efc, cv, mmax, prox.as<uint32_t>(),
+                k_phase_a<1><<<g, cw * 32, sm, ls>>>(v, a.d_q, nqq, a.d_m, a.d_ef, efc, cv, mmax, prox.as<uint32_t>(),
                                                     nprox.as<uint32_t>(), ctr, qlist, m_over, ef_over, m_keep, proxd,
                                                     ctrq);
             else
-                k_phase_a<0><<<g, cw * 32, sm, s>>>(v, a.d_q, nqq, a.d_m, a.d_ef, efc, cv, mmax, prox.as<uint32_t>(),
+                k_phase_a<0><<<g, cw * 32, sm, ls>>>(v, a.d_q, nqq, a.d_m, a.d_ef, efc, cv, mmax, prox.as<uint32_t>(),
                                                     nprox.as<uint32_t>(), ctr, qlist, m_over, ef_over, m_keep, proxd,
                                                     ctrq);
             CUDA_LAUNCH_CHECK();
@@ -706,67 +736,91 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
                 ix.kcol.as<float>(), b.proj.as<float>(), b.feat.as<float>());
             CUDA_LAUNCH_CHECK();
             b.mlp.forward(b.feat.as<float>(), (int)nq, s);
+            const bool may_split = two_pass && fast && stream_bc && !learned_serial();
+            if (may_split) {
+                ix.scratch[9].ensure(nq + 16);
+                grp = ix.scratch[9].as<uint8_t>();
+            }
             k_budget_decide<<<(unsigned)((nq + 255) / 256), 256, 0, s>>>(
                 b.mlp.z3.as<float>(), (uint32_t)nq, b.confidence, b.m[0], b.m[1], a.d_m, two_pass ? 1 : 0,
-                nprox.as<uint32_t>(), b.fallback_list.as<uint32_t>(), fb_count, levels);
+                nprox.as<uint32_t>(), b.fallback_list.as<uint32_t>(), fb_count, levels, grp);
             CUDA_LAUNCH_CHECK();
             if (two_pass) {
                 uint32_t nfb = 0;
                 CUDA_CHECK(cudaMemcpyAsync(&nfb, fb_count, 4, cudaMemcpyDeviceToHost, s));
                 CUDA_CHECK(cudaStreamSynchronize(s));
+                split = may_split && nfb > 0 && nfb < nq;
+                if (split) {
+                    if (!ix.aux) CUDA_CHECK(cudaStreamCreateWithFlags(&ix.aux, cudaStreamNonBlocking));
+                    for (auto& e : ix.aux_ev)
+                        if (!e) CUDA_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+                    CUDA_CHECK(cudaEventRecord(ix.aux_ev[0], s));
+                    CUDA_CHECK(cudaStreamWaitEvent(ix.aux, ix.aux_ev[0], 0));
+                    ls = ix.aux;
+                }
                 if (nfb)
                     launch(grid_for(nfb), wpb, vc, smem_a, nfb, b.fallback_list.as<uint32_t>(), 0, 0, 0, nullptr,
                            d_qa + 1, save_cap, st_cnt, st_d, st_i, save_cap ? 1 : 0);
+                if (split) {
+                    CUDA_CHECK(cudaEventRecord(ix.aux_ev[1], ix.aux));
+                    ls = s;
+                }
             }
         }
     }
     CUDA_CHECK(cudaEventRecord(ev[1], s));
-    {
-        size_t tot = nq * mmax;
-        auto kern = ix.wide ? k_phase_b_count<uint64_t> : k_phase_b_count<uint32_t>;
-        kern<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(v, (uint32_t)nq, a.d_Kp, mmax, prox.as<uint32_t>(),
-                                                           nprox.as<uint32_t>(), plen.as<uint32_t>(), d_total);
-        CUDA_LAUNCH_CHECK();
-    }
-    exclusive_scan_u64(d_total, d_resoff, nq + 1, s, tmp);
-    std::vector<uint64_t> htot(nq);
-    uint64_t sum_total = 0;
-    CUDA_CHECK(cudaMemcpyAsync(htot.data(), d_total, nq * 8, cudaMemcpyDeviceToHost, s));
-    CUDA_CHECK(cudaMemcpyAsync(&sum_total, d_resoff + nq, 8, cudaMemcpyDeviceToHost, s));
-    CUDA_CHECK(cudaStreamSynchronize(s));
-    DevMem& hkey = ix.scratch[5];
-    DevMem& hcnt = ix.scratch[6];
-    DevMem& res = ix.scratch[7];
-    const size_t res_bytes = std::max<uint64_t>(sum_total, 1) * 8;
-    res.ensure(res_bytes + (nq + 1) * 4 + 256);
-    uint64_t* resbuf = res.as<uint64_t>();
-    uint32_t* ovl = (uint32_t*)(res.as<char>() + ((res_bytes + 255) & ~(size_t)255));
-    uint32_t* d_nov = d_next + 1;  // spare counters after d_next, zeroed with d_rcount
-    CUDA_CHECK(cudaEventRecord(ev[2], s));
-    {
-        // Per-call column of kdist(p, k-1) (hrnn.h:286-293), then one CTA per query.
+    // Phase B (posting counts, staging) and C (verification) of the queries with
+    // g[q] == want (all of them for g null), staged in `resm` at offsets d_off.
+    auto run_bc = [&](const uint8_t* g, uint8_t want, uint64_t* d_tot, uint64_t* d_off, DevMem& resm,
+                      bool first) -> uint64_t* {
+        {
+            size_t tot = nq * mmax;
+            auto kern = ix.wide ? k_phase_b_count<uint64_t> : k_phase_b_count<uint32_t>;
+            kern<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(v, (uint32_t)nq, a.d_Kp, mmax, prox.as<uint32_t>(),
+                                                               nprox.as<uint32_t>(), plen.as<uint32_t>(), d_tot, g,
+                                                               want);
+            CUDA_LAUNCH_CHECK();
+        }
+        exclusive_scan_u64(d_tot, d_off, nq + 1, s, tmp);
+        std::vector<uint64_t> htot(nq);
+        uint64_t sum_total = 0;
+        CUDA_CHECK(cudaMemcpyAsync(htot.data(), d_tot, nq * 8, cudaMemcpyDeviceToHost, s));
+        CUDA_CHECK(cudaMemcpyAsync(&sum_total, d_off + nq, 8, cudaMemcpyDeviceToHost, s));
+        CUDA_CHECK(cudaStreamSynchronize(s));
+        DevMem& hkey = ix.scratch[5];
+        DevMem& hcnt = ix.scratch[6];
+        const size_t res_bytes = std::max<uint64_t>(sum_total, 1) * 8;
+        resm.ensure(res_bytes + (nq + 1) * 4 + 256);
+        uint64_t* rbuf = resm.as<uint64_t>();
+        uint32_t* ovl = (uint32_t*)(resm.as<char>() + ((res_bytes + 255) & ~(size_t)255));
+        uint32_t* d_nov = d_next + 1;  // spare counters after d_next, zeroed with d_rcount
+        if (first) CUDA_CHECK(cudaEventRecord(ev[2], s));
+        // Per-call column of kdist(p, k-1) (hrnn.h:286-293), then the verification.
         const uint32_t kidx = (uint32_t)(a.k - 1);
-        ix.kcol.ensure((size_t)std::max<size_t>(ix.cur, 1) * 4);
-        k_kdist_column<<<(unsigned)((ix.cur + 255) / 256), 256, 0, s>>>(v, kidx, ix.kcol.as<float>());
-        CUDA_LAUNCH_CHECK();
-        const bool counts = a.threshold > 1.0f;
-        if (int8 && mixed && !counts && stream_supported(v) && !verify_table_forced()) {
+        if (first) {
+            ix.kcol.ensure((size_t)std::max<size_t>(ix.cur, 1) * 4);
+            k_kdist_column<<<(unsigned)((ix.cur + 255) / 256), 256, 0, s>>>(v, kidx, ix.kcol.as<float>());
+            CUDA_LAUNCH_CHECK();
+        }
+        if (stream_bc) {
             // INT8 form: postings verified as they are read, in chunks spread over
             // persistent warps
             const size_t npairs = nq * mmax;
             ix.sb.reserve((uint32_t)nq, v.dim, npairs, stream_max_chunks(sum_total, npairs));
             stream_verify(v, ix.wide, fusedsimd, a.d_q, (uint32_t)nq, mmax, prox.as<uint32_t>(), plen.as<uint32_t>(),
-                          d_resoff, ix.kcol.as<float>(), kidx, resbuf, d_rcount, ovl, d_nov, ctr, ix.sb, nsm, s);
+                          d_off, ix.kcol.as<float>(), kidx, rbuf, d_rcount, ovl, d_nov, ctr, ix.sb, nsm, s, g, want);
         } else {
-            const size_t smem = bc_cta_smem(v.dim, counts, mixed);
-            KCta kc = ix.wide ? pick_bc<uint64_t>(fusedsimd, counts, mixed) : pick_bc<uint32_t>(fusedsimd, counts, mixed);
+            // one CTA per query (every query: the CTA path verifies a batch in one group)
+            const size_t smem = bc_cta_smem(v.dim, counts_mode, mixed);
+            KCta kc = ix.wide ? pick_bc<uint64_t>(fusedsimd, counts_mode, mixed)
+                              : pick_bc<uint32_t>(fusedsimd, counts_mode, mixed);
             CUDA_CHECK(cudaFuncSetAttribute(kc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             int per_sm = 1;
             CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kc, 256, smem));
             unsigned grid = (unsigned)std::min<size_t>(nq, (size_t)nsm * std::max(per_sm, 1));
             kc<<<grid, 256, smem, s>>>(v, a.d_q, (uint32_t)nq, mmax, prox.as<uint32_t>(), nprox.as<uint32_t>(),
-                                       plen.as<uint32_t>(), d_total, d_resoff, a.threshold, ix.kcol.as<float>(), kidx,
-                                       resbuf, d_rcount, d_next, ovl, d_nov, ctr);
+                                       plen.as<uint32_t>(), d_tot, d_off, a.threshold, ix.kcol.as<float>(), kidx,
+                                       rbuf, d_rcount, d_next, ovl, d_nov, ctr);
             CUDA_LAUNCH_CHECK();
         }
         // Queries whose shared-memory table or accepted list overflowed: the
@@ -799,16 +853,31 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
             size_t smem_w = 4 * (v.dim * 4 + 16);
             void (*kern)(DevView, const float*, uint32_t, uint32_t, const uint32_t*, const uint32_t*, const uint32_t*,
                          const uint64_t*, float, uint32_t, uint32_t, uint32_t*, uint32_t*, uint32_t*, size_t,
-                         uint64_t*, uint32_t*, uint32_t*, const uint32_t*, SearchCounters*, const uint32_t*);
+                         uint64_t*, uint32_t*, uint32_t*, const uint32_t*, SearchCounters*, const uint32_t*,
+                         uint32_t*);
             if (ix.wide) kern = fusedsimd ? k_phase_bc<uint64_t, true> : k_phase_bc<uint64_t, false>;
             else kern = fusedsimd ? k_phase_bc<uint32_t, true> : k_phase_bc<uint32_t, false>;
             kern<<<(unsigned)(slots / 4), 128, smem_w, s>>>(v, a.d_q, nov, mmax, prox.as<uint32_t>(),
-                                                            nprox.as<uint32_t>(), plen.as<uint32_t>(), d_resoff,
+                                                            nprox.as<uint32_t>(), plen.as<uint32_t>(), d_off,
                                                             a.threshold, kidx, hcap, hkey.as<uint32_t>(),
                                                             hcnt.as<uint32_t>(), lp.as<uint32_t>(), (size_t)tmax,
-                                                            resbuf, d_rcount, d_next2, ovl, ctr, nullptr);
+                                                            rbuf, d_rcount, d_next2, ovl, ctr, nullptr, nullptr);
             CUDA_LAUNCH_CHECK();
         }
+        return rbuf;
+    };
+    uint64_t* resbuf = run_bc(split ? grp : nullptr, 0, d_total, d_resoff, ix.scratch[7], true);
+    uint64_t *resbuf2 = nullptr, *d_total2 = nullptr, *d_resoff2 = nullptr;
+    if (split) {
+        // group 1 once its second search is done
+        // after d_next's max(nq + 1, 8) counters, 8-byte aligned
+        const uintptr_t at = (uintptr_t)(d_next + std::max<size_t>(nq + 1, 8));
+        d_total2 = (uint64_t*)((at + 7) & ~(uintptr_t)7);
+        d_resoff2 = d_total2 + (nq + 1);
+        CUDA_CHECK(cudaStreamWaitEvent(s, ix.aux_ev[1], 0));
+        CUDA_CHECK(cudaMemsetAsync(d_total2, 0, (nq + 1) * 8, s));
+        CUDA_CHECK(cudaMemsetAsync(d_next, 0, 12, s));  // the verification's counters of group 0
+        resbuf2 = run_bc(grp, 1, d_total2, d_resoff2, ix.scratch[8], false);
     }
     exclusive_scan_u32_to_u64(d_rcount, a.d_out_offsets, nq + 1, s, tmp);
     uint64_t total = 0;
@@ -816,8 +885,13 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
     CUDA_CHECK(cudaStreamSynchronize(s));
     if (total <= a.cap && total > 0) {
         k_pack_results<<<(unsigned)nq, 128, 0, s>>>((uint32_t)nq, d_resoff, d_rcount, a.d_out_offsets, resbuf,
-                                                     a.d_out_labels);
+                                                     a.d_out_labels, split ? grp : nullptr, 0);
         CUDA_LAUNCH_CHECK();
+        if (split) {
+            k_pack_results<<<(unsigned)nq, 128, 0, s>>>((uint32_t)nq, d_resoff2, d_rcount, a.d_out_offsets, resbuf2,
+                                                         a.d_out_labels, grp, 1);
+            CUDA_LAUNCH_CHECK();
+        }
     }
     CUDA_CHECK(cudaEventRecord(ev[3], s));
     CUDA_CHECK(cudaStreamSynchronize(s));
@@ -1001,6 +1075,15 @@ PlanLaunch plan_launch_shape(Index& ix, const SearchPlan& p) {
 
 }  // namespace
 
+// The smallest result slice of a captured plan (>= the finishing passes' 16384).
+constexpr size_t kPlanMinSlice = 16384;
+
+// Slice lengths of a captured plan: each query's posting count, at most qcap.
+__global__ void k_cap_totals(const uint64_t* __restrict__ total, uint32_t n, uint64_t qcap, uint64_t* __restrict__ out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = min(total[i], qcap);
+}
+
 void plan_create(SearchPlan& p, cudaStream_t s) {
     Index& ix = *p.ix;
     if (!ix.rknng_built) fail(HRNN_ERR_STATE, "searchRknn: RKNNG not built");
@@ -1026,11 +1109,23 @@ void plan_create(SearchPlan& p, cudaStream_t s) {
     uint64_t maxdeg = 1;
     for (size_t i = 0; i < ix.cur; ++i) maxdeg = std::max<uint64_t>(maxdeg, off[i + 1] - off[i]);
     L.tmax = (size_t)L.mmax * maxdeg;
-    const size_t res_entries = nq * L.tmax;
+    // Result staging: every query's slice holds its postings, up to qcap -- the
+    // full bound nq * m_max * (longest reverse list) where it takes at most a
+    // quarter of the free memory, else as many as fit (at least kPlanMinSlice).  A
+    // query whose acceptances pass its slice is answered by the overflow pass; an
+    // answer longer than its slice is cut and raises the clamp flag.
     size_t free_b = 0, total_b = 0;
     CUDA_CHECK(cudaMemGetInfo(&free_b, &total_b));
+    size_t qcap = L.tmax;
+    if (nq * qcap * 8 > free_b / 4) qcap = std::max<size_t>(kPlanMinSlice, (free_b / 4) / (nq * 8));
+    qcap = std::min(qcap, L.tmax);
+    if (const char* e = std::getenv("HRNN_PLAN_MAX_SLICE")) {  // a smaller bound (tests of the bounded path)
+        const size_t v = std::strtoull(e, nullptr, 10);
+        if (v >= 1) qcap = std::min(qcap, v);
+    }
+    const size_t res_entries = nq * qcap;
     if (res_entries * 8 > free_b / 2)
-        fail(HRNN_ERR_NOMEM, "search plan: result bound nq * m_max * longest reverse list does not fit; lower m_max or nq");
+        fail(HRNN_ERR_NOMEM, "search plan: the result staging (nq * 16384 entries at least) does not fit; lower nq");
     const int nsm = sms(ix.device);
     // overflow tables: a fixed pool of warp slots, each sized for the bound
     uint32_t hcap = 64;
@@ -1044,7 +1139,7 @@ void plan_create(SearchPlan& p, cudaStream_t s) {
     p.prox.alloc(nq * L.mmax * 4);
     p.nprox.alloc(nq * 4);
     p.plen.alloc(nq * L.mmax * 4);
-    p.qtot.alloc((nq + 1) * 8 * 2 + (nq + 1) * 4 + 64);
+    p.qtot.alloc((nq + 1) * 8 * 3 + (nq + 1) * 4 + 64);
     p.res.alloc(std::max<size_t>(res_entries, 1) * 8);
     p.kcol.alloc(std::max<size_t>(ix.cur, 1) * 4);
     p.hkey.alloc(slots * hcap * 4);
@@ -1058,6 +1153,7 @@ void plan_create(SearchPlan& p, cudaStream_t s) {
     uint64_t* d_resoff = d_total + (nq + 1);
     uint32_t* d_rcount = (uint32_t*)(d_resoff + (nq + 1));
     uint32_t* d_next = d_rcount + (nq + 1);
+    uint64_t* d_totc = (uint64_t*)(d_next + 8 + ((nq + 1) & 1));  // per-query slice lengths (8-byte aligned)
     uint32_t* pm = p.inputs.as<uint32_t>();
     uint32_t* pef = pm + nq;
     uint32_t* flag = pef + nq;
@@ -1076,7 +1172,7 @@ void plan_create(SearchPlan& p, cudaStream_t s) {
     const bool stream = L.int8 && L.mixed && !L.counts && stream_supported(v) && !verify_table_forced();
     KCta kc = ix.wide ? pick_bc<uint64_t>(L.fusedsimd, L.counts, L.mixed) : pick_bc<uint32_t>(L.fusedsimd, L.counts, L.mixed);
     if (stream) {
-        p.sb.reserve((uint32_t)nq, v.dim, nq * L.mmax, stream_max_chunks(res_entries, nq * L.mmax));
+        p.sb.reserve((uint32_t)nq, v.dim, nq * L.mmax, stream_max_chunks(nq * L.tmax, nq * L.mmax));
         stream_prepare(v, ix.wide, L.fusedsimd);
         // the scan's scratch sized outside the capture
         exclusive_scan_u32_to_u64(p.sb.cnt.as<uint32_t>(), p.sb.coff.as<uint64_t>(), nq * L.mmax + 1, s, p.sb.tmp);
@@ -1088,7 +1184,7 @@ void plan_create(SearchPlan& p, cudaStream_t s) {
     }
     void (*kov)(DevView, const float*, uint32_t, uint32_t, const uint32_t*, const uint32_t*, const uint32_t*,
                 const uint64_t*, float, uint32_t, uint32_t, uint32_t*, uint32_t*, uint32_t*, size_t, uint64_t*,
-                uint32_t*, uint32_t*, const uint32_t*, SearchCounters*, const uint32_t*);
+                uint32_t*, uint32_t*, const uint32_t*, SearchCounters*, const uint32_t*, uint32_t*);
     if (ix.wide) kov = L.fusedsimd ? k_phase_bc<uint64_t, true> : k_phase_bc<uint64_t, false>;
     else kov = L.fusedsimd ? k_phase_bc<uint32_t, true> : k_phase_bc<uint32_t, false>;
     CUDA_CHECK(cudaStreamSynchronize(s));
@@ -1115,9 +1211,11 @@ void plan_create(SearchPlan& p, cudaStream_t s) {
         const size_t tot = nq * L.mmax;
         auto kb = ix.wide ? k_phase_b_count<uint64_t> : k_phase_b_count<uint32_t>;
         kb<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(v, (uint32_t)nq, p.d_kp, L.mmax, p.prox.as<uint32_t>(),
-                                                         p.nprox.as<uint32_t>(), p.plen.as<uint32_t>(), d_total);
+                                                         p.nprox.as<uint32_t>(), p.plen.as<uint32_t>(), d_total,
+                                                         nullptr, 0);
     }
-    exclusive_scan_u64(d_total, d_resoff, nq + 1, s, p.tmp);
+    k_cap_totals<<<(unsigned)((nq + 1 + 255) / 256), 256, 0, s>>>(d_total, (uint32_t)nq + 1, qcap, d_totc);
+    exclusive_scan_u64(d_totc, d_resoff, nq + 1, s, p.tmp);
     k_kdist_column<<<(unsigned)((ix.cur + 255) / 256), 256, 0, s>>>(v, L.kidx, p.kcol.as<float>());
     uint64_t* resbuf = p.res.as<uint64_t>();
     uint32_t* ovl = flag + 4;  // the overflow list (nq entries) after the clamp flag
@@ -1134,7 +1232,7 @@ void plan_create(SearchPlan& p, cudaStream_t s) {
                                                       p.nprox.as<uint32_t>(), p.plen.as<uint32_t>(), d_resoff,
                                                       p.threshold, L.kidx, L.hcap, p.hkey.as<uint32_t>(),
                                                       p.hcnt.as<uint32_t>(), p.lp.as<uint32_t>(), L.tmax, resbuf,
-                                                      d_rcount, d_next + 2, ovl, ctr, d_next + 1);
+                                                      d_rcount, d_next + 2, ovl, ctr, d_next + 1, flag);
     exclusive_scan_u32_to_u64(d_rcount, p.d_out_off, nq + 1, s, p.tmp);
     k_pack_results_capped<<<(unsigned)nq, 128, 0, s>>>((uint32_t)nq, d_resoff, d_rcount, p.d_out_off, resbuf,
                                                         p.d_out_lab, p.cap);

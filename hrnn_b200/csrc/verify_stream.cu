@@ -103,7 +103,9 @@ __global__ void k_chunk_fill(const uint32_t* __restrict__ cnt, const uint64_t* _
 }
 
 // Appends the ids of the lanes with `a` set to query qi's slice of the result
-// buffer (counted in acc_cnt).
+// buffer (counted in acc_cnt).  A slice shorter than the query's postings (a
+// captured plan's bounded staging) takes what fits; the finishing pass sends a
+// query whose count passed its slice to the overflow pass.
 __device__ __forceinline__ void stream_accept(bool a, uint32_t id, uint32_t qi, const uint64_t* res_off,
                                               uint32_t* acc_cnt, uint64_t* resbuf) {
     const uint32_t ab = __ballot_sync(0xFFFFFFFFu, a);
@@ -112,7 +114,10 @@ __device__ __forceinline__ void stream_accept(bool a, uint32_t id, uint32_t qi, 
     uint32_t base = 0;
     if (lane == 0) base = atomicAdd(&acc_cnt[qi], (uint32_t)__popc(ab));
     base = __shfl_sync(0xFFFFFFFFu, base, 0);
-    if (a) resbuf[res_off[qi] + base + __popc(ab & ((1u << lane) - 1u))] = id;
+    if (a) {
+        const uint64_t pos = res_off[qi] + base + __popc(ab & ((1u << lane) - 1u));
+        if (pos < res_off[qi + 1]) resbuf[pos] = id;
+    }
 }
 
 // Counters of one warp (summed into SearchCounters at the end).
@@ -353,14 +358,15 @@ __global__ void __launch_bounds__(256) k_stream_finish(DevView v, uint32_t nq, c
                                                        const uint32_t* __restrict__ acc_cnt,
                                                        uint64_t* __restrict__ resbuf, uint32_t* __restrict__ res_count,
                                                        uint32_t* __restrict__ big, uint32_t* __restrict__ n_big,
-                                                       SearchCounters* __restrict__ ctr) {
+                                                       SearchCounters* __restrict__ ctr,
+                                                       const uint8_t* __restrict__ grp, uint8_t want) {
     __shared__ uint32_t sm[8][kFinCap];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint32_t qi = blockIdx.x * 8 + w;
-    if (qi >= nq) return;
+    if (qi >= nq || (grp && grp[qi] != want)) return;
     uint32_t* acc = sm[w];
     const uint32_t na = acc_cnt[qi];
-    if (na > kFinCap) {  // left to the block-wide pass
+    if (na > kFinCap || na > res_off[qi + 1] - res_off[qi]) {  // left to the block-wide pass
         if (lane == 0) big[atomicAdd(n_big, 1u)] = qi;
         return;
     }
@@ -422,7 +428,7 @@ __global__ void __launch_bounds__(1024) k_stream_finish_big(DevView v, const uin
         if (b >= nb) break;
         const uint32_t qi = big[b];
         const uint32_t na = acc_cnt[qi];
-        if (na > kBigCap) {
+        if (na > kBigCap || na > res_off[qi + 1] - res_off[qi]) {  // (or not all of them were kept)
             if (tid == 0) ovl[atomicAdd(n_ovl, 1u)] = qi;
             continue;
         }
@@ -547,7 +553,7 @@ size_t stream_max_chunks(uint64_t total_postings, size_t npairs) {
 void stream_verify(const DevView& v, bool wide, bool fused, const float* Q, uint32_t nq, uint32_t mmax,
                    const uint32_t* prox, const uint32_t* plen, const uint64_t* res_off, const float* kcol,
                    uint32_t kidx, uint64_t* resbuf, uint32_t* res_count, uint32_t* ovl, uint32_t* n_ovl,
-                   SearchCounters* ctr, StreamBufs& B, int nsm, cudaStream_t s) {
+                   SearchCounters* ctr, StreamBufs& B, int nsm, cudaStream_t s, const uint8_t* grp, uint8_t want) {
     const size_t npairs = (size_t)nq * mmax;
     if (B.npairs != npairs) fail(HRNN_ERR_STATE, "stream_verify: buffers reserved for another shape");
     stream_prepare(v, wide, fused);
@@ -588,7 +594,7 @@ void stream_verify(const DevView& v, bool wide, bool fused, const float* Q, uint
     uint32_t* big_n = B.ctl.as<uint32_t>() + 2;  // [2] big queries, [3] their work counter
     uint32_t* big = B.acc_cnt.as<uint32_t>() + nq;
     k_stream_finish<<<(nq + 7) / 8, 256, 0, s>>>(v, nq, res_off, B.acc_cnt.as<uint32_t>(), resbuf, res_count, big,
-                                                 big_n, ctr);
+                                                 big_n, ctr, grp, want);
     CUDA_LAUNCH_CHECK();
     k_stream_finish_big<<<nsm, 1024, kBigCap * 4, s>>>(v, res_off, B.acc_cnt.as<uint32_t>(), big, big_n, big_n + 1,
                                                        resbuf, res_count, ovl, n_ovl, ctr);

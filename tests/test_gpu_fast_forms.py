@@ -145,3 +145,28 @@ def test_two_pass_levels_with_resume(idx128, level):
     else:           # resumed from the level beam: exact decisions, the fresh search's recall
         assert _exact_fails(X, Q, h, got, k) <= st["n_fp64_flipped"]
         assert data.macro_recall(gt, got) >= data.macro_recall(gt, fresh) - 0.01
+
+
+def test_overlapped_second_search_equals_serial(idx128, monkeypatch):
+    """Two-pass mode with a mix of levels: the fallback queries' second search runs
+    on a second stream beside the verification of the others (two verification
+    groups); the answers equal those of the serial order (HRNN_LEARNED_SERIAL=1)."""
+    from oracle import mlp as OM
+    X, Q, h = idx128
+    m, kp, ef, k, efl = 6, 64, 128, 10, 32
+    params = list(OM.init_params(5))[:6] + [np.zeros(H.BUDGET_IN, np.float32), np.ones(H.BUDGET_IN, np.float32)]
+    params[5][:] = 0.0  # logits around 0: about half the queries pass a cutoff just above 0.5
+    h.set_precision(H.PREC_INT8)
+    try:
+        h.budget_set_weights(params)
+        h.set_budget(True, 1, 3, efl, 0.5001)
+        over = h.search_rknn_batch(Q, m, kp, ef, threshold=1.0, k=k)
+        lv = h.last_search_stats()["n_budget"]
+        monkeypatch.setenv("HRNN_LEARNED_SERIAL", "1")
+        serial = h.search_rknn_batch(Q, m, kp, ef, threshold=1.0, k=k)
+        assert h.last_search_stats()["n_budget"] == lv
+    finally:
+        h.set_budget(False)
+        h.set_precision(H.PREC_FP32_EXACT)
+    assert 0 < lv[2] < len(Q) and lv[0] + lv[1] > 0, lv
+    assert all(np.array_equal(a, b) for a, b in zip(over, serial))

@@ -74,6 +74,45 @@ def test_plan_replays_equal_batch_calls(index, precision):
         h.set_precision(H.PREC_FP32_EXACT)
 
 
+@pytest.mark.parametrize("precision", [H.PREC_FP32_EXACT, H.PREC_INT8])
+def test_plan_bounded_result_slices(index, precision, monkeypatch):
+    """A plan whose per-query result slices are smaller than the queries' posting
+    counts (the bounded staging of large indexes, forced small here): queries whose
+    acceptances pass their slice go to the overflow pass, and the answers still
+    equal the batch calls'."""
+    import torch
+    h = index
+    h.set_precision(precision)
+    nq, m_max, ef_max, k, cap = 2000, 8, 120, 10, 2000 * 64
+    Q, hm, hkp, hef = _batch(5, nq, m_max, ef_max)
+    q = torch.from_numpy(Q).cuda()
+    m = torch.from_numpy(hm.astype(np.int32)).cuda()
+    kp = torch.from_numpy(hkp.astype(np.int32)).cuda()
+    ef = torch.from_numpy(hef.astype(np.int32)).cuda()
+    exp_off, exp_lab = _regular(h, torch, q, m, kp, ef, k, cap)
+    st = h.last_search_stats()
+    # slices just long enough for the longest answer, shorter than most queries'
+    # postings: acceptances (an owner counted once per proxy listing it) pass them
+    slice_len = int(np.diff(exp_off).max()) + 8
+    assert st["n_posting"] / nq > slice_len
+    monkeypatch.setenv("HRNN_PLAN_MAX_SLICE", str(slice_len))
+    off = torch.zeros(nq + 1, dtype=torch.int64, device="cuda")
+    lab = torch.zeros(cap, dtype=torch.int64, device="cuda")
+    plan = h.search_plan(q.data_ptr(), nq, m.data_ptr(), kp.data_ptr(), ef.data_ptr(), m_max, ef_max, 1.0, k,
+                         off.data_ptr(), lab.data_ptr(), cap)
+    try:
+        torch.cuda.synchronize()
+        plan.run()
+        total, clamped = plan.result()
+        assert not clamped
+        got_off, got_lab = off.cpu().numpy(), lab.cpu().numpy()[:total]
+        assert np.array_equal(got_off, exp_off)
+        assert np.array_equal(got_lab, exp_lab[:total])
+    finally:
+        plan.close()
+        h.set_precision(H.PREC_FP32_EXACT)
+
+
 def test_plan_clamps_capacity_and_index_changes(index):
     import torch
     h = index
