@@ -207,7 +207,8 @@ def rknn_gt_fp64(torch, X, Q, kth, dev):
 # reported rather than a stale one.
 NCU_TRAFFIC = {}
 NCU_TRAFFIC_QUERIES = 10_000
-SEARCH_SOURCES = ("common.cuh", "beam.cuh", "search_plain.cu", "search_bc.cu", "mixed.cu", "budget.cu")
+SEARCH_SOURCES = ("common.cuh", "beam.cuh", "beam_fast.cuh", "search_plain.cu", "search_bc.cu", "verify_stream.cu",
+                  "mixed.cu", "budget.cu")
 
 
 def search_src_hash() -> str:
@@ -436,7 +437,10 @@ def main():
         return
 
     # ---- timed device steps, per form ----
-    stream = torch.cuda.current_stream(dev)
+    # A stream of its own for every timed launch and its events: the library runs
+    # a call given the null handle on the index's own (non-blocking) stream, which
+    # events on torch's default stream would not order against.
+    stream = torch.cuda.Stream(dev)
     hbm, bf16, peak_kind = load_peaks()
     maxM0 = 2 * W["M"]
     qsets = {}
@@ -459,11 +463,18 @@ def main():
         if learned:
             h.set_budget(True, **BUDGET)
         m_dev = torch.full((nq_,), m_star, dtype=torch.int32, device=dev)
+        dev_sync()  # made on the default stream, read on `stream`
+
+        # The batch search recorded once as a CUDA graph over the step's buffers
+        # (hrnn_search_plan_*, the serving path: no host synchronisation inside a
+        # step), replayed once per step.
+        plan = h.search_plan(S["q"].data_ptr(), nq_, m_dev.data_ptr(), S["kp"].data_ptr(), S["ef"].data_ptr(),
+                             m_star, W["ef"], 1.0, W["k"], S["off"].data_ptr(), S["lab"].data_ptr(), S["cap"],
+                             stream.cuda_stream)
+        per_run = plan.kernels()
 
         def step():
-            return h.search_rknn_batch_device(S["q"].data_ptr(), nq_, m_dev.data_ptr(), S["kp"].data_ptr(),
-                                              S["ef"].data_ptr(), 1.0, W["k"], S["off"].data_ptr(),
-                                              S["lab"].data_ptr(), S["cap"], stream.cuda_stream)
+            plan.run(stream.cuda_stream)
 
         for _ in range(args.warmup):
             step()
@@ -474,19 +485,28 @@ def main():
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.nvtx.range_push("timed")  # profilers select the timed steps with this range
         e0.record(stream)
-        launches, tot = 0, 0
+        launches = 0
         for _ in range(steps):
-            tot = step()
-            launches += h.last_search_stats()["n_launches"]
+            step()
+            launches += per_run
         e1.record(stream)
         dev_sync()
         torch.cuda.nvtx.range_pop()
         ck = clocks.stop()
         ms = max_over_ranks(torch, e0.elapsed_time(e1), dev, world)
-        st = h.last_search_stats()
+        tot, clamped = plan.result(stream.cuda_stream)
+        plan.close()
         offs = S["off"].cpu().numpy()
         labs = S["lab"][:tot].cpu().numpy()
         recall = macro_recall(S["gt"], [labs[offs[i]:offs[i + 1]] for i in range(nq_)])
+        # counts and per-phase times of the same search: one stream-ordered batch
+        # call after the timed steps (its answers must equal the plan's)
+        tot_b = h.search_rknn_batch_device(S["q"].data_ptr(), nq_, m_dev.data_ptr(), S["kp"].data_ptr(),
+                                           S["ef"].data_ptr(), 1.0, W["k"], S["off"].data_ptr(), S["lab"].data_ptr(),
+                                           S["cap"], stream.cuda_stream)
+        st = h.last_search_stats()
+        if tot_b != tot or clamped or not np.array_equal(S["off"].cpu().numpy(), offs):
+            raise RuntimeError(f"bench: plan and batch call disagree ({tot} vs {tot_b} results, clamped {clamped})")
         # algorithmic bytes of the two phases: rows of 4 bytes/element (FP32), 2 (BF16)
         # or 1 plus 16 bytes of scale / error terms (INT8); the k-distance of each
         # verified id; the FP32 rows of the screens' undecided ids
@@ -583,8 +603,11 @@ def main():
     if head == "learned":
         h.set_budget(True, **BUDGET)
     # Pinned host buffers; every step copies the queries and their (m, K', ef) in,
-    # searches, copies the offsets and the labels out and waits (the C ABI's
-    # hrnn_search_rknn_batch on host pointers).
+    # searches, copies the offsets and the labels out and waits: one call of the
+    # C ABI's hrnn_search_plan_run_host on a plan made for the batch shape (the
+    # serving path; plan creation is setup, outside the timed region).  The
+    # one-call batch entry point hrnn_search_rknn_batch on the same host buffers
+    # is timed beside it.
     e2e_steps = max(1, args.steps)
     q_pin = torch.from_numpy(np.ascontiguousarray(Q)).pin_memory()
     p_m = torch.full((nq,), m_star, dtype=torch.int32).pin_memory()
@@ -593,22 +616,40 @@ def main():
     p_off = torch.zeros(nq + 1, dtype=torch.int64).pin_memory()
     e2e_cap = nq * 512
     p_lab = torch.zeros(e2e_cap, dtype=torch.int64).pin_memory()
+    d_in = {"q": torch.zeros((nq, d), dtype=torch.float32, device=dev),
+            **{k_: torch.zeros(nq, dtype=torch.int32, device=dev) for k_ in ("m", "kp", "ef")},
+            "off": torch.zeros(nq + 1, dtype=torch.int64, device=dev),
+            "lab": torch.zeros(e2e_cap, dtype=torch.int64, device=dev)}
+    dev_sync()  # made on the default stream, written on `stream`
+    e2e_plan = h.search_plan(d_in["q"].data_ptr(), nq, d_in["m"].data_ptr(), d_in["kp"].data_ptr(),
+                             d_in["ef"].data_ptr(), m_star, W["ef"], 1.0, W["k"], d_in["off"].data_ptr(),
+                             d_in["lab"].data_ptr(), e2e_cap, stream.cuda_stream)
 
     def e2e_step():
+        return e2e_plan.run_host(q_pin.data_ptr(), p_m.data_ptr(), p_kp.data_ptr(), p_ef.data_ptr(),
+                                 p_off.data_ptr(), p_lab.data_ptr(), e2e_cap, stream.cuda_stream)[0]
+
+    def e2e_batch_step():
         return h.search_rknn_batch_host(q_pin.data_ptr(), nq, p_m.data_ptr(), p_kp.data_ptr(), p_ef.data_ptr(), 1.0,
                                         W["k"], p_off.data_ptr(), p_lab.data_ptr(), e2e_cap)
 
-    for _ in range(max(1, args.warmup)):
-        e2e_step()
-    dev_sync()
-    t0 = time.perf_counter()
-    total_res = 0
-    for _ in range(e2e_steps):
-        total_res = e2e_step()
-    e2e_s = max_over_ranks(torch, time.perf_counter() - t0, dev, world)
+    e2e_batch = None
+    for fn in (e2e_batch_step, e2e_step):  # the plan's run last: its answers are read below
+        for _ in range(max(1, args.warmup)):
+            fn()
+        dev_sync()
+        t0 = time.perf_counter()
+        total_res = 0
+        for _ in range(e2e_steps):
+            total_res = fn()
+        e2e_s = max_over_ranks(torch, time.perf_counter() - t0, dev, world)
+        if fn is e2e_batch_step:
+            e2e_batch = round(world * nq * e2e_steps / e2e_s, 1)
+    e2e_plan.close()
     e2e = {"value": world * nq * e2e_steps / e2e_s, "unit": "queries/s",
            "h2d_bytes_per_step": int(nq * d * 4 + 3 * nq * 4), "d2h_bytes_per_step": int((nq + 1) * 8 + total_res * 8),
-           "host_buffers": "pinned"}
+           "host_buffers": "pinned", "call": "hrnn_search_plan_run_host",
+           "batch_call_value": e2e_batch, "batch_call": "hrnn_search_rknn_batch"}
     offs = p_off.numpy().astype(np.int64)
     labs = p_lab.numpy()[:total_res]
     out = [labs[offs[i]:offs[i + 1]] for i in range(nq)]

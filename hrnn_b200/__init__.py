@@ -30,7 +30,9 @@ EXPORTS = [
     "hrnn_last_error", "hrnn_version", "hrnn_create", "hrnn_load", "hrnn_save", "hrnn_destroy",
     "hrnn_add_points", "hrnn_refine_knng", "hrnn_build_rknng", "hrnn_build_rknng_mutable",
     "hrnn_search_rknn", "hrnn_search_rknn_batch", "hrnn_search_rknn_batch_device",
-    "hrnn_search_plan_create", "hrnn_search_plan_run", "hrnn_search_plan_result", "hrnn_search_plan_destroy",
+    "hrnn_search_plan_create", "hrnn_search_plan_run", "hrnn_search_plan_result", "hrnn_search_plan_run_host",
+    "hrnn_search_plan_kernels",
+    "hrnn_search_plan_destroy",
     "hrnn_compact_for_serving", "hrnn_insert_dynamic", "hrnn_set_ef", "hrnn_get_info",
     "hrnn_get_search_stats", "hrnn_get_refine_stats", "hrnn_set_precision", "hrnn_set_join_mode", "hrnn_set_autotune", "hrnn_set_l2_order", "hrnn_detect_l2_order", "hrnn_get_knng",
     "hrnn_set_knng", "hrnn_get_rknng", "hrnn_l2_batch", "hrnn_build_rknng_noalloc",
@@ -116,6 +118,9 @@ _lib.hrnn_search_plan_create.argtypes = [_vp, _vp, _sz, _vp, _vp, _vp, C.c_uint3
                                          C.c_uint32, _vp, _vp, _sz, _vp, C.POINTER(_vp)]
 _lib.hrnn_search_plan_run.argtypes = [_vp, _vp]
 _lib.hrnn_search_plan_result.argtypes = [_vp, _vp, C.POINTER(C.c_uint64), C.POINTER(C.c_int)]
+_lib.hrnn_search_plan_kernels.argtypes = [_vp, C.POINTER(_sz)]
+_lib.hrnn_search_plan_run_host.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _sz, C.POINTER(C.c_uint64),
+                                           C.POINTER(C.c_int), _vp]
 _lib.hrnn_search_plan_destroy.argtypes = [_vp]
 _lib.hrnn_search_plan_destroy.restype = None
 _lib.hrnn_search_rknn_batch_device.argtypes = [_vp, _vp, _sz, _vp, _vp, _vp, C.c_float, C.c_uint32, _vp,
@@ -506,6 +511,21 @@ class SearchPlan:
         tot, cl = C.c_uint64(0), C.c_int(0)
         _check(_lib.hrnn_search_plan_result(self._p, _vp(stream), C.byref(tot), C.byref(cl)))
         return tot.value, bool(cl.value)
+
+    def run_host(self, q_ptr, m_ptr, kp_ptr, ef_ptr, off_ptr, lab_ptr, cap, stream=0):
+        """One run on a host batch (ints are raw host pointers): copies in, replays,
+        waits, copies the offsets and labels out; returns (total, clamped)."""
+        tot, cl = C.c_uint64(0), C.c_int(0)
+        _check(_lib.hrnn_search_plan_run_host(self._p, _vp(q_ptr), _vp(m_ptr), _vp(kp_ptr), _vp(ef_ptr),
+                                              _vp(off_ptr), _vp(lab_ptr), cap, C.byref(tot), C.byref(cl),
+                                              _vp(stream)))
+        return tot.value, bool(cl.value)
+
+    def kernels(self) -> int:
+        """Kernel launches one run makes (the graph's kernel nodes)."""
+        n = C.c_size_t(0)
+        _check(_lib.hrnn_search_plan_kernels(self._p, C.byref(n)))
+        return n.value
 
     def close(self):
         if self._p:

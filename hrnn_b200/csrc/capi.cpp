@@ -287,6 +287,48 @@ hrnn_status hrnn_search_plan_result(hrnn_search_plan* plan, void* stream, uint64
     });
 }
 
+hrnn_status hrnn_search_plan_run_host(hrnn_search_plan* plan, const float* queries, const uint32_t* m,
+                                      const uint32_t* K_prime, const uint32_t* ef_search, uint64_t* out_offsets,
+                                      uint64_t* out_labels, size_t cap, uint64_t* total, int* clamped, void* stream) {
+    return guard([&] {
+        need(plan, "plan");
+        need(queries, "queries");
+        need(m, "m");
+        need(K_prime, "K_prime");
+        need(ef_search, "ef_search");
+        need(out_offsets, "out_offsets");
+        set_device(plan->h);
+        hrnn::SearchPlan& p = plan->p;
+        cudaStream_t s = stream ? (cudaStream_t)stream : plan->h->ix.stream;
+        const size_t nq = p.nq;
+        // the host batch into the plan's input buffers, the graph, the outputs back
+        CUDA_CHECK(cudaMemcpyAsync(const_cast<float*>(p.d_q), queries, nq * plan->h->ix.dim * 4,
+                                   cudaMemcpyHostToDevice, s));
+        CUDA_CHECK(cudaMemcpyAsync(const_cast<uint32_t*>(p.d_m), m, nq * 4, cudaMemcpyHostToDevice, s));
+        CUDA_CHECK(cudaMemcpyAsync(const_cast<uint32_t*>(p.d_kp), K_prime, nq * 4, cudaMemcpyHostToDevice, s));
+        CUDA_CHECK(cudaMemcpyAsync(const_cast<uint32_t*>(p.d_ef), ef_search, nq * 4, cudaMemcpyHostToDevice, s));
+        hrnn::plan_run(p, s);
+        const uint64_t t = hrnn::plan_result(p, s, clamped);
+        if (total) *total = t;
+        if (t > cap || t > p.cap)
+            hrnn::fail(HRNN_ERR_CAPACITY, "search plan: results exceed the capacity; labels not written");
+        CUDA_CHECK(cudaMemcpyAsync(out_offsets, p.d_out_off, (nq + 1) * 8, cudaMemcpyDeviceToHost, s));
+        if (t) {
+            need(out_labels, "out_labels");
+            CUDA_CHECK(cudaMemcpyAsync(out_labels, p.d_out_lab, t * 8, cudaMemcpyDeviceToHost, s));
+        }
+        CUDA_CHECK(cudaStreamSynchronize(s));
+    });
+}
+
+hrnn_status hrnn_search_plan_kernels(hrnn_search_plan* plan, size_t* n) {
+    return guard([&] {
+        need(plan, "plan");
+        need(n, "n");
+        *n = plan->p.kernel_nodes;
+    });
+}
+
 void hrnn_search_plan_destroy(hrnn_search_plan* plan) {
     if (!plan) return;
     cudaSetDevice(plan->h->ix.device);
@@ -409,6 +451,7 @@ hrnn_status hrnn_set_budget(hrnn_index* h, int enable, uint32_t m0, uint32_t m1,
                             float confidence) {
     return guard([&] {
         need(h, "index");
+        h->ix.generation++;  // captured plans record the budget's settings
         set_device(h);
         hrnn::budget_set(h->ix, enable != 0, m0, m1, ef, confidence);
     });
@@ -441,6 +484,7 @@ hrnn_status hrnn_budget_train(hrnn_index* h, const float* feat, const uint8_t* l
         need(h, "index");
         need(feat, "feat");
         need(labels, "labels");
+        h->ix.generation++;  // new weights: captured plans record the old ones
         set_device(h);
         const float l = hrnn::budget_train(h->ix, feat, labels, n, epochs, batch, lr, seed);
         if (final_loss) *final_loss = l;
@@ -483,6 +527,7 @@ hrnn_status hrnn_budget_set_weights(hrnn_index* h, const float* params) {
     return guard([&] {
         need(h, "index");
         need(params, "params");
+        h->ix.generation++;  // new weights: captured plans record the old ones
         set_device(h);
         hrnn::budget_set_weights(h->ix, params);
     });

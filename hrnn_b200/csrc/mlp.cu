@@ -193,13 +193,19 @@ void Mlp::ensure_work(int B) {
 
 void Mlp::forward(const float* X, int B, cudaStream_t s) {
     ensure_work(B);
-    k_normalize<<<blocks((size_t)B * kMlpIn), 256, 0, s>>>(X, norm.as<float>(), xn.as<float>(), (size_t)B * kMlpIn);
+    forward_into(X, B, xn.as<float>(), z1.as<float>(), a1.as<float>(), z2.as<float>(), a2.as<float>(), z3.as<float>(),
+                 s);
+}
+
+void Mlp::forward_into(const float* X, int B, float* xn_, float* z1_, float* a1_, float* z2_, float* a2_, float* z3_,
+                       cudaStream_t s) const {
+    k_normalize<<<blocks((size_t)B * kMlpIn), 256, 0, s>>>(X, norm.as<float>(), xn_, (size_t)B * kMlpIn);
     CUDA_LAUNCH_CHECK();
     // the two 256 x 256 layers on the tensor cores (GELU in the epilogue), the
     // 2-output layer on the CUDA cores
-    mlp_layer_tc(xn.as<float>(), B, w(0), b(0), nullptr, z1.as<float>(), a1.as<float>(), true, tc_err.as<int>(), s);
-    mlp_layer_tc(a1.as<float>(), B, w(1), b(1), nullptr, z2.as<float>(), a2.as<float>(), true, tc_err.as<int>(), s);
-    gemm(false, true, a2.as<float>(), w(2), z3.as<float>(), b(2), B, kMlpOut, kMlpH, kMlpH, kMlpH, 0.f, s);
+    mlp_layer_tc(xn_, B, w(0), b(0), nullptr, z1_, a1_, true, tc_err.as<int>(), s);
+    mlp_layer_tc(a1_, B, w(1), b(1), nullptr, z2_, a2_, true, tc_err.as<int>(), s);
+    gemm(false, true, a2_, w(2), z3_, b(2), B, kMlpOut, kMlpH, kMlpH, kMlpH, 0.f, s);
 }
 
 // Gradients of the mean BCE over the batch into gr[] (forward must have run on X;

@@ -27,6 +27,10 @@ struct Mlp {
     void init(uint64_t seed, cudaStream_t s);  // random weights, identity normalisation
     void ensure_work(int B);
     void forward(const float* X, int B, cudaStream_t s);  // logits in z3
+    // The same into caller buffers (xn [B x In], z1 a1 z2 a2 [B x H], z3 [B x Out]):
+    // no allocation, so it can be recorded in a graph that outlives the members'.
+    void forward_into(const float* X, int B, float* xn_, float* z1_, float* a1_, float* z2_, float* a2_, float* z3_,
+                      cudaStream_t s) const;
     void backward(const float* X, const uint8_t* Y, int B, float* loss, cudaStream_t s);
     void adam(float lr, float wd, cudaStream_t s);
     void check_tc();  // after a synchronisation: fails if a tensor-core wait ran out
@@ -50,6 +54,9 @@ struct Budget {
 // mlp_tc.cu: tcgen05 layer out = act(norm(A) W^T + b), A [M x 256], W [256 x 256]
 void mlp_layer_tc(const float* A, int M, const float* W, const float* bias, const float* nrm, float* out_z,
                   float* out_a, bool gelu, int* err, cudaStream_t s);
+// The layer kernel's launch attributes on the current device (before a stream
+// capture that records the layer).
+void mlp_layer_tc_prepare();
 
 // search_plain.cu
 Budget& budget_of(Index& ix);

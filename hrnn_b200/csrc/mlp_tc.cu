@@ -188,12 +188,19 @@ __global__ void __launch_bounds__(128, 1) k_mlp_layer_tc(const float* __restrict
 
 }  // namespace
 
+void mlp_layer_tc_prepare() {
+    CUDA_CHECK(cudaFuncSetAttribute(k_mlp_layer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemTC));
+}
+
 // out_z / out_a (either may be null): [M x 256] FP32.  nrm: input normalisation
 // (mean[256], inv[256]) or null.  err: device int set to 1 if a wait ran out.
 void mlp_layer_tc(const float* A, int M, const float* W, const float* bias, const float* nrm, float* out_z,
                   float* out_a, bool gelu, int* err, cudaStream_t s) {
     if (M <= 0) return;
-    CUDA_CHECK(cudaFuncSetAttribute(k_mlp_layer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemTC));
+    // a stream being recorded into a graph gets the launch alone (mlp_layer_tc_prepare ran before the capture)
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    CUDA_CHECK(cudaStreamIsCapturing(s, &cs));
+    if (cs == cudaStreamCaptureStatusNone) mlp_layer_tc_prepare();
     k_mlp_layer_tc<<<(unsigned)((M + kTM - 1) / kTM), 128, kSmemTC, s>>>(A, M, W, bias, nrm, out_z, out_a,
                                                                           gelu ? 1 : 0, err);
     CUDA_LAUNCH_CHECK();

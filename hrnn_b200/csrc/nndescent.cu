@@ -1424,6 +1424,7 @@ void refine_knng(Index& ix, int iters, int sample) {
     // Fewer, larger chunks are cheaper: every merge pass reads and writes the
     // lists of all targets it touches.
     double prop_per_pair = 0.0;
+    uint32_t retry_cap = UINT32_MAX;  // set when a chunk overflowed the buffer, until it is done
     const size_t merge_smem = merge_cta_bytes(K);
     if (merge_smem > 227 * 1024 || merge_window(K) < 256)
         fail(HRNN_ERR_ARG, "refineKNNG: K_knng too large for the merge kernel");
@@ -1491,6 +1492,7 @@ void refine_knng(Index& ix, int iters, int sample) {
             if (prop_per_pair > 0.0 && pairs_per_node > 0.0)
                 chunk = (uint32_t)std::max(1.0, std::min((double)n, 0.7 * (double)ptarget /
                                                                        (prop_per_pair * pairs_per_node)));
+            chunk = std::min(chunk, retry_cap);  // a chunk that overflowed is redone at most this large
             uint32_t node1 = std::min<uint32_t>(n, node0 + chunk);
             k_thresholds<<<(n + 255) / 256, 256, 0, s>>>(hdr, dist, n, K, thr.as<float>());
             CUDA_LAUNCH_CHECK();
@@ -1527,13 +1529,20 @@ void refine_knng(Index& ix, int iters, int sample) {
             t_join += elapsed(ev[3], ev[4]);
             if (np > pcap) {
                 if (chunk == 1) fail(HRNN_ERR_NOMEM, "refineKNNG: proposal buffer too small for one node");
-                chunk = std::max<uint32_t>(1, chunk / 4);  // redo this chunk smaller (the join is pure)
+                // Redo this chunk smaller (the join is pure): np counts every proposal
+                // the attempt reserved, so half the buffer at the attempt's own density
+                // bounds the retry (the rate that sized the chunk is an average and
+                // would size it the same again).
+                retry_cap = (uint32_t)std::max(1.0, std::min((double)chunk / 4.0,
+                                                             (double)chunk * 0.5 * (double)pcap / (double)np));
+                chunk = retry_cap;
                 // the pair and screen counts of the dropped attempt start over
                 CUDA_CHECK(cudaMemcpyAsync(d_njoin, &njoin_ok, 8, cudaMemcpyHostToDevice, s));
                 if (tcj) CUDA_CHECK(cudaMemcpyAsync(d_jc, &jc_ok, sizeof(jc_ok), cudaMemcpyHostToDevice, s));
                 CUDA_CHECK(cudaStreamSynchronize(s));
                 continue;
             }
+            retry_cap = UINT32_MAX;
             const unsigned long long njoin_prev = njoin_ok, nprop_prev = nprop_ok;
             CUDA_CHECK(cudaMemcpyAsync(&njoin_ok, d_njoin, 8, cudaMemcpyDeviceToHost, s));
             if (tcj) CUDA_CHECK(cudaMemcpyAsync(&jc_ok, d_jc, sizeof(jc_ok), cudaMemcpyDeviceToHost, s));

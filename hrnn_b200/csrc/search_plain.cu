@@ -82,8 +82,11 @@ __global__ void __launch_bounds__(128) k_phase_a(DevView v, const float* __restr
                                                  SearchCounters* __restrict__ ctr,
                                                  const uint32_t* __restrict__ qlist, uint32_t m_over,
                                                  uint32_t ef_over, uint32_t m_keep, float* __restrict__ proxd,
-                                                 uint32_t* __restrict__ next_q) {
-    // qlist: search only the listed queries (nq = list length); m_over / ef_over:
+                                                 uint32_t* __restrict__ next_q,
+                                                 const uint32_t* __restrict__ nq_dev) {
+    // qlist: search only the listed queries (nq = list length; nq_dev, when not
+    // null, holds the length in device memory, at most nq -- a launch recorded
+    // before the list is made); m_over / ef_over:
     // one (m, ef) for every query instead of the arrays (the beam is
     // max(ef, m) as in the reference); m_keep: write at least this many beam
     // entries (the learned budget's frontier; at most mmax); proxd: also write
@@ -93,6 +96,7 @@ __global__ void __launch_bounds__(128) k_phase_a(DevView v, const float* __restr
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     WarpSmem s = carve(smem_raw + (size_t)w * warp_smem_bytes(v.dim, efc, vc), v.dim, efc, vc);
     unsigned long long c_dist = 0, c_exp = 0;
+    if (nq_dev) nq = min(nq, *nq_dev);
     for (;;) {
         uint32_t j = 0;
         if (lane == 0) j = atomicAdd(next_q, 1u);
@@ -135,7 +139,8 @@ __global__ void __launch_bounds__(128) k_phase_a(DevView v, const float* __restr
 //     save_cap) -- the learned budget's frontier pass, which a fallback can
 //     resume;
 //   resume: start from the stored beam instead of the descent (its ids seed the
-//     visited cache), continue with the query's own ef, store nothing.
+//     visited cache), continue with the query's own ef, store nothing;
+//   nq_dev: as k_phase_a.
 template <int DM, bool R2>
 __global__ void __launch_bounds__(128, R2 ? 4 : 1) k_phase_a_fast(DevView v, const float* __restrict__ Q, uint32_t nq,
                                                       const uint32_t* __restrict__ qm,
@@ -146,11 +151,13 @@ __global__ void __launch_bounds__(128, R2 ? 4 : 1) k_phase_a_fast(DevView v, con
                                                       uint32_t ef_over, uint32_t m_keep, float* __restrict__ proxd,
                                                       uint32_t* __restrict__ next_q, uint32_t save_cap,
                                                       uint32_t* __restrict__ st_cnt, float* __restrict__ st_d,
-                                                      uint32_t* __restrict__ st_i, int resume) {
+                                                      uint32_t* __restrict__ st_i, int resume,
+                                                      const uint32_t* __restrict__ nq_dev) {
     extern __shared__ char smem_raw[];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     WarpSmem s = carve_fast(smem_raw + (size_t)w * fast_smem_bytes(v.dim, efc, vc), v.dim, efc, vc);
     unsigned long long c_dist = 0, c_exp = 0;
+    if (nq_dev) nq = min(nq, *nq_dev);
     for (;;) {
         uint32_t j = 0;
         if (lane == 0) j = atomicAdd(next_q, 1u);
@@ -485,6 +492,48 @@ DevView make_view(Index& ix) {
     return v;
 }
 
+// The phase-A kernel of a batch: distance mode dm (0/1 exact FP32, 2 BF16, 3
+// INT8), the reference-order beam (k_phase_a) or, for the reduced-precision
+// forms, the two-parent search (k_phase_a_fast; r2: its INT8 two-rows-per-lane
+// shape); the batch's queries, parameter arrays and proxy outputs.
+struct PhaseA {
+    bool fast;
+    int dm;
+    bool r2;
+    DevView v;
+    const float* q;
+    const uint32_t *qm, *qef;
+    uint32_t efc, mmax;
+    uint32_t *prox, *nprox;
+    SearchCounters* ctr;
+};
+
+static const void* phase_a_kernel(bool fast, int dm, bool r2) {
+    return fast ? (dm == 3 ? (r2 ? (const void*)k_phase_a_fast<3, true> : (const void*)k_phase_a_fast<3, false>)
+                           : (const void*)k_phase_a_fast<2, false>)
+                : (dm == 3 ? (const void*)k_phase_a<3>
+                           : dm == 2 ? (const void*)k_phase_a<2>
+                                     : dm == 1 ? (const void*)k_phase_a<1> : (const void*)k_phase_a<0>);
+}
+
+// One launch; qlist / m_over / ef_over / m_keep / proxd / save / resume / nq_dev as
+// documented at k_phase_a_fast (the exact kernel takes no save or resume).
+static void launch_phase_a(const PhaseA& p, unsigned g, int cw, uint32_t cv, size_t sm, cudaStream_t ls, uint32_t nqq,
+                    const uint32_t* qlist, uint32_t m_over, uint32_t ef_over, uint32_t m_keep, float* proxd,
+                    uint32_t* ctrq, uint32_t save_cap, uint32_t* st_cnt, float* st_d, uint32_t* st_i, int resume,
+                    const uint32_t* nq_dev) {
+    if (p.fast) {
+        auto k = p.dm == 3 ? (p.r2 ? k_phase_a_fast<3, true> : k_phase_a_fast<3, false>) : k_phase_a_fast<2, false>;
+        k<<<g, cw * 32, sm, ls>>>(p.v, p.q, nqq, p.qm, p.qef, p.efc, cv, p.mmax, p.prox, p.nprox, p.ctr, qlist, m_over,
+                                  ef_over, m_keep, proxd, ctrq, save_cap, st_cnt, st_d, st_i, resume, nq_dev);
+    } else {
+        auto k = p.dm == 3 ? k_phase_a<3> : p.dm == 2 ? k_phase_a<2> : p.dm == 1 ? k_phase_a<1> : k_phase_a<0>;
+        k<<<g, cw * 32, sm, ls>>>(p.v, p.q, nqq, p.qm, p.qef, p.efc, cv, p.mmax, p.prox, p.nprox, p.ctr, qlist, m_over,
+                                  ef_over, m_keep, proxd, ctrq, nq_dev);
+    }
+    CUDA_LAUNCH_CHECK();
+}
+
 uint64_t search_batch(Index& ix, const SearchArgs& a) {
     if (!ix.rknng_built) fail(HRNN_ERR_STATE, "searchRknn: RKNNG not built");
     ensure_flat_rknng(ix);
@@ -525,7 +574,12 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
     // (two-pass mode) the frontier beam is that ef.
     const bool two_pass = learned && ix.budget->ef > 0;
     if (learned) mmax = std::max<uint32_t>(mmax, kFrontier);
-    if (two_pass) efmax = std::max<uint32_t>(efmax, ix.budget->ef);
+    // two-pass mode: the frontier pass stores its beam with a reserve beyond the
+    // level ef for the second search to resume (the reduced-precision forms); the
+    // batch's beam capacity holds it, so the stored beam does not depend on the
+    // batch's largest ef
+    const uint32_t reserve = two_pass ? (std::max(2 * ix.budget->ef, ix.budget->ef + 32) + 31) & ~31u : 0;
+    if (two_pass) efmax = std::max<uint32_t>(efmax, reserve);
     DevView v = make_view(ix);
     const uint32_t efc = (efmax + 31) & ~31u;
     // Visited-cache slots (lossy; a miss costs a recomputed row).  1024 rather than
@@ -579,13 +633,7 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
         const int dm = int8 ? 3 : mixed ? 2 : fusedsimd ? 1 : 0;
         // r2: the INT8 two-parent search loads all 64 rows of a step at once (a launch-shape choice)
         bool r2 = false;
-        auto kfun_of = [&](bool two) {
-            return fast ? (dm == 3 ? (two ? (const void*)k_phase_a_fast<3, true> : (const void*)k_phase_a_fast<3, false>)
-                                   : (const void*)k_phase_a_fast<2, false>)
-                        : (dm == 3 ? (const void*)k_phase_a<3>
-                                   : dm == 2 ? (const void*)k_phase_a<2>
-                                             : dm == 1 ? (const void*)k_phase_a<1> : (const void*)k_phase_a<0>);
-        };
+        auto kfun_of = [&](bool two) { return phase_a_kernel(fast, dm, two); };
         auto smem_for = [&](uint32_t cv, int cw) {
             return (fast ? fast_smem_bytes(v.dim, efc, cv) : warp_smem_bytes(v.dim, efc, cv)) * (size_t)cw;
         };
@@ -596,38 +644,9 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
         auto launch = [&](unsigned g, int cw, uint32_t cv, size_t sm, uint32_t nqq, const uint32_t* qlist,
                           uint32_t m_over, uint32_t ef_over, uint32_t m_keep, float* proxd, uint32_t* ctrq,
                           uint32_t save_cap, uint32_t* st_cnt, float* st_d, uint32_t* st_i, int resume) {
-            if (fast && dm == 3 && r2)
-                k_phase_a_fast<3, true><<<g, cw * 32, sm, ls>>>(v, a.d_q, nqq, a.d_m, a.d_ef, efc, cv, mmax,
-                                                               prox.as<uint32_t>(), nprox.as<uint32_t>(), ctr, qlist,
-                                                               m_over, ef_over, m_keep, proxd, ctrq, save_cap, st_cnt,
-                                                               st_d, st_i, resume);
-            else if (fast && dm == 3)
-                k_phase_a_fast<3, false><<<g, cw * 32, sm, ls>>>(v, a.d_q, nqq, a.d_m, a.d_ef, efc, cv, mmax,
-                                                                prox.as<uint32_t>(), nprox.as<uint32_t>(), ctr, qlist,
-                                                                m_over, ef_over, m_keep, proxd, ctrq, save_cap, st_cnt,
-                                                                st_d, st_i, resume);
-            else if (fast)
-                k_phase_a_fast<2, false><<<g, cw * 32, sm, ls>>>(v, a.d_q, nqq, a.d_m, a.d_ef, efc, cv, mmax,
-                                                         prox.as<uint32_t>(), nprox.as<uint32_t>(), ctr, qlist,
-                                                         m_over, ef_over, m_keep, proxd, ctrq, save_cap, st_cnt, st_d,
-                                                         st_i, resume);
-            else if (dm == 3)
-                k_phase_a<3><<<g, cw * 32, sm, ls>>>(v, a.d_q, nqq, a.d_m, a.d_ef, efc, cv, mmax, prox.as<uint32_t>(),
-                                                    nprox.as<uint32_t>(), ctr, qlist, m_over, ef_over, m_keep, proxd,
-                                                    ctrq);
-            else if (dm == 2)
-                k_phase_a<2><<<g, cw * 32, sm, ls>>>(v, a.d_q, nqq, a.d_m, a.d_ef, efc, cv, mmax, prox.as<uint32_t>(),
-                                                    nprox.as<uint32_t>(), ctr, qlist, m_over, ef_over, m_keep, proxd,
-                                                    ctrq);
-            else if (dm == 1)
-                k_phase_a<1><<<g, cw * 32, sm, ls>>>(v, a.d_q, nqq, a.d_m, a.d_ef, efc, cv, mmax, prox.as<uint32_t>(),
-                                                    nprox.as<uint32_t>(), ctr, qlist, m_over, ef_over, m_keep, proxd,
-                                                    ctrq);
-            else
-                k_phase_a<0><<<g, cw * 32, sm, ls>>>(v, a.d_q, nqq, a.d_m, a.d_ef, efc, cv, mmax, prox.as<uint32_t>(),
-                                                    nprox.as<uint32_t>(), ctr, qlist, m_over, ef_over, m_keep, proxd,
-                                                    ctrq);
-            CUDA_LAUNCH_CHECK();
+            PhaseA pa{fast, dm, r2, v, a.d_q, a.d_m, a.d_ef, efc, mmax, prox.as<uint32_t>(), nprox.as<uint32_t>(), ctr};
+            launch_phase_a(pa, g, cw, cv, sm, ls, nqq, qlist, m_over, ef_over, m_keep, proxd, ctrq, save_cap, st_cnt,
+                           st_d, st_i, resume, nullptr);
         };
         uint32_t* d_qa = d_next + 4;  // work counters of the phase-A launches (zeroed with d_rcount)
         // Launch shape: the tuned one of this (distance mode, beam size), else timed
@@ -717,10 +736,9 @@ uint64_t search_batch(Index& ix, const SearchArgs& a) {
             uint32_t* fb_count = b.decided.as<uint32_t>();
             unsigned long long* levels = (unsigned long long*)(b.decided.as<char>() + 8);
             CUDA_CHECK(cudaMemsetAsync(b.decided.p, 0, 64, s));
-            // the stored frontier beam: the level beam plus a reserve (up to twice
-            // the level ef, within the batch's largest beam) that the fallback resumes
-            const uint32_t save_cap =
-                (two_pass && fast) ? std::min<uint32_t>(efc, (std::max(2 * b.ef, b.ef + 32) + 31) & ~31u) : 0;
+            // the stored frontier beam: the level beam plus a reserve (twice the
+            // level ef, at least 32 more entries) that the fallback resumes
+            const uint32_t save_cap = (two_pass && fast) ? reserve : 0;
             uint32_t *st_cnt = nullptr, *st_i = nullptr;
             float* st_d = nullptr;
             if (save_cap) {
@@ -1001,14 +1019,15 @@ void budget_features(Index& ix, const float* d_q, size_t nq, uint32_t k, uint32_
         kern<<<grid, wpb * 32, smem_a, s>>>(v, d_q, (uint32_t)nq, nullptr, nullptr, efc, vc, mmax,
                                             prox.as<uint32_t>(), nprox.as<uint32_t>(),
                                             ix.counters.as<SearchCounters>(), nullptr, m, ef, kFrontier,
-                                            proxd.as<float>(), next.as<uint32_t>(), 0, nullptr, nullptr, nullptr, 0);
+                                            proxd.as<float>(), next.as<uint32_t>(), 0, nullptr, nullptr, nullptr, 0,
+                                            nullptr);
     } else {
         auto kern = int8 ? k_phase_a<3> : mixed ? k_phase_a<2> : ((ix.order.fused & 1) != 0) ? k_phase_a<1> : k_phase_a<0>;
         CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_a));
         kern<<<grid, wpb * 32, smem_a, s>>>(v, d_q, (uint32_t)nq, nullptr, nullptr, efc, vc, mmax,
                                             prox.as<uint32_t>(), nprox.as<uint32_t>(),
                                             ix.counters.as<SearchCounters>(), nullptr, m, ef, kFrontier,
-                                            proxd.as<float>(), next.as<uint32_t>());
+                                            proxd.as<float>(), next.as<uint32_t>(), nullptr);
     }
     CUDA_LAUNCH_CHECK();
     k_budget_features<<<(unsigned)((nq * 32 + 255) / 256), 256, 0, s>>>(v, d_q, (uint32_t)nq, prox.as<uint32_t>(),
@@ -1035,17 +1054,26 @@ void budget_features(Index& ix, const float* d_q, size_t nq, uint32_t k, uint32_
 
 namespace {
 
+// mmax: the bound of a query's verified proxies (m_max); mstride: the row stride
+// of the proxy arrays (the learned budget's frontier keeps kFrontier entries).
 struct PlanLaunch {
-    uint32_t efc, vc, mmax, wpb, grid_a, grid_bc, kidx, slots, hcap;
+    uint32_t efc, vc, mmax, mstride, reserve, wpb, grid_a, grid_bc, kidx, slots, hcap;
     size_t smem_a, smem_bc, smem_w, tmax;
-    bool mixed, int8, fusedsimd, counts, fast, r2;
+    bool mixed, int8, fusedsimd, counts, fast, r2, learned, two_pass;
 };
 
 PlanLaunch plan_launch_shape(Index& ix, const SearchPlan& p) {
     PlanLaunch L{};
     DevView v = make_view(ix);
     L.mmax = std::max<uint32_t>(1, p.m_max);
-    const uint32_t efmax = std::max(std::max<uint32_t>(1, p.ef_max), L.mmax);
+    // the learned budget as search_batch runs it: frontier pass, MLP, and in
+    // two-pass mode (level ef > 0) a second search of the other queries
+    L.learned = ix.budget && ix.budget->enabled && ix.budget->mlp.ready && ix.dim % 4 == 0;
+    L.two_pass = L.learned && ix.budget->ef > 0;
+    L.mstride = L.learned ? std::max<uint32_t>(L.mmax, kFrontier) : L.mmax;
+    uint32_t efmax = std::max(std::max<uint32_t>(1, p.ef_max), L.mmax);
+    L.reserve = L.two_pass ? (std::max(2 * ix.budget->ef, ix.budget->ef + 32) + 31) & ~31u : 0;  // as search_batch
+    if (L.two_pass) efmax = std::max(efmax, L.reserve);
     L.efc = (efmax + 31) & ~31u;
     L.vc = 512;
     L.fusedsimd = (ix.order.fused & 1) != 0;
@@ -1084,12 +1112,24 @@ __global__ void k_cap_totals(const uint64_t* __restrict__ total, uint32_t n, uin
     if (i < n) out[i] = min(total[i], qcap);
 }
 
+// A plan verified in two groups: group 1's slices follow group 0's (*base: group
+// 0's total, its offsets' last entry).
+__global__ void k_add_base(uint64_t* __restrict__ off, uint32_t n, const uint64_t* __restrict__ base) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) off[i] += *base;
+}
+
+// Each query's slice offset from its group's offsets.
+__global__ void k_merge_offsets(const uint8_t* __restrict__ grp, uint32_t nq, const uint64_t* __restrict__ off0,
+                                const uint64_t* __restrict__ off1, uint64_t* __restrict__ out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nq) out[i] = grp[i] ? off1[i] : off0[i];
+}
+
 void plan_create(SearchPlan& p, cudaStream_t s) {
     Index& ix = *p.ix;
     if (!ix.rknng_built) fail(HRNN_ERR_STATE, "searchRknn: RKNNG not built");
     ensure_flat_rknng(ix);
-    if (ix.budget && ix.budget->enabled)
-        fail(HRNN_ERR_STATE, "search plan: the learned budget is not captured; disable it first");
     if (p.nq == 0 || p.nq > (1u << 30)) fail(HRNN_ERR_ARG, "search plan: nq must be in [1, 2^30]");
     if (p.m_max == 0 || p.ef_max == 0) fail(HRNN_ERR_ARG, "search plan: m_max and ef_max must be >= 1");
     if (std::max(p.m_max, p.ef_max) > (1u << 16)) fail(HRNN_ERR_ARG, "searchRknn: ef_search/m too large (max 65536)");
@@ -1134,11 +1174,17 @@ void plan_create(SearchPlan& p, cudaStream_t s) {
     const size_t per_slot = (size_t)hcap * 8 + L.tmax * 4;
     size_t slots = std::max<size_t>(4, std::min<size_t>((size_t)nsm * 4, (free_b / 8) / per_slot) / 4 * 4);
     L.slots = (uint32_t)slots;
+    // verification: the streaming kernel of the INT8 form where search_batch takes it, else the CTA kernel
+    const bool stream = L.int8 && L.mixed && !L.counts && stream_supported(v) && !verify_table_forced();
+    // learned budget, two-pass, streaming verification: the second search runs on
+    // a second stream beside the verification of the confident queries (group 0),
+    // and its queries verify afterwards as group 1 (as search_batch)
+    const bool split = L.two_pass && L.fast && stream && !learned_serial();
     // buffers
     p.inputs.alloc((3 * nq + 8) * 4);  // m | ef | flag, 3 spare | overflow list
-    p.prox.alloc(nq * L.mmax * 4);
+    p.prox.alloc(nq * L.mstride * 4);
     p.nprox.alloc(nq * 4);
-    p.plen.alloc(nq * L.mmax * 4);
+    p.plen.alloc(nq * L.mstride * 4);
     p.qtot.alloc((nq + 1) * 8 * 3 + (nq + 1) * 4 + 64);
     p.res.alloc(std::max<size_t>(res_entries, 1) * 8);
     p.kcol.alloc(std::max<size_t>(ix.cur, 1) * 4);
@@ -1157,25 +1203,64 @@ void plan_create(SearchPlan& p, cudaStream_t s) {
     uint32_t* pm = p.inputs.as<uint32_t>();
     uint32_t* pef = pm + nq;
     uint32_t* flag = pef + nq;
+    // learned budget: features, MLP activations, frontier distances, decisions,
+    // stored frontier beams, groups and group 1's totals / offsets
+    Budget* bud = L.learned ? ix.budget.get() : nullptr;
+    uint32_t save_cap = 0;
+    uint32_t *fb_list = nullptr, *fb_count = nullptr, *st_cnt = nullptr, *st_i = nullptr;
+    float *feat = nullptr, *proxd = nullptr, *st_d = nullptr, *mlpw = nullptr;
+    unsigned long long* levels = nullptr;
+    uint8_t* grp = nullptr;
+    uint64_t *d_total2 = nullptr, *d_totc2 = nullptr, *d_resoff2 = nullptr, *d_resoffm = nullptr;
+    if (bud) {
+        ensure_projection(ix, *bud);
+        save_cap = (L.two_pass && L.fast) ? L.reserve : 0;
+        p.lfeat.alloc(nq * kMlpIn * 4);
+        p.lmlp.alloc(nq * (kMlpIn + 4 * kMlpH + kMlpOut) * 4);
+        p.lproxd.alloc(nq * L.mstride * 4);
+        p.lfb.alloc(nq * 4 + 64);
+        p.lgrp.alloc(nq + 16);
+        p.loff.alloc((nq + 1) * 8 * 4);
+        if (save_cap) p.lsaved.alloc(nq * 4 + (size_t)nq * save_cap * 8 + 256);
+        feat = p.lfeat.as<float>();
+        mlpw = p.lmlp.as<float>();
+        proxd = p.lproxd.as<float>();
+        fb_count = p.lfb.as<uint32_t>();                                  // [0] count, [2..7] level counts
+        levels = (unsigned long long*)(p.lfb.as<char>() + 8);
+        fb_list = p.lfb.as<uint32_t>() + 16;
+        grp = split ? p.lgrp.as<uint8_t>() : nullptr;
+        d_total2 = p.loff.as<uint64_t>();
+        d_totc2 = d_total2 + (nq + 1);
+        d_resoff2 = d_totc2 + (nq + 1);
+        d_resoffm = d_resoff2 + (nq + 1);
+        if (save_cap) {
+            st_cnt = p.lsaved.as<uint32_t>();
+            st_d = (float*)(p.lsaved.as<char>() + ((nq * 4 + 255) & ~(size_t)255));
+            st_i = (uint32_t*)(st_d + (size_t)nq * save_cap);
+        }
+        if (split) {
+            CUDA_CHECK(cudaStreamCreateWithFlags(&p.aux, cudaStreamNonBlocking));
+            CUDA_CHECK(cudaEventCreateWithFlags(&p.ev_fork, cudaEventDisableTiming));
+            CUDA_CHECK(cudaEventCreateWithFlags(&p.ev_join, cudaEventDisableTiming));
+        }
+        p.budget_levels = levels;
+        mlp_layer_tc_prepare();
+    }
     // scan scratch sized outside the capture (both scans take nq + 1 entries)
     exclusive_scan_u64(d_total, d_resoff, nq + 1, s, p.tmp);
     exclusive_scan_u32_to_u64(d_rcount, p.d_out_off, nq + 1, s, p.tmp);
-    auto ka = L.int8 ? k_phase_a<3> : L.mixed ? k_phase_a<2> : L.fusedsimd ? k_phase_a<1> : k_phase_a<0>;
-    auto kaf = L.int8 ? (L.r2 ? k_phase_a_fast<3, true> : k_phase_a_fast<3, false>) : k_phase_a_fast<2, false>;
-    const void* kaf_or_ka = L.fast ? (const void*)kaf : (const void*)ka;
-    CUDA_CHECK(cudaFuncSetAttribute(kaf_or_ka, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem_a));
+    const int dm = L.int8 ? 3 : L.mixed ? 2 : L.fusedsimd ? 1 : 0;
+    const void* kfun = phase_a_kernel(L.fast, dm, L.r2);
+    CUDA_CHECK(cudaFuncSetAttribute(kfun, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem_a));
     int per_sm = 1;
-    CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kaf_or_ka, L.wpb * 32, L.smem_a));
+    CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfun, L.wpb * 32, L.smem_a));
     L.grid_a = (uint32_t)std::max<size_t>(1, std::min<size_t>((nq + L.wpb - 1) / L.wpb, (size_t)nsm * std::max(per_sm, 1)));
-    // verification: the streaming kernel of the INT8 form where search_batch takes it, else the CTA kernel
-    // verification: the streaming kernel of the INT8 form where search_batch takes it, else the CTA kernel
-    const bool stream = L.int8 && L.mixed && !L.counts && stream_supported(v) && !verify_table_forced();
     KCta kc = ix.wide ? pick_bc<uint64_t>(L.fusedsimd, L.counts, L.mixed) : pick_bc<uint32_t>(L.fusedsimd, L.counts, L.mixed);
     if (stream) {
-        p.sb.reserve((uint32_t)nq, v.dim, nq * L.mmax, stream_max_chunks(nq * L.tmax, nq * L.mmax));
+        p.sb.reserve((uint32_t)nq, v.dim, nq * L.mstride, stream_max_chunks(nq * L.tmax, nq * L.mstride));
         stream_prepare(v, ix.wide, L.fusedsimd);
         // the scan's scratch sized outside the capture
-        exclusive_scan_u32_to_u64(p.sb.cnt.as<uint32_t>(), p.sb.coff.as<uint64_t>(), nq * L.mmax + 1, s, p.sb.tmp);
+        exclusive_scan_u32_to_u64(p.sb.cnt.as<uint32_t>(), p.sb.coff.as<uint64_t>(), nq * L.mstride + 1, s, p.sb.tmp);
     } else {
         CUDA_CHECK(cudaFuncSetAttribute(kc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem_bc));
         per_sm = 1;
@@ -1199,42 +1284,90 @@ void plan_create(SearchPlan& p, cudaStream_t s) {
     CUDA_CHECK(cudaMemsetAsync(flag, 0, 4, s));
     k_plan_inputs<<<(unsigned)((nq + 255) / 256), 256, 0, s>>>(p.d_m, p.d_ef, (uint32_t)nq, L.mmax, p.ef_max, pm, pef,
                                                                flag);
-    if (L.fast)
-        kaf<<<L.grid_a, L.wpb * 32, L.smem_a, s>>>(v, p.d_q, (uint32_t)nq, pm, pef, L.efc, L.vc, L.mmax,
-                                                    p.prox.as<uint32_t>(), p.nprox.as<uint32_t>(), ctr, nullptr, 0, 0,
-                                                    0, nullptr, d_next + 4, 0, nullptr, nullptr, nullptr, 0);
-    else
-        ka<<<L.grid_a, L.wpb * 32, L.smem_a, s>>>(v, p.d_q, (uint32_t)nq, pm, pef, L.efc, L.vc, L.mmax,
-                                                   p.prox.as<uint32_t>(), p.nprox.as<uint32_t>(), ctr, nullptr, 0, 0,
-                                                   0, nullptr, d_next + 4);
-    {
-        const size_t tot = nq * L.mmax;
-        auto kb = ix.wide ? k_phase_b_count<uint64_t> : k_phase_b_count<uint32_t>;
-        kb<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(v, (uint32_t)nq, p.d_kp, L.mmax, p.prox.as<uint32_t>(),
-                                                         p.nprox.as<uint32_t>(), p.plen.as<uint32_t>(), d_total,
-                                                         nullptr, 0);
-    }
-    k_cap_totals<<<(unsigned)((nq + 1 + 255) / 256), 256, 0, s>>>(d_total, (uint32_t)nq + 1, qcap, d_totc);
-    exclusive_scan_u64(d_totc, d_resoff, nq + 1, s, p.tmp);
+    // the per-call column of kdist(p, k-1) (hrnn.h:286-293): features and verification
     k_kdist_column<<<(unsigned)((ix.cur + 255) / 256), 256, 0, s>>>(v, L.kidx, p.kcol.as<float>());
+    const PhaseA pa{L.fast, dm, L.r2, v, p.d_q, pm, pef, L.efc, L.mstride, p.prox.as<uint32_t>(),
+                    p.nprox.as<uint32_t>(), ctr};
+    if (!bud) {
+        launch_phase_a(pa, L.grid_a, (int)L.wpb, L.vc, L.smem_a, s, (uint32_t)nq, nullptr, 0, 0, 0, nullptr, d_next + 4,
+                       0, nullptr, nullptr, nullptr, 0, nullptr);
+    } else {
+        // frontier pass, features, MLP, decision (search_batch's learned path)
+        CUDA_CHECK(cudaMemsetAsync(p.lfb.p, 0, 64, s));
+        launch_phase_a(pa, L.grid_a, (int)L.wpb, L.vc, L.smem_a, s, (uint32_t)nq, nullptr,
+                       L.two_pass ? bud->m[1] : 0, L.two_pass ? bud->ef : 0, kFrontier, proxd, d_next + 4, save_cap,
+                       st_cnt, st_d, st_i, 0, nullptr);
+        k_budget_features<<<(unsigned)((nq * 32 + 255) / 256), 256, 0, s>>>(
+            v, p.d_q, (uint32_t)nq, p.prox.as<uint32_t>(), proxd, p.nprox.as<uint32_t>(), L.mstride,
+            p.kcol.as<float>(), bud->proj.as<float>(), feat);
+        float* xn = mlpw;
+        float* z1 = xn + nq * kMlpIn;
+        float* a1 = z1 + nq * kMlpH;
+        float* z2 = a1 + nq * kMlpH;
+        float* a2 = z2 + nq * kMlpH;
+        float* z3 = a2 + nq * kMlpH;
+        bud->mlp.forward_into(feat, (int)nq, xn, z1, a1, z2, a2, z3, s);
+        k_budget_decide<<<(unsigned)((nq + 255) / 256), 256, 0, s>>>(z3, (uint32_t)nq, bud->confidence, bud->m[0],
+                                                                     bud->m[1], pm, L.two_pass ? 1 : 0,
+                                                                     p.nprox.as<uint32_t>(), fb_list, fb_count, levels,
+                                                                     grp);
+        if (L.two_pass) {
+            // the second search over the listed queries; their count is read on the device
+            cudaStream_t ls = s;
+            if (split) {
+                CUDA_CHECK(cudaEventRecord(p.ev_fork, s));
+                CUDA_CHECK(cudaStreamWaitEvent(p.aux, p.ev_fork, 0));
+                ls = p.aux;
+            }
+            launch_phase_a(pa, L.grid_a, (int)L.wpb, L.vc, L.smem_a, ls, (uint32_t)nq, fb_list, 0, 0, 0, nullptr,
+                           d_next + 5, save_cap, st_cnt, st_d, st_i, save_cap ? 1 : 0, fb_count);
+            if (split) CUDA_CHECK(cudaEventRecord(p.ev_join, p.aux));
+        }
+    }
     uint64_t* resbuf = p.res.as<uint64_t>();
     uint32_t* ovl = flag + 4;  // the overflow list (nq entries) after the clamp flag
-    if (stream)
-        stream_verify(v, ix.wide, L.fusedsimd, p.d_q, (uint32_t)nq, L.mmax, p.prox.as<uint32_t>(),
-                      p.plen.as<uint32_t>(), d_resoff, p.kcol.as<float>(), L.kidx, resbuf, d_rcount, ovl,
-                      d_next + 1, ctr, p.sb, nsm, s);
-    else
-        kc<<<L.grid_bc, 256, L.smem_bc, s>>>(v, p.d_q, (uint32_t)nq, L.mmax, p.prox.as<uint32_t>(),
-                                             p.nprox.as<uint32_t>(), p.plen.as<uint32_t>(), d_total, d_resoff,
-                                             p.threshold, p.kcol.as<float>(), L.kidx, resbuf, d_rcount, d_next, ovl,
-                                             d_next + 1, ctr);
-    kov<<<(unsigned)(slots / 4), 128, L.smem_w, s>>>(v, p.d_q, 0, L.mmax, p.prox.as<uint32_t>(),
-                                                      p.nprox.as<uint32_t>(), p.plen.as<uint32_t>(), d_resoff,
-                                                      p.threshold, L.kidx, L.hcap, p.hkey.as<uint32_t>(),
-                                                      p.hcnt.as<uint32_t>(), p.lp.as<uint32_t>(), L.tmax, resbuf,
-                                                      d_rcount, d_next + 2, ovl, ctr, d_next + 1, flag);
+    // posting counts, slices and verification of the queries with g[q] == want (all
+    // for g null); base: group 0's offsets, which group 1's slices follow
+    auto verify_group = [&](const uint8_t* g, uint8_t want, uint64_t* tot, uint64_t* totc, uint64_t* roff,
+                            const uint64_t* base) {
+        const size_t npairs = nq * L.mstride;
+        auto kb = ix.wide ? k_phase_b_count<uint64_t> : k_phase_b_count<uint32_t>;
+        kb<<<(unsigned)((npairs + 255) / 256), 256, 0, s>>>(v, (uint32_t)nq, p.d_kp, L.mstride, p.prox.as<uint32_t>(),
+                                                            p.nprox.as<uint32_t>(), p.plen.as<uint32_t>(), tot, g,
+                                                            want);
+        k_cap_totals<<<(unsigned)((nq + 1 + 255) / 256), 256, 0, s>>>(tot, (uint32_t)nq + 1, qcap, totc);
+        exclusive_scan_u64(totc, roff, nq + 1, s, p.tmp);
+        if (base) k_add_base<<<(unsigned)((nq + 1 + 255) / 256), 256, 0, s>>>(roff, (uint32_t)nq + 1, base);
+        if (stream)
+            stream_verify(v, ix.wide, L.fusedsimd, p.d_q, (uint32_t)nq, L.mstride, p.prox.as<uint32_t>(),
+                          p.plen.as<uint32_t>(), roff, p.kcol.as<float>(), L.kidx, resbuf, d_rcount, ovl,
+                          d_next + 1, ctr, p.sb, nsm, s, g, want);
+        else
+            kc<<<L.grid_bc, 256, L.smem_bc, s>>>(v, p.d_q, (uint32_t)nq, L.mstride, p.prox.as<uint32_t>(),
+                                                 p.nprox.as<uint32_t>(), p.plen.as<uint32_t>(), tot, roff,
+                                                 p.threshold, p.kcol.as<float>(), L.kidx, resbuf, d_rcount, d_next,
+                                                 ovl, d_next + 1, ctr);
+        kov<<<(unsigned)(slots / 4), 128, L.smem_w, s>>>(v, p.d_q, 0, L.mstride, p.prox.as<uint32_t>(),
+                                                          p.nprox.as<uint32_t>(), p.plen.as<uint32_t>(), roff,
+                                                          p.threshold, L.kidx, L.hcap, p.hkey.as<uint32_t>(),
+                                                          p.hcnt.as<uint32_t>(), p.lp.as<uint32_t>(), L.tmax, resbuf,
+                                                          d_rcount, d_next + 2, ovl, ctr, d_next + 1, flag);
+    };
+    const uint64_t* pack_off = d_resoff;
+    if (split) {
+        verify_group(grp, 0, d_total, d_totc, d_resoff, nullptr);
+        CUDA_CHECK(cudaStreamWaitEvent(s, p.ev_join, 0));
+        CUDA_CHECK(cudaMemsetAsync(d_total2, 0, (nq + 1) * 8, s));
+        CUDA_CHECK(cudaMemsetAsync(d_next, 0, 12, s));  // the verification's counters of group 0
+        verify_group(grp, 1, d_total2, d_totc2, d_resoff2, d_resoff + nq);
+        k_merge_offsets<<<(unsigned)((nq + 255) / 256), 256, 0, s>>>(grp, (uint32_t)nq, d_resoff, d_resoff2,
+                                                                     d_resoffm);
+        pack_off = d_resoffm;
+    } else {
+        verify_group(nullptr, 0, d_total, d_totc, d_resoff, nullptr);
+    }
     exclusive_scan_u32_to_u64(d_rcount, p.d_out_off, nq + 1, s, p.tmp);
-    k_pack_results_capped<<<(unsigned)nq, 128, 0, s>>>((uint32_t)nq, d_resoff, d_rcount, p.d_out_off, resbuf,
+    k_pack_results_capped<<<(unsigned)nq, 128, 0, s>>>((uint32_t)nq, pack_off, d_rcount, p.d_out_off, resbuf,
                                                         p.d_out_lab, p.cap);
     } catch (...) {
         cudaGraph_t g = nullptr;
@@ -1245,6 +1378,17 @@ void plan_create(SearchPlan& p, cudaStream_t s) {
     const cudaError_t ce = cudaStreamEndCapture(s, &p.graph);
     if (ce != cudaSuccess) fail(HRNN_ERR_CUDA, std::string("search plan: capture failed: ") + cudaGetErrorString(ce));
     CUDA_CHECK(cudaGraphInstantiate(&p.exec, p.graph, 0));
+    // kernel nodes of the graph (the launches of one run)
+    size_t nn = 0;
+    CUDA_CHECK(cudaGraphGetNodes(p.graph, nullptr, &nn));
+    std::vector<cudaGraphNode_t> nodes(nn);
+    if (nn) CUDA_CHECK(cudaGraphGetNodes(p.graph, nodes.data(), &nn));
+    p.kernel_nodes = 0;
+    for (auto nd : nodes) {
+        cudaGraphNodeType t;
+        CUDA_CHECK(cudaGraphNodeGetType(nd, &t));
+        if (t == cudaGraphNodeTypeKernel) ++p.kernel_nodes;
+    }
     p.generation = ix.generation;
 }
 

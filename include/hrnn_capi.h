@@ -197,10 +197,13 @@ hrnn_status hrnn_search_rknn_batch_device(hrnn_index* h, const float* d_queries,
  * reported by hrnn_search_plan_result), threshold and k fixed.  Staging is sized
  * for nq * m_max * (the index's longest reverse list) postings (HRNN_ERR_NOMEM
  * when that exceeds half the free device memory).  The precision form is the
- * index's at creation; the learned budget must be disabled.  A plan is bound to
- * the index as it was: any later call that changes the index (add, refine, build,
- * insert, compact, set_knng, set_l2_order, set_precision, set_ef) makes run fail
- * with HRNN_ERR_STATE.  Answers equal hrnn_search_rknn_batch_device's.
+ * index's at creation, and so is the learned budget when it is enabled (its
+ * frontier pass, MLP, levels and second search are recorded with the budget's
+ * settings and weights).  A plan is bound to the index as it was: any later call
+ * that changes the index or those settings (add, refine, build, insert, compact,
+ * set_knng, set_l2_order, set_precision, set_ef, set_budget, budget_train,
+ * budget_set_weights) makes run fail with HRNN_ERR_STATE.  Answers equal
+ * hrnn_search_rknn_batch_device's.
  *   hrnn_search_plan_result: waits for `stream`; *total = out_offsets[nq];
  *     *clamped = 1 if some query's m or ef_search was above the maxima;
  *     HRNN_ERR_CAPACITY when total > cap (labels then not written). */
@@ -211,6 +214,17 @@ hrnn_status hrnn_search_plan_create(hrnn_index* h, const float* d_queries, size_
                                     uint64_t* d_out_labels, size_t cap, void* stream, hrnn_search_plan** out);
 hrnn_status hrnn_search_plan_run(hrnn_search_plan* plan, void* stream);
 hrnn_status hrnn_search_plan_result(hrnn_search_plan* plan, void* stream, uint64_t* total, int* clamped);
+/* One run of a plan on a host batch: copies the nq queries and their m / K' /
+ * ef_search from host memory into the plan's input buffers (the device buffers
+ * given at creation), replays the graph, waits, and copies out_offsets (nq + 1)
+ * and the labels (at most cap; HRNN_ERR_CAPACITY beyond, labels not written) back
+ * to host memory.  The serving call of hrnn_search_rknn_batch for a fixed batch
+ * shape; *clamped as hrnn_search_plan_result. */
+hrnn_status hrnn_search_plan_run_host(hrnn_search_plan* plan, const float* queries, const uint32_t* m,
+                                      const uint32_t* K_prime, const uint32_t* ef_search, uint64_t* out_offsets,
+                                      uint64_t* out_labels, size_t cap, uint64_t* total, int* clamped, void* stream);
+/* Kernel launches one run of the plan makes (the graph's kernel nodes). */
+hrnn_status hrnn_search_plan_kernels(hrnn_search_plan* plan, size_t* n);
 void hrnn_search_plan_destroy(hrnn_search_plan* plan);
 
 /* compactForServing(max_k_serve) -- hrnn.h:299-364: dense kdist[n x max_k_serve]. */

@@ -69,8 +69,76 @@ def test_plan_replays_equal_batch_calls(index, precision):
             assert total == exp_off[-1] and total > 0
             assert np.array_equal(got_off, exp_off)
             assert np.array_equal(got_lab, exp_lab)
+        # the host-buffer run: the same batch copied in from host memory
+        hq = np.ascontiguousarray(Q, np.float32)
+        hm32, hkp32, hef32 = (np.ascontiguousarray(x, np.uint32) for x in (hm, hkp, hef))
+        hoff = np.zeros(nq + 1, np.uint64)
+        hlab = np.zeros(cap, np.uint64)
+        total, clamped = plan.run_host(hq.ctypes.data, hm32.ctypes.data, hkp32.ctypes.data, hef32.ctypes.data,
+                                       hoff.ctypes.data, hlab.ctypes.data, cap)
+        assert not clamped and total == exp_off[-1]
+        assert np.array_equal(hoff.astype(np.int64), exp_off)
+        assert np.array_equal(hlab[:total].astype(np.int64), exp_lab)
     finally:
         plan.close()
+        h.set_precision(H.PREC_FP32_EXACT)
+
+
+@pytest.mark.parametrize("efl", [0, 48])
+@pytest.mark.parametrize("precision", [H.PREC_INT8, H.PREC_BF16])
+def test_plan_learned_budget_replays_equal_batch_calls(index, precision, efl):
+    """The learned budget recorded in a plan (frontier pass, features, MLP, levels;
+    in two-pass mode the second search, beside the first group's verification in
+    the INT8 form): replays of two batches answer as the batch calls with the
+    budget on, and a later change of the budget invalidates the plan."""
+    import torch
+    from oracle import mlp
+    h = index
+    h.set_precision(precision)
+    nq, m_max, ef_max, k, cap = 3000, 8, 120, 10, 3000 * 64
+    # labels a linear function of one input feature decides, so the model's
+    # levels spread over the queries: level 0 above the median, level 1 above
+    # the lower quartile, the caller's m below it
+    Qtr = data.mixture(3000, 128, 32, 1.0, 7, 55)
+    h.budget_set_weights(mlp.init_params(3))
+    feat = h.budget_features(Qtr, k, 6, 100)
+    f0 = feat[:, 0]
+    Y = np.stack([f0 > np.median(f0), f0 > np.quantile(f0, 0.25)], 1).astype(np.uint8)
+    h.budget_train(feat, Y, epochs=30, batch=256, lr=2e-3, seed=2)
+    h.set_budget(True, 2, 4, efl, 0.8)
+    q = torch.zeros((nq, 128), dtype=torch.float32, device="cuda")
+    m = torch.zeros(nq, dtype=torch.int32, device="cuda")
+    kp = torch.zeros(nq, dtype=torch.int32, device="cuda")
+    ef = torch.zeros(nq, dtype=torch.int32, device="cuda")
+    off = torch.zeros(nq + 1, dtype=torch.int64, device="cuda")
+    lab = torch.zeros(cap, dtype=torch.int64, device="cuda")
+    plan = h.search_plan(q.data_ptr(), nq, m.data_ptr(), kp.data_ptr(), ef.data_ptr(), m_max, ef_max, 1.0, k,
+                         off.data_ptr(), lab.data_ptr(), cap)
+    try:
+        for seed in (1, 2):
+            Q, hm, hkp, hef = _batch(seed, nq, m_max, ef_max)
+            q.copy_(torch.from_numpy(Q))
+            m.copy_(torch.from_numpy(hm.astype(np.int32)))
+            kp.copy_(torch.from_numpy(hkp.astype(np.int32)))
+            ef.copy_(torch.from_numpy(hef.astype(np.int32)))
+            torch.cuda.synchronize()
+            plan.run()
+            total, clamped = plan.result()
+            assert not clamped
+            got_off, got_lab = off.cpu().numpy(), lab.cpu().numpy()[:total]
+            exp_off, exp_lab = _regular(h, torch, q, m, kp, ef, k, cap)
+            levels = h.last_search_stats()["n_budget"]
+            assert sum(levels) == nq and levels[2] > 0 and levels[0] + levels[1] > 0, levels
+            assert total == exp_off[-1] and total > 0
+            assert np.array_equal(got_off, exp_off)
+            assert np.array_equal(got_lab, exp_lab)
+        h.set_budget(True, 2, 4, efl, 0.9)  # other settings: the plan records the old ones
+        with pytest.raises(H.HrnnError) as e:
+            plan.run()
+        assert e.value.code == H.ERR_STATE
+    finally:
+        plan.close()
+        h.set_budget(False)
         h.set_precision(H.PREC_FP32_EXACT)
 
 
