@@ -199,14 +199,14 @@ def rknn_gt_fp64(torch, X, Q, kth, dev):
     return [np.sort(ids) for ids, _ in groundtruth.rknn_fp64(X, Q, kth, dev)]
 
 
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch of the two
-# search kernels, from a one-pass ncu capture (a couple of launches of each kernel)
-# of the bench command on the named workload, keyed by (precision form, phase,
-# learned budget) and tied to the kernel sources it was captured on: when the
-# sources have changed since (SEARCH_SOURCES hash differs), no traffic figure is
-# reported rather than a stale one.
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of the search kernels
+# per unit of work -- per beam distance for the beam search, per posting for the
+# verification -- from an ncu capture of the bench command on the 500k x 128
+# profiling case (the 1M index's capture would exceed the few GB a capture may
+# hold), keyed by (precision form, phase) and tied to the kernel sources it was
+# captured on: the bench line scales it by the units of its own launch, and
+# reports none when the sources have changed since (SEARCH_SOURCES hash differs).
 NCU_TRAFFIC = {}
-NCU_TRAFFIC_QUERIES = 10_000
 SEARCH_SOURCES = ("common.cuh", "beam.cuh", "beam_fast.cuh", "search_plain.cu", "search_bc.cu", "verify_stream.cu",
                   "mixed.cu", "budget.cu")
 
@@ -220,19 +220,21 @@ def search_src_hash() -> str:
     return hsh.hexdigest()[:16]
 
 
-def ncu_traffic(workload, form, phase, learned, nq):
-    """(DRAM bytes of one launch of that kernel scaled from the capture's queries to
-    nq, source note); (None, why) when not captured on the current kernels."""
-    cap = NCU_TRAFFIC.get(workload)
-    if not cap:
-        return None, "no capture of this workload"
-    if cap["src_hash"] != search_src_hash():
-        return None, f"capture {cap['src_hash']} predates the current kernel sources"
-    v = cap["bytes"].get((form, phase, bool(learned)))
-    if v is None:
+def ncu_traffic(form, phase, st):
+    """(DRAM bytes of one launch of that phase's kernel: the capture's bytes per
+    unit times this launch's units, source note); (None, why) when not captured on
+    the current kernel sources."""
+    if not NCU_TRAFFIC:
+        return None, "no capture of the current kernels"
+    if NCU_TRAFFIC["src_hash"] != search_src_hash():
+        return None, f"capture {NCU_TRAFFIC['src_hash']} predates the current kernel sources"
+    per_unit = NCU_TRAFFIC["per_unit"].get((form, phase))
+    if per_unit is None:
         return None, "form not captured"
-    return int(v * nq / cap["queries"]), (f"ncu dram__bytes_read.sum + dram__bytes_write.sum, one-pass capture of "
-                                          f"{cap['command']} on kernel sources {cap['src_hash']}, scaled by queries")
+    units = st["n_dist"] if phase == "a" else st["n_posting"]
+    return int(per_unit * units), (f"ncu dram__bytes_read.sum + dram__bytes_write.sum per "
+                                   f"{'beam distance' if phase == 'a' else 'posting'} on {NCU_TRAFFIC['command']} "
+                                   f"(kernel sources {NCU_TRAFFIC['src_hash']}), times this launch's units")
 
 
 def knng_quality(torch, h, X, K, dev, sample=1000, seed=5):
@@ -522,8 +524,7 @@ def main():
         tms, tb = phases[dom]
         achieved = tb / (tms / 1e3) / 1e9 if tms > 0 else 0.0
         form = {H.PREC_FP32_EXACT: "fp32", H.PREC_BF16: "bf16", H.PREC_INT8: "int8"}[prec]
-        traffic, traffic_src = ncu_traffic(args.workload, form, "a" if dom.startswith("phase_a") else "bc", learned,
-                                           nq_)
+        traffic, traffic_src = ncu_traffic(form, "a" if dom.startswith("phase_a") else "bc", st)
         roof = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
                 "frac": round(achieved / hbm, 4), "peak_source": peak_kind, "traffic": traffic,
                 "traffic_source": traffic_src,

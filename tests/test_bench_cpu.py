@@ -64,18 +64,22 @@ def test_workloads_are_well_formed():
 
 
 def test_ncu_traffic_is_tied_to_the_kernel_sources():
+    """The captured DRAM bytes per unit scale with this launch's units, and are
+    not reported once the kernel sources differ from the captured ones."""
     b = _bench()
     saved = dict(b.NCU_TRAFFIC)
+    st = {"n_dist": 1_000_000, "n_posting": 3_000_000}
     try:
         b.NCU_TRAFFIC.clear()
-        b.NCU_TRAFFIC["w"] = {"src_hash": b.search_src_hash(), "queries": 10_000, "command": "c",
-                              "bytes": {("int8", "a", True): 2_819_000_000}}
-        v, src = b.ncu_traffic("w", "int8", "a", True, 5_000)
-        assert v == 1_409_500_000 and "c" in src
-        assert b.ncu_traffic("w", "int8", "bc", True, 5_000)[0] is None
-        assert b.ncu_traffic("other", "int8", "a", True, 5_000)[0] is None
-        b.NCU_TRAFFIC["w"]["src_hash"] = "0" * 16          # captured on other sources: not reported
-        v, src = b.ncu_traffic("w", "int8", "a", True, 5_000)
+        assert b.ncu_traffic("int8", "a", st)[0] is None
+        b.NCU_TRAFFIC.update({"src_hash": b.search_src_hash(), "command": "c",
+                              "per_unit": {("int8", "a"): 23.5, ("int8", "bc"): 25.0}})
+        v, src = b.ncu_traffic("int8", "a", st)
+        assert v == 23_500_000 and "c" in src and "beam distance" in src
+        assert b.ncu_traffic("int8", "bc", st)[0] == 75_000_000
+        assert b.ncu_traffic("fp32", "a", st)[0] is None
+        b.NCU_TRAFFIC["src_hash"] = "0" * 16          # captured on other sources: not reported
+        v, src = b.ncu_traffic("int8", "a", st)
         assert v is None and "predates" in src
     finally:
         b.NCU_TRAFFIC.clear()
