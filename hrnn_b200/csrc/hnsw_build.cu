@@ -25,6 +25,7 @@
 // multi-threaded build does), while every stored distance is the exact FP32 value
 // of the reference's L2 order.
 #include <algorithm>
+#include <cstdlib>
 #include <cfloat>
 #include <cmath>
 #include <random>
@@ -352,7 +353,14 @@ void add_points(Index& ix, const float* data, const uint64_t* labels, size_t n_a
     CUDA_CHECK(cudaMemsetAsync(kcnt.p, 0, kcnt.bytes, s));
     const int nsm = nsm_of(ix.device);
     const bool fused = (ix.order.fused & 1) != 0;
-    const uint32_t efc = (uint32_t)((ix.ef_construction + 31) & ~(size_t)31), vc = 2048;
+    const uint32_t efc = (uint32_t)((ix.ef_construction + 31) & ~(size_t)31);
+    // Visited-cache slots per warp (lossy: a miss only re-scores a node, so the
+    // graph does not depend on it); HRNN_BUILD_VC overrides, for measurements.
+    uint32_t vc = 2048;
+    if (const char* e = std::getenv("HRNN_BUILD_VC")) {
+        const unsigned long v = std::strtoul(e, nullptr, 10);
+        if (v >= 256 && v <= 8192 && (v & (v - 1)) == 0) vc = (uint32_t)v;
+    }
     const size_t per_warp_b = warp_smem_bytes((uint32_t)dim, efc, vc) + dim * 4 + kMaxSel * 12 + 128;
     const int wpb = (int)std::max<size_t>(1, std::min<size_t>(4, (200 * 1024) / per_warp_b));
     const size_t smem_b = per_warp_b * wpb;

@@ -304,10 +304,9 @@ __global__ void k_sample_rev(uint32_t n, uint32_t R, uint32_t cap, const uint64_
 // accumulators (element e into accumulator e mod 16, then summed left to right),
 // so the tiling leaves every distance bit-identical.
 //
+// NBUF 1 (256 threads, two blocks per SM): one stage per block, the default.
 // NBUF 2 (512 threads, one block per SM): two stages, the next node's rows
-// copied asynchronously while the current node is computed -- for iterations
-// with many pairs per node.  NBUF 1 (256 threads, two blocks per SM): one stage,
-// for iterations with few pairs per node (and dims whose two stages do not fit).
+// copied asynchronously while the current node is computed (a measured option).
 // Nodes without new entries have no pairs and are skipped.  Proposals go to
 // ranges of the buffer a warp reserves kReserve slots at a time (one atomic per
 // range instead of one per tile; a tile's proposals continue in a new range when
@@ -1370,9 +1369,13 @@ void refine_knng(Index& ix, int iters, int sample) {
     // (20 bytes per proposal: the record and its bucket key).
     size_t free_b = 0, total_b = 0;
     CUDA_CHECK(cudaMemGetInfo(&free_b, &total_b));
-    const unsigned long long pcap = std::max<unsigned long long>(
+    unsigned long long pcap = std::max<unsigned long long>(
         1 << 20, std::min<unsigned long long>({(unsigned long long)n * 2048, 1ull << 31,
                                                (unsigned long long)(free_b * 0.4 / 20)}));
+    if (const char* e = std::getenv("HRNN_REFINE_PCAP")) {  // a smaller buffer (tests of the chunk retries)
+        const unsigned long long v = std::strtoull(e, nullptr, 10);
+        if (v >= 4096) pcap = std::min(pcap, v);
+    }
     // Proposals one chunk aims for (HRNN_REFINE_CHUNK_PROPOSALS, default the whole
     // buffer): smaller chunks merge more often, so lists that start short fill
     // sooner and later chunks are filtered by finite thresholds.
@@ -1401,6 +1404,14 @@ void refine_knng(Index& ix, int iters, int sample) {
     // block resident).
     const bool jf = (ix.order.fused & 1) != 0;
     const bool join2_fits = join_smem_bytes((uint32_t)ix.dim, cap, 2) <= 227 * 1024;
+    // The one-stage form (two blocks of 8 warps per SM, each on its own node)
+    // measured faster than the two-stage form (16 warps on one node) in every
+    // iteration of the 1M x 128, K = 500 build (1.40 s against 1.48 s): the other
+    // block's node hides the row loads, and 8 warps share a node's work units
+    // with less waiting at its barriers.  HRNN_JOIN2_MIN_PAIRS selects the
+    // two-stage form from that many pairs per node (for measurements).
+    double join2_min_pairs = 1e300;
+    if (const char* e = std::getenv("HRNN_JOIN2_MIN_PAIRS")) join2_min_pairs = std::strtod(e, nullptr);
     const size_t join_smem1 = join_smem_bytes((uint32_t)ix.dim, cap, 1);
     const size_t join_smem2 = join_smem_bytes((uint32_t)ix.dim, cap, 2);
     auto kj1 = jf ? k_join<true, 1> : k_join<false, 1>;
@@ -1486,7 +1497,7 @@ void refine_knng(Index& ix, int iters, int sample) {
         unsigned long long njoin_ok = 0;  // pair count after the last accepted chunk
         unsigned long long nprop_ok = 0;  // proposal count after the last accepted chunk
         JoinTcCounters jc_ok{};           // screen counts after the last accepted chunk
-        const bool join2 = join2_fits && pairs_per_node >= 1000.0;
+        const bool join2 = join2_fits && pairs_per_node >= join2_min_pairs;
         // ---- phase 2, chunk by chunk ----
         for (uint32_t node0 = 0; node0 < n;) {
             if (prop_per_pair > 0.0 && pairs_per_node > 0.0)

@@ -132,3 +132,22 @@ def test_refine_odd_list_widths_match_oracle(golden_refine, tmp_path, K):
     flags = (np.arange(K)[None, :] < oc[:, None]).astype(np.uint8)
     port.refine(X, oi, od, oc, flags, 3, 10)
     _same_lists(*got, oi, od, oc)
+
+
+def test_refine_with_a_small_proposal_buffer_keeps_the_lists(monkeypatch):
+    """A proposal buffer far smaller than one chunk's proposals: chunks overflow,
+    are redone smaller (each retry at most a quarter of the one before) and the
+    refinement ends with the lists of the unconstrained run, up to the order of
+    exactly equal distances."""
+    n, K = 20000, 60
+    X = data.mixture(n, 128, 24, 1.0, 9, 9)
+    h = H.HRNN(dim=128, max_elements=n, M=16, ef_construction=60, random_seed=100, K_knng=K)
+    h.add_points(X)
+    start = [np.ascontiguousarray(a).copy() for a in h.get_knng()]
+    h.refineKNNG(2, 20)
+    full = h.get_knng()
+    h.set_knng(*start)
+    monkeypatch.setenv("HRNN_REFINE_PCAP", "20000")
+    h.refineKNNG(2, 20)
+    small = h.get_knng()
+    _same_lists_up_to_ties(*small, *full, K, X)
