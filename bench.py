@@ -206,7 +206,16 @@ def rknn_gt_fp64(torch, X, Q, kth, dev):
 # hold), keyed by (precision form, phase) and tied to the kernel sources it was
 # captured on: the bench line scales it by the units of its own launch, and
 # reports none when the sources have changed since (SEARCH_SOURCES hash differs).
-NCU_TRAFFIC = {}
+NCU_TRAFFIC = {
+    "src_hash": "3d3f921bb1720653",
+    "command": ("ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum --nvtx "
+                "--nvtx-include timed/ -k regex:k_phase_a_fast|k_verify_chunks python bench.py --workload "
+                "mixed-500k-d128-K250 --queries 10000 --no-learned --no-cpu-baseline --steps 1 --warmup 3"),
+    # bytes per beam distance (phase a) / per posting (phase bc): 842.9 MB over 35.72 M
+    # distances (INT8 beam), 1,101.0 MB over 43.83 M postings (streaming verification),
+    # 2,854.9 MB over 35.72 M distances (BF16 beam)
+    "per_unit": {("int8", "a"): 23.60, ("int8", "bc"): 25.12, ("bf16", "a"): 79.93},
+}
 SEARCH_SOURCES = ("common.cuh", "beam.cuh", "beam_fast.cuh", "search_plain.cu", "search_bc.cu", "verify_stream.cu",
                   "mixed.cu", "budget.cu")
 

@@ -614,20 +614,39 @@ __global__ void k_bucket_count(const Prop* __restrict__ prop, unsigned long long
     }
 }
 
+// Each warp takes kFillU consecutive runs of 32 proposals at a time: their loads,
+// then their cursor atomics (independent of each other), then their stores, so a
+// warp has kFillU atomic round trips in flight instead of one.
+constexpr int kFillU = 4;
+
 __global__ void k_bucket_fill(const Prop* __restrict__ prop, unsigned long long np, const uint64_t* __restrict__ toff,
                               uint32_t* __restrict__ tcur, uint64_t* __restrict__ bucket) {
     const uint32_t lt = lanemask_lt_();
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < np; i += (size_t)gridDim.x * blockDim.x) {
-        const Prop p = prop[i];
-        const uint32_t peers = __match_any_sync(__activemask(), p.target);
-        const int leader = __ffs(peers) - 1;
-        uint32_t base = 0;
-        const bool real = p.target != kNoTarget;
-        if ((peers & lt) == 0 && real) base = atomicAdd(&tcur[p.target], (uint32_t)__popc(peers));
-        base = __shfl_sync(peers, base, leader);
-        if (!real) continue;
-        const uint64_t pos = toff[p.target] + base + (uint32_t)__popc(peers & lt);
-        bucket[pos] = ((uint64_t)__float_as_uint(p.d) << 32) | p.source;  // d >= 0: bit order = value order
+    const int lane = threadIdx.x & 31;
+    const size_t warp = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const size_t nwarps = ((size_t)gridDim.x * blockDim.x) >> 5;
+    for (size_t b = warp * (32 * kFillU); b < np; b += nwarps * (32 * kFillU)) {  // uniform over the warp
+        Prop p[kFillU];
+#pragma unroll
+        for (int r = 0; r < kFillU; ++r) {
+            const size_t i = b + (size_t)r * 32 + lane;
+            p[r] = i < np ? prop[i] : Prop{kNoTarget, 0u, 0.f};
+        }
+        uint32_t peers[kFillU], base[kFillU];
+#pragma unroll
+        for (int r = 0; r < kFillU; ++r) {
+            peers[r] = __match_any_sync(0xFFFFFFFFu, p[r].target);
+            base[r] = 0;
+            if ((peers[r] & lt) == 0 && p[r].target != kNoTarget)
+                base[r] = atomicAdd(&tcur[p[r].target], (uint32_t)__popc(peers[r]));
+        }
+#pragma unroll
+        for (int r = 0; r < kFillU; ++r) {
+            base[r] = __shfl_sync(0xFFFFFFFFu, base[r], __ffs(peers[r]) - 1);
+            if (p[r].target == kNoTarget) continue;
+            const uint64_t pos = toff[p[r].target] + base[r] + (uint32_t)__popc(peers[r] & lt);
+            bucket[pos] = ((uint64_t)__float_as_uint(p[r].d) << 32) | p[r].source;  // d >= 0: bit order = value order
+        }
     }
 }
 
@@ -933,13 +952,14 @@ __global__ void __launch_bounds__(kMT) k_merge_cta(uint32_t n, uint32_t K, const
 // of distance <= its own, each list entry after the survivors below it, and the
 // first K are kept.  Targets with more survivors are listed in ovl for the CTA
 // merge, their lists untouched.
-constexpr uint32_t kWS = 1024;  // survivors a warp merge holds
-constexpr int kWW = 8;          // warps per block of the warp merge
+constexpr int kWW = 8;  // warps per block of the warp merge
 
-__host__ __device__ inline size_t merge_warp_bytes(uint32_t K) {
-    return (size_t)kWS * 8 + (((size_t)K * 9 + 15) & ~(size_t)15);
+// Per-warp shared memory of the warp merge holding WS survivors.
+__host__ __device__ inline size_t merge_warp_bytes(uint32_t K, uint32_t WS) {
+    return (size_t)WS * 8 + (((size_t)K * 9 + 15) & ~(size_t)15);
 }
 
+template <uint32_t kWS>  // survivors a warp merge holds
 __global__ void __launch_bounds__(kWW * 32) k_merge_warp(uint32_t n, uint32_t K, const uint64_t* __restrict__ toff,
                                                          const uint64_t* __restrict__ bucket,
                                                          uint32_t* __restrict__ hdr, uint32_t* __restrict__ ids,
@@ -949,7 +969,7 @@ __global__ void __launch_bounds__(kWW * 32) k_merge_warp(uint32_t n, uint32_t K,
                                                          uint32_t* __restrict__ n_ovl) {
     extern __shared__ __align__(16) char smraw[];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    char* base = smraw + (size_t)w * merge_warp_bytes(K);
+    char* base = smraw + (size_t)w * merge_warp_bytes(K, kWS);
     uint64_t* sk = (uint64_t*)base;  // survivor keys: d bits << 32 | source
     float* Ld = (float*)(base + (size_t)kWS * 8);
     uint32_t* Li = (uint32_t*)(Ld + K);
@@ -1109,17 +1129,26 @@ void bucket_and_merge(uint32_t n, uint32_t K, const Prop* prop, unsigned long lo
     CUDA_LAUNCH_CHECK();
     if (mid) CUDA_CHECK(cudaEventRecord(mid, s));
     CUDA_CHECK(cudaMemsetAsync(d_nextt, 0, 4, s));
-    if (!ops && merge_warp_bytes(K) * kWW <= 227 * 1024) {
+    // Survivors a warp merge holds: 512 (less shared memory per warp, so three
+    // blocks per SM instead of two; targets with more survivors go to the CTA
+    // merge) measured 15-20 % faster in the heavy iterations of the 1M x 128,
+    // K = 500 build than 1024 (HRNN_MERGE_WS = 1024 selects it, for measurements).
+    static const uint32_t ws = [] {
+        const char* e = std::getenv("HRNN_MERGE_WS");
+        return (e && std::strtoul(e, nullptr, 10) == 1024) ? 1024u : 512u;
+    }();
+    if (!ops && merge_warp_bytes(K, ws) * kWW <= 227 * 1024) {
         // warp merge for every target, then the CTA merge for the targets it left
         // (tcur and tcount are free after the scatter: the left targets and their count)
-        static int per_sm = 0;
-        const size_t wsm = merge_warp_bytes(K) * kWW;
-        CUDA_CHECK(cudaFuncSetAttribute(k_merge_warp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm));
-        if (!per_sm) CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_merge_warp, kWW * 32, wsm));
+        const size_t wsm = merge_warp_bytes(K, ws) * kWW;
+        auto kmw = ws == 512 ? k_merge_warp<512> : k_merge_warp<1024>;
+        int per_sm = 1;
+        CUDA_CHECK(cudaFuncSetAttribute(kmw, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm));
+        CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kmw, kWW * 32, wsm));
         uint32_t* left = tcur.as<uint32_t>();
         uint32_t* n_left = tcount.as<uint32_t>();
         CUDA_CHECK(cudaMemsetAsync(n_left, 0, 4, s));
-        k_merge_warp<<<(unsigned)(nsm * std::max(per_sm, 1)), kWW * 32, wsm, s>>>(
+        kmw<<<(unsigned)(nsm * std::max(per_sm, 1)), kWW * 32, wsm, s>>>(
             n, K, toff.as<uint64_t>(), bucket, hdr, ids, dist, isnew, d_nupd, d_nextt, left, n_left);
         CUDA_LAUNCH_CHECK();
         CUDA_CHECK(cudaMemsetAsync(d_nextt, 0, 4, s));
