@@ -1132,16 +1132,18 @@ void bucket_and_merge(uint32_t n, uint32_t K, const Prop* prop, unsigned long lo
     // Survivors a warp merge holds: 512 (less shared memory per warp, so three
     // blocks per SM instead of two; targets with more survivors go to the CTA
     // merge) measured 15-20 % faster in the heavy iterations of the 1M x 128,
-    // K = 500 build than 1024 (HRNN_MERGE_WS = 1024 selects it, for measurements).
+    // K = 500 build than 1024 (HRNN_MERGE_WS = 256 / 1024 selects another, for
+    // measurements).
     static const uint32_t ws = [] {
         const char* e = std::getenv("HRNN_MERGE_WS");
-        return (e && std::strtoul(e, nullptr, 10) == 1024) ? 1024u : 512u;
+        const unsigned long v = e ? std::strtoul(e, nullptr, 10) : 0;
+        return (v == 256 || v == 1024) ? (uint32_t)v : 512u;
     }();
     if (!ops && merge_warp_bytes(K, ws) * kWW <= 227 * 1024) {
         // warp merge for every target, then the CTA merge for the targets it left
         // (tcur and tcount are free after the scatter: the left targets and their count)
         const size_t wsm = merge_warp_bytes(K, ws) * kWW;
-        auto kmw = ws == 512 ? k_merge_warp<512> : k_merge_warp<1024>;
+        auto kmw = ws == 256 ? k_merge_warp<256> : ws == 512 ? k_merge_warp<512> : k_merge_warp<1024>;
         int per_sm = 1;
         CUDA_CHECK(cudaFuncSetAttribute(kmw, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm));
         CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kmw, kWW * 32, wsm));
