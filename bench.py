@@ -60,10 +60,12 @@ WORKLOADS = {
     # K_knng=200 (8 GB of ids + 8 GB of distances), reverse CSR of 2e9 entries;
     # 100,000 queries per step, recall against a float64 ground truth of the first
     # 5,000 (radii computed only for the points the stored k-th distances let a
-    # query reach).
+    # query reach); the learned budget's levels are 5 / 10 proxies from a beam of
+    # 100 (this size needs more proxies than the 1M mixture).
     "large-10M-d96-K200": dict(n=10_000_000, d=96, C=1024, sigma=1.0, seed=4, dirichlet=False, nq=100_000,
                                qseed=1004, M=16, efc=200, K=200, iters=10, S=50, k=10, Kp=200, ef=200,
-                               m_sweep=[1, 2, 3, 4, 5, 6, 8, 10, 20, 50], gt_subset=5000, val_n=2000),
+                               m_sweep=[1, 2, 3, 4, 5, 6, 8, 10, 15, 20, 50], gt_subset=5000, val_n=4000,
+                               budget_levels=(5, 10, 100)),
     # Learned search budget: 1M x 256, 512 equal Gaussians (sigma 1.5, seed 3),
     # K_knng=500; the MLP trained on 200,000 seeded queries (draw seed 1003) labelled
     # by the method itself, evaluated on 20,000 held-out queries (draw seed 2003);
