@@ -104,12 +104,6 @@ __device__ __forceinline__ uint32_t jt_idesc(uint32_t n) {
     return (1u << 4) | (1u << 7) | (1u << 10) | ((n >> 3) << 17) | ((kMaxNew >> 4) << 24);
 }
 
-__device__ __forceinline__ uint32_t lanemask_lt_jt() {
-    uint32_t m;
-    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
-    return m;
-}
-
 // Exact FP32 distance of two shared-memory rows in the reference's order.
 template <bool FUSED>
 __device__ __forceinline__ float exact_pair(const float* ra, const float* rb, uint32_t d4) {
