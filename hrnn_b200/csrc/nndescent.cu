@@ -63,39 +63,52 @@ __global__ void k_init_flags(const uint32_t* __restrict__ hdr, uint32_t n, uint3
 
 // Counts reverse-sample candidates per (target, type) segment: seg = 2*nbr + (old?1:0).
 // thr[nbr]: the farthest entry of nbr's list, FLT_MAX when not full (so an empty
-// list never passes `d > thr`).
+// list never passes `d > thr`).  The decision of every entry is kept in rbits
+// (bit j % 32 of word i * ceil(K / 32) + j / 32), so the fill pass reads one word
+// per 32 entries instead of their distances and the thresholds of their ids.
 __global__ void k_sample_count(const uint32_t* __restrict__ ids, const float* __restrict__ dist,
                                const uint32_t* __restrict__ hdr, const uint8_t* __restrict__ isnew, uint32_t n,
-                               uint32_t K, const float* __restrict__ thr, uint32_t* __restrict__ rcount) {
+                               uint32_t K, const float* __restrict__ thr, uint32_t* __restrict__ rcount,
+                               uint32_t* __restrict__ rbits) {
     size_t warp = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     int lane = threadIdx.x & 31;
     size_t nw = ((size_t)gridDim.x * blockDim.x) >> 5;
+    const uint32_t wpn = (K + 31) >> 5;
     for (size_t i = warp; i < n; i += nw) {
         uint32_t c = hdr[i] & 0xFFFFu;
-        for (uint32_t j = lane; j < c; j += 32) {
-            uint32_t nbr = ids[i * K + j];
-            if (dist[i * K + j] > thr[nbr]) atomicAdd(&rcount[2 * (size_t)nbr + (isnew[i * K + j] ? 0 : 1)], 1u);
+        for (uint32_t base = 0; base < c; base += 32) {  // uniform over the warp
+            const uint32_t j = base + lane;
+            bool rc = false;
+            if (j < c) {
+                const uint32_t nbr = ids[i * K + j];
+                rc = dist[i * K + j] > thr[nbr];
+                if (rc) atomicAdd(&rcount[2 * (size_t)nbr + (isnew[i * K + j] ? 0 : 1)], 1u);
+            }
+            const uint32_t b = __ballot_sync(0xFFFFFFFFu, rc);
+            if (lane == 0) rbits[i * wpn + (base >> 5)] = b;
         }
     }
 }
 
 // Forward samples (first S new / first S old by rank), reverse-candidate scatter,
 // and clearing of the new flags.
-__global__ void k_sample_fill(const uint32_t* __restrict__ ids, const float* __restrict__ dist,
+__global__ void k_sample_fill(const uint32_t* __restrict__ ids, const uint32_t* __restrict__ rbits,
                               const uint32_t* __restrict__ hdr, uint8_t* __restrict__ isnew, uint32_t n, uint32_t K,
-                              const float* __restrict__ thr, uint32_t S, uint32_t cap, uint32_t* __restrict__ newl, uint32_t* __restrict__ newc,
+                              uint32_t S, uint32_t cap, uint32_t* __restrict__ newl, uint32_t* __restrict__ newc,
                               uint32_t* __restrict__ oldl, uint32_t* __restrict__ oldc,
                               const uint64_t* __restrict__ roff, uint32_t* __restrict__ rcur,
                               uint32_t* __restrict__ rbuf) {
     size_t warp = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     int lane = threadIdx.x & 31;
     size_t nw = ((size_t)gridDim.x * blockDim.x) >> 5;
+    const uint32_t wpn = (K + 31) >> 5;
     for (size_t i = warp; i < n; i += nw) {
         uint32_t c = hdr[i] & 0xFFFFu;
         uint32_t nn = 0, no = 0;
         for (uint32_t base = 0; base < c; base += 32) {
             uint32_t j = base + lane;
             bool valid = j < c;
+            const uint32_t rb = rbits[i * wpn + (base >> 5)];  // the count pass's decisions
             uint32_t nbr = valid ? ids[i * K + j] : 0;
             bool isn = valid && isnew[i * K + j];
             uint32_t bn = __ballot_sync(0xFFFFFFFFu, isn);
@@ -110,7 +123,7 @@ __global__ void k_sample_fill(const uint32_t* __restrict__ ids, const float* __r
             }
             nn += __popc(bn);
             no += __popc(bo);
-            if (valid && dist[i * K + j] > thr[nbr]) {
+            if (valid && ((rb >> lane) & 1u)) {
                 size_t seg = 2 * (size_t)nbr + (isn ? 0 : 1);
                 rbuf[roff[seg] + atomicAdd(&rcur[seg], 1u)] = (uint32_t)i;
             }
@@ -1372,9 +1385,11 @@ void refine_knng(Index& ix, int iters, int sample) {
     }
     const int nsm = smcount(ix.device);
     // Device state of the refinement.
-    DevMem isnew, newl, newc, oldl, oldc, rcount, roff, rcur, rbuf, thr, prop, tcount, toff, tcur, bucket, tmp, ctr;
+    DevMem isnew, newl, newc, oldl, oldc, rcount, roff, rcur, rbuf, rbits, thr, prop, tcount, toff, tcur, bucket, tmp,
+        ctr;
     isnew.alloc((size_t)n * K + 16);
     rbuf.alloc((size_t)n * K * 4 + 16);
+    rbits.alloc((size_t)n * ((K + 31) / 32) * 4 + 16);
     // INIT (hrnn.h:1744-1748): every existing entry is new.
     if (n) {
         size_t tot = (size_t)n * K;
@@ -1496,14 +1511,14 @@ void refine_knng(Index& ix, int iters, int sample) {
         k_thresholds<<<(n + 255) / 256, 256, 0, s>>>(hdr, dist, n, K, thr.as<float>());
         CUDA_LAUNCH_CHECK();
         k_sample_count<<<g1, 256, 0, s>>>(ids, dist, hdr, isnew.as<uint8_t>(), n, K, thr.as<float>(),
-                                           rcount.as<uint32_t>());
+                                           rcount.as<uint32_t>(), rbits.as<uint32_t>());
         CUDA_LAUNCH_CHECK();
         exclusive_scan_u32_to_u64(rcount.as<uint32_t>(), roff.as<uint64_t>(), (size_t)2 * n + 1, s, tmp);
         uint64_t rtot = 0;
         CUDA_CHECK(cudaMemcpyAsync(&rtot, roff.as<uint64_t>() + (size_t)2 * n, 8, cudaMemcpyDeviceToHost, s));
         CUDA_CHECK(cudaStreamSynchronize(s));
         rbuf.ensure(std::max<uint64_t>(rtot, 1) * 4);  // rtot <= n K: allocated once up front
-        k_sample_fill<<<g1, 256, 0, s>>>(ids, dist, hdr, isnew.as<uint8_t>(), n, K, thr.as<float>(), S, cap,
+        k_sample_fill<<<g1, 256, 0, s>>>(ids, rbits.as<uint32_t>(), hdr, isnew.as<uint8_t>(), n, K, S, cap,
                                           newl.as<uint32_t>(),
                                           newc.as<uint32_t>(), oldl.as<uint32_t>(), oldc.as<uint32_t>(),
                                           roff.as<uint64_t>(), rcur.as<uint32_t>(), rbuf.as<uint32_t>());
